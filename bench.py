@@ -1,0 +1,330 @@
+"""Benchmark: time to a 1e-8 FP64 relative residual of AMG-preconditioned CG
+on the 3-D 7-point variable-coefficient heat-conduction problem, 128^3 cells
+(2,097,152 rows, 14,581,760 nonzeros), log-normal conductivity, Dirichlet on
+one face, Neumann elsewhere (seeded synthetic input).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl thermofem|reference]
+
+A step is one solve (Solver::apply) from a zero initial guess with the
+hierarchy already built; `value` is seconds per solve of the mixed-precision
+path (FP32 AMG hierarchy and V-cycle, FP64 PCG), `plain_fp64` the same with an
+FP64 hierarchy.  Inputs stay resident in HBM (the 217 MB FP64 operator is
+larger than the 126 MB L2, so nothing is flushed between steps).  `e2e` runs
+the same solve through the C ABI with pinned host buffers (rhs upload, x
+upload and download inside the timed region).  With N > 1 every rank solves
+its own replica (the solve does not shard) and the time is the max over
+ranks.  `--impl reference` times the CPU oracle (the reference has no CPU
+solver; its host restatement is the baseline) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+SIZE = 128
+SEED_MATRIX, SEED_RHS = 1001, 1002
+AMG = dict(jacobi_weight=2.0 / 3.0, pre_sweeps=1, post_sweeps=1, cycle="v", coarse_rows=64)
+METRIC = "time-to-1e-8 FP64 relative residual (s), AMG-PCG V-cycle, FP32 hierarchy / FP64 outer"
+WORKLOAD = f"heat3d {SIZE}^3 7-point FV, log-normal k (seed {SEED_MATRIX}), Dirichlet x=0, rhs U[-1,1] (seed {SEED_RHS})"
+
+
+def spmv_bytes(n, nnz, vsize=8, isize=4):
+    """Algorithmic bytes of one CSR SpMV: values + column indices, row
+    offsets, x and y each once."""
+    return nnz * (vsize + isize) + n * (isize + 2 * vsize) + isize
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index),
+                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap", "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 7:
+                    try:
+                        rows.append((float(parts[0]), float(parts[1]), float(parts[2]), parts[3:7]))
+                    except ValueError:
+                        pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k, v in enumerate(r[3]) if v.lower() == "active"})
+        return {"sm_mhz": float(np.median([r[0] for r in rows])), "sm_max_mhz": max(r[1] for r in rows),
+                "power_w_max": max(r[2] for r in rows), "samples": len(rows), "reasons": reasons}
+
+
+def cpu_solve_once(A, amg, b, O):
+    t0 = time.perf_counter()
+    x, rep = O.cg(A, amg, b, np.zeros(A.rows))
+    return time.perf_counter() - t0, rep
+
+
+def run_reference(args):
+    """CPU oracle (OpenMP, all host cores) on the same workload and metric."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle")], check=True)
+    from oracle import oracle as O
+    from thermofem_b200 import problems as P
+    off, idx, val = P.heat3d(SIZE, SEED_MATRIX)
+    n = len(off) - 1
+    b = P.rhs_uniform(n, SEED_RHS)
+    A = O.Csr(n, off, idx, val)
+    t0 = time.perf_counter()
+    amg = O.Amg(A, **{k: (0 if v == "v" else v) for k, v in AMG.items() if k != "cycle"}, cycle=0)
+    setup_s = time.perf_counter() - t0
+    # First warm-up step: one full solve gives the iteration count and cost.
+    t_full, rep = cpu_solve_once(A, amg, b, O)
+    budget = 240.0
+    full = (args.steps + args.warmup) * t_full <= budget
+    sample = "full solve per step" if full else "20 PCG iterations per step, scaled to the full iteration count"
+    times = []
+    for k in range(args.warmup - 1 + args.steps):
+        if full:
+            t, _ = cpu_solve_once(A, amg, b, O)
+        else:
+            t0 = time.perf_counter()
+            O.cg(A, amg, b, np.zeros(n), max_iterations=20)
+            t = (time.perf_counter() - t0) * rep["iterations"] / 20.0
+        if k >= args.warmup - 1:
+            times.append(t)
+    value = float(np.median(times))
+    cores = O.num_threads()
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
+            "config": {"workload": WORKLOAD + ", CPU oracle FP64 AMG-PCG", "rows": n, "nnz": int(len(idx)),
+                       "parallelism": "host OpenMP"},
+            "iterations": rep["iterations"], "setup_s": setup_s,
+            "cpu_baseline": {"value": value, "unit": "s", "cores": cores, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="thermofem", choices=["thermofem", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import thermofem_b200 as tf
+    from thermofem_b200 import problems as P
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+
+    off, idx, val = P.heat3d(SIZE, SEED_MATRIX)
+    n, nnz = len(off) - 1, len(idx)
+    b_host = torch.tensor(P.rhs_uniform(n, SEED_RHS))
+    ctx = tf.Context(local)
+    a = tf.DeviceCsr.from_host(off, idx, val, device=dev)
+    b = b_host.to(dev)
+    x = torch.zeros(n, dtype=torch.float64, device=dev)
+    opts = tf.solver_options(torch.float64)
+
+    def make(hier):
+        s = tf.Cg(opts, "amg", tf.amg_options(hierarchy_type=hier, **AMG), ctx=ctx)
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        s.setup(a)
+        ctx.synchronize()
+        return s, time.perf_counter() - t0
+
+    mixed, setup_mixed = make("f32")
+    plain, setup_plain = make("f64")
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def maxover(v):
+        if dist is None:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def solve(s):
+        x.zero_()
+        rep = s.apply(b, x)
+        assert rep["status"] == "Converged", rep
+        return rep
+
+    def timed(s, steps, clocks=None):
+        for _ in range(args.warmup):
+            rep = solve(s)
+        barrier()
+        torch.cuda.synchronize(dev)
+        launches0 = ctx.launches
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(ctx.stream)
+        for _ in range(steps):
+            rep = solve(s)
+        e1.record(ctx.stream)
+        torch.cuda.synchronize(dev)
+        barrier()
+        ms = e0.elapsed_time(e1) / steps
+        return maxover(ms), rep, ctx.launches - launches0
+
+    with Clocks(local) as clk:
+        ms_mixed, rep_mixed, launches_mixed = timed(mixed, args.steps)
+    clocks = clk.summary()
+    ms_plain, rep_plain, launches_plain = timed(plain, args.steps)
+
+    # true FP64 residual of the last mixed solve
+    r = tf.residual(a, b, x, ctx=ctx)
+    true_rel = float(torch.linalg.norm(r) / torch.linalg.norm(b))
+
+    # e2e: public C ABI call with pinned host buffers, copies inside the timed region
+    hb = b_host.pin_memory()
+    hx = torch.zeros(n, dtype=torch.float64).pin_memory()
+    for _ in range(2):
+        hx.zero_()
+        mixed.apply(hb, hx)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        hx.zero_()
+        rep_e2e = mixed.apply(hb, hx)
+    e2e_s = maxover((time.perf_counter() - t0) / args.steps)
+    assert rep_e2e["status"] == "Converged"
+
+    # roofline of the dominant kernel family: the row-tile SpMV on the FP64 operator
+    y = torch.empty_like(b)
+    for _ in range(5):
+        tf.spmv(a, b, y, ctx=ctx)
+    reps = 50
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(ctx.stream)
+    for _ in range(reps):
+        tf.spmv(a, b, y, ctx=ctx)
+    e1.record(ctx.stream)
+    torch.cuda.synchronize(dev)
+    spmv_ms = e0.elapsed_time(e1) / reps
+    peak, peak_kind = measured_peaks()
+    algo = spmv_bytes(n, nnz)
+    achieved = algo / (spmv_ms * 1e-3) / 1e9
+    a32 = a.to(torch.float32)
+    b32 = b.float()
+    y32 = torch.empty_like(b32)
+    for _ in range(5):
+        tf.spmv(a32, b32, y32, ctx=ctx)
+    e0.record(ctx.stream)
+    for _ in range(reps):
+        tf.spmv(a32, b32, y32, ctx=ctx)
+    e1.record(ctx.stream)
+    torch.cuda.synchronize(dev)
+    spmv32_ms = e0.elapsed_time(e1) / reps
+    achieved32 = spmv_bytes(n, nnz, 4, 4) / (spmv32_ms * 1e-3) / 1e9
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle")], check=True)
+            from oracle import oracle as O
+            A = O.Csr(n, off, idx, val)
+            amg = O.Amg(A, jacobi_weight=AMG["jacobi_weight"], coarse_rows=AMG["coarse_rows"])
+            t_cpu, rep_cpu = cpu_solve_once(A, amg, b_host.numpy(), O)
+            cpu = {"value": t_cpu, "unit": "s", "cores": O.num_threads(), "kind": "port",
+                   "sample": f"one full FP64 AMG-PCG solve of the same 128^3 problem ({rep_cpu['iterations']} iterations)"}
+        except Exception as e:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": "s", "cores": None, "kind": "port", "sample": f"failed: {e}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": ms_mixed / 1e3, "unit": "s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_mixed, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64 outer / f32 hierarchy", "data": "synthetic (seeded generator)",
+            "config": {"workload": WORKLOAD, "rows": n, "nnz": nnz,
+                       "solver": "PCG + aggregation AMG V(1,1), Jacobi w=2/3, coarse LU <= 64 rows, rtol 1e-8",
+                       "parallelism": "replicas" if world > 1 else "single GPU",
+                       "l2": "inputs larger than L2 (217 MB FP64 operator), no flush"},
+            "iterations": rep_mixed["iterations"], "true_relative_residual": true_rel,
+            "setup_s": setup_mixed,
+            "plain_fp64": {"value": ms_plain / 1e3, "unit": "s", "iterations": rep_plain["iterations"],
+                           "setup_s": setup_plain},
+            "speedup_mixed_vs_fp64": ms_plain / ms_mixed,
+            "spmv_gbs": {"f64": achieved, "f32": achieved32},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "kernel": "csr_tile_kernel (SpMV, FP64 operator)", "peak_source": peak_kind,
+                         "algorithmic_bytes": algo, "launch_ms": spmv_ms},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": 2 * n * 8, "d2h_bytes_per_step": n * 8},
+            "gpu_launches": int(launches_mixed),
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    del mixed, plain
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

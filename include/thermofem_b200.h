@@ -1,0 +1,302 @@
+/*
+ * thermofem_b200.h -- C ABI of the B200 (sm_100a) sparse solve path.
+ *
+ * Plain pointers and sizes, int status returns (TF_OK == 0, negative codes
+ * below), no exceptions across the boundary.  Device pointers are caller
+ * owned unless a function returns an opaque handle; every launch goes to the
+ * stream of the tf_ctx it is given.  Reference citations are paths inside
+ * the Mgepahmge/ThermoFEM project and name the interface each entry point
+ * replaces.  Nothing here falls back to the CPU: a missing GPU is an error.
+ */
+#ifndef THERMOFEM_B200_H
+#define THERMOFEM_B200_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+/* Map onto the reference's exception classes (include/DataStructure/
+ * Memory.cuh:52-66 CudaError; std::invalid_argument / logic_error /
+ * length_error thrown by the component constructors and setup). */
+#define TF_OK 0
+#define TF_ERR_INVALID (-1)   /* std::invalid_argument */
+#define TF_ERR_CUDA (-2)      /* CudaError */
+#define TF_ERR_LENGTH (-3)    /* std::length_error / overflow_error */
+#define TF_ERR_LOGIC (-4)     /* std::logic_error (e.g. apply before setup) */
+#define TF_ERR_TIMEOUT (-5)   /* a bounded device wait gave up */
+#define TF_ERR_NOMEM (-6)     /* allocation failure */
+#define TF_ERR_RUNTIME (-7)   /* std::runtime_error (I/O, parse) */
+
+/* ---- element types ----------------------------------------------------- */
+#define TF_F32 0
+#define TF_F64 1
+#define TF_I32 2
+#define TF_I64 3
+
+/* Solve status, values of thermofem::SolveStatus (include/Solver/
+ * Interfaces.cuh:10). */
+#define TF_CONVERGED 0
+#define TF_MAX_ITERATIONS 1
+#define TF_BREAKDOWN 2
+#define TF_NONFINITE 3
+
+/* Cycle kinds, thermofem::multigrid::Cycle (include/Multigrid/Cycle.cuh:10). */
+#define TF_CYCLE_V 0
+#define TF_CYCLE_W 1
+#define TF_CYCLE_F 2
+
+const char *tf_version(void);
+/* Message of the last failing call on this thread. */
+const char *tf_last_error(void);
+const char *tf_status_string(int status);
+
+/* ---- execution context ------------------------------------------------- */
+/* Owns (or borrows) a stream and a grow-only scratch arena on one device.
+ * Not thread safe; one per solver instance.  Replaces the reference's
+ * per-object handles (src/LinearAlgebra/IterationContext.cu:35-122) and the
+ * CUB workspace of GpuAggregation (src/Multigrid/GpuAggregation.cu:84-126). */
+typedef struct tf_ctx tf_ctx;
+int tf_ctx_create(int device, void *stream /* cudaStream_t or NULL */, tf_ctx **out);
+int tf_ctx_destroy(tf_ctx *ctx);
+int tf_ctx_synchronize(tf_ctx *ctx);
+void *tf_ctx_stream(tf_ctx *ctx);
+int tf_ctx_device(tf_ctx *ctx);
+/* Number of kernels this context has launched (all entry points). */
+int64_t tf_ctx_launch_count(tf_ctx *ctx);
+int tf_device_count(int *count);
+
+/* ---- CSR descriptor ---------------------------------------------------- */
+/* Device CSR view (include/DataStructure/CsrMatrix.cuh:36-217): offsets
+ * rows+1, indices/values nnz, index_type TF_I32|TF_I64, value_type
+ * TF_F32|TF_F64. */
+typedef struct {
+    int64_t rows, cols, nnz;
+    int index_type, value_type;
+    const void *offsets;
+    const void *indices;
+    const void *values;
+} tf_csr;
+
+/* Device CSR owned by the library (outputs of setup stages). */
+typedef struct tf_dcsr tf_dcsr;
+int tf_dcsr_view(const tf_dcsr *m, tf_csr *out);
+int tf_dcsr_free(tf_dcsr *m);
+
+/* ---- data-structure checks -------------------------------------------- */
+/* Structural validation on the device: offsets monotone and bounded, indices
+ * in range.  Replaces detail::validateDeviceCsr (src/DataStructure/
+ * CsrMatrix.cu:12-58).  TF_ERR_INVALID when malformed. */
+int tf_csr_validate(tf_ctx *ctx, const tf_csr *a);
+/* Canonical-form check (src/Multigrid/GpuAggregation.cu:283-304): *flags
+ * bit 1 = unsorted/duplicate columns, bit 2 = invalid structure or
+ * nonfinite value.  Host int written after a stream sync. */
+int tf_csr_check_canonical(tf_ctx *ctx, const tf_csr *a, int *flags);
+/* Sorted, duplicate-summed copy, explicit zeros kept
+ * (GpuAggregation::canonical, GpuAggregation.cu:991-1007). */
+int tf_canonicalize(tf_ctx *ctx, const tf_csr *a, tf_dcsr **out);
+/* Element-type conversion of a device array (GpuAggregation.cu:1101-1108). */
+int tf_convert(tf_ctx *ctx, int64_t n, int src_type, const void *src, int dst_type, void *dst);
+
+/* ---- SpMV family (IterationContext::multiply/residual/jacobi,
+ *      src/LinearAlgebra/IterationContext.cu:140-269) --------------------- */
+/* y = A x.  x, y have A's value type; y must not alias x. */
+int tf_spmv(tf_ctx *ctx, const tf_csr *a, const void *x, void *y);
+int tf_spmv_f64(tf_ctx *ctx, int64_t rows, int64_t cols, int64_t nnz, const int32_t *offsets,
+                const int32_t *indices, const double *values, const double *x, double *y);
+int tf_spmv_f32(tf_ctx *ctx, int64_t rows, int64_t cols, int64_t nnz, const int32_t *offsets,
+                const int32_t *indices, const float *values, const float *x, float *y);
+/* r = b - A x in one pass (replaces SpMV + scal + axpy, IterationContext.cu:167-175). */
+int tf_residual(tf_ctx *ctx, const tf_csr *a, const void *b, const void *x, void *r);
+/* One fused weighted-Jacobi sweep x_out = x + w * Dinv (b - A x)
+ * (Jacobi.cuh:60-74 with IterationContext.cu:26-32).  row_weight (float,
+ * nullable) replaces w per row.  When map/coarse are given the sweep reads
+ * x~ = x + coarse[map] (prolongation fused, GpuAggregation.cu:970-976).
+ * x_out must not alias x. */
+int tf_jacobi_sweep(tf_ctx *ctx, const tf_csr *a, const void *dinv, const void *b, const void *x, void *x_out,
+                    double weight, const float *row_weight, const int32_t *map, const void *coarse);
+/* Zero-guess sweep x = w * Dinv * b (no SpMV). */
+int tf_jacobi_zero(tf_ctx *ctx, int64_t n, int value_type, const void *dinv, const void *b, void *x, double weight,
+                   const float *row_weight);
+/* Inverse diagonal with duplicate diagonals summed; TF_ERR_INVALID on a
+ * missing, zero or nonfinite diagonal or reciprocal (LinearAlgebra/
+ * Diagonal.cuh:13-36), computed on the device. */
+int tf_inverse_diagonal(tf_ctx *ctx, const tf_csr *a, void *dinv);
+
+/* ---- aggregate transfers (GpuAggregation.cu:950-976,1050-1067) --------- */
+/* coarse[c] = sum of fine[members] in member order (no float atomics). */
+int tf_restrict(tf_ctx *ctx, int value_type, int64_t coarse_rows, const int32_t *offsets, const int32_t *members,
+                const void *fine, void *coarse);
+/* fine[i] += coarse[map[i]]. */
+int tf_prolong(tf_ctx *ctx, int value_type, int64_t fine_rows, const int32_t *map, const void *coarse,
+               void *fine);
+
+/* ---- BLAS-1 and fused Krylov steps (IterationContext.cu:161-249) ------- */
+/* out[k] = sum_i x_k[i] * y_k[i] for k < count (count <= 4), FP64
+ * accumulation with a deterministic two-stage reduction; out is a device
+ * double array.  Partial sums live in the context's scratch arena. */
+int tf_dot_multi(tf_ctx *ctx, int value_type, int64_t n, int count, const void *const *xs, const void *const *ys,
+                 double *out);
+/* y = a x + b y (FP64 scalars). */
+int tf_axpby(tf_ctx *ctx, int value_type, int64_t n, double a, const void *x, double b, void *y);
+
+/* ---- setup stages (GpuAggregation, include/Multigrid/GpuAggregation.cuh:47-64) */
+/* Row validation (finite values, nonzero diagonal with finite reciprocal)
+ * and row max |offdiag| (GpuAggregation.cu:247-271); *bad set on failure. */
+int tf_row_stats(tf_ctx *ctx, const tf_csr *a, double *row_max, int *bad);
+/* Symmetric strength graph, max-merged (GpuAggregation.cu:339-390). */
+int tf_strength(tf_ctx *ctx, const tf_csr *a, const double *row_max, double threshold, tf_dcsr **graph);
+/* Synchronous handshake matching, rounds 1..8 (GpuAggregation.cu:402-505):
+ * map[rows] gets consecutive pair ids, *count their number. */
+int tf_match(tf_ctx *ctx, const tf_csr *graph, int rounds, int32_t *map, int *count);
+/* Graph quotient by map, intra edges dropped, max-merged
+ * (GpuAggregation.cu:534-576). */
+int tf_contract(tf_ctx *ctx, const tf_csr *graph, const int32_t *map, int count, tf_dcsr **out);
+
+/* Aggregate transfer (AggregateTransfer, GpuAggregation.cuh:13-17). */
+typedef struct tf_transfer tf_transfer;
+/* Two-stage matching + optional two absorption rounds, compaction, member
+ * table and histogram (GpuAggregation::aggregate, GpuAggregation.cu:766-818). */
+int tf_aggregate(tf_ctx *ctx, const tf_csr *graph, int rounds, int absorb_singletons, tf_transfer **out);
+int tf_transfer_info(const tf_transfer *t, int *fine_rows, int *coarse_rows, int32_t histogram[4]);
+/* Device arrays owned by the transfer: map[fine], offsets[coarse+1], members[fine]. */
+int tf_transfer_arrays(const tf_transfer *t, const int32_t **map, const int32_t **offsets,
+                       const int32_t **members);
+int tf_transfer_free(tf_transfer *t);
+/* Ac = P^T A P by coordinate mapping and sum (GpuAggregation.cu:136-234). */
+int tf_galerkin(tf_ctx *ctx, const tf_csr *a, const tf_transfer *t, tf_dcsr **out);
+
+/* ---- sort / reduce / scan primitives (replace CUB, GpuAggregation.cu:116-211) */
+/* Stable LSD radix sort of (u64 key, f64 value) pairs on bits
+ * [0, end_bit).  Outputs must not alias inputs. */
+int tf_radix_sort_pairs_u64f64(tf_ctx *ctx, int64_t n, const uint64_t *keys_in, const double *values_in,
+                               uint64_t *keys_out, double *values_out, int end_bit);
+/* Reduce runs of equal keys left to right: op 0 = sum, 1 = max.
+ * *count (host) receives the number of unique keys. */
+int tf_reduce_by_key_u64f64(tf_ctx *ctx, int64_t n, const uint64_t *keys, const double *values, int op,
+                            uint64_t *keys_out, double *values_out, int64_t *count);
+/* Exclusive prefix sum of int32 (out may alias in). */
+int tf_scan_exclusive_i32(tf_ctx *ctx, int64_t n, const int32_t *in, int32_t *out);
+
+/* ---- coarse dense LU (GpuAggregation.cu:827-939,1068-1098) ------------- */
+/* Partial-pivot LU of a canonical FP64 CSR with rows <= 256 (reference:
+ * <= 64); pivot threshold 64*DBL_EPSILON*max|A|.  lu: rows*rows doubles,
+ * pivots: rows ints (device).  *factored = 1 on success, 0 when singular. */
+int tf_coarse_lu_factor(tf_ctx *ctx, const tf_csr *a, double *lu, int32_t *pivots, int *factored);
+/* x = A^-1 b from the factor; b and x may alias; value_type of b/x. */
+int tf_coarse_lu_solve(tf_ctx *ctx, int rows, const double *lu, const int32_t *pivots, int value_type,
+                       const void *b, void *x);
+
+/* ---- components (include/Smoother/Jacobi.cuh, include/Preconditioner/
+ *      Amg.cuh, include/Solver/{Cg,BiCgStab}.cuh) ------------------------ */
+/* AmgOptions (Amg.cuh:14-25) plus the precision extension. */
+typedef struct {
+    int max_levels;          /* 1..20, default 20 */
+    int coarse_rows;         /* 1..256, default 64 */
+    int matching_rounds;     /* 1..8, default 8 */
+    int pre_sweeps, post_sweeps; /* default 1, 1 */
+    int coarse_sweeps;       /* default 8 */
+    double jacobi_weight;    /* default 0.75 */
+    double strength_threshold; /* default 0.25 */
+    int absorb_singletons;   /* default 1 */
+    int compact_sort_keys;   /* default 0; does not change results */
+    int cycle;               /* TF_CYCLE_V */
+    int hierarchy_type;      /* TF_F64 or TF_F32 storage/arithmetic of the cycle; -1 = same as vectors */
+    int coarse_lu_rows;      /* LU when the last level has <= this many rows; default 64, max 256 */
+} tf_amg_options;
+void tf_amg_options_default(tf_amg_options *o);
+
+typedef struct tf_amg tf_amg;
+/* value_type/index_type: the component's T and I (vectors and matrix). */
+int tf_amg_create(tf_ctx *ctx, int value_type, int index_type, const tf_amg_options *opt, tf_amg **out);
+int tf_amg_destroy(tf_amg *m);
+/* Amg::setup (Amg.cuh:81-143); transactional: on failure the previous
+ * hierarchy is kept. */
+int tf_amg_setup(tf_amg *m, const tf_csr *a);
+/* Amg::apply (Amg.cuh:149-161): x = M^-1 rhs from a zero guess; device
+ * vectors of the component's T; rhs and x may alias. */
+int tf_amg_apply(tf_amg *m, const void *rhs, void *x);
+int tf_amg_level_count(const tf_amg *m);
+/* Level statistics (AmgLevelStatistics, Amg.cuh:27-31). */
+int tf_amg_level_stats(const tf_amg *m, int level, int64_t *rows, int64_t *nnz, int32_t histogram[4]);
+const char *tf_amg_stop_reason(const tf_amg *m);
+const char *tf_amg_coarse_solver(const tf_amg *m);
+/* Visits per level of the last apply (Amg::lastCycleVisits). */
+int tf_amg_last_visits(const tf_amg *m, int64_t *visits, int capacity);
+/* Level operator and transfer of the hierarchy (read-only device views). */
+int tf_amg_level_matrix(const tf_amg *m, int level, tf_csr *out);
+int tf_amg_level_transfer(const tf_amg *m, int level, const int32_t **map, const int32_t **offsets,
+                          const int32_t **members, int *coarse_rows);
+
+/* Jacobi smoother component (Jacobi.cuh:26-93). */
+typedef struct tf_jacobi tf_jacobi;
+int tf_jacobi_create(tf_ctx *ctx, int value_type, int index_type, int sweeps, double weight, tf_jacobi **out);
+int tf_jacobi_destroy(tf_jacobi *j);
+int tf_jacobi_setup(tf_jacobi *j, const tf_csr *a);
+/* x updated from its current value; rhs and x may alias. */
+int tf_jacobi_apply(tf_jacobi *j, const void *rhs, void *x);
+
+/* Solver components: kind 0 = PCG (Cg.cuh), 1 = right-preconditioned
+ * BiCGStab (BiCgStab.cuh).  precond 0 = Identity, 1 = AMG with amg_opt. */
+typedef struct {
+    int max_iterations;          /* default 1000 */
+    double relative_tolerance;   /* default 1e-8 (f64) / 1e-5 (f32) */
+    double absolute_tolerance;   /* default 0 */
+    int residual_refresh_interval; /* default 50 */
+} tf_solver_options;
+void tf_solver_options_default(int value_type, tf_solver_options *o);
+
+typedef struct {
+    int status;      /* TF_CONVERGED ... */
+    int iterations;
+    double residual_norm;
+    double relative_residual;
+} tf_solve_result;
+
+#define TF_SOLVER_CG 0
+#define TF_SOLVER_BICGSTAB 1
+#define TF_PRECOND_IDENTITY 0
+#define TF_PRECOND_AMG 1
+typedef struct tf_solver tf_solver;
+int tf_solver_create(tf_ctx *ctx, int kind, int value_type, int index_type, const tf_solver_options *opt,
+                     int precond, const tf_amg_options *amg_opt, tf_solver **out);
+int tf_solver_destroy(tf_solver *s);
+/* Solver::setup (Cg.cuh:63-70, BiCgStab.cuh:70-77); a failed setup leaves
+ * the solver unusable until the next successful setup. */
+int tf_solver_setup(tf_solver *s, const tf_csr *a);
+/* Solver::apply: x holds the initial guess on entry; rhs and x may alias.
+ * Device or host pointers: host_buffers != 0 means rhs/x are host memory
+ * (pinned or pageable) and the copies run inside the call. */
+int tf_solver_apply(tf_solver *s, const void *rhs, void *x, int host_buffers, tf_solve_result *result);
+/* The AMG preconditioner owned by the solver, or NULL for Identity. */
+tf_amg *tf_solver_amg(tf_solver *s);
+/* Device time of the last apply in milliseconds (CUDA events on the ctx stream). */
+double tf_solver_last_apply_ms(const tf_solver *s);
+
+/* ---- Matrix Market input (include/IO/MatrixMarket.cuh:14-31) ----------- */
+typedef struct {
+    int rows, cols;
+    int64_t nnz;
+    int32_t *offsets;
+    int32_t *indices;
+    double *values;
+} tf_host_csr;
+/* Parses coordinate real|integer general|symmetric text; duplicates kept in
+ * input order, symmetric triangles expanded (src/IO/MatrixMarket.cu:35-122).
+ * TF_ERR_RUNTIME with tf_last_error() on malformed input. */
+int tf_read_matrix_market(const char *text, size_t length, tf_host_csr *out);
+int tf_read_matrix_market_file(const char *path, tf_host_csr *out);
+void tf_host_csr_free(tf_host_csr *m);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,282 @@
+"""GPU parity of the kernel layer against the CPU oracle (FP64) and a plain
+numpy FP64 evaluation of the same formula (FP32 kernels).  Tolerances:
+FP64 kernels 1e-13 relative to the row's magnitude (FMA contraction and
+summation order are the only differences); FP32 kernels 2e-6 relative."""
+import numpy as np
+import pytest
+import torch
+
+import thermofem_b200 as tf
+from conftest import to_device
+from oracle import oracle as O
+from thermofem_b200 import problems as P
+
+pytestmark = pytest.mark.gpu
+
+
+def irregular(n=3000, seed=7):
+    """Rows of very different lengths, including rows longer than one staged
+    chunk (4096 entries) and empty rows."""
+    rng = np.random.default_rng(seed)
+    lens = rng.integers(0, 12, n)
+    lens[5] = 9000
+    lens[17] = 0
+    lens[n - 1] = 5000
+    off = np.zeros(n + 1, np.int64)
+    np.cumsum(lens, out=off[1:])
+    idx = np.concatenate([np.sort(rng.choice(n, size=l, replace=l > n)) for l in lens]).astype(np.int32)
+    val = rng.standard_normal(off[-1])
+    for i in range(n):  # make every row have a diagonal where nonempty
+        if lens[i]:
+            idx[off[i]] = i
+    return off.astype(np.int32), idx, val
+
+
+def mats():
+    yield "heat3d16", P.heat3d(16)
+    yield "laplace2d40", P.laplace2d(40)
+    yield "irregular", irregular()
+    s = O.sample_matrix(61)
+    yield "sample61", (s.offsets, s.indices, s.values)
+
+
+def host_spmv(m, x):
+    off, idx, val = m
+    n = len(off) - 1
+    y = np.zeros(n)
+    np.add.at(y, np.repeat(np.arange(n), np.diff(off)), val * x[idx])
+    return y
+
+
+def rel_err(a, b):
+    return np.max(np.abs(a - b)) / max(1e-300, np.max(np.abs(b)))
+
+
+@pytest.mark.parametrize("name,m", list(mats()))
+@pytest.mark.parametrize("index_dtype", [torch.int32, torch.int64])
+def test_spmv_f64_matches_oracle(ctx, name, m, index_dtype):
+    off, idx, val = m
+    n = len(off) - 1
+    x = np.random.default_rng(1).standard_normal(n)
+    a = to_device(m, index_dtype=index_dtype)
+    y = tf.spmv(a, torch.tensor(x, device="cuda"), ctx=ctx).cpu().numpy()
+    ref = O.spmv(O.Csr(n, off, idx, val), x)
+    scale = host_spmv((off, idx, np.abs(val)), np.abs(x)) + 1e-300
+    assert np.max(np.abs(y - ref) / scale) < 1e-13
+
+
+@pytest.mark.parametrize("name,m", list(mats()))
+def test_spmv_f32_matches_fp64_reference(ctx, name, m):
+    off, idx, val = m
+    n = len(off) - 1
+    x = np.random.default_rng(2).standard_normal(n).astype(np.float32)
+    a = to_device(m, dtype=torch.float32)
+    y = tf.spmv(a, torch.tensor(x, device="cuda"), ctx=ctx).cpu().numpy().astype(np.float64)
+    ref = host_spmv((off, idx, val.astype(np.float32).astype(np.float64)), x.astype(np.float64))
+    scale = host_spmv((off, idx, np.abs(val)), np.abs(x.astype(np.float64))) + 1e-30
+    assert np.max(np.abs(y - ref) / scale) < 2e-6
+
+
+def test_spmv_empty_pattern_and_typed_entry(ctx):
+    a = to_device((np.zeros(4, np.int32), np.zeros(0, np.int32), np.zeros(0)))
+    y = tf.spmv(a, torch.ones(3, dtype=torch.float64, device="cuda"), ctx=ctx)
+    assert y.abs().max().item() == 0.0
+    off, idx, val = P.laplace2d(20)
+    d = to_device((off, idx, val))
+    x = torch.randn(400, dtype=torch.float64, device="cuda")
+    y1 = tf.spmv(d, x, ctx=ctx)
+    y2 = torch.empty_like(x)
+    with ctx:
+        tf.check(tf.lib().tf_spmv_f64(ctx.h, 400, 400, len(idx), d.offsets.data_ptr(), d.indices.data_ptr(),
+                                      d.values.data_ptr(), x.data_ptr(), y2.data_ptr()))
+    assert torch.equal(y1, y2)
+    with pytest.raises(tf.InvalidArgument):
+        tf.spmv(d, x, y=x, ctx=ctx)
+
+
+@pytest.mark.parametrize("dtype,tol", [(torch.float64, 1e-13), (torch.float32, 3e-6)])
+def test_residual_and_jacobi_family(ctx, dtype, tol):
+    off, idx, val = P.heat3d(12, seed=5)
+    n = len(off) - 1
+    rng = np.random.default_rng(3)
+    b, x = rng.standard_normal(n), rng.standard_normal(n)
+    hb = b.astype(np.float32).astype(np.float64) if dtype == torch.float32 else b
+    hx = x.astype(np.float32).astype(np.float64) if dtype == torch.float32 else x
+    hv = val.astype(np.float32).astype(np.float64) if dtype == torch.float32 else val
+    a = to_device((off, idx, val), dtype=dtype)
+    tb, tx = torch.tensor(b, dtype=dtype, device="cuda"), torch.tensor(x, dtype=dtype, device="cuda")
+    ax = host_spmv((off, idx, hv), hx)
+    scale = host_spmv((off, idx, np.abs(hv)), np.abs(hx)) + np.abs(hb)
+    r = tf.residual(a, tb, tx, ctx=ctx).cpu().numpy()
+    assert np.max(np.abs(r - (hb - ax)) / scale) < tol
+    dinv = tf.inverse_diagonal(a, ctx=ctx)
+    hd = dinv.cpu().numpy().astype(np.float64)
+    diag = np.array([hv[off[i]:off[i + 1]][idx[off[i]:off[i + 1]] == i].sum() for i in range(n)])
+    assert np.max(np.abs(hd * diag - 1)) < tol * 10
+    w = 2.0 / 3.0
+    xo = tf.jacobi_sweep(a, dinv, tb, tx, w, ctx=ctx).cpu().numpy()
+    want = hx + w * hd * (hb - ax)
+    assert np.max(np.abs(xo - want) / (np.abs(hx) + w * np.abs(hd) * scale)) < tol * 4
+    # per-row weights
+    rw = torch.linspace(0.3, 0.9, n, device="cuda", dtype=torch.float32)
+    xo = tf.jacobi_sweep(a, dinv, tb, tx, w, row_weight=rw, ctx=ctx).cpu().numpy()
+    hw = rw.cpu().numpy().astype(np.float64)
+    want = hx + hw * hd * (hb - ax)
+    assert np.max(np.abs(xo - want) / (np.abs(hx) + np.abs(hd) * scale)) < tol * 4
+    # prolongation fused: x~ = x + e[map]
+    nc = 97
+    mp = rng.integers(0, nc, n).astype(np.int32)
+    e = rng.standard_normal(nc)
+    he = e.astype(np.float32).astype(np.float64) if dtype == torch.float32 else e
+    xt = hx + he[mp]
+    if dtype == torch.float32:
+        xt = xt.astype(np.float32).astype(np.float64)
+    axt = host_spmv((off, idx, hv), xt)
+    xo = tf.jacobi_sweep(a, dinv, tb, tx, w, map=torch.tensor(mp, device="cuda"),
+                         coarse=torch.tensor(e, dtype=dtype, device="cuda"), ctx=ctx).cpu().numpy()
+    want = xt + w * hd * (hb - axt)
+    scale2 = host_spmv((off, idx, np.abs(hv)), np.abs(xt)) + np.abs(hb)
+    assert np.max(np.abs(xo - want) / (np.abs(xt) + w * np.abs(hd) * scale2)) < tol * 4
+    z = tf.jacobi_zero(dinv, tb, w, ctx=ctx).cpu().numpy()
+    assert np.max(np.abs(z - w * hd * hb) / (np.abs(w * hd * hb) + 1e-300)) < tol
+
+
+def test_jacobi_sweep_matches_oracle_jacobi(ctx):
+    # two sweeps of the fused kernel == Jacobi<double>(2, 1) on poisson(2): 0.5/0.25 (solver_test.cpp:56-74)
+    off, idx, val = P.poisson1d(2)
+    a = to_device((off, idx, val))
+    dinv = tf.inverse_diagonal(a, ctx=ctx)
+    b = torch.tensor([1.0, 0.0], dtype=torch.float64, device="cuda")
+    x = torch.zeros(2, dtype=torch.float64, device="cuda")
+    x = tf.jacobi_sweep(a, dinv, b, x, 1.0, ctx=ctx)
+    x = tf.jacobi_sweep(a, dinv, b, x, 1.0, ctx=ctx)
+    assert x.cpu().tolist() == [0.5, 0.25]
+
+
+def test_inverse_diagonal_rejects_bad_diagonals(ctx):
+    # duplicate diagonal entries are summed (multigrid_operations_test.cpp:63-83)
+    a = to_device((np.array([0, 2, 4], np.int32), np.array([0, 0, 0, 1], np.int32), np.array([1.0, 1, 4, 3])))
+    d = tf.inverse_diagonal(a, ctx=ctx).cpu().numpy()
+    assert abs(d[0] - 0.5) < 1e-15 and abs(d[1] - 1 / 3) < 1e-15
+    bad = to_device((np.array([0, 2, 4], np.int32), np.array([0, 0, 0, 1], np.int32), np.array([0.0, 0, 4, 3])))
+    with pytest.raises(tf.InvalidArgument):
+        tf.inverse_diagonal(bad, ctx=ctx)
+
+
+def test_restrict_prolong_and_blas1(ctx):
+    n = 5000
+    rng = np.random.default_rng(4)
+    nc = 1500
+    mp = np.sort(rng.integers(0, nc, n)).astype(np.int32)
+    mp[:nc] = np.arange(nc)  # every aggregate nonempty
+    mp = np.sort(mp)
+    off = np.zeros(nc + 1, np.int32)
+    np.cumsum(np.bincount(mp, minlength=nc), out=off[1:])
+    mem = np.argsort(mp, kind="stable").astype(np.int32)
+    t = tf.Transfer(torch.tensor(mp, device="cuda"), torch.tensor(off, device="cuda"), torch.tensor(mem, device="cuda"),
+                    n, nc, np.zeros(4))
+    f = rng.standard_normal(n)
+    c = tf.restrict_aggregates(t, torch.tensor(f, device="cuda"), ctx=ctx).cpu().numpy()
+    want = np.array([sum(f[mem[off[k]:off[k + 1]]]) for k in range(nc)])  # member order, left to right
+    assert np.array_equal(c, want)
+    fine = torch.tensor(f, device="cuda")
+    tf.prolong_aggregates(t, torch.tensor(want, device="cuda"), fine, ctx=ctx)
+    assert np.array_equal(fine.cpu().numpy(), f + want[mp])
+    xs = [torch.tensor(rng.standard_normal(n), device="cuda") for _ in range(3)]
+    ys = [torch.tensor(rng.standard_normal(n), device="cuda") for _ in range(3)]
+    d = tf.dot_multi(xs, ys, ctx=ctx).cpu().numpy()
+    want = [float(np.dot(a.cpu().numpy(), b.cpu().numpy())) for a, b in zip(xs, ys)]
+    assert np.allclose(d, want, rtol=1e-13, atol=1e-12)
+    d2 = tf.dot_multi(xs, ys, ctx=ctx).cpu().numpy()
+    assert np.array_equal(d, d2)  # deterministic
+    y = ys[0].clone()
+    tf.axpby(2.0, xs[0], -0.5, y, ctx=ctx)
+    assert torch.allclose(y, 2.0 * xs[0] - 0.5 * ys[0], rtol=1e-15, atol=1e-15)
+
+
+@pytest.mark.parametrize("n", [1, 7, 2048, 2049, 100000, 5_000_000])
+def test_scan_exclusive(ctx, n):
+    rng = np.random.default_rng(n)
+    x = rng.integers(0, 5, n).astype(np.int32)
+    out = tf.scan_exclusive(torch.tensor(x, device="cuda"), ctx=ctx).cpu().numpy()
+    want = np.concatenate([[0], np.cumsum(x)[:-1]]).astype(np.int32)
+    assert np.array_equal(out, want)
+    t = torch.tensor(x, device="cuda")
+    tf.scan_exclusive(t, out=t, ctx=ctx)  # in place
+    assert np.array_equal(t.cpu().numpy(), want)
+
+
+@pytest.mark.parametrize("n,bits", [(1, 8), (1000, 12), (70000, 40), (1_000_003, 64)])
+def test_radix_sort_is_stable_and_reduce_by_key(ctx, n, bits):
+    rng = np.random.default_rng(n)
+    hi = 1 << min(bits, 62)
+    keys = rng.integers(0, min(hi, max(2, n // 3)), n, dtype=np.int64).astype(np.uint64)
+    if bits == 64:
+        keys = keys | (np.uint64(1) << np.uint64(63))
+    vals = np.arange(n, dtype=np.float64)  # original positions expose stability
+    tk = torch.tensor(keys.view(np.int64), device="cuda")
+    tv = torch.tensor(vals, device="cuda")
+    sk, sv = tf.radix_sort_pairs(tk, tv, end_bit=bits, ctx=ctx)
+    order = np.argsort(keys, kind="stable")
+    assert np.array_equal(sk.cpu().numpy().view(np.uint64), keys[order])
+    assert np.array_equal(sv.cpu().numpy(), vals[order])
+    w = rng.standard_normal(n)
+    uk, uv = tf.reduce_by_key(sk, torch.tensor(w, device="cuda"), "sum", ctx=ctx)
+    ks = keys[order]
+    heads = np.flatnonzero(np.r_[True, ks[1:] != ks[:-1]])
+    want = [float(sum(w[h:e])) for h, e in zip(heads, list(heads[1:]) + [n])] if n < 100000 else None
+    assert np.array_equal(uk.cpu().numpy().view(np.uint64), ks[heads])
+    if want is not None:
+        assert np.array_equal(uv.cpu().numpy(), np.array(want))  # left-to-right sums: bit exact
+    uk, um = tf.reduce_by_key(sk, torch.tensor(w, device="cuda"), "max", ctx=ctx)
+    assert np.array_equal(um.cpu().numpy(), np.maximum.reduceat(w, heads))
+
+
+def test_csr_validation_and_canonical(ctx):
+    good = to_device(P.laplace2d(8))
+    tf.csr_validate(good, ctx=ctx)
+    assert tf.check_canonical(good, ctx=ctx) == 0
+    bad = to_device((np.array([0, 7, 6], np.int32), np.array([1, 0, 0, 1, 0, 1], np.int32), np.ones(6)))
+    with pytest.raises(tf.InvalidArgument):
+        tf.csr_validate(bad, ctx=ctx)
+    dup = to_device((np.array([0, 3, 6], np.int32), np.array([1, 0, 0, 1, 0, 1], np.int32),
+                     np.array([-1.0, 1, 1, 1, -1, 1])))
+    assert tf.check_canonical(dup, ctx=ctx) == 1
+    c = tf.canonicalize(dup, ctx=ctx)
+    assert c.values.cpu().tolist() == [2, -1, -1, 2]  # amg_native_test.cpp:115-121
+    nan = to_device((np.array([0, 1, 2], np.int32), np.array([0, 1], np.int32), np.array([1.0, np.nan])))
+    assert tf.check_canonical(nan, ctx=ctx) & 2
+
+
+@pytest.mark.parametrize("n", [2, 17, 64, 150, 256])
+def test_coarse_lu_matches_oracle(ctx, n):
+    rng = np.random.default_rng(n)
+    dense = rng.standard_normal((n, n)) + n * np.eye(n) * 0.1
+    dense[rng.random((n, n)) < 0.3] = 0.0
+    np.fill_diagonal(dense, np.diag(dense) + 1.0)
+    off = np.concatenate([[0], np.cumsum((dense != 0).sum(axis=1))]).astype(np.int32)
+    idx = np.concatenate([np.flatnonzero(r) for r in dense]).astype(np.int32)
+    val = dense[dense != 0]
+    ok, lu, piv = tf.coarse_lu_factor(to_device((off, idx, val)), ctx=ctx)
+    ook, olu, opiv = O.lu_factor(O.Csr(n, off, idx, val))
+    assert ok and ook
+    assert np.array_equal(piv.cpu().numpy(), opiv)
+    assert np.allclose(lu.cpu().numpy(), olu, rtol=1e-10, atol=1e-12)
+    b = rng.standard_normal(n)
+    x = tf.coarse_lu_solve(lu, piv, torch.tensor(b, device="cuda"), ctx=ctx).cpu().numpy()
+    assert np.allclose(dense @ x, b, rtol=1e-10, atol=1e-10)
+
+
+def test_coarse_lu_scale_invariance_and_singular(ctx):
+    # amg_native_test.cpp:133-153
+    off, idx = np.array([0, 2, 4], np.int32), np.array([0, 1, 0, 1], np.int32)
+    for scale in (1e-100, 1.0, 1e100):
+        ok, lu, piv = tf.coarse_lu_factor(to_device((off, idx, np.array([1, 2, 4, 3.0]) * scale)), ctx=ctx)
+        assert ok
+        b = torch.tensor([5 * scale, 10 * scale], dtype=torch.float64, device="cuda")
+        x = tf.coarse_lu_solve(lu, piv, b, ctx=ctx).cpu().numpy()
+        assert abs(x[0] - 1) < 1e-12 and abs(x[1] - 2) < 1e-12
+        tf.coarse_lu_solve(lu, piv, b, x=b, ctx=ctx)  # rhs and x alias
+        assert np.array_equal(b.cpu().numpy(), x)
+    ok, _, _ = tf.coarse_lu_factor(to_device((off, idx, np.ones(4))), ctx=ctx)
+    assert not ok

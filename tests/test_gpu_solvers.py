@@ -1,0 +1,241 @@
+"""GPU AMG cycles and Krylov solvers against the CPU oracle and the
+reference's known answers.  Tolerances follow the reference tests: cycle vs
+host recursion 2e-10 (FP64) and 2e-3 (FP32) (amg_native_test.cpp:348);
+solver solutions to the exact 1-D Poisson solution (solver_test.cpp:196-205)."""
+import numpy as np
+import pytest
+import torch
+
+import thermofem_b200 as tf
+from conftest import to_device
+from oracle import oracle as O
+from thermofem_b200 import problems as P
+
+pytestmark = pytest.mark.gpu
+
+
+def poisson(n, dtype=torch.float64, index_dtype=torch.int32, nonsymmetric=False):
+    off, idx, val = P.poisson1d(n)
+    if nonsymmetric:
+        val = np.where(idx == np.repeat(np.arange(n), np.diff(off)), 3.0, np.where(idx > np.repeat(np.arange(n), np.diff(off)), -0.5, -1.0))
+    return (off, idx, val), to_device((off, idx, val), dtype=dtype, index_dtype=index_dtype)
+
+
+@pytest.mark.parametrize("cycle", ["v", "w", "f"])
+@pytest.mark.parametrize("dtype,index_dtype,tol", [(torch.float64, torch.int32, 2e-10),
+                                                    (torch.float32, torch.int64, 2e-3)])
+def test_cycles_match_host_recursion(ctx, cycle, dtype, index_dtype, tol):
+    # amg_native_test.cpp:303-395
+    host, a = poisson(127, dtype, index_dtype)
+    n = 127
+    i = np.arange(n)
+    b = (np.sin(0.13 * i) + 0.4).astype(np.float32 if dtype == torch.float32 else np.float64).astype(np.float64)
+    c = np.cos(0.07 * i)
+    amg = tf.Amg(tf.amg_options(coarse_rows=4, cycle=cycle), dtype=dtype, index_dtype=index_dtype, ctx=ctx)
+    amg.setup(a)
+    assert amg.level_count() >= 3
+    ora = O.Amg(O.Csr(n, *host), coarse_rows=4, cycle={"v": 0, "w": 1, "f": 2}[cycle])
+    x = amg.apply(torch.tensor(b, dtype=dtype, device="cuda")).cpu().numpy()
+    want, visits = ora.apply(b)
+    assert np.max(np.abs(x - want)) < tol
+    assert amg.last_cycle_visits() == list(visits)
+    L = amg.level_count()
+    if cycle == "v":
+        assert list(visits) == [1] * L
+    elif cycle == "w":
+        assert list(visits) == [2 ** d for d in range(L)]
+    else:
+        assert list(visits) == [d + 2 if d + 1 < L else L for d in range(L)]
+    # linearity and rhs/x aliasing
+    xc = amg.apply(torch.tensor(c, dtype=dtype, device="cuda")).cpu().numpy()
+    xs = amg.apply(torch.tensor(b + c, dtype=dtype, device="cuda")).cpu().numpy()
+    assert np.max(np.abs(xs - (x + xc))) < tol
+    r = torch.tensor(b, dtype=dtype, device="cuda")
+    amg.apply(r, r)
+    assert np.max(np.abs(r.cpu().numpy() - x)) < tol
+
+
+@pytest.mark.parametrize("cycle", ["v", "w", "f"])
+def test_mixed_precision_cycle_tracks_fp64(ctx, cycle):
+    m = P.heat3d(16, seed=3)
+    n = len(m[0]) - 1
+    b = P.rhs_uniform(n, 9)
+    opts = dict(coarse_rows=64, cycle=cycle)
+    a64 = to_device(m)
+    full = tf.Amg(tf.amg_options(**opts), ctx=ctx)
+    mixed = tf.Amg(tf.amg_options(hierarchy_type=tf.F32, **opts), ctx=ctx)
+    full.setup(a64)
+    mixed.setup(a64)
+    tb = torch.tensor(b, device="cuda")
+    x64, x32 = full.apply(tb).cpu().numpy(), mixed.apply(tb).cpu().numpy()
+    assert np.max(np.abs(x32 - x64)) / np.max(np.abs(x64)) < 1e-4
+    ora = O.Amg(O.Csr(n, *m), **opts | {"cycle": {"v": 0, "w": 1, "f": 2}[cycle]})
+    assert np.max(np.abs(x64 - ora.apply(b)[0])) / np.max(np.abs(x64)) < 1e-12
+
+
+def test_fallback_jacobi_equals_standalone_jacobi_and_zero_sweeps(ctx):
+    # amg_native_test.cpp:398-424
+    host, a = poisson(100)
+    b = torch.ones(100, dtype=torch.float64, device="cuda")
+    amg = tf.Amg(tf.amg_options(max_levels=1, coarse_sweeps=8), ctx=ctx)
+    amg.setup(a)
+    assert amg.coarse_solver() == "Jacobi (coarsening stopped)"
+    x = amg.apply(b)
+    j = tf.Jacobi(8, 0.75, ctx=ctx)
+    j.setup(a)
+    y = j.apply(b, torch.zeros(100, dtype=torch.float64, device="cuda"))
+    assert torch.equal(x, y)
+    for cycle in "vwf":
+        m = tf.Amg(tf.amg_options(coarse_rows=4, pre_sweeps=0, post_sweeps=0, cycle=cycle), ctx=ctx)
+        m.setup(a)
+        first = m.apply(b).clone()
+        assert torch.equal(first, m.apply(b))
+
+
+def test_amg_lifecycle_and_coarse_paths(ctx):
+    # solver_test.cpp:134-162
+    a = to_device((np.array([0, 2, 4], np.int32), np.array([0, 1, 0, 1], np.int32), np.array([1.0, 2, 4, 3])))
+    amg = tf.Amg(ctx=ctx)
+    with pytest.raises(tf.LogicError):
+        amg.apply(torch.ones(2, dtype=torch.float64, device="cuda"))
+    amg.setup(a)
+    x = amg.apply(torch.tensor([5.0, 10.0], dtype=torch.float64, device="cuda")).cpu().numpy()
+    assert np.allclose(x, [1, 2], atol=1e-12)
+    invalid = to_device((np.array([0, 2, 4], np.int32), np.array([0, 1, 0, 1], np.int32), np.array([0.0, 1, 1, 1])))
+    with pytest.raises(tf.InvalidArgument):
+        amg.setup(invalid)
+    x = amg.apply(torch.tensor([5.0, 10.0], dtype=torch.float64, device="cuda")).cpu().numpy()
+    assert np.allclose(x, [1, 2], atol=1e-12)  # failed setup kept the previous state
+    amg.setup(to_device((np.array([0, 2, 4], np.int32), np.array([0, 1, 0, 1], np.int32), np.ones(4))))
+    assert amg.coarse_solver() == "Jacobi (singular LU)"
+    bounded = tf.Amg(tf.amg_options(max_levels=1, coarse_rows=2), ctx=ctx)
+    bounded.setup(poisson(100)[1])
+    assert bounded.level_count() == 1 and bounded.coarse_solver() == "Jacobi (coarsening stopped)"
+    with pytest.raises(tf.InvalidArgument):
+        tf.Amg(tf.amg_options(max_levels=0), ctx=ctx)
+
+
+@pytest.mark.parametrize("solver", [tf.Cg, tf.BiCgStab])
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
+def test_amg_solves_poisson_known_answer(ctx, solver, dtype):
+    # solver_test.cpp:180-213, cg_test.cpp:51-75
+    n = 63
+    _, a = poisson(n, dtype)
+    rtol = 1e-9 if dtype == torch.float64 else 2e-4
+    s = solver(tf.solver_options(dtype, relative_tolerance=rtol), "amg", tf.amg_options(coarse_rows=8), dtype=dtype,
+               ctx=ctx)
+    s.setup(a)
+    b = torch.ones(n, dtype=dtype, device="cuda")
+    x = torch.zeros(n, dtype=dtype, device="cuda")
+    rep = s.apply(b, x)
+    assert rep["status"] == "Converged" and rep["iterations"] < 100
+    exact = np.array([(i + 1) * (n - i) / 2 for i in range(n)])
+    xv = x.cpu().numpy().astype(np.float64)
+    assert np.allclose(xv, exact, rtol=1e-8 if dtype == torch.float64 else 1e-3)
+    r = 1 - 2 * xv + np.r_[0, xv[:-1]] + np.r_[xv[1:], 0]
+    assert abs(rep["residual_norm"] - np.linalg.norm(r)) <= (1e-10 if dtype == torch.float64 else 1e-3)
+    assert rep["relative_residual"] <= rtol
+    again = s.apply(b, x)
+    assert again["status"] == "Converged" and again["iterations"] == 0
+    alias = torch.ones(n, dtype=dtype, device="cuda")
+    assert s.apply(alias, alias)["status"] == "Converged"
+
+
+@pytest.mark.parametrize("dtype,tol", [(torch.float64, 1e-11), (torch.float32, 1e-5)])
+def test_bicgstab_identity_nonsymmetric_refresh(ctx, dtype, tol):
+    # solver_test.cpp:214-237
+    n = 80
+    host, a = poisson(n, dtype, nonsymmetric=True)
+    exact = 1 + (np.arange(n) % 7) / 7
+    b = 3 * exact - np.r_[0, exact[:-1]] - 0.5 * np.r_[exact[1:], 0]
+    s = tf.BiCgStab(tf.solver_options(dtype, residual_refresh_interval=3, relative_tolerance=tol), "identity",
+                    dtype=dtype, ctx=ctx)
+    s.setup(a)
+    x = torch.full((n,), 0.2, dtype=dtype, device="cuda")
+    rep = s.apply(torch.tensor(b, dtype=dtype, device="cuda"), x)
+    assert rep["status"] == "Converged"
+    assert np.allclose(x.cpu().numpy(), exact, atol=1e-9 if dtype == torch.float64 else 1e-4)
+
+
+@pytest.mark.parametrize("solver", [tf.Cg, tf.BiCgStab])
+def test_status_semantics(ctx, solver):
+    # solver_test.cpp:238-287, cg_test.cpp:100-170
+    _, a = poisson(5)
+    zeros = torch.zeros(5, dtype=torch.float64, device="cuda")
+    s = solver(tf.solver_options(absolute_tolerance=1e-12), "identity", ctx=ctx)
+    s.setup(a)
+    rep = s.apply(zeros.clone(), zeros.clone())
+    assert rep["status"] == "Converged" and rep["iterations"] == 0
+    rep = s.apply(zeros.clone(), torch.ones(5, dtype=torch.float64, device="cuda"))
+    assert rep["status"] == "Converged" and rep["residual_norm"] <= 1e-12
+    assert rep["relative_residual"] == rep["residual_norm"]
+    host, a3 = poisson(3, nonsymmetric=True)
+    b = torch.tensor([1.0, 2, 3], dtype=torch.float64, device="cuda")
+    lim = solver(tf.solver_options(max_iterations=0), "identity", ctx=ctx)
+    lim.setup(a3)
+    rep = lim.apply(b, torch.zeros(3, dtype=torch.float64, device="cuda"))
+    assert rep["status"] == "MaxIterations" and rep["iterations"] == 0
+    one = solver(tf.solver_options(max_iterations=1, relative_tolerance=0.0), "identity", ctx=ctx)
+    one.setup(a3)
+    rep = one.apply(b, torch.zeros(3, dtype=torch.float64, device="cuda"))
+    assert rep["status"] == "MaxIterations" and rep["iterations"] == 1
+    zero_matrix = to_device((np.zeros(4, np.int32), np.zeros(0, np.int32), np.zeros(0)))
+    z = solver(tf.solver_options(), "identity", ctx=ctx)
+    z.setup(zero_matrix)
+    rep = z.apply(b, torch.zeros(3, dtype=torch.float64, device="cuda"))
+    assert rep["status"] == "Breakdown" and abs(rep["residual_norm"] - np.sqrt(14)) < 1e-12
+    bad = torch.tensor([1.0, float("nan"), 3], dtype=torch.float64, device="cuda")
+    assert z.apply(bad, torch.zeros(3, dtype=torch.float64, device="cuda"))["status"] == "NonFinite"
+
+
+def test_solver_lifecycle_errors(ctx):
+    s = tf.BiCgStab(ctx=ctx, index_dtype=torch.int64)
+    with pytest.raises(tf.LogicError):
+        s.apply(torch.ones(2, dtype=torch.float64, device="cuda"), torch.zeros(2, dtype=torch.float64, device="cuda"))
+    s.setup(poisson(2, index_dtype=torch.int64)[1])
+    assert s.apply(torch.tensor([1.0, 0.0], dtype=torch.float64, device="cuda"),
+                   torch.zeros(2, dtype=torch.float64, device="cuda"))["status"] == "Converged"
+    with pytest.raises(tf.InvalidArgument):
+        tf.BiCgStab(tf.solver_options(relative_tolerance=-1.0), ctx=ctx)
+    with pytest.raises(tf.InvalidArgument):
+        tf.Jacobi(0, ctx=ctx)
+
+
+@pytest.mark.parametrize("kind", ["cg", "bicgstab"])
+@pytest.mark.parametrize("hierarchy", [None, "f32"])
+def test_heat3d_solve_matches_oracle(ctx, kind, hierarchy):
+    m = P.heat3d(24, seed=21)
+    n = len(m[0]) - 1
+    b = P.rhs_uniform(n, 22)
+    opts = dict(coarse_rows=64, jacobi_weight=2 / 3)
+    solver = tf.Cg if kind == "cg" else tf.BiCgStab
+    s = solver(tf.solver_options(), "amg", tf.amg_options(hierarchy_type=hierarchy, **opts), ctx=ctx)
+    a = to_device(m)
+    s.setup(a)
+    x = torch.zeros(n, dtype=torch.float64, device="cuda")
+    rep = s.apply(torch.tensor(b, device="cuda"), x)
+    assert rep["status"] == "Converged"
+    xv = x.cpu().numpy()
+    A = O.Csr(n, *m)
+    true_rel = np.linalg.norm(b - O.spmv(A, xv)) / np.linalg.norm(b)
+    assert true_rel <= 1e-8 * 1.0001
+    ora = O.Amg(A, **opts)
+    xo, orep = (O.cg if kind == "cg" else O.bicgstab)(A, ora, b, np.zeros(n))
+    assert orep["status"] == "Converged"
+    assert abs(rep["iterations"] - orep["iterations"]) <= (1 if hierarchy is None else 3)
+    assert np.linalg.norm(xv - xo) / np.linalg.norm(xo) < 1e-6
+
+
+def test_host_buffer_apply(ctx):
+    m = P.heat3d(12, seed=2)
+    n = len(m[0]) - 1
+    b = torch.tensor(P.rhs_uniform(n, 3)).pin_memory()
+    x = torch.zeros(n, dtype=torch.float64).pin_memory()
+    s = tf.Cg(ctx=ctx)
+    s.setup(to_device(m))
+    rep = s.apply(b, x)
+    assert rep["status"] == "Converged"
+    xd = torch.zeros(n, dtype=torch.float64, device="cuda")
+    rep2 = s.apply(b.cuda(), xd)
+    assert rep2["iterations"] == rep["iterations"]
+    assert torch.equal(xd.cpu(), x)

@@ -1,0 +1,241 @@
+// common.cuh -- shared host/device plumbing of the B200 sparse solve path:
+// error model of the C ABI, device scope guard, RAII device buffers, the
+// execution context and launch helpers.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <new>
+#include <stdexcept>
+#include <string>
+#include <utility>
+
+#include "thermofem_b200.h"
+
+namespace tfb {
+
+// Internal failure carrying a C ABI status code.  Thrown inside the library
+// and converted to a status at every extern "C" boundary.
+struct Failure : std::exception {
+    int code;
+    std::string message;
+    Failure(int c, std::string m) : code(c), message(std::move(m)) {}
+    const char *what() const noexcept override { return message.c_str(); }
+};
+
+[[noreturn]] inline void fail(int code, const std::string &msg) { throw Failure(code, msg); }
+inline void require(bool ok, const char *msg, int code = TF_ERR_INVALID) {
+    if (!ok) fail(code, msg);
+}
+inline void cuda_check(cudaError_t e, const char *what) {
+    if (e != cudaSuccess) {
+        if (e == cudaErrorMemoryAllocation) fail(TF_ERR_NOMEM, std::string(what) + ": " + cudaGetErrorString(e));
+        fail(TF_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+    }
+}
+
+void set_last_error(const char *msg);
+
+// Runs f and converts exceptions to a status (the ABI never throws).
+template <class F>
+int guard(F &&f) noexcept {
+    try {
+        f();
+        return TF_OK;
+    } catch (const Failure &e) {
+        set_last_error(e.message.c_str());
+        return e.code;
+    } catch (const std::bad_alloc &) {
+        set_last_error("host allocation failed");
+        return TF_ERR_NOMEM;
+    } catch (const std::exception &e) {
+        set_last_error(e.what());
+        return TF_ERR_RUNTIME;
+    } catch (...) {
+        set_last_error("unknown failure");
+        return TF_ERR_RUNTIME;
+    }
+}
+
+// Selects a device for the lifetime of the scope and restores the caller's.
+class DeviceScope {
+  public:
+    explicit DeviceScope(int device) {
+        cuda_check(cudaGetDevice(&previous_), "cudaGetDevice");
+        if (device != previous_) cuda_check(cudaSetDevice(device), "cudaSetDevice");
+    }
+    ~DeviceScope() {
+        int now = -1;
+        if (cudaGetDevice(&now) == cudaSuccess && now != previous_) cudaSetDevice(previous_);
+    }
+    DeviceScope(const DeviceScope &) = delete;
+    DeviceScope &operator=(const DeviceScope &) = delete;
+
+  private:
+    int previous_{0};
+};
+
+// Owning device allocation (cudaMalloc / cudaFree).  Allocation happens in
+// setup and workspace growth only; the solve loop never allocates.
+template <class T>
+class DeviceBuffer {
+  public:
+    DeviceBuffer() = default;
+    explicit DeviceBuffer(size_t n) { allocate(n); }
+    ~DeviceBuffer() { release(); }
+    DeviceBuffer(const DeviceBuffer &) = delete;
+    DeviceBuffer &operator=(const DeviceBuffer &) = delete;
+    DeviceBuffer(DeviceBuffer &&o) noexcept { swap(o); }
+    DeviceBuffer &operator=(DeviceBuffer &&o) noexcept {
+        if (this != &o) {
+            DeviceBuffer t(std::move(o));
+            swap(t);
+        }
+        return *this;
+    }
+    void swap(DeviceBuffer &o) noexcept {
+        std::swap(ptr_, o.ptr_);
+        std::swap(size_, o.size_);
+        std::swap(device_, o.device_);
+    }
+    void allocate(size_t n) {
+        release();
+        if (n) {
+            cuda_check(cudaGetDevice(&device_), "cudaGetDevice");
+            cuda_check(cudaMalloc(&ptr_, n * sizeof(T)), "cudaMalloc");
+        }
+        size_ = n;
+    }
+    // Grows to at least n elements (contents not preserved).
+    void reserve(size_t n) {
+        if (n > size_) allocate(n);
+    }
+    void release() noexcept {
+        if (ptr_) {
+            int now = -1;
+            cudaGetDevice(&now);
+            if (now != device_) cudaSetDevice(device_);
+            cudaFree(ptr_);
+            if (now != device_) cudaSetDevice(now);
+        }
+        ptr_ = nullptr;
+        size_ = 0;
+    }
+    T *data() const noexcept { return static_cast<T *>(ptr_); }
+    size_t size() const noexcept { return size_; }
+    bool empty() const noexcept { return size_ == 0; }
+
+  private:
+    void *ptr_{nullptr};
+    size_t size_{0};
+    int device_{-1};
+};
+
+}  // namespace tfb
+
+// Execution context: one device, one stream, a scratch arena and a pinned
+// host staging word for scalar readbacks.
+struct tf_ctx {
+    int device{0};
+    cudaStream_t stream{nullptr};
+    bool own_stream{false};
+    int sm_count{148};
+    int64_t launches{0};
+    tfb::DeviceBuffer<unsigned char> scratch;  // grow-only, reused by primitives
+    tfb::DeviceBuffer<unsigned char> scratch2;
+    void *pinned{nullptr};                      // 256 bytes of pinned host memory
+    // Returns a scratch region of at least bytes (256-byte aligned start).
+    void *arena(size_t bytes, int slot = 0) {
+        auto &b = slot ? scratch2 : scratch;
+        b.reserve(bytes + 256);
+        return b.data();
+    }
+};
+
+namespace tfb {
+
+constexpr int kBlock = 256;
+
+inline unsigned grid_for(int64_t n, int block = kBlock) {
+    int64_t g = (n + block - 1) / block;
+    if (g < 1) g = 1;
+    if (g > 0x7fffffff) g = 0x7fffffff;
+    return static_cast<unsigned>(g);
+}
+
+// Checks the launch and counts it on the context.
+inline void launched(tf_ctx *ctx, const char *name) {
+    ++ctx->launches;
+    cuda_check(cudaGetLastError(), name);
+}
+
+// Synchronises the context stream and reads a device scalar.
+template <class T>
+T read_scalar(tf_ctx *ctx, const T *device_ptr) {
+    static_assert(sizeof(T) <= 256, "scalar too large");
+    cuda_check(cudaMemcpyAsync(ctx->pinned, device_ptr, sizeof(T), cudaMemcpyDeviceToHost, ctx->stream),
+               "scalar readback");
+    cuda_check(cudaStreamSynchronize(ctx->stream), "scalar readback sync");
+    T v;
+    std::memcpy(&v, ctx->pinned, sizeof(T));
+    return v;
+}
+
+inline void memset_async(tf_ctx *ctx, void *p, int value, size_t bytes) {
+    if (bytes) cuda_check(cudaMemsetAsync(p, value, bytes, ctx->stream), "cudaMemsetAsync");
+}
+
+inline void copy_async(tf_ctx *ctx, void *dst, const void *src, size_t bytes) {
+    if (bytes && dst != src) cuda_check(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, ctx->stream), "cudaMemcpyAsync");
+}
+
+inline size_t type_size(int t) {
+    switch (t) {
+        case TF_F32: return 4;
+        case TF_F64: return 8;
+        case TF_I32: return 4;
+        case TF_I64: return 8;
+    }
+    fail(TF_ERR_INVALID, "unknown element type");
+}
+
+inline void check_ctx(tf_ctx *ctx) { require(ctx != nullptr, "null context"); }
+
+inline void check_csr(const tf_csr *a) {
+    require(a != nullptr, "null CSR descriptor");
+    require(a->rows >= 0 && a->cols >= 0 && a->nnz >= 0, "negative CSR dimension");
+    require(a->index_type == TF_I32 || a->index_type == TF_I64, "CSR index type must be TF_I32 or TF_I64");
+    require(a->value_type == TF_F32 || a->value_type == TF_F64, "CSR value type must be TF_F32 or TF_F64");
+    require(a->offsets != nullptr || a->rows == 0, "null CSR offsets");
+    require((a->indices != nullptr && a->values != nullptr) || a->nnz == 0, "null CSR entries");
+    if (a->index_type == TF_I32) require(a->nnz <= INT32_MAX && a->rows < INT32_MAX, "CSR exceeds int32 indices", TF_ERR_LENGTH);
+}
+
+}  // namespace tfb
+
+// Owned device CSR returned by setup stages.
+struct tf_dcsr {
+    int64_t rows{0}, cols{0}, nnz{0};
+    int index_type{TF_I32}, value_type{TF_F64};
+    tfb::DeviceBuffer<unsigned char> offsets, indices, values;
+    tf_csr view() const {
+        tf_csr v;
+        v.rows = rows;
+        v.cols = cols;
+        v.nnz = nnz;
+        v.index_type = index_type;
+        v.value_type = value_type;
+        v.offsets = offsets.data();
+        v.indices = indices.data();
+        v.values = values.data();
+        return v;
+    }
+};
+
+struct tf_transfer {
+    int fine_rows{0}, coarse_rows{0};
+    int32_t histogram[4]{0, 0, 0, 0};
+    tfb::DeviceBuffer<int32_t> map, offsets, members;
+};

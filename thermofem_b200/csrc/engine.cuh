@@ -1,0 +1,72 @@
+// engine.cuh -- the AMG hierarchy and the Krylov solvers behind the
+// component API (include/Preconditioner/Amg.cuh, include/Solver/Cg.cuh,
+// include/Solver/BiCgStab.cuh of the reference).
+#pragma once
+#include <string>
+#include <vector>
+
+#include "ops.cuh"
+
+namespace tfb {
+
+struct LevelStats {
+    int64_t rows{0}, nnz{0};
+    int32_t histogram[4]{0, 0, 0, 0};
+};
+
+// Validated copy of tf_amg_options.
+struct AmgConfig {
+    tf_amg_options o;
+    explicit AmgConfig(const tf_amg_options &opt);
+};
+
+// Canonical FP64/int32 copy of a square CSR (GpuAggregation::canonical after
+// toNativeMatrix, src/Multigrid/GpuAggregation.cu:991-1007,1099-1136).
+std::unique_ptr<tf_dcsr> to_native(tf_ctx *ctx, const tf_csr &a);
+
+// A built hierarchy; the storage/arithmetic type of the cycle is fixed at
+// construction (TF_F64 or TF_F32).
+class Hierarchy {
+  public:
+    virtual ~Hierarchy() = default;
+    // x = M^-1 rhs (zero initial guess); enqueued on the context stream.
+    // rhs may alias x.  Vector type T is the caller's (float or double).
+    virtual void apply(tf_ctx *ctx, const double *rhs, double *x) = 0;
+    virtual void apply(tf_ctx *ctx, const float *rhs, float *x) = 0;
+    virtual int storage_type() const = 0;
+    virtual int64_t rows() const = 0;
+    virtual int level_count() const = 0;
+    virtual tf_csr level_matrix(int d) const = 0;
+    virtual void level_transfer(int d, const int32_t **map, const int32_t **off, const int32_t **mem,
+                                int *coarse) const = 0;
+    // Kernels launched by one cycle (graph replay counts them too).
+    virtual int64_t kernels_per_cycle() const = 0;
+
+    std::vector<LevelStats> stats;
+    std::vector<int64_t> visits;
+    std::string stop_reason, coarse_solver;
+};
+
+// Builds the hierarchy from the canonical native fine matrix (Amg::setup,
+// include/Preconditioner/Amg.cuh:81-143).  row_weights (optional, per level)
+// give per-row Jacobi damping for the smoothers.
+std::unique_ptr<Hierarchy> build_hierarchy(tf_ctx *ctx, const AmgConfig &cfg, int storage_type,
+                                           const tf_dcsr &native);
+
+// Krylov solver (kind TF_SOLVER_CG or TF_SOLVER_BICGSTAB) over vectors of T.
+class Krylov {
+  public:
+    virtual ~Krylov() = default;
+    virtual void setup(tf_ctx *ctx, const tf_csr &a) = 0;
+    // rhs/x are device pointers of T; x holds the initial guess.
+    virtual tf_solve_result solve(tf_ctx *ctx, const void *rhs, void *x) = 0;
+    virtual Hierarchy *amg() = 0;
+    virtual int64_t rows() const = 0;
+    double last_ms{0};
+};
+
+std::unique_ptr<Krylov> make_krylov(int kind, int value_type, int index_type, const tf_solver_options &opt,
+                                    int precond, const tf_amg_options *amg_opt);
+void validate_solver_options(const tf_solver_options &o);
+
+}  // namespace tfb

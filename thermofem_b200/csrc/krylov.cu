@@ -1,0 +1,710 @@
+// krylov.cu -- PCG and right-preconditioned BiCGStab with the scalar
+// recurrences on the device.
+//
+// The control flow is the reference's (PCG: include/Solver/Cg.cuh:123-189;
+// BiCGStab: include/Solver/BiCgStab.cuh:144-247), including the
+// breakdown/non-finite checks, the true-residual confirmation of a candidate
+// convergence and the periodic refresh with restart.  The difference is
+// where it runs: each scalar decision is a one-CTA kernel that finishes a
+// deterministic reduction and updates a device-resident state record, and
+// the vector kernels are gated on that record, so one iteration is a fixed
+// kernel sequence captured once into a CUDA graph.  Reductions are fused
+// into the producing pass (p.Ap into the SpMV that makes Ap, ||r||^2 into the
+// x/r update, t.t and t.s into the SpMV that makes t).  The host reads one
+// word per iteration to stop the loop.
+#include "engine.cuh"
+#include "tile.cuh"
+
+namespace tfb {
+namespace {
+
+enum : int { kRunning = -1 };
+
+struct KState {
+    double normB, tol, res, rho, rho_prev, alpha, omega, beta, curv;
+    int it, status, running, fresh, pmode, refresh, early, normal, copy_shadow, max_it, interval;
+};
+
+constexpr int kParts = 1184;  // upper bound of grid-stride partial sums
+
+int parts_for(int64_t n) {
+    int64_t p = (n + 2047) / 2048;
+    return static_cast<int>(p < 1 ? 1 : (p > kParts ? kParts : p));
+}
+
+// Fixed-order sum of K partial arrays [K][parts]; valid in thread 0.
+template <int K>
+__device__ __forceinline__ void sum_partials(const double *part, int parts, double (&v)[K]) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        v[k] = 0.0;
+        for (int p = threadIdx.x; p < parts; p += blockDim.x) v[k] += part[k * parts + p];
+    }
+    tile::block_reduce<K>(v);
+}
+
+__device__ __forceinline__ void stop(KState *s, int status) {
+    s->status = status;
+    s->running = 0;
+}
+
+// ---- shared steps --------------------------------------------------------
+
+// After r = b - A x0 and ||b||^2 partials: initial decisions (Cg.cuh:125-137).
+__global__ void k_init(KState *s, const double *pb, int nb, const double *pr, int nr, int bicg) {
+    double vb[1], vr[1];
+    sum_partials<1>(pb, nb, vb);
+    __syncthreads();
+    sum_partials<1>(pr, nr, vr);
+    if (threadIdx.x) return;
+    s->normB = sqrt(vb[0]);
+    s->tol = fmax(s->tol, s->res * s->normB);  // s->res carries rtol in, tol carries atol in
+    s->res = sqrt(vr[0]);
+    s->it = 0;
+    s->fresh = 1;
+    s->refresh = s->early = s->copy_shadow = 0;
+    s->normal = 1;
+    s->rho_prev = 1;
+    s->alpha = 1;
+    s->omega = 1;
+    if (!isfinite(s->normB) || !isfinite(s->res)) stop(s, TF_NONFINITE);
+    else if (s->res <= s->tol) stop(s, TF_CONVERGED);
+    else {
+        s->status = kRunning;
+        s->running = 1;
+        s->copy_shadow = bicg;  // BiCGStab: shadow = r
+    }
+}
+
+// Final report from the true residual (Cg.cuh:105-121, BiCgStab.cuh:122-136).
+__global__ void k_finish(KState *s, const double *pr, int nr) {
+    double v[1];
+    sum_partials<1>(pr, nr, v);
+    if (threadIdx.x) return;
+    const double res = sqrt(v[0]);
+    int status = s->status == kRunning ? TF_MAX_ITERATIONS : s->status;
+    if (!isfinite(res) || !isfinite(s->normB)) status = TF_NONFINITE;
+    else if (res <= s->tol) status = TF_CONVERGED;
+    else if (status == TF_CONVERGED) status = TF_MAX_ITERATIONS;
+    s->status = status;
+    s->res = res;
+    s->running = 0;
+}
+
+template <class T>
+__global__ void k_copy_if(const int *flag, int64_t n, const T *__restrict__ src, T *__restrict__ dst) {
+    if (!*flag) return;
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        dst[i] = src[i];
+}
+
+__global__ void k_clear_flag(int *flag) { *flag = 0; }
+
+template <class T>
+__global__ void k_dot(int64_t n, const T *__restrict__ x, const T *__restrict__ y, double *part) {
+    double v[1] = {0.0};
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        v[0] += static_cast<double>(x[i]) * static_cast<double>(y[i]);
+    tile::block_reduce<1>(v);
+    if (threadIdx.x == 0) part[blockIdx.x] = v[0];
+}
+
+// y = A x with sum_i w_i y_i; gated on *gate.
+template <class T>
+struct SpmvDot {
+    static constexpr int kReduce = 1;
+    T *__restrict__ y;
+    const T *__restrict__ w;
+    const int *gate;
+    double *partial;
+    __device__ __forceinline__ bool skip() const { return gate && !*gate; }
+    template <class XS>
+    __device__ __forceinline__ void operator()(int64_t i, T acc, const XS &, double (&red)[1]) const {
+        y[i] = acc;
+        red[0] += static_cast<double>(w[i]) * static_cast<double>(acc);
+    }
+};
+
+// t = A x with sum t_i^2 and sum t_i s_i; gated.
+template <class T>
+struct SpmvDot2 {
+    static constexpr int kReduce = 2;
+    T *__restrict__ y;
+    const T *__restrict__ s;
+    const int *gate;
+    double *partial;
+    __device__ __forceinline__ bool skip() const { return gate && !*gate; }
+    template <class XS>
+    __device__ __forceinline__ void operator()(int64_t i, T acc, const XS &, double (&red)[2]) const {
+        y[i] = acc;
+        const double t = static_cast<double>(acc);
+        red[0] += t * t;
+        red[1] += t * static_cast<double>(s[i]);
+    }
+};
+
+// r = b - A x with sum r_i^2; gated (gate may be null).
+template <class T>
+struct ResidualNorm {
+    static constexpr int kReduce = 1;
+    const T *__restrict__ b;
+    T *__restrict__ r;
+    const int *gate;
+    double *partial;
+    __device__ __forceinline__ bool skip() const { return gate && !*gate; }
+    template <class XS>
+    __device__ __forceinline__ void operator()(int64_t i, T acc, const XS &, double (&red)[1]) const {
+        const T v = b[i] - acc;
+        r[i] = v;
+        red[0] += static_cast<double>(v) * static_cast<double>(v);
+    }
+};
+
+// ---- PCG -----------------------------------------------------------------
+
+__global__ void cg_rho(KState *s, const double *part, int parts) {
+    if (!s->running) return;
+    double v[1];
+    sum_partials<1>(part, parts, v);
+    if (threadIdx.x) return;
+    s->it += 1;
+    const double rho = v[0];
+    s->rho = rho;
+    if (!isfinite(rho)) return stop(s, TF_NONFINITE);
+    if (rho <= 0) return stop(s, TF_BREAKDOWN);
+    if (s->fresh) {
+        s->pmode = 0;
+        s->fresh = 0;
+    } else {
+        const double beta = rho / s->rho_prev;
+        if (!isfinite(beta)) return stop(s, TF_NONFINITE);
+        s->beta = beta;
+        s->pmode = 1;
+    }
+}
+
+template <class T>
+__global__ void cg_p(const KState *s, int64_t n, const T *__restrict__ z, T *__restrict__ p) {
+    if (!s->running) return;
+    const int mode = s->pmode;
+    const T beta = static_cast<T>(s->beta);
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        p[i] = mode ? z[i] + beta * p[i] : z[i];
+}
+
+__global__ void cg_curv(KState *s, const double *part, int parts) {
+    if (!s->running) return;
+    double v[1];
+    sum_partials<1>(part, parts, v);
+    if (threadIdx.x) return;
+    const double c = v[0];
+    s->curv = c;
+    if (!isfinite(c)) return stop(s, TF_NONFINITE);
+    if (c <= 0) return stop(s, TF_BREAKDOWN);
+    const double alpha = s->rho / c;
+    if (!isfinite(alpha)) return stop(s, TF_NONFINITE);
+    s->alpha = alpha;
+}
+
+template <class T>
+__global__ void cg_xr(const KState *s, int64_t n, const T *__restrict__ p, const T *__restrict__ ap, T *__restrict__ x,
+                      T *__restrict__ r, double *part) {
+    if (!s->running) return;
+    const T alpha = static_cast<T>(s->alpha);
+    double v[1] = {0.0};
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        x[i] += alpha * p[i];
+        const T ri = r[i] - alpha * ap[i];
+        r[i] = ri;
+        v[0] += static_cast<double>(ri) * static_cast<double>(ri);
+    }
+    tile::block_reduce<1>(v);
+    if (threadIdx.x == 0) part[blockIdx.x] = v[0];
+}
+
+// ||r|| check, refresh decision (Cg.cuh:170-178).
+__global__ void cg_res(KState *s, const double *part, int parts) {
+    if (!s->running) return;
+    double v[1];
+    sum_partials<1>(part, parts, v);
+    if (threadIdx.x) return;
+    const double res = sqrt(v[0]);
+    s->res = res;
+    if (!isfinite(res)) return stop(s, TF_NONFINITE);
+    if (res <= s->tol || s->it % s->interval == 0) s->refresh = 1;
+}
+
+// After a gated true residual: confirm or restart (Cg.cuh:178-185), then
+// close the iteration.
+__global__ void cg_end(KState *s, const double *part, int parts) {
+    if (!s->running) return;
+    double v[1];
+    if (s->refresh) sum_partials<1>(part, parts, v);
+    if (threadIdx.x) return;
+    if (s->refresh) {
+        s->refresh = 0;
+        const double res = sqrt(v[0]);
+        s->res = res;
+        if (!isfinite(res) || res <= s->tol) return stop(s, TF_MAX_ITERATIONS);
+        s->fresh = 1;
+    }
+    s->rho_prev = s->rho;
+    if (s->it >= s->max_it) stop(s, TF_MAX_ITERATIONS);
+}
+
+// ---- BiCGStab ------------------------------------------------------------
+
+__global__ void bi_rho(KState *s, const double *part, int parts) {
+    if (!s->running) return;
+    double v[1];
+    sum_partials<1>(part, parts, v);
+    if (threadIdx.x) return;
+    s->it += 1;
+    s->normal = 1;
+    s->early = 0;
+    s->copy_shadow = 0;
+    const double rho = v[0];
+    s->rho = rho;
+    if (!isfinite(rho)) return stop(s, TF_NONFINITE);
+    if (rho == 0) return stop(s, TF_BREAKDOWN);
+    if (s->fresh) {
+        s->pmode = 0;
+        s->fresh = 0;
+    } else {
+        const double beta = (rho / s->rho_prev) * (s->alpha / s->omega);
+        if (!isfinite(beta)) return stop(s, TF_NONFINITE);
+        s->beta = beta;
+        s->pmode = 1;
+    }
+}
+
+// p = r (fresh) or p = r + beta (p - omega v) (BiCgStab.cuh:176-184).
+template <class T>
+__global__ void bi_p(const KState *s, int64_t n, const T *__restrict__ r, const T *__restrict__ v, T *__restrict__ p) {
+    if (!s->running) return;
+    const int mode = s->pmode;
+    const T beta = static_cast<T>(s->beta), omega = static_cast<T>(s->omega);
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        if (mode) {
+            const T t = p[i] - omega * v[i];
+            p[i] = r[i] + beta * t;
+        } else {
+            p[i] = r[i];
+        }
+    }
+}
+
+__global__ void bi_alpha(KState *s, const double *part, int parts) {
+    if (!s->running) return;
+    double v[1];
+    sum_partials<1>(part, parts, v);
+    if (threadIdx.x) return;
+    const double den = v[0];
+    if (!isfinite(den)) return stop(s, TF_NONFINITE);
+    if (den == 0) return stop(s, TF_BREAKDOWN);
+    const double alpha = s->rho / den;
+    if (!isfinite(alpha)) return stop(s, TF_NONFINITE);
+    s->alpha = alpha;
+}
+
+// s = r - alpha v, x += alpha phat, sum s_i^2.
+template <class T>
+__global__ void bi_s(const KState *st, int64_t n, const T *__restrict__ r, const T *__restrict__ v,
+                     const T *__restrict__ ph, T *__restrict__ sv, T *__restrict__ x, double *part) {
+    if (!st->running) return;
+    const T alpha = static_cast<T>(st->alpha);
+    double acc[1] = {0.0};
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const T si = r[i] - alpha * v[i];
+        sv[i] = si;
+        x[i] += alpha * ph[i];
+        acc[0] += static_cast<double>(si) * static_cast<double>(si);
+    }
+    tile::block_reduce<1>(acc);
+    if (threadIdx.x == 0) part[blockIdx.x] = acc[0];
+}
+
+// ||s|| check: candidate convergence takes the early path (BiCgStab.cuh:199-211).
+__global__ void bi_snorm(KState *s, const double *part, int parts) {
+    if (!s->running) return;
+    double v[1];
+    sum_partials<1>(part, parts, v);
+    if (threadIdx.x) return;
+    const double ns = sqrt(v[0]);
+    if (!isfinite(ns)) return stop(s, TF_NONFINITE);
+    if (ns <= s->tol) {
+        s->early = 1;
+        s->normal = 0;
+    }
+}
+
+// Early path after the gated true residual: confirm or restart, skipping the
+// omega half and the rho_prev update of this iteration.
+__global__ void bi_early(KState *s, const double *part, int parts) {
+    if (!s->running || !s->early) return;
+    double v[1];
+    sum_partials<1>(part, parts, v);
+    if (threadIdx.x) return;
+    const double res = sqrt(v[0]);
+    s->res = res;
+    if (res <= s->tol || !isfinite(res)) return stop(s, TF_MAX_ITERATIONS);
+    s->copy_shadow = 1;
+    s->fresh = 1;
+}
+
+__global__ void bi_omega(KState *s, const double *part, int parts) {
+    if (!s->running || !s->normal) return;
+    double v[2];
+    sum_partials<2>(part, parts, v);
+    if (threadIdx.x) return;
+    const double tt = v[0], ts = v[1];
+    if (!isfinite(tt) || !isfinite(ts)) return stop(s, TF_NONFINITE);
+    if (tt == 0) return stop(s, TF_BREAKDOWN);
+    const double omega = ts / tt;
+    if (!isfinite(omega)) return stop(s, TF_NONFINITE);
+    if (omega == 0) return stop(s, TF_BREAKDOWN);
+    s->omega = omega;
+}
+
+// x += omega shat, r = s - omega t, sum r_i^2.
+template <class T>
+__global__ void bi_xr(const KState *st, int64_t n, const T *__restrict__ sh, const T *__restrict__ sv,
+                      const T *__restrict__ t, T *__restrict__ x, T *__restrict__ r, double *part) {
+    if (!st->running || !st->normal) return;
+    const T omega = static_cast<T>(st->omega);
+    double acc[1] = {0.0};
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        x[i] += omega * sh[i];
+        const T ri = sv[i] - omega * t[i];
+        r[i] = ri;
+        acc[0] += static_cast<double>(ri) * static_cast<double>(ri);
+    }
+    tile::block_reduce<1>(acc);
+    if (threadIdx.x == 0) part[blockIdx.x] = acc[0];
+}
+
+__global__ void bi_res(KState *s, const double *part, int parts) {
+    if (!s->running || !s->normal) return;
+    double v[1];
+    sum_partials<1>(part, parts, v);
+    if (threadIdx.x) return;
+    const double res = sqrt(v[0]);
+    s->res = res;
+    if (!isfinite(res)) return stop(s, TF_NONFINITE);
+    if (res <= s->tol || s->it % s->interval == 0) s->refresh = 1;
+}
+
+__global__ void bi_end(KState *s, const double *part, int parts) {
+    if (!s->running) return;
+    double v[1];
+    const bool refresh = s->normal && s->refresh;
+    if (refresh) sum_partials<1>(part, parts, v);
+    if (threadIdx.x) return;
+    if (refresh) {
+        s->refresh = 0;
+        const double res = sqrt(v[0]);
+        s->res = res;
+        if (res <= s->tol || !isfinite(res)) return stop(s, TF_MAX_ITERATIONS);
+        s->copy_shadow = 1;
+        s->fresh = 1;
+    }
+    if (s->normal) s->rho_prev = s->rho;
+    if (s->it >= s->max_it) stop(s, TF_MAX_ITERATIONS);
+}
+
+// ---- solver object --------------------------------------------------------
+
+template <class T, class I>
+class KrylovImpl final : public Krylov {
+  public:
+    KrylovImpl(int kind, const tf_solver_options &opt, int precond, const tf_amg_options *amg)
+        : kind_(kind), opt_(opt), precond_(precond) {
+        validate_solver_options(opt);
+        if (precond == TF_PRECOND_AMG) {
+            require(amg != nullptr, "AMG options required");
+            amg_cfg_ = std::make_unique<AmgConfig>(*amg);
+        } else {
+            require(precond == TF_PRECOND_IDENTITY, "unknown preconditioner");
+        }
+    }
+    ~KrylovImpl() override {
+        if (exec_) cudaGraphExecDestroy(exec_);
+        if (ev0_) cudaEventDestroy(ev0_);
+        if (ev1_) cudaEventDestroy(ev1_);
+    }
+
+    void setup(tf_ctx *ctx, const tf_csr &a) override {
+        ready_ = false;
+        if (exec_) {
+            cudaGraphExecDestroy(exec_);
+            exec_ = nullptr;
+        }
+        check_csr(&a);
+        require(a.rows > 0 && a.rows == a.cols, "Solver requires a nonempty square matrix");
+        require(sizeof(T) == type_size(a.value_type) && sizeof(I) == type_size(a.index_type),
+                "matrix types differ from the solver's");
+        // Snapshot: canonical copy (duplicates summed), finite values.
+        std::unique_ptr<tf_dcsr> native;
+        try {
+            native = to_native(ctx, a);
+        } catch (const Failure &f) {
+            if (f.code == TF_ERR_INVALID) fail(TF_ERR_INVALID, "Matrix contains nonfinite entries");
+            throw;
+        }
+        n_ = a.rows;
+        nnz_ = native->nnz;
+        rp_.allocate(static_cast<size_t>(n_) + 1);
+        ci_.allocate(static_cast<size_t>(nnz_));
+        val_.allocate(static_cast<size_t>(nnz_));
+        const auto nc = csr_of(*native);
+        convert(ctx, n_ + 1, nc.rp, rp_.data());
+        convert(ctx, nnz_, nc.ci, ci_.data());
+        convert(ctx, nnz_, nc.val, val_.data());
+        hier_.reset();
+        if (precond_ == TF_PRECOND_AMG) {
+            const int storage = amg_cfg_->o.hierarchy_type == -1 ? (sizeof(T) == 8 ? TF_F64 : TF_F32)
+                                                                 : amg_cfg_->o.hierarchy_type;
+            hier_ = build_hierarchy(ctx, *amg_cfg_, storage, *native);
+        }
+        for (auto *b : {&rhs_, &x_, &r_, &z_, &p_, &q_, &shadow_, &s_, &t_, &sh_})
+            b->allocate(static_cast<size_t>(n_));
+        const auto shape = spmv_shape(n_, nnz_, sizeof(T), sizeof(I));
+        tiles_ = static_cast<int>(tile::grid(shape, n_));
+        parts_ = parts_for(n_);
+        part_.allocate(static_cast<size_t>(2 * std::max(tiles_, parts_)));
+        partb_.allocate(static_cast<size_t>(std::max(tiles_, parts_)));
+        state_.allocate(1);
+        if (!ev0_) {
+            cuda_check(cudaEventCreate(&ev0_), "event");
+            cuda_check(cudaEventCreate(&ev1_), "event");
+        }
+        cuda_check(cudaStreamSynchronize(ctx->stream), "solver setup");
+        ready_ = true;
+    }
+
+    tf_solve_result solve(tf_ctx *ctx, const void *rhs, void *x) override {
+        if (!ready_) fail(TF_ERR_LOGIC, kind_ == TF_SOLVER_CG ? "CG requires setup" : "BiCGStab requires setup");
+        cuda_check(cudaEventRecord(ev0_, ctx->stream), "event");
+        copy_async(ctx, rhs_.data(), rhs, n_ * sizeof(T));
+        copy_async(ctx, x_.data(), x, n_ * sizeof(T));
+        KState init{};
+        init.tol = opt_.absolute_tolerance;
+        init.res = opt_.relative_tolerance;
+        init.max_it = opt_.max_iterations;
+        init.interval = opt_.residual_refresh_interval;
+        init.status = TF_MAX_ITERATIONS;
+        cuda_check(cudaMemcpyAsync(state_.data(), &init, sizeof(KState), cudaMemcpyHostToDevice, ctx->stream),
+                   "state upload");
+        // ||b||^2 and r = b - A x with ||r||^2.
+        k_dot<T><<<parts_, 256, 0, ctx->stream>>>(n_, rhs_.data(), rhs_.data(), partb_.data());
+        launched(ctx, "dot");
+        tile::launch(ctx, csr(), tile::PlainX<T>{x_.data()},
+                     ResidualNorm<T>{rhs_.data(), r_.data(), nullptr, part_.data()}, "residual_norm");
+        k_init<<<1, 256, 0, ctx->stream>>>(state_.data(), partb_.data(), parts_, part_.data(), tiles_,
+                                          kind_ == TF_SOLVER_BICGSTAB ? 1 : 0);
+        launched(ctx, "k_init");
+        if (kind_ == TF_SOLVER_BICGSTAB) {
+            k_copy_if<T><<<parts_, 256, 0, ctx->stream>>>(&state_.data()->copy_shadow, n_, r_.data(), shadow_.data());
+            launched(ctx, "copy_if");
+        }
+        int *running = static_cast<int *>(ctx->pinned);
+        cuda_check(cudaMemcpyAsync(running, &state_.data()->running, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream),
+                   "state readback");
+        cuda_check(cudaStreamSynchronize(ctx->stream), "solve init");
+        for (int k = 0; k < opt_.max_iterations && *running; ++k) {
+            run_iteration(ctx);
+            cuda_check(cudaMemcpyAsync(running, &state_.data()->running, sizeof(int), cudaMemcpyDeviceToHost,
+                                       ctx->stream),
+                       "state readback");
+            cuda_check(cudaStreamSynchronize(ctx->stream), "iteration");
+        }
+        // Final true residual and report.
+        tile::launch(ctx, csr(), tile::PlainX<T>{x_.data()},
+                     ResidualNorm<T>{rhs_.data(), r_.data(), nullptr, part_.data()}, "residual_norm");
+        k_finish<<<1, 256, 0, ctx->stream>>>(state_.data(), part_.data(), tiles_);
+        launched(ctx, "k_finish");
+        copy_async(ctx, x, x_.data(), n_ * sizeof(T));
+        KState fin;
+        cuda_check(cudaMemcpyAsync(ctx->pinned, state_.data(), sizeof(KState) <= 256 ? sizeof(KState) : 256,
+                                   cudaMemcpyDeviceToHost, ctx->stream),
+                   "state readback");
+        cuda_check(cudaEventRecord(ev1_, ctx->stream), "event");
+        cuda_check(cudaStreamSynchronize(ctx->stream), "solve");
+        std::memcpy(&fin, ctx->pinned, sizeof(KState));
+        float ms = 0;
+        cudaEventElapsedTime(&ms, ev0_, ev1_);
+        last_ms = ms;
+        tf_solve_result out;
+        out.status = fin.status;
+        out.iterations = fin.it;
+        out.residual_norm = fin.res;
+        out.relative_residual = fin.normB > 0 ? fin.res / fin.normB : fin.res;
+        return out;
+    }
+
+    Hierarchy *amg() override { return hier_.get(); }
+    int64_t rows() const override { return n_; }
+
+  private:
+    Csr<T, I> csr() const {
+        Csr<T, I> c;
+        c.rows = c.cols = n_;
+        c.nnz = nnz_;
+        c.rp = rp_.data();
+        c.ci = ci_.data();
+        c.val = val_.data();
+        return c;
+    }
+
+    void precondition(tf_ctx *ctx, const T *in, T *out) {
+        if (hier_) hier_->apply(ctx, in, out);
+        else copy_async(ctx, out, in, n_ * sizeof(T));
+    }
+
+    void run_iteration(tf_ctx *ctx) {
+        if (!exec_ && !capture_failed_) {
+            if (cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+                const int64_t before = ctx->launches;
+                cudaGraph_t g = nullptr;
+                try {
+                    enqueue_iteration(ctx);
+                } catch (...) {
+                    cudaStreamEndCapture(ctx->stream, &g);
+                    if (g) cudaGraphDestroy(g);
+                    throw;
+                }
+                per_iteration_ = ctx->launches - before;
+                ctx->launches = before;
+                cuda_check(cudaStreamEndCapture(ctx->stream, &g), "iteration capture");
+                if (cudaGraphInstantiate(&exec_, g, 0) != cudaSuccess) {
+                    cudaGetLastError();
+                    exec_ = nullptr;
+                    capture_failed_ = true;
+                }
+                cudaGraphDestroy(g);
+            } else {
+                cudaGetLastError();
+                capture_failed_ = true;
+            }
+        }
+        if (exec_) {
+            cuda_check(cudaGraphLaunch(exec_, ctx->stream), "iteration graph");
+            ctx->launches += per_iteration_;
+        } else {
+            enqueue_iteration(ctx);
+        }
+    }
+
+    void enqueue_iteration(tf_ctx *ctx) {
+        KState *s = state_.data();
+        double *part = part_.data();
+        const unsigned pg = static_cast<unsigned>(parts_);
+        if (kind_ == TF_SOLVER_CG) {
+            precondition(ctx, r_.data(), z_.data());
+            k_dot<T><<<pg, 256, 0, ctx->stream>>>(n_, r_.data(), z_.data(), part);
+            launched(ctx, "dot");
+            cg_rho<<<1, 256, 0, ctx->stream>>>(s, part, parts_);
+            launched(ctx, "cg_rho");
+            cg_p<T><<<pg, 256, 0, ctx->stream>>>(s, n_, z_.data(), p_.data());
+            launched(ctx, "cg_p");
+            tile::launch(ctx, csr(), tile::PlainX<T>{p_.data()}, SpmvDot<T>{q_.data(), p_.data(), &s->running, part},
+                         "spmv_dot");
+            cg_curv<<<1, 256, 0, ctx->stream>>>(s, part, tiles_);
+            launched(ctx, "cg_curv");
+            cg_xr<T><<<pg, 256, 0, ctx->stream>>>(s, n_, p_.data(), q_.data(), x_.data(), r_.data(), part);
+            launched(ctx, "cg_xr");
+            cg_res<<<1, 256, 0, ctx->stream>>>(s, part, parts_);
+            launched(ctx, "cg_res");
+            tile::launch(ctx, csr(), tile::PlainX<T>{x_.data()},
+                         ResidualNorm<T>{rhs_.data(), r_.data(), &s->refresh, part}, "residual_norm");
+            cg_end<<<1, 256, 0, ctx->stream>>>(s, part, tiles_);
+            launched(ctx, "cg_end");
+            return;
+        }
+        // BiCGStab: v = q_, phat = z_
+        k_dot<T><<<pg, 256, 0, ctx->stream>>>(n_, shadow_.data(), r_.data(), part);
+        launched(ctx, "dot");
+        bi_rho<<<1, 256, 0, ctx->stream>>>(s, part, parts_);
+        launched(ctx, "bi_rho");
+        bi_p<T><<<pg, 256, 0, ctx->stream>>>(s, n_, r_.data(), q_.data(), p_.data());
+        launched(ctx, "bi_p");
+        precondition(ctx, p_.data(), z_.data());
+        tile::launch(ctx, csr(), tile::PlainX<T>{z_.data()}, SpmvDot<T>{q_.data(), shadow_.data(), &s->running, part},
+                     "spmv_dot");
+        bi_alpha<<<1, 256, 0, ctx->stream>>>(s, part, tiles_);
+        launched(ctx, "bi_alpha");
+        bi_s<T><<<pg, 256, 0, ctx->stream>>>(s, n_, r_.data(), q_.data(), z_.data(), s_.data(), x_.data(), part);
+        launched(ctx, "bi_s");
+        bi_snorm<<<1, 256, 0, ctx->stream>>>(s, part, parts_);
+        launched(ctx, "bi_snorm");
+        tile::launch(ctx, csr(), tile::PlainX<T>{x_.data()}, ResidualNorm<T>{rhs_.data(), r_.data(), &s->early, part},
+                     "residual_norm");
+        bi_early<<<1, 256, 0, ctx->stream>>>(s, part, tiles_);
+        launched(ctx, "bi_early");
+        precondition(ctx, s_.data(), sh_.data());
+        tile::launch(ctx, csr(), tile::PlainX<T>{sh_.data()}, SpmvDot2<T>{t_.data(), s_.data(), &s->normal, part},
+                     "spmv_dot2");
+        bi_omega<<<1, 256, 0, ctx->stream>>>(s, part, tiles_);
+        launched(ctx, "bi_omega");
+        bi_xr<T><<<pg, 256, 0, ctx->stream>>>(s, n_, sh_.data(), s_.data(), t_.data(), x_.data(), r_.data(), part);
+        launched(ctx, "bi_xr");
+        bi_res<<<1, 256, 0, ctx->stream>>>(s, part, parts_);
+        launched(ctx, "bi_res");
+        tile::launch(ctx, csr(), tile::PlainX<T>{x_.data()}, ResidualNorm<T>{rhs_.data(), r_.data(), &s->refresh, part},
+                     "residual_norm");
+        bi_end<<<1, 256, 0, ctx->stream>>>(s, part, tiles_);
+        launched(ctx, "bi_end");
+        k_copy_if<T><<<pg, 256, 0, ctx->stream>>>(&s->copy_shadow, n_, r_.data(), shadow_.data());
+        launched(ctx, "copy_if");
+    }
+
+    int kind_;
+    tf_solver_options opt_;
+    int precond_;
+    std::unique_ptr<AmgConfig> amg_cfg_;
+    std::unique_ptr<Hierarchy> hier_;
+    bool ready_{false};
+    int64_t n_{0}, nnz_{0};
+    DeviceBuffer<I> rp_, ci_;
+    DeviceBuffer<T> val_;
+    DeviceBuffer<T> rhs_, x_, r_, z_, p_, q_, shadow_, s_, t_, sh_;
+    DeviceBuffer<double> part_, partb_;
+    DeviceBuffer<KState> state_;
+    int tiles_{1}, parts_{1};
+    cudaGraphExec_t exec_{nullptr};
+    bool capture_failed_{false};
+    int64_t per_iteration_{0};
+    cudaEvent_t ev0_{nullptr}, ev1_{nullptr};
+};
+
+}  // namespace
+
+void validate_solver_options(const tf_solver_options &o) {
+    if (o.max_iterations < 0 || o.residual_refresh_interval < 1 || !std::isfinite(o.relative_tolerance) ||
+        o.relative_tolerance < 0 || o.relative_tolerance >= 1 || !std::isfinite(o.absolute_tolerance) ||
+        o.absolute_tolerance < 0)
+        fail(TF_ERR_INVALID, "Invalid solver options");
+}
+
+std::unique_ptr<Krylov> make_krylov(int kind, int value_type, int index_type, const tf_solver_options &opt,
+                                    int precond, const tf_amg_options *amg_opt) {
+    require(kind == TF_SOLVER_CG || kind == TF_SOLVER_BICGSTAB, "unknown solver kind");
+    if (value_type == TF_F64 && index_type == TF_I32)
+        return std::make_unique<KrylovImpl<double, int32_t>>(kind, opt, precond, amg_opt);
+    if (value_type == TF_F64 && index_type == TF_I64)
+        return std::make_unique<KrylovImpl<double, int64_t>>(kind, opt, precond, amg_opt);
+    if (value_type == TF_F32 && index_type == TF_I32)
+        return std::make_unique<KrylovImpl<float, int32_t>>(kind, opt, precond, amg_opt);
+    if (value_type == TF_F32 && index_type == TF_I64)
+        return std::make_unique<KrylovImpl<float, int64_t>>(kind, opt, precond, amg_opt);
+    fail(TF_ERR_INVALID, "unsupported solver types");
+}
+
+}  // namespace tfb

@@ -1,0 +1,340 @@
+// objects.cu -- component objects of the C ABI: AMG preconditioner, Jacobi
+// smoother and Krylov solvers (the setup/apply components of
+// include/Preconditioner/Amg.cuh, include/Smoother/Jacobi.cuh and
+// include/Solver/{Cg,BiCgStab}.cuh).  Setup is transactional for AMG and
+// Jacobi (a failure keeps the previous state) and invalidating for solvers,
+// as in the reference.
+#include "engine.cuh"
+
+using namespace tfb;
+
+struct tf_amg {
+    tf_ctx *ctx;
+    int value_type, index_type;
+    AmgConfig cfg;
+    std::unique_ptr<Hierarchy> owned;
+    Hierarchy *h{nullptr};  // owned.get(), or a solver's hierarchy for borrowed views
+};
+
+struct tf_jacobi {
+    tf_ctx *ctx;
+    int value_type, index_type;
+    int sweeps;
+    double weight;
+    bool ready{false};
+    int64_t n{0}, nnz{0};
+    DeviceBuffer<int32_t> rp, ci;
+    DeviceBuffer<unsigned char> val, dinv, rhs, x0, x1;
+};
+
+struct tf_solver {
+    tf_ctx *ctx;
+    int value_type, index_type;
+    std::unique_ptr<Krylov> k;
+    DeviceBuffer<unsigned char> hb, hx;  // staging for host-buffer applies
+    std::unique_ptr<tf_amg> view;        // borrowed view of the AMG preconditioner
+};
+
+namespace {
+
+void check_types(int value_type, int index_type) {
+    require(value_type == TF_F32 || value_type == TF_F64, "value type must be TF_F32 or TF_F64");
+    require(index_type == TF_I32 || index_type == TF_I64, "index type must be TF_I32 or TF_I64");
+}
+
+void check_matrix_types(const tf_csr *a, int value_type, int index_type) {
+    check_csr(a);
+    require(a->value_type == value_type && a->index_type == index_type, "matrix types differ from the component's");
+}
+
+}  // namespace
+
+extern "C" {
+
+void tf_amg_options_default(tf_amg_options *o) {
+    if (!o) return;
+    o->max_levels = 20;
+    o->coarse_rows = 64;
+    o->matching_rounds = 8;
+    o->pre_sweeps = 1;
+    o->post_sweeps = 1;
+    o->coarse_sweeps = 8;
+    o->jacobi_weight = 0.75;
+    o->strength_threshold = 0.25;
+    o->absorb_singletons = 1;
+    o->compact_sort_keys = 0;
+    o->cycle = TF_CYCLE_V;
+    o->hierarchy_type = -1;
+    o->coarse_lu_rows = 64;
+}
+
+void tf_solver_options_default(int value_type, tf_solver_options *o) {
+    if (!o) return;
+    o->max_iterations = 1000;
+    o->relative_tolerance = value_type == TF_F32 ? static_cast<double>(1e-5f) : 1e-8;
+    o->absolute_tolerance = 0;
+    o->residual_refresh_interval = 50;
+}
+
+int tf_amg_create(tf_ctx *ctx, int value_type, int index_type, const tf_amg_options *opt, tf_amg **out) {
+    return guard([&] {
+        check_ctx(ctx);
+        require(out && opt, "null argument");
+        *out = nullptr;
+        check_types(value_type, index_type);
+        *out = new tf_amg{ctx, value_type, index_type, AmgConfig(*opt), nullptr, nullptr};
+    });
+}
+
+int tf_amg_destroy(tf_amg *m) {
+    return guard([&] {
+        if (!m) return;
+        DeviceScope scope(m->ctx->device);
+        delete m;
+    });
+}
+
+int tf_amg_setup(tf_amg *m, const tf_csr *a) {
+    return guard([&] {
+        require(m != nullptr, "null AMG");
+        check_matrix_types(a, m->value_type, m->index_type);
+        require(a->rows > 0 && a->rows == a->cols, "Solver requires a nonempty square matrix");
+        DeviceScope scope(m->ctx->device);
+        auto native = to_native(m->ctx, *a);
+        const int storage = m->cfg.o.hierarchy_type == -1 ? m->value_type : m->cfg.o.hierarchy_type;
+        auto h = build_hierarchy(m->ctx, m->cfg, storage, *native);
+        m->owned = std::move(h);
+        m->h = m->owned.get();
+    });
+}
+
+int tf_amg_apply(tf_amg *m, const void *rhs, void *x) {
+    return guard([&] {
+        require(m != nullptr, "null AMG");
+        if (!m->h) fail(TF_ERR_LOGIC, "AMG requires setup");
+        require(rhs && x, "null vector");
+        DeviceScope scope(m->ctx->device);
+        if (m->value_type == TF_F64)
+            m->h->apply(m->ctx, static_cast<const double *>(rhs), static_cast<double *>(x));
+        else
+            m->h->apply(m->ctx, static_cast<const float *>(rhs), static_cast<float *>(x));
+        cuda_check(cudaStreamSynchronize(m->ctx->stream), "AMG apply");
+    });
+}
+
+int tf_amg_level_count(const tf_amg *m) { return m && m->h ? m->h->level_count() : 0; }
+
+int tf_amg_level_stats(const tf_amg *m, int level, int64_t *rows, int64_t *nnz, int32_t histogram[4]) {
+    return guard([&] {
+        require(m != nullptr, "null AMG");
+        if (!m->h) fail(TF_ERR_LOGIC, "AMG requires setup");
+        require(level >= 0 && level < m->h->level_count(), "level out of range");
+        const auto &s = m->h->stats[static_cast<size_t>(level)];
+        if (rows) *rows = s.rows;
+        if (nnz) *nnz = s.nnz;
+        if (histogram)
+            for (int k = 0; k < 4; ++k) histogram[k] = s.histogram[k];
+    });
+}
+
+const char *tf_amg_stop_reason(const tf_amg *m) { return m && m->h ? m->h->stop_reason.c_str() : ""; }
+const char *tf_amg_coarse_solver(const tf_amg *m) { return m && m->h ? m->h->coarse_solver.c_str() : ""; }
+
+int tf_amg_last_visits(const tf_amg *m, int64_t *visits, int capacity) {
+    return guard([&] {
+        require(m != nullptr && visits != nullptr, "null argument");
+        if (!m->h) fail(TF_ERR_LOGIC, "AMG requires setup");
+        const auto &v = m->h->visits;
+        for (int d = 0; d < capacity && d < static_cast<int>(v.size()); ++d) visits[d] = v[static_cast<size_t>(d)];
+    });
+}
+
+int tf_amg_level_matrix(const tf_amg *m, int level, tf_csr *out) {
+    return guard([&] {
+        require(m != nullptr && out != nullptr, "null argument");
+        if (!m->h) fail(TF_ERR_LOGIC, "AMG requires setup");
+        require(level >= 0 && level < m->h->level_count(), "level out of range");
+        *out = m->h->level_matrix(level);
+    });
+}
+
+int tf_amg_level_transfer(const tf_amg *m, int level, const int32_t **map, const int32_t **offsets,
+                          const int32_t **members, int *coarse_rows) {
+    return guard([&] {
+        require(m != nullptr && map && offsets && members && coarse_rows, "null argument");
+        if (!m->h) fail(TF_ERR_LOGIC, "AMG requires setup");
+        require(level >= 0 && level + 1 < m->h->level_count(), "level has no transfer");
+        m->h->level_transfer(level, map, offsets, members, coarse_rows);
+    });
+}
+
+int tf_jacobi_create(tf_ctx *ctx, int value_type, int index_type, int sweeps, double weight, tf_jacobi **out) {
+    return guard([&] {
+        check_ctx(ctx);
+        require(out != nullptr, "null output");
+        *out = nullptr;
+        check_types(value_type, index_type);
+        const double w = value_type == TF_F32 ? static_cast<double>(static_cast<float>(weight)) : weight;
+        if (sweeps < 1 || !std::isfinite(w) || w <= 0 || w >= 2) fail(TF_ERR_INVALID, "Invalid Jacobi parameters");
+        auto *j = new tf_jacobi();
+        j->ctx = ctx;
+        j->value_type = value_type;
+        j->index_type = index_type;
+        j->sweeps = sweeps;
+        j->weight = w;
+        *out = j;
+    });
+}
+
+int tf_jacobi_destroy(tf_jacobi *j) {
+    return guard([&] {
+        if (!j) return;
+        DeviceScope scope(j->ctx->device);
+        delete j;
+    });
+}
+
+int tf_jacobi_setup(tf_jacobi *j, const tf_csr *a) {
+    return guard([&] {
+        require(j != nullptr, "null Jacobi");
+        check_matrix_types(a, j->value_type, j->index_type);
+        require(a->rows > 0 && a->rows == a->cols, "Solver requires a nonempty square matrix");
+        DeviceScope scope(j->ctx->device);
+        tf_ctx *ctx = j->ctx;
+        std::unique_ptr<tf_dcsr> native;
+        try {
+            native = to_native(ctx, *a);
+        } catch (const Failure &f) {
+            if (f.code == TF_ERR_INVALID) fail(TF_ERR_INVALID, "Matrix contains nonfinite entries");
+            throw;
+        }
+        const size_t vs = type_size(j->value_type);
+        const int64_t n = native->rows, nnz = native->nnz;
+        DeviceBuffer<int32_t> rp(static_cast<size_t>(n) + 1), ci(static_cast<size_t>(nnz));
+        DeviceBuffer<unsigned char> val(static_cast<size_t>(nnz) * vs), dinv(static_cast<size_t>(n) * vs);
+        const auto nc = csr_of(*native);
+        copy_async(ctx, rp.data(), nc.rp, (n + 1) * 4);
+        copy_async(ctx, ci.data(), nc.ci, nnz * 4);
+        if (j->value_type == TF_F64) {
+            convert(ctx, nnz, nc.val, reinterpret_cast<double *>(val.data()));
+            Csr<double, int32_t> c{n, n, nnz, rp.data(), ci.data(), reinterpret_cast<const double *>(val.data())};
+            inverse_diagonal(ctx, c, reinterpret_cast<double *>(dinv.data()));
+        } else {
+            convert(ctx, nnz, nc.val, reinterpret_cast<float *>(val.data()));
+            Csr<float, int32_t> c{n, n, nnz, rp.data(), ci.data(), reinterpret_cast<const float *>(val.data())};
+            inverse_diagonal(ctx, c, reinterpret_cast<float *>(dinv.data()));
+        }
+        DeviceBuffer<unsigned char> rhs(static_cast<size_t>(n) * vs), x0(static_cast<size_t>(n) * vs),
+            x1(static_cast<size_t>(n) * vs);
+        cuda_check(cudaStreamSynchronize(ctx->stream), "Jacobi setup");
+        j->n = n;
+        j->nnz = nnz;
+        j->rp = std::move(rp);
+        j->ci = std::move(ci);
+        j->val = std::move(val);
+        j->dinv = std::move(dinv);
+        j->rhs = std::move(rhs);
+        j->x0 = std::move(x0);
+        j->x1 = std::move(x1);
+        j->ready = true;
+    });
+}
+
+int tf_jacobi_apply(tf_jacobi *j, const void *rhs, void *x) {
+    return guard([&] {
+        require(j != nullptr, "null Jacobi");
+        if (!j->ready) fail(TF_ERR_LOGIC, "Jacobi requires setup");
+        require(rhs && x, "null vector");
+        DeviceScope scope(j->ctx->device);
+        tf_ctx *ctx = j->ctx;
+        const size_t bytes = static_cast<size_t>(j->n) * type_size(j->value_type);
+        copy_async(ctx, j->rhs.data(), rhs, bytes);
+        copy_async(ctx, j->x0.data(), x, bytes);
+        auto run = [&](auto t) {
+            using T = decltype(t);
+            Csr<T, int32_t> c{j->n, j->n, j->nnz, j->rp.data(), j->ci.data(), reinterpret_cast<const T *>(j->val.data())};
+            T *xa = reinterpret_cast<T *>(j->x0.data()), *xb = reinterpret_cast<T *>(j->x1.data());
+            for (int s = 0; s < j->sweeps; ++s) {
+                jacobi_sweep(ctx, c, reinterpret_cast<const T *>(j->dinv.data()), reinterpret_cast<const T *>(j->rhs.data()),
+                             xa, xb, static_cast<T>(j->weight), nullptr, nullptr, static_cast<const T *>(nullptr));
+                std::swap(xa, xb);
+            }
+            copy_async(ctx, x, xa, bytes);
+        };
+        if (j->value_type == TF_F64) run(double{});
+        else run(float{});
+        cuda_check(cudaStreamSynchronize(ctx->stream), "Jacobi apply");
+    });
+}
+
+int tf_solver_create(tf_ctx *ctx, int kind, int value_type, int index_type, const tf_solver_options *opt, int precond,
+                     const tf_amg_options *amg_opt, tf_solver **out) {
+    return guard([&] {
+        check_ctx(ctx);
+        require(out && opt, "null argument");
+        *out = nullptr;
+        check_types(value_type, index_type);
+        auto s = std::make_unique<tf_solver>();
+        s->ctx = ctx;
+        s->value_type = value_type;
+        s->index_type = index_type;
+        s->k = make_krylov(kind, value_type, index_type, *opt, precond, amg_opt);
+        *out = s.release();
+    });
+}
+
+int tf_solver_destroy(tf_solver *s) {
+    return guard([&] {
+        if (!s) return;
+        DeviceScope scope(s->ctx->device);
+        delete s;
+    });
+}
+
+int tf_solver_setup(tf_solver *s, const tf_csr *a) {
+    return guard([&] {
+        require(s != nullptr, "null solver");
+        check_matrix_types(a, s->value_type, s->index_type);
+        DeviceScope scope(s->ctx->device);
+        s->view.reset();
+        s->k->setup(s->ctx, *a);
+    });
+}
+
+int tf_solver_apply(tf_solver *s, const void *rhs, void *x, int host_buffers, tf_solve_result *result) {
+    return guard([&] {
+        require(s != nullptr && result != nullptr, "null argument");
+        require(rhs && x, "null vector");
+        DeviceScope scope(s->ctx->device);
+        if (!host_buffers) {
+            *result = s->k->solve(s->ctx, rhs, x);
+            return;
+        }
+        const int64_t n = s->k->rows();
+        if (n == 0) fail(TF_ERR_LOGIC, "solver requires setup");
+        const size_t bytes = static_cast<size_t>(n) * type_size(s->value_type);
+        s->hb.reserve(bytes);
+        s->hx.reserve(bytes);
+        tf_ctx *ctx = s->ctx;
+        cuda_check(cudaMemcpyAsync(s->hb.data(), rhs, bytes, cudaMemcpyHostToDevice, ctx->stream), "rhs upload");
+        cuda_check(cudaMemcpyAsync(s->hx.data(), x, bytes, cudaMemcpyHostToDevice, ctx->stream), "x upload");
+        *result = s->k->solve(ctx, s->hb.data(), s->hx.data());
+        cuda_check(cudaMemcpyAsync(x, s->hx.data(), bytes, cudaMemcpyDeviceToHost, ctx->stream), "x download");
+        cuda_check(cudaStreamSynchronize(ctx->stream), "solve download");
+    });
+}
+
+tf_amg *tf_solver_amg(tf_solver *s) {
+    if (!s || !s->k || !s->k->amg()) return nullptr;
+    if (!s->view) {
+        tf_amg_options o;
+        tf_amg_options_default(&o);
+        s->view.reset(new tf_amg{s->ctx, s->value_type, s->index_type, AmgConfig(o), nullptr, s->k->amg()});
+    }
+    s->view->h = s->k->amg();
+    return s->view.get();
+}
+
+double tf_solver_last_apply_ms(const tf_solver *s) { return s && s->k ? s->k->last_ms : 0.0; }
+
+}  // extern "C"

@@ -1,0 +1,118 @@
+// ops.cuh -- typed internal entry points of the kernels (the C ABI and the
+// C++ components both call these).
+#pragma once
+#include "common.cuh"
+
+#include <memory>
+
+namespace tfb {
+
+// Device CSR view with typed arrays.
+template <class T, class I>
+struct Csr {
+    int64_t rows{0}, cols{0}, nnz{0};
+    const I *rp{nullptr};
+    const I *ci{nullptr};
+    const T *val{nullptr};
+};
+
+// Launch shape of the row-tile SpMV family: rows_per_tile consecutive rows
+// per CTA; their nonzeros are staged through shared memory in chunks of
+// chunk entries.
+struct SpmvShape {
+    int rows_per_thread{2};  // 1 or 2 (rows per tile = 256 * rows_per_thread)
+    int chunk{4096};         // staged entries per chunk
+};
+SpmvShape spmv_shape(int64_t rows, int64_t nnz, size_t value_size, size_t index_size);
+
+// y = A x
+template <class T, class I>
+void spmv(tf_ctx *ctx, const Csr<T, I> &a, const T *x, T *y);
+// r = b - A x
+template <class T, class I>
+void residual(tf_ctx *ctx, const Csr<T, I> &a, const T *b, const T *x, T *r);
+// xo = x~ + w Dinv (b - A x~), x~ = x (+ e[map] when map != nullptr)
+template <class T, class I>
+void jacobi_sweep(tf_ctx *ctx, const Csr<T, I> &a, const T *dinv, const T *b, const T *x, T *xo, T w,
+                  const float *row_w, const int32_t *map, const T *e);
+// x = w Dinv b
+template <class T>
+void jacobi_zero(tf_ctx *ctx, int64_t n, const T *dinv, const T *b, T *x, T w, const float *row_w);
+// Dinv from summed diagonal entries; throws TF_ERR_INVALID on a bad diagonal.
+template <class T, class I>
+void inverse_diagonal(tf_ctx *ctx, const Csr<T, I> &a, T *dinv);
+template <class T>
+void restrict_sum(tf_ctx *ctx, int64_t nc, const int32_t *off, const int32_t *mem, const T *fine, T *coarse);
+template <class T>
+void prolong_add(tf_ctx *ctx, int64_t nf, const int32_t *map, const T *coarse, T *fine);
+// out[k] = x_k . y_k (k < count <= 4), deterministic two-stage FP64 reduction.
+template <class T>
+void dot_multi(tf_ctx *ctx, int64_t n, int count, const T *const *xs, const T *const *ys, double *out);
+template <class T>
+void axpby(tf_ctx *ctx, int64_t n, double a, const T *x, double b, T *y);
+template <class S, class D>
+void convert(tf_ctx *ctx, int64_t n, const S *src, D *dst);
+template <class T>
+void fill_zero(tf_ctx *ctx, int64_t n, T *x);
+
+// Structural validation (offsets monotone/bounded, indices in range).
+template <class I>
+bool csr_structure_ok(tf_ctx *ctx, int64_t rows, int64_t cols, int64_t nnz, const I *rp, const I *ci);
+// bit 1 unsorted/duplicate, bit 2 invalid/nonfinite.
+template <class T, class I>
+int csr_canonical_flags(tf_ctx *ctx, const Csr<T, I> &a);
+// Finite values, nonfinite entry or bad diagonal -> false; row max |offdiag|.
+bool row_stats(tf_ctx *ctx, const Csr<double, int32_t> &a, double *row_max);
+
+// Sorting primitives (sort.cu).
+void radix_sort_pairs(tf_ctx *ctx, int64_t n, const uint64_t *kin, const double *vin, uint64_t *kout,
+                      double *vout, int end_bit);
+int64_t reduce_by_key(tf_ctx *ctx, int64_t n, const uint64_t *keys, const double *vals, int op, uint64_t *kout,
+                      double *vout);
+void scan_exclusive(tf_ctx *ctx, int64_t n, const int32_t *in, int32_t *out);
+
+// Coordinate compression (sort + reduce + unpack) into an owned CSR.
+std::unique_ptr<tf_dcsr> compress(tf_ctx *ctx, int rows, int64_t n, const uint64_t *keys, const double *vals, int col_bits, int op);
+int column_bits(int rows);
+
+// Setup stages (setup.cu), on canonical FP64/int32 operands.
+std::unique_ptr<tf_dcsr> canonicalize(tf_ctx *ctx, const Csr<double, int32_t> &a);
+std::unique_ptr<tf_dcsr> strength_graph(tf_ctx *ctx, const Csr<double, int32_t> &a, const double *row_max, double theta);
+int match_pairs(tf_ctx *ctx, const Csr<double, int32_t> &g, int rounds, int32_t *map);
+std::unique_ptr<tf_dcsr> contract_graph(tf_ctx *ctx, const Csr<double, int32_t> &g, const int32_t *map, int count);
+std::unique_ptr<tf_transfer> aggregate(tf_ctx *ctx, const Csr<double, int32_t> &g, int rounds, bool absorb);
+std::unique_ptr<tf_dcsr> galerkin(tf_ctx *ctx, const Csr<double, int32_t> &a, const int32_t *map, int coarse);
+
+// Coarse LU (coarse.cu).
+bool coarse_lu_factor(tf_ctx *ctx, const Csr<double, int32_t> &a, double *lu, int32_t *pivots);
+template <class T>
+void coarse_lu_solve(tf_ctx *ctx, int n, const double *lu, const int32_t *pivots, const T *b, T *x);
+// Explicit inverse (row major) from the factor, for the per-cycle dense apply.
+void coarse_inverse(tf_ctx *ctx, int n, const double *lu, const int32_t *pivots, double *inv);
+template <class T>
+void coarse_dense_apply(tf_ctx *ctx, int n, const double *inv, const T *b, T *x);
+
+inline Csr<double, int32_t> csr_of(const tf_dcsr &m) {
+    Csr<double, int32_t> c;
+    c.rows = m.rows;
+    c.cols = m.cols;
+    c.nnz = m.nnz;
+    c.rp = reinterpret_cast<const int32_t *>(m.offsets.data());
+    c.ci = reinterpret_cast<const int32_t *>(m.indices.data());
+    c.val = reinterpret_cast<const double *>(m.values.data());
+    return c;
+}
+
+template <class T, class I>
+Csr<T, I> csr_of(const tf_csr &m) {
+    Csr<T, I> c;
+    c.rows = m.rows;
+    c.cols = m.cols;
+    c.nnz = m.nnz;
+    c.rp = static_cast<const I *>(m.offsets);
+    c.ci = static_cast<const I *>(m.indices);
+    c.val = static_cast<const T *>(m.values);
+    return c;
+}
+
+}  // namespace tfb

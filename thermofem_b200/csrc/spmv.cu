@@ -1,0 +1,416 @@
+// spmv.cu -- the SpMV family on the row-tile kernel (tile.cuh) and the
+// vector kernels around it.
+//
+// The epilogue is a template parameter, so the residual, the weighted-Jacobi
+// sweep and the prolongation-fused sweep read A exactly once per pass: the
+// reference does SpMV + scal + axpy (src/LinearAlgebra/IterationContext.cu:
+// 167-175) and SpMV + update (:26-32,251-269) as separate passes.
+#include "tile.cuh"
+
+namespace tfb {
+namespace {
+
+using tile::PlainX;
+using tile::ProlongX;
+
+template <class T>
+struct StoreY {
+    static constexpr int kReduce = 0;
+    T *__restrict__ y;
+    double *partial{nullptr};
+    __device__ __forceinline__ bool skip() const { return false; }
+    template <class XS>
+    __device__ __forceinline__ void operator()(int64_t i, T acc, const XS &, double (&)[1]) const {
+        y[i] = acc;
+    }
+};
+
+template <class T>
+struct ResidualOut {
+    static constexpr int kReduce = 0;
+    const T *__restrict__ b;
+    T *__restrict__ r;
+    double *partial{nullptr};
+    __device__ __forceinline__ bool skip() const { return false; }
+    template <class XS>
+    __device__ __forceinline__ void operator()(int64_t i, T acc, const XS &, double (&)[1]) const {
+        r[i] = b[i] - acc;
+    }
+};
+
+// x_out = x~ + (w Dinv) (b - A x~), the reference's update expression
+// x += w * d * (b - a) (IterationContext.cu:26-32).
+template <class T>
+struct JacobiOut {
+    static constexpr int kReduce = 0;
+    const T *__restrict__ dinv;
+    const T *__restrict__ b;
+    T *__restrict__ xo;
+    const float *__restrict__ row_w;
+    T w;
+    double *partial{nullptr};
+    __device__ __forceinline__ bool skip() const { return false; }
+    template <class XS>
+    __device__ __forceinline__ void operator()(int64_t i, T acc, const XS &xs, double (&)[1]) const {
+        const T wi = row_w ? static_cast<T>(row_w[i]) : w;
+        xo[i] = xs(i) + wi * dinv[i] * (b[i] - acc);
+    }
+};
+
+template <class T, class I, class XS, class Epi>
+void launch_tile(tf_ctx *ctx, const Csr<T, I> &a, const XS &xs, const Epi &epi, const char *name) {
+    tile::launch(ctx, a, xs, epi, name);
+}
+
+
+template <class T>
+__global__ void jacobi_zero_kernel(int64_t n, const T *__restrict__ dinv, const T *__restrict__ b, T *__restrict__ x,
+                                   T w, const float *__restrict__ row_w) {
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const T wi = row_w ? static_cast<T>(row_w[i]) : w;
+        // x = 0 + w d (b - 0), the reference update from a zero guess.
+        x[i] = wi * dinv[i] * b[i];
+    }
+}
+
+template <class T, class I>
+__global__ void inverse_diagonal_kernel(int64_t n, const I *__restrict__ rp, const I *__restrict__ ci,
+                                        const T *__restrict__ val, T *__restrict__ dinv, int *bad) {
+    const int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (i >= n) return;
+    T d = 0;
+    for (I j = rp[i]; j < rp[i + 1]; ++j)
+        if (static_cast<int64_t>(ci[j]) == i) d += val[j];
+    const T inv = T(1) / d;
+    if (!isfinite(d) || d == T(0) || !isfinite(inv)) atomicExch(bad, 1);
+    dinv[i] = inv;
+}
+
+template <class T>
+__global__ void restrict_kernel(int64_t nc, const int32_t *__restrict__ off, const int32_t *__restrict__ mem,
+                                const T *__restrict__ fine, T *__restrict__ coarse) {
+    const int64_t c = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (c >= nc) return;
+    T s = 0;
+    for (int32_t j = off[c]; j < off[c + 1]; ++j) s += fine[mem[j]];
+    coarse[c] = s;
+}
+
+template <class T>
+__global__ void prolong_kernel(int64_t nf, const int32_t *__restrict__ map, const T *__restrict__ coarse,
+                               T *__restrict__ fine) {
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < nf;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        fine[i] += coarse[map[i]];
+}
+
+// Deterministic block reduction of up to 4 sums (fixed tree order).
+template <int K>
+__device__ __forceinline__ void block_sum(double (&v)[K], double *shm /* [K][32] */) {
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+        for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < K; ++k) shm[k * 32 + warp] = v[k];
+    __syncthreads();
+    if (warp == 0) {
+        const int nw = blockDim.x >> 5;
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            v[k] = lane < nw ? shm[k * 32 + lane] : 0.0;
+            for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+        }
+    }
+}
+
+struct DotArgs {
+    const void *x[4];
+    const void *y[4];
+};
+
+template <class T, int K>
+__global__ void __launch_bounds__(256) dot_partial_kernel(int64_t n, DotArgs args, double *partial) {
+    __shared__ double shm[K * 32];
+    double v[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) v[k] = 0.0;
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+            v[k] += static_cast<double>(static_cast<const T *>(args.x[k])[i]) *
+                    static_cast<double>(static_cast<const T *>(args.y[k])[i]);
+    }
+    block_sum<K>(v, shm);
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int k = 0; k < K; ++k) partial[k * gridDim.x + blockIdx.x] = v[k];
+}
+
+template <int K>
+__global__ void __launch_bounds__(256) dot_final_kernel(int parts, const double *partial, double *out) {
+    __shared__ double shm[K * 32];
+    double v[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        v[k] = 0.0;
+        for (int p = threadIdx.x; p < parts; p += blockDim.x) v[k] += partial[k * parts + p];
+    }
+    block_sum<K>(v, shm);
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int k = 0; k < K; ++k) out[k] = v[k];
+}
+
+template <class T>
+__global__ void axpby_kernel(int64_t n, double a, const T *__restrict__ x, double b, T *__restrict__ y) {
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const T ta = static_cast<T>(a), tb = static_cast<T>(b);
+        y[i] = tb == T(0) ? ta * x[i] : ta * x[i] + tb * y[i];
+    }
+}
+
+template <class S, class D>
+__global__ void convert_kernel(int64_t n, const S *__restrict__ src, D *__restrict__ dst) {
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        dst[i] = static_cast<D>(src[i]);
+}
+
+template <class I>
+__global__ void csr_structure_kernel(int64_t rows, int64_t cols, int64_t nnz, const I *__restrict__ rp,
+                                     const I *__restrict__ ci, int *bad) {
+    const int64_t r = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (r == 0 && (rp[0] != 0 || static_cast<int64_t>(rp[rows]) != nnz)) atomicExch(bad, 1);
+    if (r >= rows) return;
+    const int64_t s = rp[r], e = rp[r + 1];
+    if (s < 0 || e < s || e > nnz) {
+        atomicExch(bad, 1);
+        return;
+    }
+    for (int64_t j = s; j < e; ++j)
+        if (ci[j] < 0 || static_cast<int64_t>(ci[j]) >= cols) atomicExch(bad, 1);
+}
+
+// Canonical-form flags (src/Multigrid/GpuAggregation.cu:283-304).
+template <class T, class I>
+__global__ void canonical_flags_kernel(int64_t n, int64_t nnz, const I *__restrict__ rp, const I *__restrict__ ci,
+                                       const T *__restrict__ val, int *flags) {
+    const int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (i >= n) return;
+    if (rp[0] != 0 || static_cast<int64_t>(rp[n]) != nnz || rp[i] < 0 || rp[i] > rp[i + 1] ||
+        static_cast<int64_t>(rp[i + 1]) > nnz) {
+        atomicOr(flags, 2);
+        return;
+    }
+    int64_t previous = -1;
+    for (I j = rp[i]; j < rp[i + 1]; ++j) {
+        const int64_t c = ci[j];
+        if (c < 0 || c >= n || !isfinite(val[j])) atomicOr(flags, 2);
+        if (c <= previous) atomicOr(flags, 1);
+        previous = c;
+    }
+}
+
+// Level validation and row max |offdiag| (GpuAggregation.cu:247-271).
+__global__ void row_stats_kernel(int64_t n, const int32_t *__restrict__ rp, const int32_t *__restrict__ ci,
+                                 const double *__restrict__ a, int *bad, double *__restrict__ row_max) {
+    const int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (i >= n) return;
+    double diag = 0, mx = 0;
+    for (int32_t j = rp[i]; j < rp[i + 1]; ++j) {
+        if (!isfinite(a[j])) atomicExch(bad, 1);
+        if (ci[j] == i) diag = a[j];
+        else mx = fmax(mx, fabs(a[j]));
+    }
+    if (diag == 0 || !isfinite(diag) || !isfinite(1.0 / diag)) atomicExch(bad, 1);
+    if (row_max) row_max[i] = mx;
+}
+
+unsigned stride_grid(tf_ctx *ctx, int64_t n) {
+    const int64_t want = (n + kBlock - 1) / kBlock;
+    const int64_t cap = static_cast<int64_t>(ctx->sm_count) * 16;
+    return static_cast<unsigned>(want < 1 ? 1 : (want > cap ? cap : want));
+}
+
+}  // namespace
+
+SpmvShape spmv_shape(int64_t rows, int64_t nnz, size_t value_size, size_t index_size) {
+    SpmvShape s;
+    s.rows_per_thread = (rows > 0 && nnz <= 8 * rows) ? 2 : 1;
+    int chunk = static_cast<int>(49152 / (value_size + index_size));
+    s.chunk = chunk & ~15;
+    return s;
+}
+
+template <class T, class I>
+void spmv(tf_ctx *ctx, const Csr<T, I> &a, const T *x, T *y) {
+    launch_tile(ctx, a, PlainX<T>{x}, StoreY<T>{y, nullptr}, "spmv");
+}
+
+template <class T, class I>
+void residual(tf_ctx *ctx, const Csr<T, I> &a, const T *b, const T *x, T *r) {
+    launch_tile(ctx, a, PlainX<T>{x}, ResidualOut<T>{b, r, nullptr}, "residual");
+}
+
+template <class T, class I>
+void jacobi_sweep(tf_ctx *ctx, const Csr<T, I> &a, const T *dinv, const T *b, const T *x, T *xo, T w,
+                  const float *row_w, const int32_t *map, const T *e) {
+    JacobiOut<T> epi{dinv, b, xo, row_w, w, nullptr};
+    if (map)
+        launch_tile(ctx, a, ProlongX<T>{x, map, e}, epi, "jacobi_prolong");
+    else
+        launch_tile(ctx, a, PlainX<T>{x}, epi, "jacobi");
+}
+
+template <class T>
+void jacobi_zero(tf_ctx *ctx, int64_t n, const T *dinv, const T *b, T *x, T w, const float *row_w) {
+    if (!n) return;
+    jacobi_zero_kernel<T><<<stride_grid(ctx, n), kBlock, 0, ctx->stream>>>(n, dinv, b, x, w, row_w);
+    launched(ctx, "jacobi_zero");
+}
+
+template <class T, class I>
+void inverse_diagonal(tf_ctx *ctx, const Csr<T, I> &a, T *dinv) {
+    require(a.rows > 0 && a.rows == a.cols, "Inverse diagonal requires a nonempty square matrix");
+    int *bad = static_cast<int *>(ctx->arena(sizeof(int), 1));
+    memset_async(ctx, bad, 0, sizeof(int));
+    inverse_diagonal_kernel<T, I><<<grid_for(a.rows), kBlock, 0, ctx->stream>>>(a.rows, a.rp, a.ci, a.val, dinv, bad);
+    launched(ctx, "inverse_diagonal");
+    if (read_scalar(ctx, bad)) fail(TF_ERR_INVALID, "Missing or invalid diagonal");
+}
+
+template <class T>
+void restrict_sum(tf_ctx *ctx, int64_t nc, const int32_t *off, const int32_t *mem, const T *fine, T *coarse) {
+    if (!nc) return;
+    restrict_kernel<T><<<grid_for(nc), kBlock, 0, ctx->stream>>>(nc, off, mem, fine, coarse);
+    launched(ctx, "restrict");
+}
+
+template <class T>
+void prolong_add(tf_ctx *ctx, int64_t nf, const int32_t *map, const T *coarse, T *fine) {
+    if (!nf) return;
+    prolong_kernel<T><<<stride_grid(ctx, nf), kBlock, 0, ctx->stream>>>(nf, map, coarse, fine);
+    launched(ctx, "prolong");
+}
+
+template <class T>
+void dot_multi(tf_ctx *ctx, int64_t n, int count, const T *const *xs, const T *const *ys, double *out) {
+    require(count >= 1 && count <= 4, "dot count must be 1..4");
+    DotArgs args{};
+    for (int k = 0; k < count; ++k) {
+        args.x[k] = xs[k];
+        args.y[k] = ys[k];
+    }
+    // Fixed partition for a given n: the result does not depend on the GPU.
+    int64_t parts64 = (n + 2047) / 2048;
+    if (parts64 < 1) parts64 = 1;
+    if (parts64 > 1184) parts64 = 1184;
+    const int parts = static_cast<int>(parts64);
+    double *partial = static_cast<double *>(ctx->arena(sizeof(double) * 4 * parts));
+    switch (count) {
+        case 1: dot_partial_kernel<T, 1><<<parts, 256, 0, ctx->stream>>>(n, args, partial); break;
+        case 2: dot_partial_kernel<T, 2><<<parts, 256, 0, ctx->stream>>>(n, args, partial); break;
+        case 3: dot_partial_kernel<T, 3><<<parts, 256, 0, ctx->stream>>>(n, args, partial); break;
+        default: dot_partial_kernel<T, 4><<<parts, 256, 0, ctx->stream>>>(n, args, partial); break;
+    }
+    launched(ctx, "dot_partial");
+    switch (count) {
+        case 1: dot_final_kernel<1><<<1, 256, 0, ctx->stream>>>(parts, partial, out); break;
+        case 2: dot_final_kernel<2><<<1, 256, 0, ctx->stream>>>(parts, partial, out); break;
+        case 3: dot_final_kernel<3><<<1, 256, 0, ctx->stream>>>(parts, partial, out); break;
+        default: dot_final_kernel<4><<<1, 256, 0, ctx->stream>>>(parts, partial, out); break;
+    }
+    launched(ctx, "dot_final");
+}
+
+template <class T>
+void axpby(tf_ctx *ctx, int64_t n, double a, const T *x, double b, T *y) {
+    if (!n) return;
+    axpby_kernel<T><<<stride_grid(ctx, n), kBlock, 0, ctx->stream>>>(n, a, x, b, y);
+    launched(ctx, "axpby");
+}
+
+template <class S, class D>
+void convert(tf_ctx *ctx, int64_t n, const S *src, D *dst) {
+    if (!n) return;
+    convert_kernel<S, D><<<stride_grid(ctx, n), kBlock, 0, ctx->stream>>>(n, src, dst);
+    launched(ctx, "convert");
+}
+
+template <class T>
+void fill_zero(tf_ctx *ctx, int64_t n, T *x) {
+    memset_async(ctx, x, 0, static_cast<size_t>(n) * sizeof(T));
+}
+
+template <class I>
+bool csr_structure_ok(tf_ctx *ctx, int64_t rows, int64_t cols, int64_t nnz, const I *rp, const I *ci) {
+    int *bad = static_cast<int *>(ctx->arena(sizeof(int), 1));
+    memset_async(ctx, bad, 0, sizeof(int));
+    csr_structure_kernel<I><<<grid_for(rows > 0 ? rows : 1), kBlock, 0, ctx->stream>>>(rows, cols, nnz, rp, ci, bad);
+    launched(ctx, "csr_validate");
+    return read_scalar(ctx, bad) == 0;
+}
+
+template <class T, class I>
+int csr_canonical_flags(tf_ctx *ctx, const Csr<T, I> &a) {
+    int *flags = static_cast<int *>(ctx->arena(sizeof(int), 1));
+    memset_async(ctx, flags, 0, sizeof(int));
+    if (a.rows) {
+        canonical_flags_kernel<T, I><<<grid_for(a.rows), kBlock, 0, ctx->stream>>>(a.rows, a.nnz, a.rp, a.ci, a.val,
+                                                                                   flags);
+        launched(ctx, "check_canonical");
+    }
+    return read_scalar(ctx, flags);
+}
+
+bool row_stats(tf_ctx *ctx, const Csr<double, int32_t> &a, double *row_max) {
+    int *bad = static_cast<int *>(ctx->arena(sizeof(int), 1));
+    memset_async(ctx, bad, 0, sizeof(int));
+    if (a.rows) {
+        row_stats_kernel<<<grid_for(a.rows), kBlock, 0, ctx->stream>>>(a.rows, a.rp, a.ci, a.val, bad, row_max);
+        launched(ctx, "row_stats");
+    }
+    return read_scalar(ctx, bad) == 0;
+}
+
+#define TF_SPMV_INST(T, I)                                                                                     \
+    template void spmv<T, I>(tf_ctx *, const Csr<T, I> &, const T *, T *);                                     \
+    template void residual<T, I>(tf_ctx *, const Csr<T, I> &, const T *, const T *, T *);                      \
+    template void jacobi_sweep<T, I>(tf_ctx *, const Csr<T, I> &, const T *, const T *, const T *, T *, T,     \
+                                     const float *, const int32_t *, const T *);                               \
+    template void inverse_diagonal<T, I>(tf_ctx *, const Csr<T, I> &, T *);                                    \
+    template int csr_canonical_flags<T, I>(tf_ctx *, const Csr<T, I> &);
+TF_SPMV_INST(float, int32_t)
+TF_SPMV_INST(double, int32_t)
+TF_SPMV_INST(float, int64_t)
+TF_SPMV_INST(double, int64_t)
+#undef TF_SPMV_INST
+
+#define TF_VEC_INST(T)                                                                                        \
+    template void jacobi_zero<T>(tf_ctx *, int64_t, const T *, const T *, T *, T, const float *);              \
+    template void restrict_sum<T>(tf_ctx *, int64_t, const int32_t *, const int32_t *, const T *, T *);        \
+    template void prolong_add<T>(tf_ctx *, int64_t, const int32_t *, const T *, T *);                          \
+    template void dot_multi<T>(tf_ctx *, int64_t, int, const T *const *, const T *const *, double *);           \
+    template void axpby<T>(tf_ctx *, int64_t, double, const T *, double, T *);                                 \
+    template void fill_zero<T>(tf_ctx *, int64_t, T *);
+TF_VEC_INST(float)
+TF_VEC_INST(double)
+#undef TF_VEC_INST
+
+template void convert<float, double>(tf_ctx *, int64_t, const float *, double *);
+template void convert<double, float>(tf_ctx *, int64_t, const double *, float *);
+template void convert<int32_t, int64_t>(tf_ctx *, int64_t, const int32_t *, int64_t *);
+template void convert<int64_t, int32_t>(tf_ctx *, int64_t, const int64_t *, int32_t *);
+template void convert<float, float>(tf_ctx *, int64_t, const float *, float *);
+template void convert<double, double>(tf_ctx *, int64_t, const double *, double *);
+template void convert<int32_t, int32_t>(tf_ctx *, int64_t, const int32_t *, int32_t *);
+template void convert<int64_t, int64_t>(tf_ctx *, int64_t, const int64_t *, int64_t *);
+template bool csr_structure_ok<int32_t>(tf_ctx *, int64_t, int64_t, int64_t, const int32_t *, const int32_t *);
+template bool csr_structure_ok<int64_t>(tf_ctx *, int64_t, int64_t, int64_t, const int64_t *, const int64_t *);
+
+}  // namespace tfb
