@@ -152,6 +152,38 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_profile(args):
+    """The kernels of whole solves, for an ncu launch list: setup and warm-up
+    solves first (skip their launches with ncu -s), then args.steps solves."""
+    import torch
+    import thermofem_b200 as tf
+    from thermofem_b200 import problems as P
+    off, idx, val = P.heat3d(SIZE, SEED_MATRIX)
+    n = len(off) - 1
+    ctx = tf.Context(0)
+    a = tf.DeviceCsr.from_host(off, idx, val)
+    b = torch.tensor(P.rhs_uniform(n, SEED_RHS), device="cuda")
+    x = torch.zeros(n, dtype=torch.float64, device="cuda")
+    s = tf.Cg(tf.solver_options(), "amg",
+              tf.amg_options(hierarchy_type="f32" if args.profile == "mixed" else "f64", **AMG), ctx=ctx)
+    s.setup(a)
+    ctx.synchronize()
+    l0 = ctx.launches
+    for _ in range(args.warmup):
+        x.zero_()
+        s.apply(b, x)
+    l1 = ctx.launches
+    for _ in range(args.steps):
+        x.zero_()
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_push("solve")  # ncu --nvtx --nvtx-include "solve/"
+        rep = s.apply(b, x)
+        torch.cuda.nvtx.range_pop()
+    ctx.synchronize()
+    print(json.dumps({"profile": args.profile, "setup_launches": l0, "warmup_launches": l1 - l0,
+                      "timed_launches": ctx.launches - l1, "iterations": rep["iterations"]}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -159,9 +191,13 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="thermofem", choices=["thermofem", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    ap.add_argument("--profile", choices=["mixed", "fp64"], default=None,
+                    help="profiling run: setup, --warmup solves, then --steps solves of one path; no JSON line")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.profile:
+        return run_profile(args)
 
     import torch
     import thermofem_b200 as tf

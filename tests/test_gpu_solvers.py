@@ -222,7 +222,10 @@ def test_heat3d_solve_matches_oracle(ctx, kind, hierarchy):
     ora = O.Amg(A, **opts)
     xo, orep = (O.cg if kind == "cg" else O.bicgstab)(A, ora, b, np.zeros(n))
     assert orep["status"] == "Converged"
-    assert abs(rep["iterations"] - orep["iterations"]) <= (1 if hierarchy is None else 3)
+    if hierarchy is None:  # same precision, same recurrence: same iteration count up to rounding
+        assert abs(rep["iterations"] - orep["iterations"]) <= 1
+    else:  # FP32 cycle: a different trajectory, but no more than 25% more iterations
+        assert rep["iterations"] <= 1.25 * orep["iterations"] + 2
     assert np.linalg.norm(xv - xo) / np.linalg.norm(xo) < 1e-6
 
 

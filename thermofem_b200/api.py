@@ -139,7 +139,7 @@ class _RawDevice:
     """Wraps a raw device pointer as a uint8 tensor (via __cuda_array_interface__)."""
 
     def __init__(self, ptr, nbytes, device):
-        self.__cuda_array_interface__ = {"shape": (nbytes,), "typestr": "|u1", "data": (int(ptr), True),
+        self.__cuda_array_interface__ = {"shape": (nbytes,), "typestr": "|u1", "data": (int(ptr), False),
                                          "version": 3, "strides": None}
         self.device = device
 

@@ -143,16 +143,35 @@ inline unsigned grid(const SpmvShape &shape, int64_t rows) {
     return static_cast<unsigned>((rows + tile_rows - 1) / tile_rows);
 }
 
+// Opts the instantiation into the dynamic shared memory it is launched with
+// (the staged chunk plus the epilogue's static reduction buffer can exceed
+// the 48 KB default); done once per instantiation and device.
+template <auto Kernel>
+void allow_smem(size_t bytes) {
+    static thread_local int configured_device = -1;
+    static thread_local size_t configured_bytes = 0;
+    int dev = 0;
+    cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+    if (dev == configured_device && bytes <= configured_bytes) return;
+    cuda_check(cudaFuncSetAttribute(Kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes)),
+               "tile shared memory");
+    configured_device = dev;
+    configured_bytes = bytes;
+}
+
 template <class T, class I, class XS, class Epi>
 void launch(tf_ctx *ctx, const Csr<T, I> &a, const XS &xs, const Epi &epi, const char *name) {
     if (a.rows == 0) return;
     const SpmvShape shape = spmv_shape(a.rows, a.nnz, sizeof(T), sizeof(I));
     const unsigned g = grid(shape, a.rows);
     const size_t smem = static_cast<size_t>(shape.chunk) * (sizeof(T) + sizeof(I));
-    if (shape.rows_per_thread == 2)
+    if (shape.rows_per_thread == 2) {
+        allow_smem<csr_tile_kernel<T, I, 2, XS, Epi>>(smem);
         csr_tile_kernel<T, I, 2><<<g, kThreads, smem, ctx->stream>>>(a.rows, a.rp, a.ci, a.val, shape.chunk, xs, epi);
-    else
+    } else {
+        allow_smem<csr_tile_kernel<T, I, 1, XS, Epi>>(smem);
         csr_tile_kernel<T, I, 1><<<g, kThreads, smem, ctx->stream>>>(a.rows, a.rp, a.ci, a.val, shape.chunk, xs, epi);
+    }
     launched(ctx, name);
 }
 
