@@ -239,11 +239,20 @@ unsigned stride_grid(tf_ctx *ctx, int64_t n) {
 
 }  // namespace
 
+// One row per thread; the staged chunk holds a typical tile (mean row
+// length x 256 rows, +25%) so short-row operators keep up to 8 CTAs per SM
+// resident, capped at 48 KB of shared memory for long rows (which then take
+// several chunks).  A pure function of (rows, nnz): the Krylov kernels size
+// their per-tile partial sums from it.
 SpmvShape spmv_shape(int64_t rows, int64_t nnz, size_t value_size, size_t index_size) {
     SpmvShape s;
-    s.rows_per_thread = (rows > 0 && nnz <= 8 * rows) ? 2 : 1;
-    int chunk = static_cast<int>(49152 / (value_size + index_size));
-    s.chunk = chunk & ~15;
+    s.rows_per_thread = 1;
+    const int64_t cap = static_cast<int64_t>(49152 / (value_size + index_size)) & ~int64_t(63);
+    const int64_t mean_tile = rows > 0 ? (nnz * 256 + rows - 1) / rows : 0;
+    int64_t chunk = (mean_tile + mean_tile / 4 + 63) & ~int64_t(63);
+    if (chunk < 512) chunk = 512;
+    if (chunk > cap) chunk = cap;
+    s.chunk = static_cast<int>(chunk);
     return s;
 }
 

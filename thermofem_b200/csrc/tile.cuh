@@ -113,11 +113,43 @@ __global__ void __launch_bounds__(kThreads) csr_tile_kernel(int64_t rows, const 
         stage(sval, val + c0, cnt);
         stage(scol, ci + c0, cnt);
         __syncthreads();
+        // The first kGather entries of every row of this thread are gathered
+        // together (independent x loads in flight) before any accumulation;
+        // the sum itself stays left to right.  Padding lanes add +0.
+        constexpr int kGather = 8;
+        T xv[RPT][kGather];
+        int lo[RPT], hi[RPT];  // chunk-relative
 #pragma unroll
         for (int k = 0; k < RPT; ++k) {
-            const int64_t lo = max(rs[k], c0), hi = min(re[k], c0 + cnt);
+            lo[k] = static_cast<int>(max(rs[k], c0) - c0);
+            hi[k] = static_cast<int>(min(re[k], c0 + cnt) - c0);
+#pragma unroll
+            for (int u = 0; u < kGather; ++u) {
+                const int o = lo[k] + u;
+                xv[k][u] = o < hi[k] ? xs(static_cast<int64_t>(scol[o])) : T(0);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < RPT; ++k) {
             T s = acc[k];
-            for (int64_t j = lo; j < hi; ++j) s += sval[j - c0] * xs(static_cast<int64_t>(scol[j - c0]));
+#pragma unroll
+            for (int u = 0; u < kGather; ++u) {
+                const int o = lo[k] + u;
+                s += (o < hi[k] ? sval[o] : T(0)) * xv[k][u];
+            }
+            for (int o0 = lo[k] + kGather; o0 < hi[k]; o0 += kGather) {
+                T y[kGather];
+#pragma unroll
+                for (int u = 0; u < kGather; ++u) {
+                    const int o = o0 + u;
+                    y[u] = o < hi[k] ? xs(static_cast<int64_t>(scol[o])) : T(0);
+                }
+#pragma unroll
+                for (int u = 0; u < kGather; ++u) {
+                    const int o = o0 + u;
+                    s += (o < hi[k] ? sval[o] : T(0)) * y[u];
+                }
+            }
             acc[k] = s;
         }
     }
