@@ -1,0 +1,96 @@
+"""C ABI checks that need no GPU: the library loads, exports every entry
+point the header declares, the host-side Matrix Market reader matches the
+reference reader on the reference's own test inputs, and compute entry
+points fail loudly (no CPU fallback) when no device is present."""
+import ctypes
+import json
+import os
+import re
+
+import numpy as np
+import pytest
+import torch
+
+import thermofem_b200 as tf
+from conftest import GOLDEN, ROOT
+
+HEADER = os.path.join(ROOT, "include", "thermofem_b200.h")
+
+
+def declared():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(tf_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_entry_point():
+    names = declared()
+    assert len(names) > 60
+    lib = ctypes.CDLL(tf.LIB_PATH)
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_python_binding_covers_the_header():
+    assert sorted(tf.SIGNATURES) == declared()
+
+
+def test_version_and_status_strings():
+    assert "sm_100a" in tf.version()
+    for code in (0, -1, -2, -3, -4, -5, -6, -7):
+        assert tf.lib().tf_status_string(code)
+
+
+def test_matrix_market_matches_reference_reader():
+    g = json.load(open(os.path.join(GOLDEN, "matrix_market_golden.json")))
+    for name, case in g["accepted"].items():
+        m = tf.read_matrix_market(case["text"])
+        assert m["rows"] == case["rows"], name
+        assert m["offsets"].tolist() == case["offsets"], name
+        assert m["indices"].tolist() == case["indices"], name
+        assert m["values"].tolist() == case["values"], name
+    for text in g["rejected"]:
+        with pytest.raises(tf.ParseError):
+            tf.read_matrix_market(text)
+
+
+def test_matrix_market_file_and_known_answers(tmp_path):
+    # matrix_market_test.cpp:8-25
+    m = tf.read_matrix_market("%%MatrixMarket matrix coordinate real general\n% comment\n3 3 4\n3 1 2\n1 2 4\n1 2 -1\n3 3 5\n")
+    assert m["offsets"].tolist() == [0, 2, 2, 4]
+    assert m["indices"].tolist() == [1, 1, 0, 2]
+    assert m["values"].tolist() == [4, -1, 2, 5]
+    p = tmp_path / "poisson.mtx"
+    p.write_text("%%MatrixMarket matrix coordinate real symmetric\n4 4 7\n1 1 2\n2 1 -1\n2 2 2\n3 2 -1\n3 3 2\n4 3 -1\n4 4 2\n")
+    m = tf.read_matrix_market_file(str(p))
+    assert m["offsets"].tolist() == [0, 2, 5, 8, 10]
+    with pytest.raises(tf.ParseError):
+        tf.read_matrix_market_file(str(tmp_path / "missing.mtx"))
+
+
+@pytest.mark.skipif(torch.cuda.is_available(), reason="checks the no-device error path")
+def test_no_cpu_fallback_without_a_device():
+    h = ctypes.c_void_p()
+    status = tf.lib().tf_ctx_create(0, None, ctypes.byref(h))
+    assert status in (tf.ERR_CUDA, tf.ERR_INVALID)
+    assert tf.device_count() == 0
+    with pytest.raises(RuntimeError):
+        tf.Context(0)
+
+
+def test_null_arguments_are_rejected():
+    assert tf.lib().tf_spmv(None, None, None, None) == tf.ERR_INVALID
+    assert tf.lib().tf_solver_apply(None, None, None, 0, None) == tf.ERR_INVALID
+    assert b"null" in tf.lib().tf_last_error()
+
+
+def test_problem_generators_match_baseline_sizes():
+    from thermofem_b200 import problems as P
+    off, idx, val = P.laplace2d(128)
+    assert len(off) - 1 == 16384 and len(idx) == 81408
+    off, idx, val = P.heat3d(32, seed=1)
+    assert len(off) - 1 == 32 ** 3 and len(idx) == 7 * 32 ** 3 - 6 * 32 ** 2
+    a = np.zeros(3)
+    assert np.array_equal(P.uniform(5, 10), P.uniform(5, 10))  # pure function of (seed, index)
+    assert not np.array_equal(P.uniform(5, 10), P.uniform(6, 10))
+    del a
