@@ -182,6 +182,21 @@ int tf_reduce_by_key_u64f64(tf_ctx *ctx, int64_t n, const uint64_t *keys, const 
                             uint64_t *keys_out, double *values_out, int64_t *count);
 /* Exclusive prefix sum of int32 (out may alias in). */
 int tf_scan_exclusive_i32(tf_ctx *ctx, int64_t n, const int32_t *in, int32_t *out);
+/* The same exclusive prefix sum without allocating anything (no counterpart
+ * in the reference).  For callers that cannot allocate device memory when
+ * they need a scan (inside an allocator or memory-pool callback, under a
+ * fixed device-memory budget, or where cudaMalloc's implicit device
+ * synchronisation is not acceptable) and that may not even hold a tf_ctx.
+ * Its scratch is a 256 KB array compiled into the library, held by every
+ * device that loads the library until the process exits; n is limited to
+ * 134,217,728 (2^27) items, larger n returns TF_ERR_LENGTH.  Runs on `stream`
+ * (a cudaStream_t, NULL = legacy default stream) of the current device and
+ * returns without synchronising.  The first call on a device looks up the
+ * scratch array's device address (cudaGetSymbolAddress); make that first
+ * call before any stream capture.  All calls on a device share the array:
+ * calls whose kernels may overlap on the GPU race and give undefined results.
+ * out may alias in. */
+int tf_scan_exclusive_i32_noalloc(void *stream, int64_t n, const int32_t *in, int32_t *out);
 
 /* ---- coarse dense LU (GpuAggregation.cu:827-939,1068-1098) ------------- */
 /* Partial-pivot LU of a canonical FP64 CSR with rows <= 256 (reference:

@@ -1,0 +1,51 @@
+"""tf_scan_exclusive_i32_noalloc, the scan for callers that cannot allocate
+device memory: called through the C ABI it must give exactly the result of
+the allocating tf_scan_exclusive_i32 (integer sums: tolerance zero), on two
+calls in a row whose sizes differ, so that what the first call leaves in the
+shared scratch array cannot leak into the second.  Collected last on
+purpose, and self-contained, so it passes alone in a fresh process too."""
+import ctypes
+
+import numpy as np
+import pytest
+import torch
+
+import thermofem_b200 as tf
+
+pytestmark = pytest.mark.gpu
+
+
+def noalloc_scan(stream, x, out):
+    return tf.lib().tf_scan_exclusive_i32_noalloc(ctypes.c_void_p(stream), x.numel(), ctypes.c_void_p(x.data_ptr()),
+                                                  ctypes.c_void_p(out.data_ptr()))
+
+
+@pytest.mark.parametrize("sizes", [(5_000_003, 1_777), (2_048, 70_000_000), (4_194_305, 4_194_305)])
+def test_noalloc_scan_matches_allocating_scan_twice(ctx, sizes):
+    stream = ctx.stream.cuda_stream
+    for call, n in enumerate(sizes):
+        g = torch.Generator(device="cuda").manual_seed(100 + call)
+        x = torch.randint(0, 7, (n,), dtype=torch.int32, device="cuda", generator=g)
+        want = tf.scan_exclusive(x, ctx=ctx)
+        got = torch.full((n,), -1, dtype=torch.int32, device="cuda")
+        torch.cuda.synchronize()
+        assert noalloc_scan(stream, x, got) == tf.OK, tf.lib().tf_last_error()
+        torch.cuda.synchronize()
+        assert torch.equal(got, want), f"call {call}: n={n}"
+
+
+def test_noalloc_scan_in_place_and_limits(ctx):
+    stream = ctx.stream.cuda_stream
+    x = torch.arange(10_000, dtype=torch.int32, device="cuda") % 5
+    want = tf.scan_exclusive(x, ctx=ctx)
+    torch.cuda.synchronize()
+    assert noalloc_scan(stream, x, x) == tf.OK
+    torch.cuda.synchronize()
+    assert torch.equal(x, want)
+    big = (1 << 27) + 1
+    status = tf.lib().tf_scan_exclusive_i32_noalloc(ctypes.c_void_p(stream), big, ctypes.c_void_p(x.data_ptr()),
+                                                    ctypes.c_void_p(x.data_ptr()))
+    assert status == tf.ERR_LENGTH
+    assert b"limit" in tf.lib().tf_last_error()
+    empty = torch.empty(0, dtype=torch.int32, device="cuda")
+    assert noalloc_scan(stream, empty, empty) == tf.OK

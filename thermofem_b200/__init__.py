@@ -138,6 +138,7 @@ SIGNATURES = {
     "tf_radix_sort_pairs_u64f64": ([_P, _L, _P, _P, _P, _P, _I], _I),
     "tf_reduce_by_key_u64f64": ([_P, _L, _P, _P, _I, _P, _P, C.POINTER(C.c_int64)], _I),
     "tf_scan_exclusive_i32": ([_P, _L, _P, _P], _I),
+    "tf_scan_exclusive_i32_noalloc": ([_P, _L, _P, _P], _I),
     "tf_coarse_lu_factor": ([_P, C.POINTER(Csr), _P, _P, C.POINTER(C.c_int)], _I),
     "tf_coarse_lu_solve": ([_P, _I, _P, _P, _I, _P, _P], _I),
     "tf_amg_options_default": ([C.POINTER(AmgOptions)], None),
