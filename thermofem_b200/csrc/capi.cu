@@ -97,6 +97,9 @@ int tf_ctx_create(int device, void *stream, tf_ctx **out) {
             ctx->own_stream = true;
         }
         cuda_check(cudaMallocHost(&ctx->pinned, 256), "cudaMallocHost");
+        cuda_check(cudaMalloc(&ctx->fault, sizeof(int)), "cudaMalloc");
+        cuda_check(cudaMemsetAsync(ctx->fault, 0, sizeof(int), ctx->stream), "cudaMemsetAsync");
+        cuda_check(cudaStreamSynchronize(ctx->stream), "context setup");
         *out = ctx.release();
     });
 }
@@ -109,6 +112,7 @@ int tf_ctx_destroy(tf_ctx *ctx) {
         ctx->scratch.release();
         ctx->scratch2.release();
         if (ctx->pinned) cudaFreeHost(ctx->pinned);
+        if (ctx->fault) cudaFree(ctx->fault);
         if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
         delete ctx;
     });
@@ -118,6 +122,7 @@ int tf_ctx_synchronize(tf_ctx *ctx) {
     return guard([&] {
         check_ctx(ctx);
         cuda_check(cudaStreamSynchronize(ctx->stream), "cudaStreamSynchronize");
+        check_faults(ctx);
     });
 }
 

@@ -146,6 +146,7 @@ struct tf_ctx {
     tfb::DeviceBuffer<unsigned char> scratch;  // grow-only, reused by primitives
     tfb::DeviceBuffer<unsigned char> scratch2;
     void *pinned{nullptr};                      // 256 bytes of pinned host memory
+    int *fault{nullptr};                        // device word raised by a kernel whose bounded wait expired
     // Returns a scratch region of at least bytes (256-byte aligned start).
     void *arena(size_t bytes, int slot = 0) {
         auto &b = slot ? scratch2 : scratch;
@@ -185,6 +186,17 @@ T read_scalar(tf_ctx *ctx, const T *device_ptr) {
 
 inline void memset_async(tf_ctx *ctx, void *p, int value, size_t bytes) {
     if (bytes) cuda_check(cudaMemsetAsync(p, value, bytes, ctx->stream), "cudaMemsetAsync");
+}
+
+// Reads and clears the context's fault word; a raised word means a kernel
+// gave up a bounded wait (its results are not valid).
+inline void check_faults(tf_ctx *ctx) {
+    if (!ctx->fault) return;
+    if (read_scalar(ctx, ctx->fault)) {
+        memset_async(ctx, ctx->fault, 0, sizeof(int));
+        cudaStreamSynchronize(ctx->stream);
+        fail(TF_ERR_TIMEOUT, "a pipelined kernel gave up a bounded wait; results are invalid");
+    }
 }
 
 inline void copy_async(tf_ctx *ctx, void *dst, const void *src, size_t bytes) {

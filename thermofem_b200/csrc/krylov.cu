@@ -475,8 +475,7 @@ class KrylovImpl final : public Krylov {
         }
         for (auto *b : {&rhs_, &x_, &r_, &z_, &p_, &q_, &shadow_, &s_, &t_, &sh_})
             b->allocate(static_cast<size_t>(n_));
-        const auto shape = spmv_shape(n_, nnz_, sizeof(T), sizeof(I));
-        tiles_ = static_cast<int>(tile::grid(shape, n_));
+        tiles_ = tile::partials<T, I>(ctx, n_, nnz_);
         parts_ = parts_for(n_);
         part_.allocate(static_cast<size_t>(2 * std::max(tiles_, parts_)));
         partb_.allocate(static_cast<size_t>(std::max(tiles_, parts_)));
@@ -538,6 +537,7 @@ class KrylovImpl final : public Krylov {
         cuda_check(cudaEventRecord(ev1_, ctx->stream), "event");
         cuda_check(cudaStreamSynchronize(ctx->stream), "solve");
         std::memcpy(&fin, ctx->pinned, sizeof(KState));
+        check_faults(ctx);
         float ms = 0;
         cudaEventElapsedTime(&ms, ev0_, ev1_);
         last_ms = ms;

@@ -119,6 +119,7 @@ int tf_amg_apply(tf_amg *m, const void *rhs, void *x) {
         else
             m->h->apply(m->ctx, static_cast<const float *>(rhs), static_cast<float *>(x));
         cuda_check(cudaStreamSynchronize(m->ctx->stream), "AMG apply");
+        check_faults(m->ctx);
     });
 }
 
@@ -264,6 +265,7 @@ int tf_jacobi_apply(tf_jacobi *j, const void *rhs, void *x) {
         if (j->value_type == TF_F64) run(double{});
         else run(float{});
         cuda_check(cudaStreamSynchronize(ctx->stream), "Jacobi apply");
+        check_faults(ctx);
     });
 }
 

@@ -169,10 +169,264 @@ __global__ void __launch_bounds__(kThreads) csr_tile_kernel(int64_t rows, const 
     }
 }
 
-// Number of CTAs (= partial sums) of a tile launch over these rows.
-inline unsigned grid(const SpmvShape &shape, int64_t rows) {
-    const int64_t tile_rows = static_cast<int64_t>(kThreads) * shape.rows_per_thread;
-    return static_cast<unsigned>((rows + tile_rows - 1) / tile_rows);
+// ---------------------------------------------------------------------------
+// Pipelined persistent variant (sm_100a).
+//
+// A persistent CTA walks tiles blockIdx.x, blockIdx.x + gridDim.x, ...  One
+// producer warp (warp 8, lane 0) streams each tile's row offsets, values and
+// column indices into a ring of shared-memory stages with cp.async.bulk
+// (TMA bulk copies, completion counted in bytes on an mbarrier), staying up
+// to `stages - 1` chunks ahead; the eight consumer warps wait on the stage's
+// "full" barrier, reduce one row per thread exactly as above, and release the
+// stage on its "empty" barrier.  Bulk copies start and end on 16-byte
+// boundaries: a chunk [cs, ce) is copied from align_down(cs) to align_up(ce)
+// (the over-read lies inside the arrays except at their very end, where the
+// ragged tail is fetched with plain loads before the barrier is armed).
+// Every wait is bounded: on expiry the kernel raises *fault, skips its
+// remaining work, drains its own copies (bounded) and returns.
+// ---------------------------------------------------------------------------
+constexpr int kMaxStages = 4;
+constexpr int kPipeCtasPerSm = 2;
+constexpr long long kWaitLimit = 1ll << 20;
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+// Bounded wait for the completion of the phase with the given parity.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+    for (long long i = 0; i < kWaitLimit; ++i)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+
+// Shared-memory layout of one stage: row offsets, values, column indices.
+template <class T, class I>
+struct StageLayout {
+    static constexpr int kVT = 16 / sizeof(T), kVI = 16 / sizeof(I);
+    int rp_bytes, val_bytes, col_bytes, bytes;
+    __host__ __device__ explicit StageLayout(int cap) {
+        rp_bytes = ((kThreads + 1 + kVI) * static_cast<int>(sizeof(I)) + 15) & ~15;
+        val_bytes = ((cap + 2 * kVT) * static_cast<int>(sizeof(T)) + 15) & ~15;
+        col_bytes = ((cap + 2 * kVI) * static_cast<int>(sizeof(I)) + 15) & ~15;
+        bytes = (rp_bytes + val_bytes + col_bytes + 127) & ~127;
+    }
+};
+
+// One range [lo, hi) of an array of length len, staged at dst[j - align_down(lo)].
+template <class E>
+struct Range {
+    int64_t a0{0}, bulk_end{0}, hi{0};
+    __device__ __forceinline__ void plan(int64_t lo, int64_t hi_, int64_t len) {
+        constexpr int64_t V = 16 / sizeof(E);
+        hi = hi_;
+        a0 = lo - (lo % V);
+        const int64_t a1 = (hi_ + V - 1) / V * V;
+        bulk_end = hi_ <= lo ? a0 : (a1 <= len ? a1 : hi_ - (hi_ % V));
+        if (bulk_end < a0) bulk_end = a0;
+    }
+    __device__ __forceinline__ void plain(E *dst, const E *src) const {
+        for (int64_t j = bulk_end; j < hi; ++j) dst[j - a0] = src[j];
+    }
+    __device__ __forceinline__ uint32_t bytes() const { return static_cast<uint32_t>((bulk_end - a0) * sizeof(E)); }
+    __device__ __forceinline__ void issue(E *dst, const E *src, uint64_t *bar) const {
+        if (bulk_end > a0) bulk_load(dst, src + a0, bytes(), bar);
+    }
+};
+
+template <class T, class I, class XS, class Epi>
+__global__ void __launch_bounds__(kThreads + 32) csr_pipe_kernel(int64_t rows, int64_t nnz, const I *__restrict__ rp,
+                                                                  const I *__restrict__ ci,
+                                                                  const T *__restrict__ val, int cap, int stages,
+                                                                  XS xs, Epi epi, int *fault) {
+    constexpr int K = Epi::kReduce;
+    constexpr int kVT = 16 / sizeof(T), kVI = 16 / sizeof(I);
+    if (epi.skip()) return;
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ uint64_t full_bar[kMaxStages], empty_bar[kMaxStages];
+    const StageLayout<T, I> L(cap);
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        for (int s = 0; s < stages; ++s) {
+            mbar_init(&full_bar[s], 1);
+            mbar_init(&empty_bar[s], kThreads / 32);
+        }
+        mbar_fence_init();
+    }
+    __syncthreads();
+    auto stage_rp = [&](int s) { return reinterpret_cast<I *>(smem + static_cast<size_t>(s) * L.bytes); };
+    auto stage_val = [&](int s) {
+        return reinterpret_cast<T *>(smem + static_cast<size_t>(s) * L.bytes + L.rp_bytes);
+    };
+    auto stage_col = [&](int s) {
+        return reinterpret_cast<I *>(smem + static_cast<size_t>(s) * L.bytes + L.rp_bytes + L.val_bytes);
+    };
+    const int64_t ntiles = (rows + kThreads - 1) / kThreads;
+    double red[K > 0 ? K : 1];
+#pragma unroll
+    for (int k = 0; k < (K > 0 ? K : 1); ++k) red[k] = 0.0;
+    bool ok = true;
+    uint32_t armed[kMaxStages] = {0, 0, 0, 0};  // producer: completions requested per stage
+
+    if (tid == kThreads) {
+        // ---- producer ----
+        uint32_t it = 0;
+        for (int64_t tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+            const int64_t r0 = tile * kThreads;
+            const int nr = static_cast<int>(min(static_cast<int64_t>(kThreads), rows - r0));
+            const int64_t s = rp[r0], e = rp[r0 + nr];
+            const int64_t nch = e > s ? (e - s + cap - 1) / cap : 1;
+            for (int64_t c = 0; c < nch && ok; ++c, ++it) {
+                const int st = static_cast<int>(it % stages);
+                if (it >= static_cast<uint32_t>(stages) && !mbar_wait(&empty_bar[st], ((it / stages) + 1) & 1)) {
+                    ok = false;
+                    break;
+                }
+                const int64_t cs = s + c * cap, ce = min(e, cs + cap);
+                Range<I> rr;
+                if (c == 0) rr.plan(r0, r0 + nr + 1, rows + 1);
+                else rr.plan(r0, r0, rows + 1);
+                Range<T> rv;
+                rv.plan(cs, ce, nnz);
+                Range<I> rc;
+                rc.plan(cs, ce, nnz);
+                rr.plain(stage_rp(st), rp);
+                rv.plain(stage_val(st), val);
+                rc.plain(stage_col(st), ci);
+                mbar_arrive_expect_tx(&full_bar[st], rr.bytes() + rv.bytes() + rc.bytes());
+                ++armed[st];
+                rr.issue(stage_rp(st), rp, &full_bar[st]);
+                rv.issue(stage_val(st), val, &full_bar[st]);
+                rc.issue(stage_col(st), ci, &full_bar[st]);
+            }
+        }
+        if (!ok) atomicExch(fault, 1);
+    } else if (tid < kThreads) {
+        // ---- consumers: one row per thread ----
+        const int lane = tid & 31;
+        uint32_t it = 0;
+        for (int64_t tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+            const int64_t r0 = tile * kThreads;
+            const int nr = static_cast<int>(min(static_cast<int64_t>(kThreads), rows - r0));
+            const bool valid = tid < nr;
+            int64_t rs = 0, re = 0, s = 0, e = 0, nch = 1;
+            T acc = T(0);
+            for (int64_t c = 0; c < nch; ++c, ++it) {
+                const int st = static_cast<int>(it % stages);
+                // warp-uniform decision, so __syncwarp below never waits on a lane that left
+                if (__any_sync(0xffffffffu, !mbar_wait(&full_bar[st], (it / stages) & 1))) {
+                    ok = false;
+                    if (lane == 0) atomicExch(fault, 1);
+                    break;
+                }
+                if (c == 0) {
+                    const I *srp = stage_rp(st);
+                    s = srp[0];
+                    e = srp[nr];
+                    nch = e > s ? (e - s + cap - 1) / cap : 1;
+                    if (valid) {
+                        rs = srp[tid];
+                        re = srp[tid + 1];
+                    }
+                }
+                const int64_t cs = s + c * cap, ce = min(e, cs + cap);
+                const T *sv = stage_val(st);
+                const I *sc = stage_col(st);
+                const int64_t av = cs - (cs % kVT), ac = cs - (cs % kVI);
+                const int64_t lo = max(rs, cs), hi = min(re, ce);
+                constexpr int kGather = 8;
+                for (int64_t j0 = lo; j0 < hi; j0 += kGather) {
+                    T y[kGather];
+#pragma unroll
+                    for (int u = 0; u < kGather; ++u) {
+                        const int64_t j = j0 + u;
+                        y[u] = j < hi ? xs(static_cast<int64_t>(sc[j - ac])) : T(0);
+                    }
+#pragma unroll
+                    for (int u = 0; u < kGather; ++u) {
+                        const int64_t j = j0 + u;
+                        acc += (j < hi ? sv[j - av] : T(0)) * y[u];
+                    }
+                }
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&empty_bar[st]);
+            }
+            if (!ok) break;
+            if (valid) epi(r0 + tid, acc, xs, red);
+        }
+    }
+    __syncthreads();
+    if (tid == kThreads) {
+        // No copy of this CTA may still be in flight when it exits: wait
+        // (bounded; immediate when the consumers consumed everything) for the
+        // last phase armed on every stage.
+        for (int st = 0; st < stages; ++st)
+            if (armed[st]) mbar_wait(&full_bar[st], (armed[st] - 1) & 1);
+    }
+    if constexpr (K > 0) {
+        block_reduce<K>(red);
+        if (tid == 0)
+#pragma unroll
+            for (int k = 0; k < K; ++k) epi.partial[k * gridDim.x + blockIdx.x] = red[k];
+    }
+}
+
+// Pipelined launch shape: entries per chunk (from the operator's mean row
+// length, within a 32 KB stage) and the number of stages.
+struct PipeShape {
+    int cap, stages, grid;
+    size_t smem;
+};
+
+template <class T, class I>
+PipeShape pipe_shape(int64_t rows, int64_t nnz, int sm_count) {
+    PipeShape p;
+    const int rp_bytes = ((kThreads + 1 + 16 / static_cast<int>(sizeof(I))) * static_cast<int>(sizeof(I)) + 15) & ~15;
+    const int max_cap = ((32768 - rp_bytes) / static_cast<int>(sizeof(T) + sizeof(I)) - 8) & ~63;
+    const int64_t mean_tile = rows > 0 ? (nnz * kThreads + rows - 1) / rows : 0;
+    int64_t cap = (mean_tile + mean_tile / 4 + 63) & ~int64_t(63);
+    if (cap < 256) cap = 256;
+    if (cap > max_cap) cap = max_cap;
+    p.cap = static_cast<int>(cap);
+    p.stages = 3;
+    p.smem = static_cast<size_t>(StageLayout<T, I>(p.cap).bytes) * p.stages;
+    const int64_t ntiles = (rows + kThreads - 1) / kThreads;
+    const int64_t g = static_cast<int64_t>(sm_count) * kPipeCtasPerSm;
+    p.grid = static_cast<int>(ntiles < g ? (ntiles < 1 ? 1 : ntiles) : g);
+    return p;
+}
+
+// Number of per-CTA partial sums a reducing launch over this operator writes.
+template <class T, class I>
+inline int partials(const tf_ctx *ctx, int64_t rows, int64_t nnz) {
+    return pipe_shape<T, I>(rows, nnz, ctx->sm_count).grid;
 }
 
 // Opts the instantiation into the dynamic shared memory it is launched with
@@ -191,11 +445,28 @@ void allow_smem(size_t bytes) {
     configured_bytes = bytes;
 }
 
+inline bool aligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+// Launches the pipelined kernel when the three arrays start on 16-byte
+// boundaries (every buffer this library allocates does), the staged kernel
+// otherwise.  Reducing epilogues need the pipelined kernel: their partial
+// sums are per CTA of its persistent grid (tile::partials).
 template <class T, class I, class XS, class Epi>
 void launch(tf_ctx *ctx, const Csr<T, I> &a, const XS &xs, const Epi &epi, const char *name) {
     if (a.rows == 0) return;
+    const bool pipe = aligned16(a.rp) && (a.nnz == 0 || (aligned16(a.ci) && aligned16(a.val)));
+    if (pipe) {
+        const PipeShape p = pipe_shape<T, I>(a.rows, a.nnz, ctx->sm_count);
+        allow_smem<csr_pipe_kernel<T, I, XS, Epi>>(p.smem);
+        csr_pipe_kernel<T, I, XS, Epi><<<p.grid, kThreads + 32, p.smem, ctx->stream>>>(
+            a.rows, a.nnz, a.rp, a.ci, a.val, p.cap, p.stages, xs, epi, ctx->fault);
+        launched(ctx, name);
+        return;
+    }
+    require(Epi::kReduce == 0, "reducing SpMV epilogues need 16-byte aligned CSR arrays");
     const SpmvShape shape = spmv_shape(a.rows, a.nnz, sizeof(T), sizeof(I));
-    const unsigned g = grid(shape, a.rows);
+    const int64_t tile_rows = static_cast<int64_t>(kThreads) * shape.rows_per_thread;
+    const unsigned g = static_cast<unsigned>((a.rows + tile_rows - 1) / tile_rows);
     const size_t smem = static_cast<size_t>(shape.chunk) * (sizeof(T) + sizeof(I));
     if (shape.rows_per_thread == 2) {
         allow_smem<csr_tile_kernel<T, I, 2, XS, Epi>>(smem);
