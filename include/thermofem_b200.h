@@ -111,6 +111,15 @@ int tf_spmv_f64(tf_ctx *ctx, int64_t rows, int64_t cols, int64_t nnz, const int3
                 const int32_t *indices, const double *values, const double *x, double *y);
 int tf_spmv_f32(tf_ctx *ctx, int64_t rows, int64_t cols, int64_t nnz, const int32_t *offsets,
                 const int32_t *indices, const float *values, const float *x, float *y);
+/* SpMV autotuner (replaces the fixed library algorithm choice of
+ * cusparseSpMV ALG_DEFAULT, IterationContext.cu:140-159): times the feasible
+ * pipelined launch shapes (ring depth 2-4, 2-6 resident CTAs per SM, chunk
+ * capacity 100% or 125% of the mean tile) on this operator and caches the
+ * fastest for every later row-tile launch over an operator of the same shape
+ * (rows, nnz, types).  y is overwritten.  Outputs may be NULL; *ms is the
+ * best time per launch.  Results never depend on the shape chosen. */
+int tf_autotune_spmv(tf_ctx *ctx, const tf_csr *a, const void *x, void *y, int *stages, int *ctas_per_sm,
+                     int *cap_pct, float *ms);
 /* r = b - A x in one pass (replaces SpMV + scal + axpy, IterationContext.cu:167-175). */
 int tf_residual(tf_ctx *ctx, const tf_csr *a, const void *b, const void *x, void *r);
 /* One fused weighted-Jacobi sweep x_out = x + w * Dinv (b - A x)

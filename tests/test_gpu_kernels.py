@@ -280,3 +280,17 @@ def test_coarse_lu_scale_invariance_and_singular(ctx):
         assert np.array_equal(b.cpu().numpy(), x)
     ok, _, _ = tf.coarse_lu_factor(to_device((off, idx, np.ones(4))), ctx=ctx)
     assert not ok
+
+
+def test_autotune_changes_speed_not_results(ctx):
+    off, idx, val = P.heat3d(40, seed=8)
+    n = len(off) - 1
+    a = to_device((off, idx, val))
+    x = torch.tensor(np.random.default_rng(5).standard_normal(n), device="cuda")
+    before = tf.spmv(a, x, ctx=ctx).clone()
+    stages, ctas, cap, ms = tf.autotune_spmv(a, x, ctx=ctx)
+    assert 2 <= stages <= 4 and 2 <= ctas <= 6 and cap in (100, 125) and ms > 0
+    after = tf.spmv(a, x, ctx=ctx)
+    assert torch.equal(before, after)
+    r1 = tf.residual(a, x, x.clone(), ctx=ctx)
+    assert torch.isfinite(r1).all()

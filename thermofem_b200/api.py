@@ -13,7 +13,7 @@ from . import (AmgOptions, Csr, HostCsr, SolveResult, SolverOptions, F32, F64, I
                SOLVER_BICGSTAB, PRECOND_AMG, PRECOND_IDENTITY, check, lib)
 
 __all__ = ["Context", "DeviceCsr", "Transfer", "Amg", "Jacobi", "Cg", "BiCgStab", "amg_options", "solver_options",
-           "read_matrix_market", "read_matrix_market_file", "spmv", "residual", "jacobi_sweep", "jacobi_zero",
+           "read_matrix_market", "read_matrix_market_file", "spmv", "autotune_spmv", "residual", "jacobi_sweep", "jacobi_zero",
            "inverse_diagonal", "restrict_aggregates", "prolong_aggregates", "dot_multi", "axpby", "convert",
            "csr_validate", "check_canonical", "canonicalize", "row_stats", "strength", "match", "contract",
            "aggregate", "galerkin", "radix_sort_pairs", "reduce_by_key", "scan_exclusive", "coarse_lu_factor",
@@ -167,6 +167,19 @@ def spmv(a: DeviceCsr, x, y=None, ctx=None):
     with ctx:
         check(lib().tf_spmv(ctx.h, C.byref(d), _p(x), _p(y)))
     return y
+
+
+def autotune_spmv(a: DeviceCsr, x, y=None, ctx=None):
+    """Times the pipelined SpMV shapes on this operator and caches the best;
+    returns (stages, ctas_per_sm, cap_pct, ms_per_launch)."""
+    ctx = _ctx(ctx)
+    y = torch.empty(a.rows, dtype=a.dtype, device=x.device) if y is None else y
+    d = a.desc()
+    st, ct, cp, ms = C.c_int(), C.c_int(), C.c_int(), C.c_float()
+    with ctx:
+        check(lib().tf_autotune_spmv(ctx.h, C.byref(d), _p(x), _p(y), C.byref(st), C.byref(ct), C.byref(cp),
+                                     C.byref(ms)))
+    return st.value, ct.value, cp.value, ms.value
 
 
 def residual(a: DeviceCsr, b, x, r=None, ctx=None):

@@ -115,6 +115,10 @@ class HierarchyImpl final : public Hierarchy {
             for (auto *b : {&l.dinv, &l.rhs, &l.x0, &l.x1, &l.r}) b->allocate(static_cast<size_t>(l.n));
             // The diagonal must also invert in the iteration precision.
             inverse_diagonal(ctx, l.csr(), l.dinv.data());
+            // Launch shape of this level's row-tile kernels (cached by shape).
+            fill_zero(ctx, l.n, l.rhs.data());
+            autotune_spmv(ctx, l.csr(), static_cast<const S *>(l.rhs.data()), l.r.data(), nullptr, nullptr, nullptr,
+                          nullptr);
             LevelStats st;
             st.rows = l.n;
             st.nnz = l.nnz;

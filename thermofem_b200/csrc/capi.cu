@@ -246,6 +246,21 @@ int tf_spmv_f32(tf_ctx *ctx, int64_t rows, int64_t cols, int64_t nnz, const int3
     return tf_spmv(ctx, &a, x, y);
 }
 
+int tf_autotune_spmv(tf_ctx *ctx, const tf_csr *a, const void *x, void *y, int *stages, int *ctas_per_sm,
+                     int *cap_pct, float *ms) {
+    return guard([&] {
+        check_ctx(ctx);
+        require(x != y || a->rows == 0, "SpMV shape or alias mismatch");
+        DeviceScope scope(ctx->device);
+        with_csr_types(a, [&](auto t, auto i) {
+            using T = decltype(t);
+            using I = decltype(i);
+            autotune_spmv(ctx, csr_of<T, I>(*a), static_cast<const T *>(x), static_cast<T *>(y), stages, ctas_per_sm,
+                          cap_pct, ms);
+        });
+    });
+}
+
 int tf_residual(tf_ctx *ctx, const tf_csr *a, const void *b, const void *x, void *r) {
     return guard([&] {
         check_ctx(ctx);

@@ -115,15 +115,21 @@ __global__ void k_dot(int64_t n, const T *__restrict__ x, const T *__restrict__ 
 template <class T>
 struct SpmvDot {
     static constexpr int kReduce = 1;
+    struct Pre {
+        T w;
+    };
     T *__restrict__ y;
     const T *__restrict__ w;
     const int *gate;
     double *partial;
     __device__ __forceinline__ bool skip() const { return gate && !*gate; }
     template <class XS>
-    __device__ __forceinline__ void operator()(int64_t i, T acc, const XS &, double (&red)[1]) const {
+    __device__ __forceinline__ Pre pre(int64_t i, const XS &) const {
+        return {w[i]};
+    }
+    __device__ __forceinline__ void operator()(int64_t i, T acc, const Pre &p, double (&red)[1]) const {
         y[i] = acc;
-        red[0] += static_cast<double>(w[i]) * static_cast<double>(acc);
+        red[0] += static_cast<double>(p.w) * static_cast<double>(acc);
     }
 };
 
@@ -131,17 +137,23 @@ struct SpmvDot {
 template <class T>
 struct SpmvDot2 {
     static constexpr int kReduce = 2;
+    struct Pre {
+        T s;
+    };
     T *__restrict__ y;
     const T *__restrict__ s;
     const int *gate;
     double *partial;
     __device__ __forceinline__ bool skip() const { return gate && !*gate; }
     template <class XS>
-    __device__ __forceinline__ void operator()(int64_t i, T acc, const XS &, double (&red)[2]) const {
+    __device__ __forceinline__ Pre pre(int64_t i, const XS &) const {
+        return {s[i]};
+    }
+    __device__ __forceinline__ void operator()(int64_t i, T acc, const Pre &p, double (&red)[2]) const {
         y[i] = acc;
         const double t = static_cast<double>(acc);
         red[0] += t * t;
-        red[1] += t * static_cast<double>(s[i]);
+        red[1] += t * static_cast<double>(p.s);
     }
 };
 
@@ -149,14 +161,20 @@ struct SpmvDot2 {
 template <class T>
 struct ResidualNorm {
     static constexpr int kReduce = 1;
+    struct Pre {
+        T b;
+    };
     const T *__restrict__ b;
     T *__restrict__ r;
     const int *gate;
     double *partial;
     __device__ __forceinline__ bool skip() const { return gate && !*gate; }
     template <class XS>
-    __device__ __forceinline__ void operator()(int64_t i, T acc, const XS &, double (&red)[1]) const {
-        const T v = b[i] - acc;
+    __device__ __forceinline__ Pre pre(int64_t i, const XS &) const {
+        return {b[i]};
+    }
+    __device__ __forceinline__ void operator()(int64_t i, T acc, const Pre &p, double (&red)[1]) const {
+        const T v = p.b - acc;
         r[i] = v;
         red[0] += static_cast<double>(v) * static_cast<double>(v);
     }
@@ -475,7 +493,9 @@ class KrylovImpl final : public Krylov {
         }
         for (auto *b : {&rhs_, &x_, &r_, &z_, &p_, &q_, &shadow_, &s_, &t_, &sh_})
             b->allocate(static_cast<size_t>(n_));
-        tiles_ = tile::partials<T, I>(ctx, n_, nnz_);
+        tiles_ = tile::partials(n_);
+        fill_zero(ctx, n_, x_.data());
+        autotune_spmv(ctx, csr(), static_cast<const T *>(x_.data()), q_.data(), nullptr, nullptr, nullptr, nullptr);
         parts_ = parts_for(n_);
         part_.allocate(static_cast<size_t>(2 * std::max(tiles_, parts_)));
         partb_.allocate(static_cast<size_t>(std::max(tiles_, parts_)));

@@ -28,6 +28,12 @@ SpmvShape spmv_shape(int64_t rows, int64_t nnz, size_t value_size, size_t index_
 // y = A x
 template <class T, class I>
 void spmv(tf_ctx *ctx, const Csr<T, I> &a, const T *x, T *y);
+// Picks and caches the fastest pipelined launch shape for operators of this
+// shape (y is overwritten).  Writes the chosen ring depth, CTAs per SM, chunk
+// capacity percentage and the best time per launch (ms) when non-null.
+template <class T, class I>
+void autotune_spmv(tf_ctx *ctx, const Csr<T, I> &a, const T *x, T *y, int *stages, int *ctas_per_sm, int *cap_pct,
+                   float *ms);
 // r = b - A x
 template <class T, class I>
 void residual(tf_ctx *ctx, const Csr<T, I> &a, const T *b, const T *x, T *r);

@@ -1,10 +1,12 @@
-// spmv.cu -- the SpMV family on the row-tile kernel (tile.cuh) and the
+// spmv.cu -- the SpMV family on the row-tile kernels (tile.cuh) and the
 // vector kernels around it.
 //
 // The epilogue is a template parameter, so the residual, the weighted-Jacobi
 // sweep and the prolongation-fused sweep read A exactly once per pass: the
 // reference does SpMV + scal + axpy (src/LinearAlgebra/IterationContext.cu:
-// 167-175) and SpMV + update (:26-32,251-269) as separate passes.
+// 167-175) and SpMV + update (:26-32,251-269) as separate passes.  Each
+// epilogue's pre() loads the row's own operands (issued at the start of the
+// row's tile so their latency overlaps the gathers).
 #include "tile.cuh"
 
 namespace tfb {
@@ -16,25 +18,33 @@ using tile::ProlongX;
 template <class T>
 struct StoreY {
     static constexpr int kReduce = 0;
+    struct Pre {};
     T *__restrict__ y;
     double *partial{nullptr};
     __device__ __forceinline__ bool skip() const { return false; }
     template <class XS>
-    __device__ __forceinline__ void operator()(int64_t i, T acc, const XS &, double (&)[1]) const {
-        y[i] = acc;
+    __device__ __forceinline__ Pre pre(int64_t, const XS &) const {
+        return {};
     }
+    __device__ __forceinline__ void operator()(int64_t i, T acc, const Pre &, double (&)[1]) const { y[i] = acc; }
 };
 
 template <class T>
 struct ResidualOut {
     static constexpr int kReduce = 0;
+    struct Pre {
+        T b;
+    };
     const T *__restrict__ b;
     T *__restrict__ r;
     double *partial{nullptr};
     __device__ __forceinline__ bool skip() const { return false; }
     template <class XS>
-    __device__ __forceinline__ void operator()(int64_t i, T acc, const XS &, double (&)[1]) const {
-        r[i] = b[i] - acc;
+    __device__ __forceinline__ Pre pre(int64_t i, const XS &) const {
+        return {b[i]};
+    }
+    __device__ __forceinline__ void operator()(int64_t i, T acc, const Pre &p, double (&)[1]) const {
+        r[i] = p.b - acc;
     }
 };
 
@@ -43,6 +53,9 @@ struct ResidualOut {
 template <class T>
 struct JacobiOut {
     static constexpr int kReduce = 0;
+    struct Pre {
+        T x, d, b, w;
+    };
     const T *__restrict__ dinv;
     const T *__restrict__ b;
     T *__restrict__ xo;
@@ -51,9 +64,11 @@ struct JacobiOut {
     double *partial{nullptr};
     __device__ __forceinline__ bool skip() const { return false; }
     template <class XS>
-    __device__ __forceinline__ void operator()(int64_t i, T acc, const XS &xs, double (&)[1]) const {
-        const T wi = row_w ? static_cast<T>(row_w[i]) : w;
-        xo[i] = xs(i) + wi * dinv[i] * (b[i] - acc);
+    __device__ __forceinline__ Pre pre(int64_t i, const XS &xs) const {
+        return {xs(i), dinv[i], b[i], row_w ? static_cast<T>(row_w[i]) : w};
+    }
+    __device__ __forceinline__ void operator()(int64_t i, T acc, const Pre &p, double (&)[1]) const {
+        xo[i] = p.x + p.w * p.d * (p.b - acc);
     }
 };
 
@@ -262,6 +277,15 @@ void spmv(tf_ctx *ctx, const Csr<T, I> &a, const T *x, T *y) {
 }
 
 template <class T, class I>
+void autotune_spmv(tf_ctx *ctx, const Csr<T, I> &a, const T *x, T *y, int *stages, int *ctas_per_sm, int *cap_pct,
+                   float *ms) {
+    const tile::PipeConfig c = tile::autotune(ctx, a, x, y, ms);
+    if (stages) *stages = c.stages;
+    if (ctas_per_sm) *ctas_per_sm = c.ctas_per_sm;
+    if (cap_pct) *cap_pct = c.cap_pct;
+}
+
+template <class T, class I>
 void residual(tf_ctx *ctx, const Csr<T, I> &a, const T *b, const T *x, T *r) {
     launch_tile(ctx, a, PlainX<T>{x}, ResidualOut<T>{b, r, nullptr}, "residual");
 }
@@ -389,6 +413,7 @@ bool row_stats(tf_ctx *ctx, const Csr<double, int32_t> &a, double *row_max) {
 
 #define TF_SPMV_INST(T, I)                                                                                     \
     template void spmv<T, I>(tf_ctx *, const Csr<T, I> &, const T *, T *);                                     \
+    template void autotune_spmv<T, I>(tf_ctx *, const Csr<T, I> &, const T *, T *, int *, int *, int *, float *); \
     template void residual<T, I>(tf_ctx *, const Csr<T, I> &, const T *, const T *, T *);                      \
     template void jacobi_sweep<T, I>(tf_ctx *, const Csr<T, I> &, const T *, const T *, const T *, T *, T,     \
                                      const float *, const int32_t *, const T *);                               \

@@ -11,6 +11,10 @@
 // reduces into per-tile partial sums (deterministic: fixed tile partition and
 // fixed reduction tree), and may gate the whole launch on a device flag.
 #pragma once
+#include <map>
+#include <mutex>
+#include <tuple>
+
 #include "ops.cuh"
 
 namespace tfb {
@@ -159,13 +163,14 @@ __global__ void __launch_bounds__(kThreads) csr_tile_kernel(int64_t rows, const 
 #pragma unroll
     for (int k = 0; k < RPT; ++k) {
         const int64_t r = r0 + threadIdx.x + k * kThreads;
-        if (r < rows) epi(r, acc[k], xs, red);
+        if (r < rows) epi(r, acc[k], epi.pre(r, xs), red);
     }
     if constexpr (K > 0) {
         block_reduce<K>(red);
-        if (threadIdx.x == 0)
+        if (threadIdx.x == 0) {
 #pragma unroll
             for (int k = 0; k < K; ++k) epi.partial[k * gridDim.x + blockIdx.x] = red[k];
+        }
     }
 }
 
@@ -271,6 +276,8 @@ __global__ void __launch_bounds__(kThreads + 32) csr_pipe_kernel(int64_t rows, i
     if (epi.skip()) return;
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ uint64_t full_bar[kMaxStages], empty_bar[kMaxStages];
+    __shared__ double warp_sums[kMaxStages + 1][kThreads / 32][K > 0 ? K : 1];
+    __shared__ int warp_done[kMaxStages + 1];
     const StageLayout<T, I> L(cap);
     const int tid = threadIdx.x;
     if (tid == 0) {
@@ -278,6 +285,7 @@ __global__ void __launch_bounds__(kThreads + 32) csr_pipe_kernel(int64_t rows, i
             mbar_init(&full_bar[s], 1);
             mbar_init(&empty_bar[s], kThreads / 32);
         }
+        for (int s = 0; s < kMaxStages + 1; ++s) warp_done[s] = 0;
         mbar_fence_init();
     }
     __syncthreads();
@@ -331,13 +339,17 @@ __global__ void __launch_bounds__(kThreads + 32) csr_pipe_kernel(int64_t rows, i
     } else if (tid < kThreads) {
         // ---- consumers: one row per thread ----
         const int lane = tid & 31;
-        uint32_t it = 0;
+        uint32_t it = 0, local_tile = 0;
         for (int64_t tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
             const int64_t r0 = tile * kThreads;
             const int nr = static_cast<int>(min(static_cast<int64_t>(kThreads), rows - r0));
             const bool valid = tid < nr;
             int64_t rs = 0, re = 0, s = 0, e = 0, nch = 1;
             T acc = T(0);
+            // The row's own epilogue operands (b, D^-1, x_i, ...) are loaded
+            // now, so their latency overlaps the stage wait and the gathers.
+            typename Epi::Pre pre{};
+            if (valid) pre = epi.pre(r0 + tid, xs);
             for (int64_t c = 0; c < nch; ++c, ++it) {
                 const int st = static_cast<int>(it % stages);
                 // warp-uniform decision, so __syncwarp below never waits on a lane that left
@@ -379,7 +391,37 @@ __global__ void __launch_bounds__(kThreads + 32) csr_pipe_kernel(int64_t rows, i
                 if (lane == 0) mbar_arrive(&empty_bar[st]);
             }
             if (!ok) break;
-            if (valid) epi(r0 + tid, acc, xs, red);
+            if (valid) epi(r0 + tid, acc, pre, red);
+            if constexpr (K > 0) {
+                // Per-tile partial sums, independent of the grid: each warp
+                // reduces its rows, the last warp of the tile to finish adds
+                // the eight warp sums in warp order.  Warps are at most
+                // `stages` tiles apart, so a ring of kMaxStages + 1 slots
+                // never overwrites a slot still being read.
+#pragma unroll
+                for (int k = 0; k < K; ++k)
+                    for (int o = 16; o > 0; o >>= 1) red[k] += __shfl_down_sync(0xffffffffu, red[k], o);
+                const int slot = static_cast<int>(local_tile % (kMaxStages + 1));
+                const int warp = tid >> 5;
+                if (lane == 0) {
+#pragma unroll
+                    for (int k = 0; k < K; ++k) warp_sums[slot][warp][k] = red[k];
+                    __threadfence_block();
+                    if (atomicAdd(&warp_done[slot], 1) == kThreads / 32 - 1) {
+                        __threadfence_block();
+#pragma unroll
+                        for (int k = 0; k < K; ++k) {
+                            double v = 0.0;
+                            for (int w = 0; w < kThreads / 32; ++w) v += warp_sums[slot][w][k];
+                            epi.partial[k * ntiles + tile] = v;
+                        }
+                        warp_done[slot] = 0;
+                    }
+                }
+#pragma unroll
+                for (int k = 0; k < K; ++k) red[k] = 0.0;
+            }
+            ++local_tile;
         }
     }
     __syncthreads();
@@ -390,43 +432,72 @@ __global__ void __launch_bounds__(kThreads + 32) csr_pipe_kernel(int64_t rows, i
         for (int st = 0; st < stages; ++st)
             if (armed[st]) mbar_wait(&full_bar[st], (armed[st] - 1) & 1);
     }
-    if constexpr (K > 0) {
-        block_reduce<K>(red);
-        if (tid == 0)
-#pragma unroll
-            for (int k = 0; k < K; ++k) epi.partial[k * gridDim.x + blockIdx.x] = red[k];
-    }
 }
 
-// Pipelined launch shape: entries per chunk (from the operator's mean row
-// length, within a 32 KB stage) and the number of stages.
+// Pipelined launch shape: entries per chunk, stages in the ring, resident
+// CTAs per SM (the persistent grid is ctas_per_sm x SMs, at most one CTA per
+// tile).
 struct PipeShape {
-    int cap, stages, grid;
+    int cap, stages, ctas_per_sm, grid;
     size_t smem;
 };
 
+// Tunable part of the shape: ring depth, resident CTAs per SM and the chunk
+// capacity as a percentage of the mean tile.  The result does not depend on
+// it (rows are reduced left to right in any chunking, partial sums are per
+// 256-row tile), only the speed does.
+struct PipeConfig {
+    int stages{3}, ctas_per_sm{2}, cap_pct{125};
+};
+
 template <class T, class I>
-PipeShape pipe_shape(int64_t rows, int64_t nnz, int sm_count) {
+PipeShape pipe_shape(int64_t rows, int64_t nnz, int sm_count, const PipeConfig &cfg) {
     PipeShape p;
     const int rp_bytes = ((kThreads + 1 + 16 / static_cast<int>(sizeof(I))) * static_cast<int>(sizeof(I)) + 15) & ~15;
     const int max_cap = ((32768 - rp_bytes) / static_cast<int>(sizeof(T) + sizeof(I)) - 8) & ~63;
     const int64_t mean_tile = rows > 0 ? (nnz * kThreads + rows - 1) / rows : 0;
-    int64_t cap = (mean_tile + mean_tile / 4 + 63) & ~int64_t(63);
+    int64_t cap = (mean_tile * cfg.cap_pct / 100 + 63) & ~int64_t(63);
     if (cap < 256) cap = 256;
     if (cap > max_cap) cap = max_cap;
     p.cap = static_cast<int>(cap);
-    p.stages = 3;
+    p.stages = cfg.stages;
+    p.ctas_per_sm = cfg.ctas_per_sm;
     p.smem = static_cast<size_t>(StageLayout<T, I>(p.cap).bytes) * p.stages;
     const int64_t ntiles = (rows + kThreads - 1) / kThreads;
-    const int64_t g = static_cast<int64_t>(sm_count) * kPipeCtasPerSm;
+    const int64_t g = static_cast<int64_t>(sm_count) * cfg.ctas_per_sm;
     p.grid = static_cast<int>(ntiles < g ? (ntiles < 1 ? 1 : ntiles) : g);
     return p;
 }
 
-// Number of per-CTA partial sums a reducing launch over this operator writes.
+// Number of partial sums a reducing launch writes: one per 256-row tile.
+inline int partials(int64_t rows) { return static_cast<int>(rows > 0 ? (rows + kThreads - 1) / kThreads : 1); }
+
+// Process-wide cache of tuned configurations, keyed by the operator's shape.
+struct TuneKey {
+    int64_t rows, nnz;
+    int vsize, isize, sm_count;
+    bool operator<(const TuneKey &o) const {
+        return std::tie(rows, nnz, vsize, isize, sm_count) < std::tie(o.rows, o.nnz, o.vsize, o.isize, o.sm_count);
+    }
+};
+inline std::mutex &tune_mutex() {
+    static std::mutex m;
+    return m;
+}
+inline std::map<TuneKey, PipeConfig> &tune_cache() {
+    static std::map<TuneKey, PipeConfig> m;
+    return m;
+}
 template <class T, class I>
-inline int partials(const tf_ctx *ctx, int64_t rows, int64_t nnz) {
-    return pipe_shape<T, I>(rows, nnz, ctx->sm_count).grid;
+PipeConfig tuned_config(int64_t rows, int64_t nnz, int sm_count) {
+    std::lock_guard<std::mutex> lock(tune_mutex());
+    auto it = tune_cache().find(TuneKey{rows, nnz, static_cast<int>(sizeof(T)), static_cast<int>(sizeof(I)), sm_count});
+    return it == tune_cache().end() ? PipeConfig{} : it->second;
+}
+template <class T, class I>
+void store_config(int64_t rows, int64_t nnz, int sm_count, const PipeConfig &cfg) {
+    std::lock_guard<std::mutex> lock(tune_mutex());
+    tune_cache()[TuneKey{rows, nnz, static_cast<int>(sizeof(T)), static_cast<int>(sizeof(I)), sm_count}] = cfg;
 }
 
 // Opts the instantiation into the dynamic shared memory it is launched with
@@ -452,11 +523,13 @@ inline bool aligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 
 // otherwise.  Reducing epilogues need the pipelined kernel: their partial
 // sums are per CTA of its persistent grid (tile::partials).
 template <class T, class I, class XS, class Epi>
-void launch(tf_ctx *ctx, const Csr<T, I> &a, const XS &xs, const Epi &epi, const char *name) {
+void launch(tf_ctx *ctx, const Csr<T, I> &a, const XS &xs, const Epi &epi, const char *name,
+            const PipeConfig *force = nullptr) {
     if (a.rows == 0) return;
     const bool pipe = aligned16(a.rp) && (a.nnz == 0 || (aligned16(a.ci) && aligned16(a.val)));
     if (pipe) {
-        const PipeShape p = pipe_shape<T, I>(a.rows, a.nnz, ctx->sm_count);
+        const PipeConfig cfg = force ? *force : tuned_config<T, I>(a.rows, a.nnz, ctx->sm_count);
+        const PipeShape p = pipe_shape<T, I>(a.rows, a.nnz, ctx->sm_count, cfg);
         allow_smem<csr_pipe_kernel<T, I, XS, Epi>>(p.smem);
         csr_pipe_kernel<T, I, XS, Epi><<<p.grid, kThreads + 32, p.smem, ctx->stream>>>(
             a.rows, a.nnz, a.rp, a.ci, a.val, p.cap, p.stages, xs, epi, ctx->fault);
@@ -476,6 +549,69 @@ void launch(tf_ctx *ctx, const Csr<T, I> &a, const XS &xs, const Epi &epi, const
         csr_tile_kernel<T, I, 1><<<g, kThreads, smem, ctx->stream>>>(a.rows, a.rp, a.ci, a.val, shape.chunk, xs, epi);
     }
     launched(ctx, name);
+}
+
+// y = A x epilogue used to time candidate shapes.
+template <class T>
+struct TuneStore {
+    static constexpr int kReduce = 0;
+    struct Pre {};
+    T *__restrict__ y;
+    double *partial{nullptr};
+    __device__ __forceinline__ bool skip() const { return false; }
+    template <class XS>
+    __device__ __forceinline__ Pre pre(int64_t, const XS &) const {
+        return {};
+    }
+    __device__ __forceinline__ void operator()(int64_t i, T acc, const Pre &, double (&)[1]) const { y[i] = acc; }
+};
+
+// Times the feasible ring depths, CTAs per SM and chunk capacities on this
+// operator (two warm-up and five timed launches each, CUDA events on the
+// context stream) and caches the fastest for every later launch over an
+// operator of the same shape.  y is overwritten.
+template <class T, class I>
+PipeConfig autotune(tf_ctx *ctx, const Csr<T, I> &a, const T *x, T *y, float *best_ms) {
+    PipeConfig best{};
+    float best_t = 0;
+    if (a.rows == 0 || !aligned16(a.rp) || (a.nnz && (!aligned16(a.ci) || !aligned16(a.val)))) return best;
+    cudaEvent_t e0, e1;
+    cuda_check(cudaEventCreate(&e0), "event");
+    cuda_check(cudaEventCreate(&e1), "event");
+    bool first = true;
+    for (int stages : {2, 3, 4}) {
+        for (int ctas : {2, 3, 4, 5, 6}) {
+            for (int pct : {100, 125}) {
+                const PipeConfig cfg{stages, ctas, pct};
+                const PipeShape p = pipe_shape<T, I>(a.rows, a.nnz, ctx->sm_count, cfg);
+                if (p.smem * ctas > 220 * 1024) continue;
+                allow_smem<csr_pipe_kernel<T, I, PlainX<T>, TuneStore<T>>>(p.smem);
+                int resident = 0;
+                cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                               &resident, csr_pipe_kernel<T, I, PlainX<T>, TuneStore<T>>, kThreads + 32, p.smem),
+                           "occupancy");
+                if (resident < ctas) continue;
+                for (int w = 0; w < 2; ++w) launch(ctx, a, PlainX<T>{x}, TuneStore<T>{y, nullptr}, "autotune", &cfg);
+                cuda_check(cudaEventRecord(e0, ctx->stream), "event");
+                for (int r = 0; r < 5; ++r) launch(ctx, a, PlainX<T>{x}, TuneStore<T>{y, nullptr}, "autotune", &cfg);
+                cuda_check(cudaEventRecord(e1, ctx->stream), "event");
+                cuda_check(cudaEventSynchronize(e1), "event");
+                float ms = 0;
+                cuda_check(cudaEventElapsedTime(&ms, e0, e1), "event");
+                if (first || ms < best_t) {
+                    best_t = ms;
+                    best = cfg;
+                    first = false;
+                }
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    check_faults(ctx);
+    store_config<T, I>(a.rows, a.nnz, ctx->sm_count, best);
+    if (best_ms) *best_ms = best_t / 5.0f;
+    return best;
 }
 
 }  // namespace tile
