@@ -295,13 +295,20 @@ class HierarchyImpl final : public Hierarchy {
         cycle(ctx, kind, d + 1, true);
         if (kind == TF_CYCLE_W) cycle(ctx, kind, d + 1, false);
         const int post = cfg_.o.post_sweeps;
-        if (post > 0) {
+        if (post > 0 && l.n <= kFusedProlongRows) {
+            // small level: one launch, x + P e read on the fly
             sweep(ctx, l, l.map.data(), c.x());
             smooth(ctx, l, post - 1, false);
         } else {
+            // large level: a streaming x += P e pass keeps the sweep's x
+            // gathers single-hop (x~_j = x_j + e[map_j] costs two dependent
+            // loads per nonzero)
             prolong_add(ctx, l.n, l.map.data(), c.x(), l.x());
+            smooth(ctx, l, post, false);
         }
     }
+
+    static constexpr int64_t kFusedProlongRows = 131072;
 
     AmgConfig cfg_;
     S w_;

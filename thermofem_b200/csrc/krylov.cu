@@ -101,6 +101,12 @@ __global__ void k_copy_if(const int *flag, int64_t n, const T *__restrict__ src,
 
 __global__ void k_clear_flag(int *flag) { *flag = 0; }
 
+// Re-arms the WHILE node of the solve graph: one more iteration while the
+// recurrence is running and below the iteration limit.
+__global__ void k_set_continue(cudaGraphConditionalHandle handle, const KState *s) {
+    cudaGraphSetConditional(handle, (s->running && s->it < s->max_it) ? 1u : 0u);
+}
+
 template <class T>
 __global__ void k_dot(int64_t n, const T *__restrict__ x, const T *__restrict__ y, double *part) {
     double v[1] = {0.0};
@@ -454,6 +460,7 @@ class KrylovImpl final : public Krylov {
     }
     ~KrylovImpl() override {
         if (exec_) cudaGraphExecDestroy(exec_);
+        if (solve_exec_) cudaGraphExecDestroy(solve_exec_);
         if (ev0_) cudaEventDestroy(ev0_);
         if (ev1_) cudaEventDestroy(ev1_);
     }
@@ -464,6 +471,11 @@ class KrylovImpl final : public Krylov {
             cudaGraphExecDestroy(exec_);
             exec_ = nullptr;
         }
+        if (solve_exec_) {
+            cudaGraphExecDestroy(solve_exec_);
+            solve_exec_ = nullptr;
+        }
+        capture_failed_ = solve_graph_failed_ = false;
         check_csr(&a);
         require(a.rows > 0 && a.rows == a.cols, "Solver requires a nonempty square matrix");
         require(sizeof(T) == type_size(a.value_type) && sizeof(I) == type_size(a.index_type),
@@ -521,34 +533,26 @@ class KrylovImpl final : public Krylov {
         init.status = TF_MAX_ITERATIONS;
         cuda_check(cudaMemcpyAsync(state_.data(), &init, sizeof(KState), cudaMemcpyHostToDevice, ctx->stream),
                    "state upload");
-        // ||b||^2 and r = b - A x with ||r||^2.
-        k_dot<T><<<parts_, 256, 0, ctx->stream>>>(n_, rhs_.data(), rhs_.data(), partb_.data());
-        launched(ctx, "dot");
-        tile::launch(ctx, csr(), tile::PlainX<T>{x_.data()},
-                     ResidualNorm<T>{rhs_.data(), r_.data(), nullptr, part_.data()}, "residual_norm");
-        k_init<<<1, 256, 0, ctx->stream>>>(state_.data(), partb_.data(), parts_, part_.data(), tiles_,
-                                          kind_ == TF_SOLVER_BICGSTAB ? 1 : 0);
-        launched(ctx, "k_init");
-        if (kind_ == TF_SOLVER_BICGSTAB) {
-            k_copy_if<T><<<parts_, 256, 0, ctx->stream>>>(&state_.data()->copy_shadow, n_, r_.data(), shadow_.data());
-            launched(ctx, "copy_if");
-        }
-        int *running = static_cast<int *>(ctx->pinned);
-        cuda_check(cudaMemcpyAsync(running, &state_.data()->running, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream),
-                   "state readback");
-        cuda_check(cudaStreamSynchronize(ctx->stream), "solve init");
-        for (int k = 0; k < opt_.max_iterations && *running; ++k) {
-            run_iteration(ctx);
+        if (!solve_exec_ && !solve_graph_failed_) build_solve_graph(ctx);
+        if (solve_exec_) {
+            // the whole solve, loop included, is one graph launch
+            cuda_check(cudaGraphLaunch(solve_exec_, ctx->stream), "solve graph");
+        } else {
+            enqueue_prefix(ctx);
+            int *running = static_cast<int *>(ctx->pinned);
             cuda_check(cudaMemcpyAsync(running, &state_.data()->running, sizeof(int), cudaMemcpyDeviceToHost,
                                        ctx->stream),
                        "state readback");
-            cuda_check(cudaStreamSynchronize(ctx->stream), "iteration");
+            cuda_check(cudaStreamSynchronize(ctx->stream), "solve init");
+            for (int k = 0; k < opt_.max_iterations && *running; ++k) {
+                run_iteration(ctx);
+                cuda_check(cudaMemcpyAsync(running, &state_.data()->running, sizeof(int), cudaMemcpyDeviceToHost,
+                                           ctx->stream),
+                           "state readback");
+                cuda_check(cudaStreamSynchronize(ctx->stream), "iteration");
+            }
+            enqueue_suffix(ctx);
         }
-        // Final true residual and report.
-        tile::launch(ctx, csr(), tile::PlainX<T>{x_.data()},
-                     ResidualNorm<T>{rhs_.data(), r_.data(), nullptr, part_.data()}, "residual_norm");
-        k_finish<<<1, 256, 0, ctx->stream>>>(state_.data(), part_.data(), tiles_);
-        launched(ctx, "k_finish");
         copy_async(ctx, x, x_.data(), n_ * sizeof(T));
         KState fin;
         cuda_check(cudaMemcpyAsync(ctx->pinned, state_.data(), sizeof(KState) <= 256 ? sizeof(KState) : 256,
@@ -557,6 +561,7 @@ class KrylovImpl final : public Krylov {
         cuda_check(cudaEventRecord(ev1_, ctx->stream), "event");
         cuda_check(cudaStreamSynchronize(ctx->stream), "solve");
         std::memcpy(&fin, ctx->pinned, sizeof(KState));
+        if (solve_exec_) ctx->launches += prefix_launches_ + suffix_launches_ + per_iteration_ * fin.it;
         check_faults(ctx);
         float ms = 0;
         cudaEventElapsedTime(&ms, ev0_, ev1_);
@@ -586,6 +591,99 @@ class KrylovImpl final : public Krylov {
     void precondition(tf_ctx *ctx, const T *in, T *out) {
         if (hier_) hier_->apply(ctx, in, out);
         else copy_async(ctx, out, in, n_ * sizeof(T));
+    }
+
+    // ||b||^2, r = b - A x with ||r||^2, initial decisions.
+    void enqueue_prefix(tf_ctx *ctx) {
+        k_dot<T><<<parts_, 256, 0, ctx->stream>>>(n_, rhs_.data(), rhs_.data(), partb_.data());
+        launched(ctx, "dot");
+        tile::launch(ctx, csr(), tile::PlainX<T>{x_.data()},
+                     ResidualNorm<T>{rhs_.data(), r_.data(), nullptr, part_.data()}, "residual_norm");
+        k_init<<<1, 1024, 0, ctx->stream>>>(state_.data(), partb_.data(), parts_, part_.data(), tiles_,
+                                           kind_ == TF_SOLVER_BICGSTAB ? 1 : 0);
+        launched(ctx, "k_init");
+        if (kind_ == TF_SOLVER_BICGSTAB) {
+            k_copy_if<T><<<parts_, 256, 0, ctx->stream>>>(&state_.data()->copy_shadow, n_, r_.data(), shadow_.data());
+            launched(ctx, "copy_if");
+        }
+    }
+
+    // Final true residual and report.
+    void enqueue_suffix(tf_ctx *ctx) {
+        tile::launch(ctx, csr(), tile::PlainX<T>{x_.data()},
+                     ResidualNorm<T>{rhs_.data(), r_.data(), nullptr, part_.data()}, "residual_norm");
+        k_finish<<<1, 1024, 0, ctx->stream>>>(state_.data(), part_.data(), tiles_);
+        launched(ctx, "k_finish");
+    }
+
+    // One graph for the whole solve: prefix, then a conditional WHILE node
+    // whose body is one iteration (it re-arms the condition from the device
+    // state at its end), then the suffix.  Falls back to the host loop when
+    // the driver refuses any step.
+    void build_solve_graph(tf_ctx *ctx) {
+        cudaGraph_t g = nullptr;
+        bool capturing = false;
+        const int64_t before = ctx->launches;
+        try {
+            cuda_check(cudaGraphCreate(&g, 0), "graph create");
+            cudaGraphConditionalHandle handle;
+            cuda_check(cudaGraphConditionalHandleCreate(&handle, g, 0, cudaGraphCondAssignDefault), "condition");
+            cuda_check(cudaStreamBeginCaptureToGraph(ctx->stream, g, nullptr, nullptr, 0,
+                                                     cudaStreamCaptureModeThreadLocal),
+                       "capture prefix");
+            capturing = true;
+            enqueue_prefix(ctx);
+            k_set_continue<<<1, 1, 0, ctx->stream>>>(handle, state_.data());
+            launched(ctx, "set_continue");
+            cudaStreamCaptureStatus st;
+            const cudaGraphNode_t *deps = nullptr;
+            size_t ndeps = 0;
+            cuda_check(cudaStreamGetCaptureInfo(ctx->stream, &st, nullptr, nullptr, &deps, &ndeps), "capture info");
+            std::vector<cudaGraphNode_t> last(deps, deps + ndeps);
+            cudaGraph_t out = nullptr;
+            capturing = false;
+            cuda_check(cudaStreamEndCapture(ctx->stream, &out), "capture prefix end");
+            prefix_launches_ = ctx->launches - before;
+            cudaGraphNodeParams cp = {};
+            cp.type = cudaGraphNodeTypeConditional;
+            cp.conditional.handle = handle;
+            cp.conditional.type = cudaGraphCondTypeWhile;
+            cp.conditional.size = 1;
+            cudaGraphNode_t loop;
+            cuda_check(cudaGraphAddNode(&loop, g, last.data(), last.size(), &cp), "while node");
+            cudaGraph_t body = cp.conditional.phGraph_out[0];
+            const int64_t b0 = ctx->launches;
+            cuda_check(cudaStreamBeginCaptureToGraph(ctx->stream, body, nullptr, nullptr, 0,
+                                                     cudaStreamCaptureModeThreadLocal),
+                       "capture body");
+            capturing = true;
+            enqueue_iteration(ctx);
+            k_set_continue<<<1, 1, 0, ctx->stream>>>(handle, state_.data());
+            launched(ctx, "set_continue");
+            capturing = false;
+            cuda_check(cudaStreamEndCapture(ctx->stream, &out), "capture body end");
+            per_iteration_ = ctx->launches - b0;
+            const int64_t s0 = ctx->launches;
+            cuda_check(cudaStreamBeginCaptureToGraph(ctx->stream, g, &loop, nullptr, 1,
+                                                     cudaStreamCaptureModeThreadLocal),
+                       "capture suffix");
+            capturing = true;
+            enqueue_suffix(ctx);
+            capturing = false;
+            cuda_check(cudaStreamEndCapture(ctx->stream, &out), "capture suffix end");
+            suffix_launches_ = ctx->launches - s0;
+            cuda_check(cudaGraphInstantiate(&solve_exec_, g, 0), "solve graph instantiate");
+        } catch (const Failure &) {
+            if (capturing) {
+                cudaGraph_t junk = nullptr;
+                cudaStreamEndCapture(ctx->stream, &junk);
+            }
+            cudaGetLastError();
+            solve_exec_ = nullptr;
+            solve_graph_failed_ = true;
+        }
+        if (g) cudaGraphDestroy(g);
+        ctx->launches = before;
     }
 
     void run_iteration(tf_ctx *ctx) {
@@ -630,56 +728,56 @@ class KrylovImpl final : public Krylov {
             precondition(ctx, r_.data(), z_.data());
             k_dot<T><<<pg, 256, 0, ctx->stream>>>(n_, r_.data(), z_.data(), part);
             launched(ctx, "dot");
-            cg_rho<<<1, 256, 0, ctx->stream>>>(s, part, parts_);
+            cg_rho<<<1, 1024, 0, ctx->stream>>>(s, part,parts_);
             launched(ctx, "cg_rho");
             cg_p<T><<<pg, 256, 0, ctx->stream>>>(s, n_, z_.data(), p_.data());
             launched(ctx, "cg_p");
             tile::launch(ctx, csr(), tile::PlainX<T>{p_.data()}, SpmvDot<T>{q_.data(), p_.data(), &s->running, part},
                          "spmv_dot");
-            cg_curv<<<1, 256, 0, ctx->stream>>>(s, part, tiles_);
+            cg_curv<<<1, 1024, 0, ctx->stream>>>(s, part,tiles_);
             launched(ctx, "cg_curv");
             cg_xr<T><<<pg, 256, 0, ctx->stream>>>(s, n_, p_.data(), q_.data(), x_.data(), r_.data(), part);
             launched(ctx, "cg_xr");
-            cg_res<<<1, 256, 0, ctx->stream>>>(s, part, parts_);
+            cg_res<<<1, 1024, 0, ctx->stream>>>(s, part,parts_);
             launched(ctx, "cg_res");
             tile::launch(ctx, csr(), tile::PlainX<T>{x_.data()},
                          ResidualNorm<T>{rhs_.data(), r_.data(), &s->refresh, part}, "residual_norm");
-            cg_end<<<1, 256, 0, ctx->stream>>>(s, part, tiles_);
+            cg_end<<<1, 1024, 0, ctx->stream>>>(s, part,tiles_);
             launched(ctx, "cg_end");
             return;
         }
         // BiCGStab: v = q_, phat = z_
         k_dot<T><<<pg, 256, 0, ctx->stream>>>(n_, shadow_.data(), r_.data(), part);
         launched(ctx, "dot");
-        bi_rho<<<1, 256, 0, ctx->stream>>>(s, part, parts_);
+        bi_rho<<<1, 1024, 0, ctx->stream>>>(s, part,parts_);
         launched(ctx, "bi_rho");
         bi_p<T><<<pg, 256, 0, ctx->stream>>>(s, n_, r_.data(), q_.data(), p_.data());
         launched(ctx, "bi_p");
         precondition(ctx, p_.data(), z_.data());
         tile::launch(ctx, csr(), tile::PlainX<T>{z_.data()}, SpmvDot<T>{q_.data(), shadow_.data(), &s->running, part},
                      "spmv_dot");
-        bi_alpha<<<1, 256, 0, ctx->stream>>>(s, part, tiles_);
+        bi_alpha<<<1, 1024, 0, ctx->stream>>>(s, part,tiles_);
         launched(ctx, "bi_alpha");
         bi_s<T><<<pg, 256, 0, ctx->stream>>>(s, n_, r_.data(), q_.data(), z_.data(), s_.data(), x_.data(), part);
         launched(ctx, "bi_s");
-        bi_snorm<<<1, 256, 0, ctx->stream>>>(s, part, parts_);
+        bi_snorm<<<1, 1024, 0, ctx->stream>>>(s, part,parts_);
         launched(ctx, "bi_snorm");
         tile::launch(ctx, csr(), tile::PlainX<T>{x_.data()}, ResidualNorm<T>{rhs_.data(), r_.data(), &s->early, part},
                      "residual_norm");
-        bi_early<<<1, 256, 0, ctx->stream>>>(s, part, tiles_);
+        bi_early<<<1, 1024, 0, ctx->stream>>>(s, part,tiles_);
         launched(ctx, "bi_early");
         precondition(ctx, s_.data(), sh_.data());
         tile::launch(ctx, csr(), tile::PlainX<T>{sh_.data()}, SpmvDot2<T>{t_.data(), s_.data(), &s->normal, part},
                      "spmv_dot2");
-        bi_omega<<<1, 256, 0, ctx->stream>>>(s, part, tiles_);
+        bi_omega<<<1, 1024, 0, ctx->stream>>>(s, part,tiles_);
         launched(ctx, "bi_omega");
         bi_xr<T><<<pg, 256, 0, ctx->stream>>>(s, n_, sh_.data(), s_.data(), t_.data(), x_.data(), r_.data(), part);
         launched(ctx, "bi_xr");
-        bi_res<<<1, 256, 0, ctx->stream>>>(s, part, parts_);
+        bi_res<<<1, 1024, 0, ctx->stream>>>(s, part,parts_);
         launched(ctx, "bi_res");
         tile::launch(ctx, csr(), tile::PlainX<T>{x_.data()}, ResidualNorm<T>{rhs_.data(), r_.data(), &s->refresh, part},
                      "residual_norm");
-        bi_end<<<1, 256, 0, ctx->stream>>>(s, part, tiles_);
+        bi_end<<<1, 1024, 0, ctx->stream>>>(s, part,tiles_);
         launched(ctx, "bi_end");
         k_copy_if<T><<<pg, 256, 0, ctx->stream>>>(&s->copy_shadow, n_, r_.data(), shadow_.data());
         launched(ctx, "copy_if");
@@ -699,6 +797,9 @@ class KrylovImpl final : public Krylov {
     DeviceBuffer<KState> state_;
     int tiles_{1}, parts_{1};
     cudaGraphExec_t exec_{nullptr};
+    cudaGraphExec_t solve_exec_{nullptr};
+    bool solve_graph_failed_{false};
+    int64_t prefix_launches_{0}, suffix_launches_{0};
     bool capture_failed_{false};
     int64_t per_iteration_{0};
     cudaEvent_t ev0_{nullptr}, ev1_{nullptr};

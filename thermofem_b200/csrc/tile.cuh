@@ -551,19 +551,25 @@ void launch(tf_ctx *ctx, const Csr<T, I> &a, const XS &xs, const Epi &epi, const
     launched(ctx, name);
 }
 
-// y = A x epilogue used to time candidate shapes.
+// y = b - A x epilogue used to time candidate shapes (the residual and
+// Jacobi sweeps of the cycle read a row operand besides x, as this does).
 template <class T>
 struct TuneStore {
     static constexpr int kReduce = 0;
-    struct Pre {};
+    struct Pre {
+        T b;
+    };
+    const T *__restrict__ b;
     T *__restrict__ y;
     double *partial{nullptr};
     __device__ __forceinline__ bool skip() const { return false; }
     template <class XS>
-    __device__ __forceinline__ Pre pre(int64_t, const XS &) const {
-        return {};
+    __device__ __forceinline__ Pre pre(int64_t i, const XS &) const {
+        return {b[i]};
     }
-    __device__ __forceinline__ void operator()(int64_t i, T acc, const Pre &, double (&)[1]) const { y[i] = acc; }
+    __device__ __forceinline__ void operator()(int64_t i, T acc, const Pre &p, double (&)[1]) const {
+        y[i] = p.b - acc;
+    }
 };
 
 // Times the feasible ring depths, CTAs per SM and chunk capacities on this
@@ -591,9 +597,9 @@ PipeConfig autotune(tf_ctx *ctx, const Csr<T, I> &a, const T *x, T *y, float *be
                                &resident, csr_pipe_kernel<T, I, PlainX<T>, TuneStore<T>>, kThreads + 32, p.smem),
                            "occupancy");
                 if (resident < ctas) continue;
-                for (int w = 0; w < 2; ++w) launch(ctx, a, PlainX<T>{x}, TuneStore<T>{y, nullptr}, "autotune", &cfg);
+                for (int w = 0; w < 2; ++w) launch(ctx, a, PlainX<T>{x}, TuneStore<T>{x, y, nullptr}, "autotune", &cfg);
                 cuda_check(cudaEventRecord(e0, ctx->stream), "event");
-                for (int r = 0; r < 5; ++r) launch(ctx, a, PlainX<T>{x}, TuneStore<T>{y, nullptr}, "autotune", &cfg);
+                for (int r = 0; r < 5; ++r) launch(ctx, a, PlainX<T>{x}, TuneStore<T>{x, y, nullptr}, "autotune", &cfg);
                 cuda_check(cudaEventRecord(e1, ctx->stream), "event");
                 cuda_check(cudaEventSynchronize(e1), "event");
                 float ms = 0;
