@@ -167,6 +167,7 @@ def run_profile(args):
     s = tf.Cg(tf.solver_options(), "amg",
               tf.amg_options(hierarchy_type="f32" if args.profile == "mixed" else "f64", **AMG), ctx=ctx)
     s.setup(a)
+    s.set_graph_mode(0)  # per-iteration graphs: ncu cannot profile inside conditional graph nodes
     ctx.synchronize()
     l0 = ctx.launches
     for _ in range(args.warmup):

@@ -297,6 +297,12 @@ int tf_solver_setup(tf_solver *s, const tf_csr *a);
  * Device or host pointers: host_buffers != 0 means rhs/x are host memory
  * (pinned or pageable) and the copies run inside the call. */
 int tf_solver_apply(tf_solver *s, const void *rhs, void *x, int host_buffers, tf_solve_result *result);
+/* Execution mode of apply: 1 (default) runs the whole solve as one CUDA
+ * graph whose iteration loop is a conditional WHILE node (no host round trip
+ * per iteration); 0 launches one graph per iteration from a host loop that
+ * reads a 4-byte running flag.  Same kernels, same results; mode 0 exists for
+ * profilers that cannot look inside conditional graph nodes. */
+int tf_solver_set_graph_mode(tf_solver *s, int mode);
 /* The AMG preconditioner owned by the solver, or NULL for Identity. */
 tf_amg *tf_solver_amg(tf_solver *s);
 /* Device time of the last apply in milliseconds (CUDA events on the ctx stream). */

@@ -242,3 +242,22 @@ def test_host_buffer_apply(ctx):
     rep2 = s.apply(b.cuda(), xd)
     assert rep2["iterations"] == rep["iterations"]
     assert torch.equal(xd.cpu(), x)
+
+
+@pytest.mark.parametrize("kind", ["cg", "bicgstab"])
+def test_graph_modes_give_identical_solves(ctx, kind):
+    m = P.heat3d(20, seed=31)
+    n = len(m[0]) - 1
+    b = torch.tensor(P.rhs_uniform(n, 32), device="cuda")
+    solver = tf.Cg if kind == "cg" else tf.BiCgStab
+    s = solver(tf.solver_options(), "amg", tf.amg_options(hierarchy_type="f32", jacobi_weight=2 / 3), ctx=ctx)
+    s.setup(to_device(m))
+    xs, reps = [], []
+    for mode in (1, 0, 1):
+        s.set_graph_mode(mode)
+        x = torch.zeros(n, dtype=torch.float64, device="cuda")
+        reps.append(s.apply(b, x))
+        xs.append(x)
+    assert reps[0]["status"] == "Converged"
+    assert reps[0] == reps[1] == reps[2]
+    assert torch.equal(xs[0], xs[1]) and torch.equal(xs[0], xs[2])

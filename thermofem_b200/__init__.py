@@ -165,6 +165,7 @@ SIGNATURES = {
     "tf_solver_setup": ([_P, C.POINTER(Csr)], _I),
     "tf_solver_apply": ([_P, _P, _P, _I, C.POINTER(SolveResult)], _I),
     "tf_solver_amg": ([_P], _P),
+    "tf_solver_set_graph_mode": ([_P, _I], _I),
     "tf_solver_last_apply_ms": ([_P], _D),
     "tf_read_matrix_market": ([C.c_char_p, _S, C.POINTER(HostCsr)], _I),
     "tf_read_matrix_market_file": ([C.c_char_p, C.POINTER(HostCsr)], _I),

@@ -602,6 +602,11 @@ class _Solver(_AmgView):
     def last_apply_ms(self) -> float:
         return lib().tf_solver_last_apply_ms(self.h)
 
+    def set_graph_mode(self, mode: int):
+        """1: one graph per solve with a device-side loop (default); 0: one
+        graph per iteration and a host loop (for kernel profilers)."""
+        check(lib().tf_solver_set_graph_mode(self.h, int(mode)))
+
 
 class Cg(_Solver):
     """Preconditioned CG (Cg<T,I>); preconditioner 'amg' or 'identity'."""

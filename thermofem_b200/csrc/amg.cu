@@ -16,6 +16,7 @@
 // captured once into a CUDA graph and replayed on every apply.
 #include <algorithm>
 
+#include "coarse_cycle.cuh"
 #include "engine.cuh"
 
 namespace tfb {
@@ -165,6 +166,7 @@ class HierarchyImpl final : public Hierarchy {
         }
         coarse_solver = factored_ ? "pivoted GPU LU" : (singular ? "Jacobi (singular LU)" : "Jacobi (coarsening stopped)");
         visits.assign(levels_.size(), 0);
+        plan_small_levels(ctx);
         cuda_check(cudaStreamSynchronize(ctx->stream), "AMG setup");
     }
 
@@ -225,10 +227,14 @@ class HierarchyImpl final : public Hierarchy {
         cudaGraph_t graph = nullptr;
         try {
             enqueue(ctx);
-        } catch (...) {
+        } catch (const Failure &) {
+            // a step the driver cannot capture: run uncaptured from now on
             cudaStreamEndCapture(ctx->stream, &graph);
             if (graph) cudaGraphDestroy(graph);
-            throw;
+            cudaGetLastError();
+            ctx->launches = before;
+            capture_failed_ = true;
+            return;
         }
         per_cycle_ = ctx->launches - before;
         ctx->launches = before;
@@ -249,12 +255,124 @@ class HierarchyImpl final : public Hierarchy {
     void enqueue(tf_ctx *ctx) {
         for (auto &l : levels_) l.cur = 0;
         std::fill(visits.begin(), visits.end(), 0);
+        entry_ = 0;
+        rec_.clear();
         cycle(ctx, cfg_.o.cycle, 0, true);
     }
 
+    // ---- level operations: launched, or recorded as a cooperative step ----
+    void op_jacobi_zero(tf_ctx *ctx, Level<S> &l) {
+        if (recording_) {
+            CoarseStep<S> s;
+            s.op = kStepJacobiZero;
+            s.n = static_cast<int>(l.n);
+            s.w = w_;
+            s.dinv = l.dinv.data();
+            s.rhs = l.rhs.data();
+            s.xout = l.x();
+            rec_.push_back(s);
+        } else if (!dry_) {
+            jacobi_zero(ctx, l.n, l.dinv.data(), l.rhs.data(), l.x(), w_, nullptr);
+        }
+    }
+
+    void op_zero(tf_ctx *ctx, Level<S> &l) {
+        if (recording_) {
+            CoarseStep<S> s;
+            s.op = kStepZero;
+            s.n = static_cast<int>(l.n);
+            s.xout = l.x();
+            rec_.push_back(s);
+        } else if (!dry_) {
+            fill_zero(ctx, l.n, l.x());
+        }
+    }
+
     void sweep(tf_ctx *ctx, Level<S> &l, const int32_t *map = nullptr, const S *e = nullptr) {
-        jacobi_sweep(ctx, l.csr(), l.dinv.data(), l.rhs.data(), l.x(), l.other(), w_, nullptr, map, e);
+        if (recording_) {
+            CoarseStep<S> s;
+            s.op = kStepSweep;
+            s.n = static_cast<int>(l.n);
+            s.w = w_;
+            s.rp = l.rp.data();
+            s.ci = l.ci.data();
+            s.val = l.val.data();
+            s.dinv = l.dinv.data();
+            s.rhs = l.rhs.data();
+            s.xin = l.x();
+            s.xout = l.other();
+            s.map = map;
+            s.e = e;
+            rec_.push_back(s);
+        } else if (!dry_) {
+            jacobi_sweep(ctx, l.csr(), l.dinv.data(), l.rhs.data(), l.x(), l.other(), w_, nullptr, map, e);
+        }
         l.cur ^= 1;
+    }
+
+    void op_residual_restrict(tf_ctx *ctx, Level<S> &l, Level<S> &c) {
+        if (recording_) {
+            CoarseStep<S> s;
+            s.op = kStepResidualRestrict;
+            s.n = static_cast<int>(l.n);
+            s.nc = l.coarse;
+            s.rp = l.rp.data();
+            s.ci = l.ci.data();
+            s.val = l.val.data();
+            s.rhs = l.rhs.data();
+            s.xin = l.x();
+            s.off = l.off.data();
+            s.mem = l.mem.data();
+            s.coarse_rhs = c.rhs.data();
+            rec_.push_back(s);
+        } else if (!dry_) {
+            residual(ctx, l.csr(), l.rhs.data(), l.x(), l.r.data());
+            restrict_sum(ctx, l.coarse, l.off.data(), l.mem.data(), l.r.data(), c.rhs.data());
+        }
+    }
+
+    void op_restrict_rhs(tf_ctx *ctx, Level<S> &l, Level<S> &c) {
+        if (recording_) {
+            CoarseStep<S> s;
+            s.op = kStepRestrict;
+            s.nc = l.coarse;
+            s.rhs = l.rhs.data();
+            s.off = l.off.data();
+            s.mem = l.mem.data();
+            s.coarse_rhs = c.rhs.data();
+            rec_.push_back(s);
+        } else if (!dry_) {
+            restrict_sum(ctx, l.coarse, l.off.data(), l.mem.data(), l.rhs.data(), c.rhs.data());
+        }
+    }
+
+    void op_prolong(tf_ctx *ctx, Level<S> &l, Level<S> &c) {
+        if (recording_) {
+            CoarseStep<S> s;
+            s.op = kStepProlong;
+            s.n = static_cast<int>(l.n);
+            s.xin = l.x();
+            s.xout = l.x();
+            s.map = l.map.data();
+            s.e = c.x();
+            rec_.push_back(s);
+        } else if (!dry_) {
+            prolong_add(ctx, l.n, l.map.data(), c.x(), l.x());
+        }
+    }
+
+    void op_dense(tf_ctx *ctx, Level<S> &l) {
+        if (recording_) {
+            CoarseStep<S> s;
+            s.op = kStepDense;
+            s.n = static_cast<int>(l.n);
+            s.inv = inv_.data();
+            s.rhs = l.rhs.data();
+            s.xout = l.x();
+            rec_.push_back(s);
+        } else if (!dry_) {
+            coarse_dense_apply(ctx, static_cast<int>(l.n), inv_.data(), l.rhs.data(), l.x());
+        }
     }
 
     // `sweeps` Jacobi sweeps; cleared: x is the zero vector on entry.
@@ -262,53 +380,95 @@ class HierarchyImpl final : public Hierarchy {
         int done = 0;
         if (cleared) {
             if (sweeps > 0) {
-                jacobi_zero(ctx, l.n, l.dinv.data(), l.rhs.data(), l.x(), w_, nullptr);
+                op_jacobi_zero(ctx, l);
                 done = 1;
             } else {
-                fill_zero(ctx, l.n, l.x());
+                op_zero(ctx, l);
             }
         }
         for (; done < sweeps; ++done) sweep(ctx, l);
     }
 
+    // Entering the first small level starts a recorded sub-cycle that runs as
+    // one cooperative launch (its program was recorded by the setup dry run;
+    // the recursion here replays the same steps to keep ping-pong state and
+    // visit counts).
     void cycle(tf_ctx *ctx, int kind, size_t d, bool zero) {
+        if (recording_ || d != coop_from_) return cycle_body(ctx, kind, d, zero);
+        recording_ = true;
+        const size_t start = rec_.size();
+        cycle_body(ctx, kind, d, zero);
+        recording_ = false;
+        if (dry_) {
+            entries_.emplace_back(start, rec_.size() - start);
+            return;
+        }
+        const auto [off, count] = entries_.at(entry_++);
+        rec_.resize(start);
+        launch_coarse_program<S>(ctx, programs_.data() + off, static_cast<int>(count), barrier_.data(), coop_grid_);
+    }
+
+    void cycle_body(tf_ctx *ctx, int kind, size_t d, bool zero) {
         Level<S> &l = levels_[d];
         ++visits[d];
         const bool cleared = zero || kind == TF_CYCLE_F;
         if (d + 1 == levels_.size()) {
-            if (factored_) coarse_dense_apply(ctx, static_cast<int>(l.n), inv_.data(), l.rhs.data(), l.x());
+            if (factored_) op_dense(ctx, l);
             else smooth(ctx, l, cfg_.o.coarse_sweeps, cleared);
             return;
         }
         Level<S> &c = levels_[d + 1];
         if (kind == TF_CYCLE_F) {
-            restrict_sum(ctx, l.coarse, l.off.data(), l.mem.data(), l.rhs.data(), c.rhs.data());
+            op_restrict_rhs(ctx, l, c);
             cycle(ctx, TF_CYCLE_F, d + 1, true);
-            fill_zero(ctx, l.n, l.x());
-            prolong_add(ctx, l.n, l.map.data(), c.x(), l.x());
+            op_zero(ctx, l);
+            op_prolong(ctx, l, c);
             cycle(ctx, TF_CYCLE_V, d, false);
             return;
         }
         smooth(ctx, l, cfg_.o.pre_sweeps, cleared);
-        residual(ctx, l.csr(), l.rhs.data(), l.x(), l.r.data());
-        restrict_sum(ctx, l.coarse, l.off.data(), l.mem.data(), l.r.data(), c.rhs.data());
+        op_residual_restrict(ctx, l, c);
         cycle(ctx, kind, d + 1, true);
         if (kind == TF_CYCLE_W) cycle(ctx, kind, d + 1, false);
         const int post = cfg_.o.post_sweeps;
         if (post > 0 && l.n <= kFusedProlongRows) {
-            // small level: one launch, x + P e read on the fly
+            // small level: x + P e read on the fly by the first sweep
             sweep(ctx, l, l.map.data(), c.x());
             smooth(ctx, l, post - 1, false);
         } else {
             // large level: a streaming x += P e pass keeps the sweep's x
             // gathers single-hop (x~_j = x_j + e[map_j] costs two dependent
             // loads per nonzero)
-            prolong_add(ctx, l.n, l.map.data(), c.x(), l.x());
+            op_prolong(ctx, l, c);
             smooth(ctx, l, post, false);
         }
     }
 
+    // Records the cooperative programs of every small-level sub-cycle of one
+    // cycle (a dry run: nothing is launched) and uploads them.
+    void plan_small_levels(tf_ctx *ctx) {
+        coop_from_ = levels_.size();
+        for (size_t d = 1; d < levels_.size(); ++d)
+            if (levels_[d].n <= kCoopRows) {
+                coop_from_ = d;
+                break;
+            }
+        if (coop_from_ == levels_.size()) return;
+        coop_grid_ = coarse_grid_size<S>(ctx->sm_count);
+        entries_.clear();
+        dry_ = true;
+        enqueue(ctx);
+        dry_ = false;
+        programs_.allocate(rec_.size());
+        cuda_check(cudaMemcpy(programs_.data(), rec_.data(), rec_.size() * sizeof(CoarseStep<S>), cudaMemcpyHostToDevice),
+                   "coarse program upload");
+        barrier_.allocate(3);
+        cuda_check(cudaMemset(barrier_.data(), 0, 3 * sizeof(unsigned)), "coarse barrier");
+        rec_.clear();
+    }
+
     static constexpr int64_t kFusedProlongRows = 131072;
+    static constexpr int64_t kCoopRows = 200000;
 
     AmgConfig cfg_;
     S w_;
@@ -321,6 +481,15 @@ class HierarchyImpl final : public Hierarchy {
     int64_t per_cycle_{0};
     std::vector<int> final_cur_;
     std::vector<int64_t> captured_visits_;
+    // cooperative small-level sub-cycles
+    size_t coop_from_{~size_t(0)};
+    bool recording_{false}, dry_{false};
+    std::vector<CoarseStep<S>> rec_;
+    std::vector<std::pair<size_t, size_t>> entries_;
+    size_t entry_{0};
+    DeviceBuffer<CoarseStep<S>> programs_;
+    DeviceBuffer<unsigned> barrier_;
+    int coop_grid_{0};
 };
 
 }  // namespace

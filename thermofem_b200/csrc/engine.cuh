@@ -62,6 +62,10 @@ class Krylov {
     virtual tf_solve_result solve(tf_ctx *ctx, const void *rhs, void *x) = 0;
     virtual Hierarchy *amg() = 0;
     virtual int64_t rows() const = 0;
+    // 1: the whole solve is one graph with a device-side loop (default);
+    // 0: one graph per iteration and a host loop (same kernels; profilers
+    // that cannot see inside conditional graph nodes need this).
+    int graph_mode{1};
     double last_ms{0};
 };
 

@@ -533,8 +533,9 @@ class KrylovImpl final : public Krylov {
         init.status = TF_MAX_ITERATIONS;
         cuda_check(cudaMemcpyAsync(state_.data(), &init, sizeof(KState), cudaMemcpyHostToDevice, ctx->stream),
                    "state upload");
-        if (!solve_exec_ && !solve_graph_failed_) build_solve_graph(ctx);
-        if (solve_exec_) {
+        if (graph_mode == 1 && !solve_exec_ && !solve_graph_failed_) build_solve_graph(ctx);
+        const bool whole = graph_mode == 1 && solve_exec_;
+        if (whole) {
             // the whole solve, loop included, is one graph launch
             cuda_check(cudaGraphLaunch(solve_exec_, ctx->stream), "solve graph");
         } else {
@@ -561,7 +562,7 @@ class KrylovImpl final : public Krylov {
         cuda_check(cudaEventRecord(ev1_, ctx->stream), "event");
         cuda_check(cudaStreamSynchronize(ctx->stream), "solve");
         std::memcpy(&fin, ctx->pinned, sizeof(KState));
-        if (solve_exec_) ctx->launches += prefix_launches_ + suffix_launches_ + per_iteration_ * fin.it;
+        if (whole) ctx->launches += prefix_launches_ + suffix_launches_ + per_iteration_ * fin.it;
         check_faults(ctx);
         float ms = 0;
         cudaEventElapsedTime(&ms, ev0_, ev1_);
@@ -693,10 +694,15 @@ class KrylovImpl final : public Krylov {
                 cudaGraph_t g = nullptr;
                 try {
                     enqueue_iteration(ctx);
-                } catch (...) {
+                } catch (const Failure &) {
+                    // a step the driver cannot capture: run uncaptured from now on
                     cudaStreamEndCapture(ctx->stream, &g);
                     if (g) cudaGraphDestroy(g);
-                    throw;
+                    cudaGetLastError();
+                    ctx->launches = before;
+                    capture_failed_ = true;
+                    enqueue_iteration(ctx);
+                    return;
                 }
                 per_iteration_ = ctx->launches - before;
                 ctx->launches = before;
