@@ -454,7 +454,7 @@ class HierarchyImpl final : public Hierarchy {
                 break;
             }
         if (coop_from_ == levels_.size()) return;
-        coop_grid_ = coarse_grid_size<S>(ctx->sm_count);
+        coop_grid_ = coarse_grid_size<S>(ctx->sm_count, levels_[coop_from_].n);
         entries_.clear();
         dry_ = true;
         enqueue(ctx);
@@ -468,7 +468,7 @@ class HierarchyImpl final : public Hierarchy {
     }
 
     static constexpr int64_t kFusedProlongRows = 131072;
-    static constexpr int64_t kCoopRows = 200000;
+    static constexpr int64_t kCoopRows = 20000;
 
     AmgConfig cfg_;
     S w_;

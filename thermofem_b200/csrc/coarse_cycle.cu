@@ -26,14 +26,21 @@ __device__ __forceinline__ T ldcg(const T *p) {
     return __ldcg(p);
 }
 
-// Bounded sense barrier over all CTAs of the grid.  Returns false when the
-// wait expired or another CTA already gave up.
-__device__ bool grid_barrier(unsigned *count, unsigned *generation, int *abort_flag, int *fault) {
+__device__ __forceinline__ unsigned load_acquire(const unsigned *p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Bounded sense barrier over all CTAs of the grid: one atomic arrival per CTA,
+// waiters poll the generation word with acquire loads.  Returns false when
+// the wait expired or another CTA already gave up.
+__device__ bool grid_barrier(unsigned *count, unsigned *generation, unsigned *abort_flag, int *fault) {
     __shared__ int ok;
     __syncthreads();
     if (threadIdx.x == 0) {
         ok = 1;
-        const unsigned gen = atomicAdd(generation, 0u);
+        const unsigned gen = load_acquire(generation);
         __threadfence();
         if (atomicAdd(count, 1u) == gridDim.x - 1) {
             atomicExch(count, 0u);
@@ -41,9 +48,9 @@ __device__ bool grid_barrier(unsigned *count, unsigned *generation, int *abort_f
             atomicAdd(generation, 1u);
         } else {
             long long spins = 0;
-            while (atomicAdd(generation, 0u) == gen) {
-                if (atomicAdd(abort_flag, 0) || ++spins > (1ll << 22)) {
-                    atomicExch(abort_flag, 1);
+            while (load_acquire(generation) == gen) {
+                if ((++spins & 255) == 0 && (load_acquire(abort_flag) || spins > (1ll << 24))) {
+                    atomicExch(abort_flag, 1u);
                     atomicExch(fault, 1);
                     ok = 0;
                     break;
@@ -51,7 +58,7 @@ __device__ bool grid_barrier(unsigned *count, unsigned *generation, int *abort_f
             }
         }
         __threadfence();
-        if (atomicAdd(abort_flag, 0)) ok = 0;
+        if (load_acquire(abort_flag)) ok = 0;
     }
     __syncthreads();
     return ok != 0;
@@ -106,17 +113,36 @@ __global__ void __launch_bounds__(kCoarseThreads) coarse_program_kernel(const Co
                     st.xout[i] = xi + st.w * __ldg(st.dinv + i) * (ldcg(st.rhs + i) - ax);
                 }
                 break;
-            case kStepResidualRestrict:
-                for (int c = tid; c < st.nc; c += stride) {
-                    S sum = S(0);
-                    for (int j = __ldg(st.off + c); j < __ldg(st.off + c + 1); ++j) {
-                        const int m = __ldg(st.mem + j);
-                        const S r = ldcg(st.rhs + m) - row_dot(st, m, st.xin);
-                        sum += r;
+            case kStepResidualRestrict: {
+                // a quad of lanes per coarse row, one member (<= 4) per lane;
+                // lane 0 of the quad adds the member residuals in member order
+                const int quads = stride >> 2, quad = tid >> 2, k4 = tid & 3;
+                for (int base = 0; base < st.nc; base += quads) {
+                    const int c = base + quad;
+                    int count = 0;
+                    S r = S(0);
+                    if (c < st.nc) {
+                        const int j0 = __ldg(st.off + c);
+                        count = __ldg(st.off + c + 1) - j0;
+                        if (k4 < count) {
+                            const int m = __ldg(st.mem + j0 + k4);
+                            r = ldcg(st.rhs + m) - row_dot(st, m, st.xin);
+                        }
                     }
-                    st.coarse_rhs[c] = sum;
+                    const S r1 = __shfl_sync(0xffffffffu, r, 1, 4);
+                    const S r2 = __shfl_sync(0xffffffffu, r, 2, 4);
+                    const S r3 = __shfl_sync(0xffffffffu, r, 3, 4);
+                    if (c < st.nc && k4 == 0) {
+                        S sum = S(0);
+                        if (count > 0) sum += r;
+                        if (count > 1) sum += r1;
+                        if (count > 2) sum += r2;
+                        if (count > 3) sum += r3;
+                        st.coarse_rhs[c] = sum;
+                    }
                 }
                 break;
+            }
             case kStepRestrict:
                 for (int c = tid; c < st.nc; c += stride) {
                     S sum = S(0);
@@ -142,19 +168,24 @@ __global__ void __launch_bounds__(kCoarseThreads) coarse_program_kernel(const Co
             default:
                 break;
         }
-        if (k + 1 < steps && !grid_barrier(barrier, barrier + 1, reinterpret_cast<int *>(barrier + 2), fault)) return;
+        if (k + 1 < steps && !grid_barrier(barrier, barrier + 1, barrier + 2, fault)) return;
     }
 }
 
 }  // namespace
 
+// One thread per row of the largest level of the region (at least one CTA,
+// at most one per SM): fewer CTAs make every barrier cheaper.
 template <class S>
-int coarse_grid_size(int sm_count) {
+int coarse_grid_size(int sm_count, int64_t max_rows) {
     int per_sm = 0;
     cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, coarse_program_kernel<S>, kCoarseThreads, 0),
                "coarse occupancy");
     if (per_sm < 1) fail(TF_ERR_CUDA, "coarse-cycle kernel cannot be resident");
-    return sm_count * (per_sm < 2 ? per_sm : 2);
+    int64_t g = (max_rows + kCoarseThreads - 1) / kCoarseThreads;
+    if (g < 1) g = 1;
+    if (g > sm_count) g = sm_count;
+    return static_cast<int>(g);
 }
 
 template <class S>
@@ -175,8 +206,8 @@ void launch_coarse_program(tf_ctx *ctx, const CoarseStep<S> *program, int steps,
     launched(ctx, "coarse_program");
 }
 
-template int coarse_grid_size<float>(int);
-template int coarse_grid_size<double>(int);
+template int coarse_grid_size<float>(int, int64_t);
+template int coarse_grid_size<double>(int, int64_t);
 template void launch_coarse_program<float>(tf_ctx *, const CoarseStep<float> *, int, unsigned *, int);
 template void launch_coarse_program<double>(tf_ctx *, const CoarseStep<double> *, int, unsigned *, int);
 

@@ -36,7 +36,7 @@ struct CoarseStep {
 
 // CTAs of the cooperative launch (all resident at once).
 template <class S>
-int coarse_grid_size(int sm_count);
+int coarse_grid_size(int sm_count, int64_t max_rows);
 
 // barrier: 3 device words (arrival count, generation, abort), zeroed once.
 template <class S>
