@@ -73,7 +73,7 @@ class AmgOptions(C.Structure):
                 ("pre_sweeps", C.c_int), ("post_sweeps", C.c_int), ("coarse_sweeps", C.c_int),
                 ("jacobi_weight", C.c_double), ("strength_threshold", C.c_double),
                 ("absorb_singletons", C.c_int), ("compact_sort_keys", C.c_int), ("cycle", C.c_int),
-                ("hierarchy_type", C.c_int), ("coarse_lu_rows", C.c_int)]
+                ("hierarchy_type", C.c_int), ("coarse_lu_rows", C.c_int), ("small_level_rows", C.c_int)]
 
 
 class SolverOptions(C.Structure):

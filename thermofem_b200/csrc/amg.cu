@@ -29,7 +29,7 @@ AmgConfig::AmgConfig(const tf_amg_options &opt) : o(opt) {
         !std::isfinite(p.jacobi_weight) || p.jacobi_weight <= 0 || p.jacobi_weight >= 2 ||
         (p.cycle != TF_CYCLE_V && p.cycle != TF_CYCLE_W && p.cycle != TF_CYCLE_F) ||
         (p.hierarchy_type != -1 && p.hierarchy_type != TF_F32 && p.hierarchy_type != TF_F64) ||
-        p.coarse_lu_rows < 1 || p.coarse_lu_rows > 256)
+        p.coarse_lu_rows < 1 || p.coarse_lu_rows > 256 || p.small_level_rows < 0)
         fail(TF_ERR_INVALID, "Invalid AMG options");
 }
 
@@ -448,8 +448,8 @@ class HierarchyImpl final : public Hierarchy {
     // cycle (a dry run: nothing is launched) and uploads them.
     void plan_small_levels(tf_ctx *ctx) {
         coop_from_ = levels_.size();
-        for (size_t d = 1; d < levels_.size(); ++d)
-            if (levels_[d].n <= kCoopRows) {
+        for (size_t d = 1; d < levels_.size() && cfg_.o.small_level_rows > 0; ++d)
+            if (levels_[d].n <= cfg_.o.small_level_rows) {
                 coop_from_ = d;
                 break;
             }
@@ -468,7 +468,6 @@ class HierarchyImpl final : public Hierarchy {
     }
 
     static constexpr int64_t kFusedProlongRows = 131072;
-    static constexpr int64_t kCoopRows = 20000;
 
     AmgConfig cfg_;
     S w_;

@@ -11,6 +11,8 @@
 // reduces into per-tile partial sums (deterministic: fixed tile partition and
 // fixed reduction tree), and may gate the whole launch on a device flag.
 #pragma once
+#include <cstdio>
+#include <cstdlib>
 #include <map>
 #include <mutex>
 #include <tuple>
@@ -572,6 +574,15 @@ struct TuneStore {
     }
 };
 
+// THERMOFEM_B200_TUNE_LOG=1 prints every timed candidate to stderr.
+inline bool tune_log() {
+    static const bool on = [] {
+        const char *v = std::getenv("THERMOFEM_B200_TUNE_LOG");
+        return v && v[0] == '1';
+    }();
+    return on;
+}
+
 // Times the feasible ring depths, CTAs per SM and chunk capacities on this
 // operator (two warm-up and five timed launches each, CUDA events on the
 // context stream) and caches the fastest for every later launch over an
@@ -604,6 +615,10 @@ PipeConfig autotune(tf_ctx *ctx, const Csr<T, I> &a, const T *x, T *y, float *be
                 cuda_check(cudaEventSynchronize(e1), "event");
                 float ms = 0;
                 cuda_check(cudaEventElapsedTime(&ms, e0, e1), "event");
+                if (tune_log())
+                    std::fprintf(stderr, "tf_autotune_spmv rows=%lld nnz=%lld T=%d stages=%d ctas=%d cap=%d%% %.2f us\n",
+                                 static_cast<long long>(a.rows), static_cast<long long>(a.nnz),
+                                 static_cast<int>(sizeof(T)), stages, ctas, pct, ms * 1e3f / 5);
                 if (first || ms < best_t) {
                     best_t = ms;
                     best = cfg;
