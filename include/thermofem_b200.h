@@ -113,13 +113,21 @@ int tf_spmv_f32(tf_ctx *ctx, int64_t rows, int64_t cols, int64_t nnz, const int3
                 const int32_t *indices, const float *values, const float *x, float *y);
 /* SpMV autotuner (replaces the fixed library algorithm choice of
  * cusparseSpMV ALG_DEFAULT, IterationContext.cu:140-159): times the feasible
- * pipelined launch shapes (ring depth 2-4, 2-6 resident CTAs per SM, chunk
- * capacity 100% or 125% of the mean tile) on this operator and caches the
- * fastest for every later row-tile launch over an operator of the same shape
- * (rows, nnz, types).  y is overwritten.  Outputs may be NULL; *ms is the
- * best time per launch.  Results never depend on the shape chosen. */
+ * pipelined launch shapes (1 or 2 rows per thread, ring depth 2-4, 1-6
+ * resident CTAs per SM, chunk capacity 100% or 125% of the mean tile) on this
+ * operator and caches the fastest for every later row-tile launch over an
+ * operator of the same shape (rows, nnz, types).  y is overwritten.  Outputs
+ * may be NULL; *ms is the best time per launch.  Results never depend on the
+ * shape chosen. */
 int tf_autotune_spmv(tf_ctx *ctx, const tf_csr *a, const void *x, void *y, int *stages, int *ctas_per_sm,
-                     int *cap_pct, float *ms);
+                     int *cap_pct, int *rows_per_thread, float *ms);
+/* Sets the cached launch shape for operators of a's shape without timing
+ * (no reference counterpart: the library picks its own algorithm).
+ * stages 2-4, ctas_per_sm 1-8, cap_pct 50-400, rows_per_thread 1 or 2;
+ * TF_ERR_INVALID otherwise or when the stage ring does not fit in shared
+ * memory.  Applies to launches enqueued or captured afterwards. */
+int tf_spmv_set_config(tf_ctx *ctx, const tf_csr *a, int stages, int ctas_per_sm, int cap_pct,
+                       int rows_per_thread);
 /* r = b - A x in one pass (replaces SpMV + scal + axpy, IterationContext.cu:167-175). */
 int tf_residual(tf_ctx *ctx, const tf_csr *a, const void *b, const void *x, void *r);
 /* One fused weighted-Jacobi sweep x_out = x + w * Dinv (b - A x)

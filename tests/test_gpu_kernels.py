@@ -288,9 +288,63 @@ def test_autotune_changes_speed_not_results(ctx):
     a = to_device((off, idx, val))
     x = torch.tensor(np.random.default_rng(5).standard_normal(n), device="cuda")
     before = tf.spmv(a, x, ctx=ctx).clone()
-    stages, ctas, cap, ms = tf.autotune_spmv(a, x, ctx=ctx)
-    assert 2 <= stages <= 4 and 2 <= ctas <= 6 and cap in (100, 125) and ms > 0
+    stages, ctas, cap, rpt, ms = tf.autotune_spmv(a, x, ctx=ctx)
+    assert 2 <= stages <= 4 and 1 <= ctas <= 6 and cap in (100, 125) and rpt in (1, 2) and ms > 0
     after = tf.spmv(a, x, ctx=ctx)
     assert torch.equal(before, after)
     r1 = tf.residual(a, x, x.clone(), ctx=ctx)
     assert torch.isfinite(r1).all()
+
+
+# Launch shapes: (stages, ctas_per_sm, cap_pct, rows_per_thread).  cap 50%
+# splits most tiles into several chunks, so rows straddle chunk boundaries.
+SHAPES = [(2, 4, 125, 1), (4, 2, 100, 1), (2, 3, 100, 2), (3, 1, 125, 2), (2, 2, 50, 2), (3, 5, 50, 1)]
+
+
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
+def test_every_launch_shape_gives_identical_results(ctx, dtype):
+    off, idx, val = P.heat3d(40, seed=9)
+    n = len(off) - 1
+    a = to_device((off, idx, val), dtype=dtype)
+    rng = np.random.default_rng(6)
+    x = torch.tensor(rng.standard_normal(n), dtype=dtype, device="cuda")
+    b = torch.tensor(rng.standard_normal(n), dtype=dtype, device="cuda")
+    dinv = tf.inverse_diagonal(a, ctx=ctx)
+    outs = []
+    for shape in SHAPES:
+        tf.set_spmv_config(a, *shape, ctx=ctx)
+        outs.append((tf.spmv(a, x, ctx=ctx).clone(), tf.residual(a, b, x, ctx=ctx).clone(),
+                     tf.jacobi_sweep(a, dinv, b, x, 0.7, ctx=ctx).clone()))
+    for o in outs[1:]:
+        for u, v in zip(outs[0], o):
+            assert torch.equal(u, v)
+    ref = O.spmv(O.Csr(n, off, idx, val.astype(np.float64)), x.double().cpu().numpy())
+    tol = 1e-12 if dtype == torch.float64 else 1e-4
+    assert np.abs(outs[0][0].double().cpu().numpy() - ref).max() <= tol * np.abs(ref).max()
+
+
+def test_launch_shape_does_not_change_reductions(ctx):
+    # The Krylov solve reduces r.z and p.Ap inside the SpMV epilogue: its
+    # iterates must be bit-identical under every launch shape.
+    m = P.heat3d(24, seed=41)
+    n = len(m[0]) - 1
+    a = to_device(m)
+    b = torch.tensor(P.rhs_uniform(n, 42), device="cuda")
+    xs, reps = [], []
+    for shape in SHAPES[:4]:
+        s = tf.Cg(tf.solver_options(), "amg", tf.amg_options(jacobi_weight=2 / 3), ctx=ctx)
+        s.setup(a)
+        tf.set_spmv_config(a, *shape, ctx=ctx)  # after setup's own tuning
+        x = torch.zeros(n, dtype=torch.float64, device="cuda")
+        reps.append(s.apply(b, x))
+        xs.append(x)
+    assert reps[0]["status"] == "Converged"
+    assert all(r == reps[0] for r in reps)
+    assert all(torch.equal(xs[0], v) for v in xs[1:])
+
+
+def test_set_spmv_config_rejects_bad_shapes(ctx):
+    a = to_device(P.heat3d(8, seed=1))
+    for bad in [(1, 2, 100, 1), (5, 2, 100, 1), (2, 0, 100, 1), (2, 9, 100, 1), (2, 2, 40, 1), (2, 2, 100, 3)]:
+        with pytest.raises(tf.InvalidArgument):
+            tf.set_spmv_config(a, *bad, ctx=ctx)

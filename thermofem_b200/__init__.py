@@ -120,7 +120,8 @@ SIGNATURES = {
     "tf_spmv_f32": ([_P, _L, _L, _L, _P, _P, _P, _P, _P], _I),
     "tf_residual": ([_P, C.POINTER(Csr), _P, _P, _P], _I),
     "tf_autotune_spmv": ([_P, C.POINTER(Csr), _P, _P, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
-                          C.POINTER(C.c_float)], _I),
+                          C.POINTER(C.c_int), C.POINTER(C.c_float)], _I),
+    "tf_spmv_set_config": ([_P, C.POINTER(Csr), _I, _I, _I, _I], _I),
     "tf_jacobi_sweep": ([_P, C.POINTER(Csr), _P, _P, _P, _P, _D, _P, _P, _P], _I),
     "tf_jacobi_zero": ([_P, _L, _I, _P, _P, _P, _D, _P], _I),
     "tf_inverse_diagonal": ([_P, C.POINTER(Csr), _P], _I),

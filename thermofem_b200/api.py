@@ -13,7 +13,7 @@ from . import (AmgOptions, Csr, HostCsr, SolveResult, SolverOptions, F32, F64, I
                SOLVER_BICGSTAB, PRECOND_AMG, PRECOND_IDENTITY, check, lib)
 
 __all__ = ["Context", "DeviceCsr", "Transfer", "Amg", "Jacobi", "Cg", "BiCgStab", "amg_options", "solver_options",
-           "read_matrix_market", "read_matrix_market_file", "spmv", "autotune_spmv", "residual", "jacobi_sweep", "jacobi_zero",
+           "read_matrix_market", "read_matrix_market_file", "spmv", "autotune_spmv", "set_spmv_config", "residual", "jacobi_sweep", "jacobi_zero",
            "inverse_diagonal", "restrict_aggregates", "prolong_aggregates", "dot_multi", "axpby", "convert",
            "csr_validate", "check_canonical", "canonicalize", "row_stats", "strength", "match", "contract",
            "aggregate", "galerkin", "radix_sort_pairs", "reduce_by_key", "scan_exclusive", "coarse_lu_factor",
@@ -25,6 +25,14 @@ _IT = {torch.int32: I32, torch.int64: I64}
 
 def _p(t):
     return C.c_void_p(t.data_ptr()) if t is not None else None
+
+
+def _release(fn: str, handle):
+    """Destroys a handle; at interpreter shutdown the library may already be gone."""
+    try:
+        getattr(lib(), fn)(handle)
+    except Exception:  # module globals cleared during shutdown
+        pass
 
 
 class Context:
@@ -45,7 +53,7 @@ class Context:
 
     def close(self):
         if getattr(self, "h", None):
-            lib().tf_ctx_destroy(self.h)
+            _release("tf_ctx_destroy", self.h)
             self.h = None
 
     __del__ = close
@@ -171,15 +179,23 @@ def spmv(a: DeviceCsr, x, y=None, ctx=None):
 
 def autotune_spmv(a: DeviceCsr, x, y=None, ctx=None):
     """Times the pipelined SpMV shapes on this operator and caches the best;
-    returns (stages, ctas_per_sm, cap_pct, ms_per_launch)."""
+    returns (stages, ctas_per_sm, cap_pct, rows_per_thread, ms_per_launch)."""
     ctx = _ctx(ctx)
     y = torch.empty(a.rows, dtype=a.dtype, device=x.device) if y is None else y
     d = a.desc()
-    st, ct, cp, ms = C.c_int(), C.c_int(), C.c_int(), C.c_float()
+    st, ct, cp, rpt, ms = C.c_int(), C.c_int(), C.c_int(), C.c_int(), C.c_float()
     with ctx:
         check(lib().tf_autotune_spmv(ctx.h, C.byref(d), _p(x), _p(y), C.byref(st), C.byref(ct), C.byref(cp),
-                                     C.byref(ms)))
-    return st.value, ct.value, cp.value, ms.value
+                                     C.byref(rpt), C.byref(ms)))
+    return st.value, ct.value, cp.value, rpt.value, ms.value
+
+
+def set_spmv_config(a: DeviceCsr, stages: int, ctas_per_sm: int, cap_pct: int, rows_per_thread: int, ctx=None):
+    """Caches a launch shape for operators of a's shape (no timing)."""
+    ctx = _ctx(ctx)
+    d = a.desc()
+    check(lib().tf_spmv_set_config(ctx.h, C.byref(d), int(stages), int(ctas_per_sm), int(cap_pct),
+                                   int(rows_per_thread)))
 
 
 def residual(a: DeviceCsr, b, x, r=None, ctx=None):
@@ -343,7 +359,7 @@ class Transfer:
 
     def __del__(self):
         if self._handle is not None:
-            lib().tf_transfer_free(self._handle)
+            _release("tf_transfer_free", self._handle)
             self._handle = None
 
 
@@ -515,7 +531,7 @@ class Amg(_AmgView):
 
     def __del__(self):
         if getattr(self, "h", None):
-            lib().tf_amg_destroy(self.h)
+            _release("tf_amg_destroy", self.h)
             self.h = None
 
     def setup(self, a: DeviceCsr):
@@ -542,7 +558,7 @@ class Jacobi:
 
     def __del__(self):
         if getattr(self, "h", None):
-            lib().tf_jacobi_destroy(self.h)
+            _release("tf_jacobi_destroy", self.h)
             self.h = None
 
     def setup(self, a: DeviceCsr):
@@ -578,7 +594,7 @@ class _Solver(_AmgView):
 
     def __del__(self):
         if getattr(self, "h", None):
-            lib().tf_solver_destroy(self.h)
+            _release("tf_solver_destroy", self.h)
             self.h = None
 
     def setup(self, a: DeviceCsr):

@@ -119,7 +119,7 @@ class HierarchyImpl final : public Hierarchy {
             // Launch shape of this level's row-tile kernels (cached by shape).
             fill_zero(ctx, l.n, l.rhs.data());
             autotune_spmv(ctx, l.csr(), static_cast<const S *>(l.rhs.data()), l.r.data(), nullptr, nullptr, nullptr,
-                          nullptr);
+                          nullptr, nullptr);
             LevelStats st;
             st.rows = l.n;
             st.nnz = l.nnz;

@@ -247,7 +247,7 @@ int tf_spmv_f32(tf_ctx *ctx, int64_t rows, int64_t cols, int64_t nnz, const int3
 }
 
 int tf_autotune_spmv(tf_ctx *ctx, const tf_csr *a, const void *x, void *y, int *stages, int *ctas_per_sm,
-                     int *cap_pct, float *ms) {
+                     int *cap_pct, int *rows_per_thread, float *ms) {
     return guard([&] {
         check_ctx(ctx);
         require(x != y || a->rows == 0, "SpMV shape or alias mismatch");
@@ -256,7 +256,19 @@ int tf_autotune_spmv(tf_ctx *ctx, const tf_csr *a, const void *x, void *y, int *
             using T = decltype(t);
             using I = decltype(i);
             autotune_spmv(ctx, csr_of<T, I>(*a), static_cast<const T *>(x), static_cast<T *>(y), stages, ctas_per_sm,
-                          cap_pct, ms);
+                          cap_pct, rows_per_thread, ms);
+        });
+    });
+}
+
+int tf_spmv_set_config(tf_ctx *ctx, const tf_csr *a, int stages, int ctas_per_sm, int cap_pct, int rows_per_thread) {
+    return guard([&] {
+        check_ctx(ctx);
+        DeviceScope scope(ctx->device);
+        with_csr_types(a, [&](auto t, auto i) {
+            using T = decltype(t);
+            using I = decltype(i);
+            set_spmv_config(ctx, csr_of<T, I>(*a), stages, ctas_per_sm, cap_pct, rows_per_thread);
         });
     });
 }

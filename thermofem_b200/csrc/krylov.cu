@@ -507,7 +507,8 @@ class KrylovImpl final : public Krylov {
             b->allocate(static_cast<size_t>(n_));
         tiles_ = tile::partials(n_);
         fill_zero(ctx, n_, x_.data());
-        autotune_spmv(ctx, csr(), static_cast<const T *>(x_.data()), q_.data(), nullptr, nullptr, nullptr, nullptr);
+        autotune_spmv(ctx, csr(), static_cast<const T *>(x_.data()), q_.data(), nullptr, nullptr, nullptr, nullptr,
+                      nullptr);
         parts_ = parts_for(n_);
         part_.allocate(static_cast<size_t>(2 * std::max(tiles_, parts_)));
         partb_.allocate(static_cast<size_t>(std::max(tiles_, parts_)));

@@ -30,10 +30,14 @@ template <class T, class I>
 void spmv(tf_ctx *ctx, const Csr<T, I> &a, const T *x, T *y);
 // Picks and caches the fastest pipelined launch shape for operators of this
 // shape (y is overwritten).  Writes the chosen ring depth, CTAs per SM, chunk
-// capacity percentage and the best time per launch (ms) when non-null.
+// capacity percentage, rows per thread and the best time per launch (ms)
+// when non-null.
 template <class T, class I>
 void autotune_spmv(tf_ctx *ctx, const Csr<T, I> &a, const T *x, T *y, int *stages, int *ctas_per_sm, int *cap_pct,
-                   float *ms);
+                   int *rows_per_thread, float *ms);
+// Stores a launch shape for operators of a's shape (validated, not timed).
+template <class T, class I>
+void set_spmv_config(tf_ctx *ctx, const Csr<T, I> &a, int stages, int ctas_per_sm, int cap_pct, int rows_per_thread);
 // r = b - A x
 template <class T, class I>
 void residual(tf_ctx *ctx, const Csr<T, I> &a, const T *b, const T *x, T *r);

@@ -278,11 +278,17 @@ void spmv(tf_ctx *ctx, const Csr<T, I> &a, const T *x, T *y) {
 
 template <class T, class I>
 void autotune_spmv(tf_ctx *ctx, const Csr<T, I> &a, const T *x, T *y, int *stages, int *ctas_per_sm, int *cap_pct,
-                   float *ms) {
+                   int *rows_per_thread, float *ms) {
     const tile::PipeConfig c = tile::autotune(ctx, a, x, y, ms);
     if (stages) *stages = c.stages;
     if (ctas_per_sm) *ctas_per_sm = c.ctas_per_sm;
     if (cap_pct) *cap_pct = c.cap_pct;
+    if (rows_per_thread) *rows_per_thread = c.rpt;
+}
+
+template <class T, class I>
+void set_spmv_config(tf_ctx *ctx, const Csr<T, I> &a, int stages, int ctas_per_sm, int cap_pct, int rows_per_thread) {
+    tile::configure(ctx, a, tile::PipeConfig{stages, ctas_per_sm, cap_pct, rows_per_thread});
 }
 
 template <class T, class I>
@@ -413,7 +419,8 @@ bool row_stats(tf_ctx *ctx, const Csr<double, int32_t> &a, double *row_max) {
 
 #define TF_SPMV_INST(T, I)                                                                                     \
     template void spmv<T, I>(tf_ctx *, const Csr<T, I> &, const T *, T *);                                     \
-    template void autotune_spmv<T, I>(tf_ctx *, const Csr<T, I> &, const T *, T *, int *, int *, int *, float *); \
+    template void autotune_spmv<T, I>(tf_ctx *, const Csr<T, I> &, const T *, T *, int *, int *, int *, int *, float *); \
+    template void set_spmv_config<T, I>(tf_ctx *, const Csr<T, I> &, int, int, int, int); \
     template void residual<T, I>(tf_ctx *, const Csr<T, I> &, const T *, const T *, T *);                      \
     template void jacobi_sweep<T, I>(tf_ctx *, const Csr<T, I> &, const T *, const T *, const T *, T *, T,     \
                                      const float *, const int32_t *, const T *);                               \

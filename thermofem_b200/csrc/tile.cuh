@@ -239,8 +239,8 @@ template <class T, class I>
 struct StageLayout {
     static constexpr int kVT = 16 / sizeof(T), kVI = 16 / sizeof(I);
     int rp_bytes, val_bytes, col_bytes, bytes;
-    __host__ __device__ explicit StageLayout(int cap) {
-        rp_bytes = ((kThreads + 1 + kVI) * static_cast<int>(sizeof(I)) + 15) & ~15;
+    __host__ __device__ StageLayout(int cap, int tile_rows) {
+        rp_bytes = ((tile_rows + 1 + kVI) * static_cast<int>(sizeof(I)) + 15) & ~15;
         val_bytes = ((cap + 2 * kVT) * static_cast<int>(sizeof(T)) + 15) & ~15;
         col_bytes = ((cap + 2 * kVI) * static_cast<int>(sizeof(I)) + 15) & ~15;
         bytes = (rp_bytes + val_bytes + col_bytes + 127) & ~127;
@@ -268,24 +268,32 @@ struct Range {
     }
 };
 
-template <class T, class I, class XS, class Epi>
+// RPT rows per consumer thread: a tile is 256 * RPT rows, thread t owns rows
+// t, t + 256, ... of it, and issues the first gathers of all its rows before
+// accumulating any (more loads in flight per register).  Partial sums stay
+// per 256-row block in the same warp and lane order, so reductions do not
+// depend on RPT.
+template <class T, class I, int RPT, class XS, class Epi>
 __global__ void __launch_bounds__(kThreads + 32) csr_pipe_kernel(int64_t rows, int64_t nnz, const I *__restrict__ rp,
                                                                   const I *__restrict__ ci,
                                                                   const T *__restrict__ val, int cap, int stages,
                                                                   XS xs, Epi epi, int *fault) {
     constexpr int K = Epi::kReduce;
+    constexpr int KK = K > 0 ? K : 1;
     constexpr int kVT = 16 / sizeof(T), kVI = 16 / sizeof(I);
+    constexpr int kTileRows = kThreads * RPT;
+    constexpr int kWarps = kThreads / 32;
     if (epi.skip()) return;
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ uint64_t full_bar[kMaxStages], empty_bar[kMaxStages];
-    __shared__ double warp_sums[kMaxStages + 1][kThreads / 32][K > 0 ? K : 1];
+    __shared__ double warp_sums[kMaxStages + 1][RPT][kWarps][KK];
     __shared__ int warp_done[kMaxStages + 1];
-    const StageLayout<T, I> L(cap);
+    const StageLayout<T, I> L(cap, kTileRows);
     const int tid = threadIdx.x;
     if (tid == 0) {
         for (int s = 0; s < stages; ++s) {
             mbar_init(&full_bar[s], 1);
-            mbar_init(&empty_bar[s], kThreads / 32);
+            mbar_init(&empty_bar[s], kWarps);
         }
         for (int s = 0; s < kMaxStages + 1; ++s) warp_done[s] = 0;
         mbar_fence_init();
@@ -298,10 +306,8 @@ __global__ void __launch_bounds__(kThreads + 32) csr_pipe_kernel(int64_t rows, i
     auto stage_col = [&](int s) {
         return reinterpret_cast<I *>(smem + static_cast<size_t>(s) * L.bytes + L.rp_bytes + L.val_bytes);
     };
-    const int64_t ntiles = (rows + kThreads - 1) / kThreads;
-    double red[K > 0 ? K : 1];
-#pragma unroll
-    for (int k = 0; k < (K > 0 ? K : 1); ++k) red[k] = 0.0;
+    const int64_t ntiles = (rows + kTileRows - 1) / kTileRows;
+    const int64_t nblocks = (rows + kThreads - 1) / kThreads;  // 256-row blocks = partial sums
     bool ok = true;
     uint32_t armed[kMaxStages] = {0, 0, 0, 0};  // producer: completions requested per stage
 
@@ -309,8 +315,8 @@ __global__ void __launch_bounds__(kThreads + 32) csr_pipe_kernel(int64_t rows, i
         // ---- producer ----
         uint32_t it = 0;
         for (int64_t tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
-            const int64_t r0 = tile * kThreads;
-            const int nr = static_cast<int>(min(static_cast<int64_t>(kThreads), rows - r0));
+            const int64_t r0 = tile * kTileRows;
+            const int nr = static_cast<int>(min(static_cast<int64_t>(kTileRows), rows - r0));
             const int64_t s = rp[r0], e = rp[r0 + nr];
             const int64_t nch = e > s ? (e - s + cap - 1) / cap : 1;
             for (int64_t c = 0; c < nch && ok; ++c, ++it) {
@@ -339,19 +345,27 @@ __global__ void __launch_bounds__(kThreads + 32) csr_pipe_kernel(int64_t rows, i
         }
         if (!ok) atomicExch(fault, 1);
     } else if (tid < kThreads) {
-        // ---- consumers: one row per thread ----
-        const int lane = tid & 31;
+        // ---- consumers: RPT rows per thread ----
+        const int lane = tid & 31, warp = tid >> 5;
         uint32_t it = 0, local_tile = 0;
+        double red[RPT][KK];
         for (int64_t tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
-            const int64_t r0 = tile * kThreads;
-            const int nr = static_cast<int>(min(static_cast<int64_t>(kThreads), rows - r0));
-            const bool valid = tid < nr;
-            int64_t rs = 0, re = 0, s = 0, e = 0, nch = 1;
-            T acc = T(0);
-            // The row's own epilogue operands (b, D^-1, x_i, ...) are loaded
+            const int64_t r0 = tile * kTileRows;
+            const int nr = static_cast<int>(min(static_cast<int64_t>(kTileRows), rows - r0));
+            int64_t rs[RPT], re[RPT], s = 0, e = 0, nch = 1;
+            T acc[RPT];
+            // The rows' own epilogue operands (b, D^-1, x_i, ...) are loaded
             // now, so their latency overlaps the stage wait and the gathers.
-            typename Epi::Pre pre{};
-            if (valid) pre = epi.pre(r0 + tid, xs);
+            typename Epi::Pre pre[RPT];
+#pragma unroll
+            for (int k = 0; k < RPT; ++k) {
+                rs[k] = re[k] = 0;
+                acc[k] = T(0);
+                pre[k] = typename Epi::Pre{};
+                if (tid + k * kThreads < nr) pre[k] = epi.pre(r0 + tid + k * kThreads, xs);
+#pragma unroll
+                for (int q = 0; q < KK; ++q) red[k][q] = 0.0;
+            }
             for (int64_t c = 0; c < nch; ++c, ++it) {
                 const int st = static_cast<int>(it % stages);
                 // warp-uniform decision, so __syncwarp below never waits on a lane that left
@@ -365,63 +379,92 @@ __global__ void __launch_bounds__(kThreads + 32) csr_pipe_kernel(int64_t rows, i
                     s = srp[0];
                     e = srp[nr];
                     nch = e > s ? (e - s + cap - 1) / cap : 1;
-                    if (valid) {
-                        rs = srp[tid];
-                        re = srp[tid + 1];
-                    }
+#pragma unroll
+                    for (int k = 0; k < RPT; ++k)
+                        if (tid + k * kThreads < nr) {
+                            rs[k] = srp[tid + k * kThreads];
+                            re[k] = srp[tid + k * kThreads + 1];
+                        }
                 }
                 const int64_t cs = s + c * cap, ce = min(e, cs + cap);
-                const T *sv = stage_val(st);
-                const I *sc = stage_col(st);
-                const int64_t av = cs - (cs % kVT), ac = cs - (cs % kVI);
-                const int64_t lo = max(rs, cs), hi = min(re, ce);
+                const T *sv = stage_val(st) + (cs % kVT);  // sv[j - cs]
+                const I *sc = stage_col(st) + (cs % kVI);  // sc[j - cs]
                 constexpr int kGather = 8;
-                for (int64_t j0 = lo; j0 < hi; j0 += kGather) {
-                    T y[kGather];
+                int lo[RPT], hi[RPT];
+                T y[RPT][kGather];
+#pragma unroll
+                for (int k = 0; k < RPT; ++k) {
+                    lo[k] = static_cast<int>(max(rs[k], cs) - cs);
+                    hi[k] = static_cast<int>(max(min(re[k], ce) - cs, int64_t(0)));
 #pragma unroll
                     for (int u = 0; u < kGather; ++u) {
-                        const int64_t j = j0 + u;
-                        y[u] = j < hi ? xs(static_cast<int64_t>(sc[j - ac])) : T(0);
+                        const int o = lo[k] + u;
+                        y[k][u] = o < hi[k] ? xs(static_cast<int64_t>(sc[o])) : T(0);
                     }
+                }
+#pragma unroll
+                for (int k = 0; k < RPT; ++k) {
+                    T a = acc[k];
 #pragma unroll
                     for (int u = 0; u < kGather; ++u) {
-                        const int64_t j = j0 + u;
-                        acc += (j < hi ? sv[j - av] : T(0)) * y[u];
+                        const int o = lo[k] + u;
+                        a += (o < hi[k] ? sv[o] : T(0)) * y[k][u];
                     }
+                    for (int o0 = lo[k] + kGather; o0 < hi[k]; o0 += kGather) {
+                        T z[kGather];
+#pragma unroll
+                        for (int u = 0; u < kGather; ++u) {
+                            const int o = o0 + u;
+                            z[u] = o < hi[k] ? xs(static_cast<int64_t>(sc[o])) : T(0);
+                        }
+#pragma unroll
+                        for (int u = 0; u < kGather; ++u) {
+                            const int o = o0 + u;
+                            a += (o < hi[k] ? sv[o] : T(0)) * z[u];
+                        }
+                    }
+                    acc[k] = a;
                 }
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&empty_bar[st]);
             }
             if (!ok) break;
-            if (valid) epi(r0 + tid, acc, pre, red);
-            if constexpr (K > 0) {
-                // Per-tile partial sums, independent of the grid: each warp
-                // reduces its rows, the last warp of the tile to finish adds
-                // the eight warp sums in warp order.  Warps are at most
-                // `stages` tiles apart, so a ring of kMaxStages + 1 slots
-                // never overwrites a slot still being read.
 #pragma unroll
-                for (int k = 0; k < K; ++k)
-                    for (int o = 16; o > 0; o >>= 1) red[k] += __shfl_down_sync(0xffffffffu, red[k], o);
+            for (int k = 0; k < RPT; ++k)
+                if (tid + k * kThreads < nr) epi(r0 + tid + k * kThreads, acc[k], pre[k], red[k]);
+            if constexpr (K > 0) {
+                // Per-256-row-block partial sums, independent of the grid and
+                // of RPT: each warp reduces its rows of every block, the last
+                // warp of the tile to finish adds the eight warp sums in warp
+                // order.  Warps are at most `stages` tiles apart, so a ring of
+                // kMaxStages + 1 slots never overwrites a slot still being read.
                 const int slot = static_cast<int>(local_tile % (kMaxStages + 1));
-                const int warp = tid >> 5;
+#pragma unroll
+                for (int k = 0; k < RPT; ++k)
+#pragma unroll
+                    for (int q = 0; q < K; ++q)
+                        for (int o = 16; o > 0; o >>= 1) red[k][q] += __shfl_down_sync(0xffffffffu, red[k][q], o);
                 if (lane == 0) {
 #pragma unroll
-                    for (int k = 0; k < K; ++k) warp_sums[slot][warp][k] = red[k];
-                    __threadfence_block();
-                    if (atomicAdd(&warp_done[slot], 1) == kThreads / 32 - 1) {
-                        __threadfence_block();
+                    for (int k = 0; k < RPT; ++k)
 #pragma unroll
-                        for (int k = 0; k < K; ++k) {
-                            double v = 0.0;
-                            for (int w = 0; w < kThreads / 32; ++w) v += warp_sums[slot][w][k];
-                            epi.partial[k * ntiles + tile] = v;
+                        for (int q = 0; q < K; ++q) warp_sums[slot][k][warp][q] = red[k][q];
+                    __threadfence_block();
+                    if (atomicAdd(&warp_done[slot], 1) == kWarps - 1) {
+                        __threadfence_block();
+                        for (int k = 0; k < RPT; ++k) {
+                            const int64_t block = tile * RPT + k;
+                            if (block >= nblocks) break;
+#pragma unroll
+                            for (int q = 0; q < K; ++q) {
+                                double v = 0.0;
+                                for (int w = 0; w < kWarps; ++w) v += warp_sums[slot][k][w][q];
+                                epi.partial[q * nblocks + block] = v;
+                            }
                         }
                         warp_done[slot] = 0;
                     }
                 }
-#pragma unroll
-                for (int k = 0; k < K; ++k) red[k] = 0.0;
             }
             ++local_tile;
         }
@@ -436,42 +479,45 @@ __global__ void __launch_bounds__(kThreads + 32) csr_pipe_kernel(int64_t rows, i
     }
 }
 
-// Pipelined launch shape: entries per chunk, stages in the ring, resident
-// CTAs per SM (the persistent grid is ctas_per_sm x SMs, at most one CTA per
-// tile).
+// Pipelined launch shape: rows per thread, entries per chunk, stages in the
+// ring, resident CTAs per SM (the persistent grid is ctas_per_sm x SMs, at
+// most one CTA per tile).
 struct PipeShape {
-    int cap, stages, ctas_per_sm, grid;
+    int rpt, cap, stages, ctas_per_sm, grid;
     size_t smem;
 };
 
-// Tunable part of the shape: ring depth, resident CTAs per SM and the chunk
-// capacity as a percentage of the mean tile.  The result does not depend on
-// it (rows are reduced left to right in any chunking, partial sums are per
-// 256-row tile), only the speed does.
+// Tunable part of the shape: rows per thread, ring depth, resident CTAs per
+// SM and the chunk capacity as a percentage of the mean tile.  The result
+// does not depend on it (rows are reduced left to right in any chunking,
+// partial sums are per 256-row block), only the speed does.
 struct PipeConfig {
-    int stages{3}, ctas_per_sm{2}, cap_pct{125};
+    int stages{2}, ctas_per_sm{4}, cap_pct{125}, rpt{1};
 };
 
 template <class T, class I>
 PipeShape pipe_shape(int64_t rows, int64_t nnz, int sm_count, const PipeConfig &cfg) {
     PipeShape p;
-    const int rp_bytes = ((kThreads + 1 + 16 / static_cast<int>(sizeof(I))) * static_cast<int>(sizeof(I)) + 15) & ~15;
-    const int max_cap = ((32768 - rp_bytes) / static_cast<int>(sizeof(T) + sizeof(I)) - 8) & ~63;
-    const int64_t mean_tile = rows > 0 ? (nnz * kThreads + rows - 1) / rows : 0;
+    p.rpt = cfg.rpt == 2 ? 2 : 1;
+    const int tile_rows = kThreads * p.rpt;
+    const int rp_bytes = ((tile_rows + 1 + 16 / static_cast<int>(sizeof(I))) * static_cast<int>(sizeof(I)) + 15) & ~15;
+    const int stage_limit = 32768 * p.rpt;
+    const int max_cap = ((stage_limit - rp_bytes) / static_cast<int>(sizeof(T) + sizeof(I)) - 8) & ~63;
+    const int64_t mean_tile = rows > 0 ? (nnz * tile_rows + rows - 1) / rows : 0;
     int64_t cap = (mean_tile * cfg.cap_pct / 100 + 63) & ~int64_t(63);
     if (cap < 256) cap = 256;
     if (cap > max_cap) cap = max_cap;
     p.cap = static_cast<int>(cap);
     p.stages = cfg.stages;
     p.ctas_per_sm = cfg.ctas_per_sm;
-    p.smem = static_cast<size_t>(StageLayout<T, I>(p.cap).bytes) * p.stages;
-    const int64_t ntiles = (rows + kThreads - 1) / kThreads;
+    p.smem = static_cast<size_t>(StageLayout<T, I>(p.cap, tile_rows).bytes) * p.stages;
+    const int64_t ntiles = (rows + tile_rows - 1) / tile_rows;
     const int64_t g = static_cast<int64_t>(sm_count) * cfg.ctas_per_sm;
     p.grid = static_cast<int>(ntiles < g ? (ntiles < 1 ? 1 : ntiles) : g);
     return p;
 }
 
-// Number of partial sums a reducing launch writes: one per 256-row tile.
+// Number of partial sums a reducing launch writes: one per 256-row block.
 inline int partials(int64_t rows) { return static_cast<int>(rows > 0 ? (rows + kThreads - 1) / kThreads : 1); }
 
 // Process-wide cache of tuned configurations, keyed by the operator's shape.
@@ -502,6 +548,18 @@ void store_config(int64_t rows, int64_t nnz, int sm_count, const PipeConfig &cfg
     tune_cache()[TuneKey{rows, nnz, static_cast<int>(sizeof(T)), static_cast<int>(sizeof(I)), sm_count}] = cfg;
 }
 
+// Validates and caches a launch shape for operators of a's shape.
+template <class T, class I>
+void configure(tf_ctx *ctx, const Csr<T, I> &a, const PipeConfig &cfg) {
+    require(cfg.rpt == 1 || cfg.rpt == 2, "rows_per_thread must be 1 or 2");
+    require(cfg.stages >= 2 && cfg.stages <= kMaxStages, "stages must be 2..4");
+    require(cfg.ctas_per_sm >= 1 && cfg.ctas_per_sm <= 8, "ctas_per_sm must be 1..8");
+    require(cfg.cap_pct >= 50 && cfg.cap_pct <= 400, "cap_pct must be 50..400");
+    const PipeShape p = pipe_shape<T, I>(a.rows, a.nnz, ctx->sm_count, cfg);
+    require(p.smem <= 200 * 1024, "stage ring exceeds shared memory");
+    store_config<T, I>(a.rows, a.nnz, ctx->sm_count, cfg);
+}
+
 // Opts the instantiation into the dynamic shared memory it is launched with
 // (the staged chunk plus the epilogue's static reduction buffer can exceed
 // the 48 KB default); done once per instantiation and device.
@@ -522,8 +580,8 @@ inline bool aligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 
 
 // Launches the pipelined kernel when the three arrays start on 16-byte
 // boundaries (every buffer this library allocates does), the staged kernel
-// otherwise.  Reducing epilogues need the pipelined kernel: their partial
-// sums are per CTA of its persistent grid (tile::partials).
+// otherwise.  Reducing epilogues need the pipelined kernel: it writes their
+// partial sums per 256-row block (tile::partials).
 template <class T, class I, class XS, class Epi>
 void launch(tf_ctx *ctx, const Csr<T, I> &a, const XS &xs, const Epi &epi, const char *name,
             const PipeConfig *force = nullptr) {
@@ -532,9 +590,15 @@ void launch(tf_ctx *ctx, const Csr<T, I> &a, const XS &xs, const Epi &epi, const
     if (pipe) {
         const PipeConfig cfg = force ? *force : tuned_config<T, I>(a.rows, a.nnz, ctx->sm_count);
         const PipeShape p = pipe_shape<T, I>(a.rows, a.nnz, ctx->sm_count, cfg);
-        allow_smem<csr_pipe_kernel<T, I, XS, Epi>>(p.smem);
-        csr_pipe_kernel<T, I, XS, Epi><<<p.grid, kThreads + 32, p.smem, ctx->stream>>>(
-            a.rows, a.nnz, a.rp, a.ci, a.val, p.cap, p.stages, xs, epi, ctx->fault);
+        if (p.rpt == 2) {
+            allow_smem<csr_pipe_kernel<T, I, 2, XS, Epi>>(p.smem);
+            csr_pipe_kernel<T, I, 2, XS, Epi><<<p.grid, kThreads + 32, p.smem, ctx->stream>>>(
+                a.rows, a.nnz, a.rp, a.ci, a.val, p.cap, p.stages, xs, epi, ctx->fault);
+        } else {
+            allow_smem<csr_pipe_kernel<T, I, 1, XS, Epi>>(p.smem);
+            csr_pipe_kernel<T, I, 1, XS, Epi><<<p.grid, kThreads + 32, p.smem, ctx->stream>>>(
+                a.rows, a.nnz, a.rp, a.ci, a.val, p.cap, p.stages, xs, epi, ctx->fault);
+        }
         launched(ctx, name);
         return;
     }
@@ -583,7 +647,7 @@ inline bool tune_log() {
     return on;
 }
 
-// Times the feasible ring depths, CTAs per SM and chunk capacities on this
+// Times the feasible rows per thread, ring depths, CTAs per SM and chunk capacities on this
 // operator (two warm-up and five timed launches each, CUDA events on the
 // context stream) and caches the fastest for every later launch over an
 // operator of the same shape.  y is overwritten.
@@ -596,33 +660,48 @@ PipeConfig autotune(tf_ctx *ctx, const Csr<T, I> &a, const T *x, T *y, float *be
     cuda_check(cudaEventCreate(&e0), "event");
     cuda_check(cudaEventCreate(&e1), "event");
     bool first = true;
-    for (int stages : {2, 3, 4}) {
-        for (int ctas : {2, 3, 4, 5, 6}) {
-            for (int pct : {100, 125}) {
-                const PipeConfig cfg{stages, ctas, pct};
-                const PipeShape p = pipe_shape<T, I>(a.rows, a.nnz, ctx->sm_count, cfg);
-                if (p.smem * ctas > 220 * 1024) continue;
-                allow_smem<csr_pipe_kernel<T, I, PlainX<T>, TuneStore<T>>>(p.smem);
-                int resident = 0;
-                cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                               &resident, csr_pipe_kernel<T, I, PlainX<T>, TuneStore<T>>, kThreads + 32, p.smem),
-                           "occupancy");
-                if (resident < ctas) continue;
-                for (int w = 0; w < 2; ++w) launch(ctx, a, PlainX<T>{x}, TuneStore<T>{x, y, nullptr}, "autotune", &cfg);
-                cuda_check(cudaEventRecord(e0, ctx->stream), "event");
-                for (int r = 0; r < 5; ++r) launch(ctx, a, PlainX<T>{x}, TuneStore<T>{x, y, nullptr}, "autotune", &cfg);
-                cuda_check(cudaEventRecord(e1, ctx->stream), "event");
-                cuda_check(cudaEventSynchronize(e1), "event");
-                float ms = 0;
-                cuda_check(cudaEventElapsedTime(&ms, e0, e1), "event");
-                if (tune_log())
-                    std::fprintf(stderr, "tf_autotune_spmv rows=%lld nnz=%lld T=%d stages=%d ctas=%d cap=%d%% %.2f us\n",
-                                 static_cast<long long>(a.rows), static_cast<long long>(a.nnz),
-                                 static_cast<int>(sizeof(T)), stages, ctas, pct, ms * 1e3f / 5);
-                if (first || ms < best_t) {
-                    best_t = ms;
-                    best = cfg;
-                    first = false;
+    for (int rpt : {1, 2}) {
+        for (int stages : {2, 3, 4}) {
+            for (int ctas : {1, 2, 3, 4, 5, 6}) {
+                for (int pct : {100, 125}) {
+                    const PipeConfig cfg{stages, ctas, pct, rpt};
+                    const PipeShape p = pipe_shape<T, I>(a.rows, a.nnz, ctx->sm_count, cfg);
+                    if (p.smem * ctas > 220 * 1024) continue;
+                    if ((rpt == 1 && ctas < 2) || (rpt == 2 && ctas > 3)) continue;
+                    int resident = 0;
+                    if (rpt == 2) {
+                        allow_smem<csr_pipe_kernel<T, I, 2, PlainX<T>, TuneStore<T>>>(p.smem);
+                        cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                                       &resident, csr_pipe_kernel<T, I, 2, PlainX<T>, TuneStore<T>>, kThreads + 32,
+                                       p.smem),
+                                   "occupancy");
+                    } else {
+                        allow_smem<csr_pipe_kernel<T, I, 1, PlainX<T>, TuneStore<T>>>(p.smem);
+                        cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                                       &resident, csr_pipe_kernel<T, I, 1, PlainX<T>, TuneStore<T>>, kThreads + 32,
+                                       p.smem),
+                                   "occupancy");
+                    }
+                    if (resident < ctas) continue;
+                    for (int w = 0; w < 2; ++w)
+                        launch(ctx, a, PlainX<T>{x}, TuneStore<T>{x, y, nullptr}, "autotune", &cfg);
+                    cuda_check(cudaEventRecord(e0, ctx->stream), "event");
+                    for (int r = 0; r < 5; ++r)
+                        launch(ctx, a, PlainX<T>{x}, TuneStore<T>{x, y, nullptr}, "autotune", &cfg);
+                    cuda_check(cudaEventRecord(e1, ctx->stream), "event");
+                    cuda_check(cudaEventSynchronize(e1), "event");
+                    float ms = 0;
+                    cuda_check(cudaEventElapsedTime(&ms, e0, e1), "event");
+                    if (tune_log())
+                        std::fprintf(stderr,
+                                     "tf_autotune_spmv rows=%lld nnz=%lld T=%d rpt=%d stages=%d ctas=%d cap=%d%% %.2f us\n",
+                                     static_cast<long long>(a.rows), static_cast<long long>(a.nnz),
+                                     static_cast<int>(sizeof(T)), rpt, stages, ctas, pct, ms * 1e3f / 5);
+                    if (first || ms < best_t) {
+                        best_t = ms;
+                        best = cfg;
+                        first = false;
+                    }
                 }
             }
         }
