@@ -313,6 +313,11 @@ int tf_solver_apply(tf_solver *s, const void *rhs, void *x, int host_buffers, tf
  * reads a 4-byte running flag.  Same kernels, same results; mode 0 exists for
  * profilers that cannot look inside conditional graph nodes. */
 int tf_solver_set_graph_mode(tf_solver *s, int mode);
+/* How the last apply ran: 2 as one whole-solve graph, 1 as one graph per
+ * iteration, 0 as uncaptured launches (a step the driver refused to
+ * capture), -1 before the first apply or for a NULL solver.  No reference
+ * counterpart (the reference launches from the host). */
+int tf_solver_last_execution(const tf_solver *s);
 /* The AMG preconditioner owned by the solver, or NULL for Identity. */
 tf_amg *tf_solver_amg(tf_solver *s);
 /* Device time of the last apply in milliseconds (CUDA events on the ctx stream). */

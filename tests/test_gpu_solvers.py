@@ -252,12 +252,41 @@ def test_graph_modes_give_identical_solves(ctx, kind):
     solver = tf.Cg if kind == "cg" else tf.BiCgStab
     s = solver(tf.solver_options(), "amg", tf.amg_options(hierarchy_type="f32", jacobi_weight=2 / 3), ctx=ctx)
     s.setup(to_device(m))
-    xs, reps = [], []
+    assert s.last_execution == -1
+    xs, reps, runs = [], [], []
     for mode in (1, 0, 1):
         s.set_graph_mode(mode)
         x = torch.zeros(n, dtype=torch.float64, device="cuda")
         reps.append(s.apply(b, x))
         xs.append(x)
+        runs.append(s.last_execution)
+    assert runs == [2, 1, 2]  # no silent fallback to uncaptured launches
     assert reps[0]["status"] == "Converged"
     assert reps[0] == reps[1] == reps[2]
     assert torch.equal(xs[0], xs[1]) and torch.equal(xs[0], xs[2])
+
+
+@pytest.mark.parametrize("kind", ["cg", "bicgstab"])
+def test_dependent_launch_gives_identical_solves(ctx, kind, monkeypatch):
+    # Kernels overlap their predecessor's tail under programmatic dependent
+    # launch; THERMOFEM_B200_PDL=0 restores plain stream order.  Both must
+    # give the same bits.
+    m = P.heat3d(20, seed=51)
+    n = len(m[0]) - 1
+    b = torch.tensor(P.rhs_uniform(n, 52), device="cuda")
+    solver = tf.Cg if kind == "cg" else tf.BiCgStab
+    out = []
+    for pdl in ("1", "0"):
+        monkeypatch.setenv("THERMOFEM_B200_PDL", pdl)
+        c = tf.Context(0)
+        s = solver(tf.solver_options(), "amg", tf.amg_options(hierarchy_type="f32", jacobi_weight=2 / 3), ctx=c)
+        s.setup(to_device(m))
+        x = torch.zeros(n, dtype=torch.float64, device="cuda")
+        rep = s.apply(b, x)
+        assert s.last_execution == 2
+        out.append((rep, x.cpu()))
+        del s
+        c.close()
+    assert out[0][0]["status"] == "Converged"
+    assert out[0][0] == out[1][0]
+    assert torch.equal(out[0][1], out[1][1])

@@ -623,6 +623,12 @@ class _Solver(_AmgView):
         graph per iteration and a host loop (for kernel profilers)."""
         check(lib().tf_solver_set_graph_mode(self.h, int(mode)))
 
+    @property
+    def last_execution(self) -> int:
+        """2: the last apply ran as one graph; 1: a graph per iteration;
+        0: uncaptured launches; -1: no apply yet."""
+        return lib().tf_solver_last_execution(self.h)
+
 
 class Cg(_Solver):
     """Preconditioned CG (Cg<T,I>); preconditioner 'amg' or 'identity'."""

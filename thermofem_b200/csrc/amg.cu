@@ -193,6 +193,7 @@ class HierarchyImpl final : public Hierarchy {
   private:
     template <class T>
     void apply_t(tf_ctx *ctx, const T *rhs, T *x) {
+        StableScope stable(ctx);  // level operators are read-only from here on
         Level<S> &f = levels_.front();
         convert(ctx, f.n, rhs, f.rhs.data());
         run_cycle(ctx);

@@ -90,6 +90,9 @@ int tf_ctx_create(int device, void *stream, tf_ctx **out) {
         auto ctx = std::make_unique<tf_ctx>();
         ctx->device = device;
         cuda_check(cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device), "SM count");
+        // THERMOFEM_B200_PDL=0 launches every kernel with plain stream order.
+        const char *pdl = std::getenv("THERMOFEM_B200_PDL");
+        ctx->pdl = !(pdl && pdl[0] == '0');
         if (stream) {
             ctx->stream = static_cast<cudaStream_t>(stream);
         } else {

@@ -27,6 +27,7 @@ __global__ void __launch_bounds__(kLuThreads) lu_factor_kernel(int n, const int3
                                                                  const int32_t *__restrict__ ci,
                                                                  const double *__restrict__ a, double *lu,
                                                                  int32_t *pivots, int *bad, int use_smem) {
+    pdl_enter();
     extern __shared__ __align__(16) double dyn[];
     __shared__ double red_v[kLuThreads / 32];
     __shared__ int red_i[kLuThreads / 32];
@@ -126,6 +127,7 @@ __global__ void __launch_bounds__(kLuThreads) lu_factor_kernel(int n, const int3
 template <class T>
 __global__ void lu_solve_kernel(int n, const double *__restrict__ lu, const int32_t *__restrict__ pivots, const T *b,
                                 T *x) {
+    pdl_enter();
     __shared__ double v[256];
     const int row = threadIdx.x;
     if (row < n) v[row] = static_cast<double>(b[row]);
@@ -153,6 +155,7 @@ __global__ void lu_solve_kernel(int n, const double *__restrict__ lu, const int3
 // Column c of A^-1 = U^-1 L^-1 P e_c, one thread per column.
 __global__ void lu_inverse_kernel(int n, const double *__restrict__ lu, const int32_t *__restrict__ pivots,
                                   double *__restrict__ inv /* row major */, double *__restrict__ work) {
+    pdl_enter();
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= n) return;
     double *v = work + static_cast<int64_t>(c) * n;
@@ -174,6 +177,7 @@ __global__ void lu_inverse_kernel(int n, const double *__restrict__ lu, const in
 // x = inv * b, one warp per row, FP64 accumulation.
 template <class T>
 __global__ void dense_apply_kernel(int n, const double *__restrict__ inv, const T *__restrict__ b, T *__restrict__ x) {
+    pdl_enter();
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (warp >= n) return;
     double s = 0;
@@ -194,28 +198,26 @@ bool coarse_lu_factor(tf_ctx *ctx, const Csr<double, int32_t> &a, double *lu, in
                                         static_cast<int>(bytes)),
                    "LU shared memory");
     int *bad = static_cast<int *>(ctx->arena(sizeof(int), 1));
-    lu_factor_kernel<<<1, kLuThreads, bytes, ctx->stream>>>(n, a.rp, a.ci, a.val, lu, pivots, bad, smem ? 1 : 0);
-    launched(ctx, "lu_factor");
+    launch_kernel(ctx, "lu_factor", lu_factor_kernel, 1, kLuThreads, bytes, n, a.rp, a.ci, a.val, lu, pivots, bad,
+                  smem ? 1 : 0);
     return read_scalar(ctx, bad) == 0;
 }
 
 template <class T>
 void coarse_lu_solve(tf_ctx *ctx, int n, const double *lu, const int32_t *pivots, const T *b, T *x) {
     require(n >= 1 && n <= 256, "Invalid GPU coarse solve");
-    lu_solve_kernel<T><<<1, 256, 0, ctx->stream>>>(n, lu, pivots, b, x);
-    launched(ctx, "lu_solve");
+    launch_kernel(ctx, "lu_solve", lu_solve_kernel<T>, 1, 256, 0, n, lu, pivots, b, x);
 }
 
 void coarse_inverse(tf_ctx *ctx, int n, const double *lu, const int32_t *pivots, double *inv) {
     double *work = static_cast<double *>(ctx->arena(static_cast<size_t>(n) * n * sizeof(double), 1));
-    lu_inverse_kernel<<<grid_for(n, 64), 64, 0, ctx->stream>>>(n, lu, pivots, inv, work);
-    launched(ctx, "lu_inverse");
+    launch_kernel(ctx, "lu_inverse", lu_inverse_kernel, grid_for(n, 64), 64, 0, n, lu, pivots, inv, work);
 }
 
 template <class T>
 void coarse_dense_apply(tf_ctx *ctx, int n, const double *inv, const T *b, T *x) {
-    dense_apply_kernel<T><<<grid_for(static_cast<int64_t>(n) * 32), kBlock, 0, ctx->stream>>>(n, inv, b, x);
-    launched(ctx, "coarse_apply");
+    launch_kernel(ctx, "coarse_apply", dense_apply_kernel<T>, grid_for(static_cast<int64_t>(n) * 32), kBlock, 0, n, inv,
+                  b, x);
 }
 
 template void coarse_lu_solve<float>(tf_ctx *, int, const double *, const int32_t *, const float *, float *);

@@ -147,6 +147,8 @@ struct tf_ctx {
     tfb::DeviceBuffer<unsigned char> scratch2;
     void *pinned{nullptr};                      // 256 bytes of pinned host memory
     int *fault{nullptr};                        // device word raised by a kernel whose bounded wait expired
+    bool pdl{true};                             // launch_kernel adds programmatic dependent launch
+    bool stable{false};                         // operators are read-only (solve / cycle enqueue)
     // Returns a scratch region of at least bytes (256-byte aligned start).
     void *arena(size_t bytes, int slot = 0) {
         auto &b = slot ? scratch2 : scratch;
@@ -171,6 +173,51 @@ inline void launched(tf_ctx *ctx, const char *name) {
     ++ctx->launches;
     cuda_check(cudaGetLastError(), name);
 }
+
+// Programmatic dependent launch.  A kernel started by launch_kernel may be
+// scheduled while the kernel before it in the stream is still running:
+// pdl_wait() returns once that kernel has completed and its writes are
+// visible, so such a kernel calls it before any access to memory an earlier
+// kernel writes or reads; pdl_trigger() lets the next kernel be scheduled
+// (its CTAs then wait in their own pdl_wait).  Both are no-ops in a kernel
+// launched without the attribute.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_enter() {
+    pdl_wait();
+    pdl_trigger();
+}
+
+// Launches kernel<<<grid, block, smem, ctx->stream>>>(args...) with the
+// programmatic-serialization attribute (when ctx->pdl) and counts it.  Every
+// kernel launched here calls pdl_wait() (pdl_enter()) before touching memory
+// that another kernel of the stream uses.
+template <class... P, class... A>
+void launch_kernel(tf_ctx *ctx, const char *name, void (*kernel)(P...), dim3 grid, dim3 block, size_t smem,
+                   A &&...args) {
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = ctx->stream;
+    cfg.attrs = attr;
+    cfg.numAttrs = ctx->pdl ? 1 : 0;
+    cuda_check(cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...), name);
+    ++ctx->launches;
+}
+
+// Marks the context's operators read-only while a solve or cycle is
+// enqueued: pipelined kernels may then stream the matrix before their
+// predecessor has finished.
+struct StableScope {
+    tf_ctx *ctx;
+    bool old;
+    explicit StableScope(tf_ctx *c) : ctx(c), old(c->stable) { c->stable = true; }
+    ~StableScope() { ctx->stable = old; }
+};
 
 // Synchronises the context stream and reads a device scalar.
 template <class T>

@@ -67,6 +67,9 @@ class Krylov {
     // that cannot see inside conditional graph nodes need this).
     int graph_mode{1};
     double last_ms{0};
+    // How the last solve ran: 2 one whole-solve graph, 1 one graph per
+    // iteration, 0 uncaptured launches, -1 no solve yet.
+    int last_execution{-1};
 };
 
 std::unique_ptr<Krylov> make_krylov(int kind, int value_type, int index_type, const tf_solver_options &opt,

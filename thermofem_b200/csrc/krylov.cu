@@ -52,6 +52,7 @@ __device__ __forceinline__ void stop(KState *s, int status) {
 
 // After r = b - A x0 and ||b||^2 partials: initial decisions (Cg.cuh:125-137).
 __global__ void k_init(KState *s, const double *pb, int nb, const double *pr, int nr, int bicg) {
+    pdl_enter();
     double vb[1], vr[1];
     sum_partials<1>(pb, nb, vb);
     __syncthreads();
@@ -78,6 +79,7 @@ __global__ void k_init(KState *s, const double *pb, int nb, const double *pr, in
 
 // Final report from the true residual (Cg.cuh:105-121, BiCgStab.cuh:122-136).
 __global__ void k_finish(KState *s, const double *pr, int nr) {
+    pdl_enter();
     double v[1];
     sum_partials<1>(pr, nr, v);
     if (threadIdx.x) return;
@@ -93,22 +95,23 @@ __global__ void k_finish(KState *s, const double *pr, int nr) {
 
 template <class T>
 __global__ void k_copy_if(const int *flag, int64_t n, const T *__restrict__ src, T *__restrict__ dst) {
+    pdl_enter();
     if (!*flag) return;
     for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
          i += static_cast<int64_t>(gridDim.x) * blockDim.x)
         dst[i] = src[i];
 }
 
-__global__ void k_clear_flag(int *flag) { *flag = 0; }
-
 // Re-arms the WHILE node of the solve graph: one more iteration while the
 // recurrence is running and below the iteration limit.
 __global__ void k_set_continue(cudaGraphConditionalHandle handle, const KState *s) {
+    pdl_enter();
     cudaGraphSetConditional(handle, (s->running && s->it < s->max_it) ? 1u : 0u);
 }
 
 template <class T>
 __global__ void k_dot(int64_t n, const T *__restrict__ x, const T *__restrict__ y, double *part) {
+    pdl_enter();
     double v[1] = {0.0};
     for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
          i += static_cast<int64_t>(gridDim.x) * blockDim.x)
@@ -189,6 +192,7 @@ struct ResidualNorm {
 // ---- PCG -----------------------------------------------------------------
 
 __global__ void cg_rho(KState *s, const double *part, int parts) {
+    pdl_enter();
     if (!s->running) return;
     double v[1];
     sum_partials<1>(part, parts, v);
@@ -211,6 +215,7 @@ __global__ void cg_rho(KState *s, const double *part, int parts) {
 
 template <class T>
 __global__ void cg_p(const KState *s, int64_t n, const T *__restrict__ z, T *__restrict__ p) {
+    pdl_enter();
     if (!s->running) return;
     const int mode = s->pmode;
     const T beta = static_cast<T>(s->beta);
@@ -220,6 +225,7 @@ __global__ void cg_p(const KState *s, int64_t n, const T *__restrict__ z, T *__r
 }
 
 __global__ void cg_curv(KState *s, const double *part, int parts) {
+    pdl_enter();
     if (!s->running) return;
     double v[1];
     sum_partials<1>(part, parts, v);
@@ -236,6 +242,7 @@ __global__ void cg_curv(KState *s, const double *part, int parts) {
 template <class T>
 __global__ void cg_xr(const KState *s, int64_t n, const T *__restrict__ p, const T *__restrict__ ap, T *__restrict__ x,
                       T *__restrict__ r, double *part) {
+    pdl_enter();
     if (!s->running) return;
     const T alpha = static_cast<T>(s->alpha);
     double v[1] = {0.0};
@@ -252,6 +259,7 @@ __global__ void cg_xr(const KState *s, int64_t n, const T *__restrict__ p, const
 
 // ||r|| check, refresh decision (Cg.cuh:170-178).
 __global__ void cg_res(KState *s, const double *part, int parts) {
+    pdl_enter();
     if (!s->running) return;
     double v[1];
     sum_partials<1>(part, parts, v);
@@ -265,6 +273,7 @@ __global__ void cg_res(KState *s, const double *part, int parts) {
 // After a gated true residual: confirm or restart (Cg.cuh:178-185), then
 // close the iteration.
 __global__ void cg_end(KState *s, const double *part, int parts) {
+    pdl_enter();
     if (!s->running) return;
     double v[1];
     if (s->refresh) sum_partials<1>(part, parts, v);
@@ -283,6 +292,7 @@ __global__ void cg_end(KState *s, const double *part, int parts) {
 // ---- BiCGStab ------------------------------------------------------------
 
 __global__ void bi_rho(KState *s, const double *part, int parts) {
+    pdl_enter();
     if (!s->running) return;
     double v[1];
     sum_partials<1>(part, parts, v);
@@ -309,6 +319,7 @@ __global__ void bi_rho(KState *s, const double *part, int parts) {
 // p = r (fresh) or p = r + beta (p - omega v) (BiCgStab.cuh:176-184).
 template <class T>
 __global__ void bi_p(const KState *s, int64_t n, const T *__restrict__ r, const T *__restrict__ v, T *__restrict__ p) {
+    pdl_enter();
     if (!s->running) return;
     const int mode = s->pmode;
     const T beta = static_cast<T>(s->beta), omega = static_cast<T>(s->omega);
@@ -324,6 +335,7 @@ __global__ void bi_p(const KState *s, int64_t n, const T *__restrict__ r, const 
 }
 
 __global__ void bi_alpha(KState *s, const double *part, int parts) {
+    pdl_enter();
     if (!s->running) return;
     double v[1];
     sum_partials<1>(part, parts, v);
@@ -340,6 +352,7 @@ __global__ void bi_alpha(KState *s, const double *part, int parts) {
 template <class T>
 __global__ void bi_s(const KState *st, int64_t n, const T *__restrict__ r, const T *__restrict__ v,
                      const T *__restrict__ ph, T *__restrict__ sv, T *__restrict__ x, double *part) {
+    pdl_enter();
     if (!st->running) return;
     const T alpha = static_cast<T>(st->alpha);
     double acc[1] = {0.0};
@@ -356,6 +369,7 @@ __global__ void bi_s(const KState *st, int64_t n, const T *__restrict__ r, const
 
 // ||s|| check: candidate convergence takes the early path (BiCgStab.cuh:199-211).
 __global__ void bi_snorm(KState *s, const double *part, int parts) {
+    pdl_enter();
     if (!s->running) return;
     double v[1];
     sum_partials<1>(part, parts, v);
@@ -371,6 +385,7 @@ __global__ void bi_snorm(KState *s, const double *part, int parts) {
 // Early path after the gated true residual: confirm or restart, skipping the
 // omega half and the rho_prev update of this iteration.
 __global__ void bi_early(KState *s, const double *part, int parts) {
+    pdl_enter();
     if (!s->running || !s->early) return;
     double v[1];
     sum_partials<1>(part, parts, v);
@@ -383,6 +398,7 @@ __global__ void bi_early(KState *s, const double *part, int parts) {
 }
 
 __global__ void bi_omega(KState *s, const double *part, int parts) {
+    pdl_enter();
     if (!s->running || !s->normal) return;
     double v[2];
     sum_partials<2>(part, parts, v);
@@ -400,6 +416,7 @@ __global__ void bi_omega(KState *s, const double *part, int parts) {
 template <class T>
 __global__ void bi_xr(const KState *st, int64_t n, const T *__restrict__ sh, const T *__restrict__ sv,
                       const T *__restrict__ t, T *__restrict__ x, T *__restrict__ r, double *part) {
+    pdl_enter();
     if (!st->running || !st->normal) return;
     const T omega = static_cast<T>(st->omega);
     double acc[1] = {0.0};
@@ -415,6 +432,7 @@ __global__ void bi_xr(const KState *st, int64_t n, const T *__restrict__ sh, con
 }
 
 __global__ void bi_res(KState *s, const double *part, int parts) {
+    pdl_enter();
     if (!s->running || !s->normal) return;
     double v[1];
     sum_partials<1>(part, parts, v);
@@ -426,6 +444,7 @@ __global__ void bi_res(KState *s, const double *part, int parts) {
 }
 
 __global__ void bi_end(KState *s, const double *part, int parts) {
+    pdl_enter();
     if (!s->running) return;
     double v[1];
     const bool refresh = s->normal && s->refresh;
@@ -523,6 +542,7 @@ class KrylovImpl final : public Krylov {
 
     tf_solve_result solve(tf_ctx *ctx, const void *rhs, void *x) override {
         if (!ready_) fail(TF_ERR_LOGIC, kind_ == TF_SOLVER_CG ? "CG requires setup" : "BiCGStab requires setup");
+        StableScope stable(ctx);  // the operator and the hierarchy are read-only during a solve
         cuda_check(cudaEventRecord(ev0_, ctx->stream), "event");
         copy_async(ctx, rhs_.data(), rhs, n_ * sizeof(T));
         copy_async(ctx, x_.data(), x, n_ * sizeof(T));
@@ -539,6 +559,7 @@ class KrylovImpl final : public Krylov {
         if (whole) {
             // the whole solve, loop included, is one graph launch
             cuda_check(cudaGraphLaunch(solve_exec_, ctx->stream), "solve graph");
+            last_execution = 2;
         } else {
             enqueue_prefix(ctx);
             int *running = static_cast<int *>(ctx->pinned);
@@ -597,16 +618,14 @@ class KrylovImpl final : public Krylov {
 
     // ||b||^2, r = b - A x with ||r||^2, initial decisions.
     void enqueue_prefix(tf_ctx *ctx) {
-        k_dot<T><<<parts_, 256, 0, ctx->stream>>>(n_, rhs_.data(), rhs_.data(), partb_.data());
-        launched(ctx, "dot");
+        launch_kernel(ctx, "dot", k_dot<T>, parts_, 256, 0, n_, rhs_.data(), rhs_.data(), partb_.data());
         tile::launch(ctx, csr(), tile::PlainX<T>{x_.data()},
                      ResidualNorm<T>{rhs_.data(), r_.data(), nullptr, part_.data()}, "residual_norm");
-        k_init<<<1, 1024, 0, ctx->stream>>>(state_.data(), partb_.data(), parts_, part_.data(), tiles_,
-                                           kind_ == TF_SOLVER_BICGSTAB ? 1 : 0);
-        launched(ctx, "k_init");
+        launch_kernel(ctx, "k_init", k_init, 1, 1024, 0, state_.data(), partb_.data(), parts_, part_.data(), tiles_,
+                      kind_ == TF_SOLVER_BICGSTAB ? 1 : 0);
         if (kind_ == TF_SOLVER_BICGSTAB) {
-            k_copy_if<T><<<parts_, 256, 0, ctx->stream>>>(&state_.data()->copy_shadow, n_, r_.data(), shadow_.data());
-            launched(ctx, "copy_if");
+            launch_kernel(ctx, "copy_if", k_copy_if<T>, parts_, 256, 0, &state_.data()->copy_shadow, n_, r_.data(),
+                          shadow_.data());
         }
     }
 
@@ -614,8 +633,7 @@ class KrylovImpl final : public Krylov {
     void enqueue_suffix(tf_ctx *ctx) {
         tile::launch(ctx, csr(), tile::PlainX<T>{x_.data()},
                      ResidualNorm<T>{rhs_.data(), r_.data(), nullptr, part_.data()}, "residual_norm");
-        k_finish<<<1, 1024, 0, ctx->stream>>>(state_.data(), part_.data(), tiles_);
-        launched(ctx, "k_finish");
+        launch_kernel(ctx, "k_finish", k_finish, 1, 1024, 0, state_.data(), part_.data(), tiles_);
     }
 
     // One graph for the whole solve: prefix, then a conditional WHILE node
@@ -635,8 +653,7 @@ class KrylovImpl final : public Krylov {
                        "capture prefix");
             capturing = true;
             enqueue_prefix(ctx);
-            k_set_continue<<<1, 1, 0, ctx->stream>>>(handle, state_.data());
-            launched(ctx, "set_continue");
+            launch_kernel(ctx, "set_continue", k_set_continue, 1, 1, 0, handle, state_.data());
             cudaStreamCaptureStatus st;
             const cudaGraphNode_t *deps = nullptr;
             size_t ndeps = 0;
@@ -660,8 +677,7 @@ class KrylovImpl final : public Krylov {
                        "capture body");
             capturing = true;
             enqueue_iteration(ctx);
-            k_set_continue<<<1, 1, 0, ctx->stream>>>(handle, state_.data());
-            launched(ctx, "set_continue");
+            launch_kernel(ctx, "set_continue", k_set_continue, 1, 1, 0, handle, state_.data());
             capturing = false;
             cuda_check(cudaStreamEndCapture(ctx->stream, &out), "capture body end");
             per_iteration_ = ctx->launches - b0;
@@ -722,8 +738,10 @@ class KrylovImpl final : public Krylov {
         if (exec_) {
             cuda_check(cudaGraphLaunch(exec_, ctx->stream), "iteration graph");
             ctx->launches += per_iteration_;
+            last_execution = 1;
         } else {
             enqueue_iteration(ctx);
+            last_execution = 0;
         }
     }
 
@@ -733,61 +751,44 @@ class KrylovImpl final : public Krylov {
         const unsigned pg = static_cast<unsigned>(parts_);
         if (kind_ == TF_SOLVER_CG) {
             precondition(ctx, r_.data(), z_.data());
-            k_dot<T><<<pg, 256, 0, ctx->stream>>>(n_, r_.data(), z_.data(), part);
-            launched(ctx, "dot");
-            cg_rho<<<1, 1024, 0, ctx->stream>>>(s, part,parts_);
-            launched(ctx, "cg_rho");
-            cg_p<T><<<pg, 256, 0, ctx->stream>>>(s, n_, z_.data(), p_.data());
-            launched(ctx, "cg_p");
+            launch_kernel(ctx, "dot", k_dot<T>, pg, 256, 0, n_, r_.data(), z_.data(), part);
+            launch_kernel(ctx, "cg_rho", cg_rho, 1, 1024, 0, s, part, parts_);
+            launch_kernel(ctx, "cg_p", cg_p<T>, pg, 256, 0, s, n_, z_.data(), p_.data());
             tile::launch(ctx, csr(), tile::PlainX<T>{p_.data()}, SpmvDot<T>{q_.data(), p_.data(), &s->running, part},
                          "spmv_dot");
-            cg_curv<<<1, 1024, 0, ctx->stream>>>(s, part,tiles_);
-            launched(ctx, "cg_curv");
-            cg_xr<T><<<pg, 256, 0, ctx->stream>>>(s, n_, p_.data(), q_.data(), x_.data(), r_.data(), part);
-            launched(ctx, "cg_xr");
-            cg_res<<<1, 1024, 0, ctx->stream>>>(s, part,parts_);
-            launched(ctx, "cg_res");
+            launch_kernel(ctx, "cg_curv", cg_curv, 1, 1024, 0, s, part, tiles_);
+            launch_kernel(ctx, "cg_xr", cg_xr<T>, pg, 256, 0, s, n_, p_.data(), q_.data(), x_.data(), r_.data(), part);
+            launch_kernel(ctx, "cg_res", cg_res, 1, 1024, 0, s, part, parts_);
             tile::launch(ctx, csr(), tile::PlainX<T>{x_.data()},
                          ResidualNorm<T>{rhs_.data(), r_.data(), &s->refresh, part}, "residual_norm");
-            cg_end<<<1, 1024, 0, ctx->stream>>>(s, part,tiles_);
-            launched(ctx, "cg_end");
+            launch_kernel(ctx, "cg_end", cg_end, 1, 1024, 0, s, part, tiles_);
             return;
         }
         // BiCGStab: v = q_, phat = z_
-        k_dot<T><<<pg, 256, 0, ctx->stream>>>(n_, shadow_.data(), r_.data(), part);
-        launched(ctx, "dot");
-        bi_rho<<<1, 1024, 0, ctx->stream>>>(s, part,parts_);
-        launched(ctx, "bi_rho");
-        bi_p<T><<<pg, 256, 0, ctx->stream>>>(s, n_, r_.data(), q_.data(), p_.data());
-        launched(ctx, "bi_p");
+        launch_kernel(ctx, "dot", k_dot<T>, pg, 256, 0, n_, shadow_.data(), r_.data(), part);
+        launch_kernel(ctx, "bi_rho", bi_rho, 1, 1024, 0, s, part, parts_);
+        launch_kernel(ctx, "bi_p", bi_p<T>, pg, 256, 0, s, n_, r_.data(), q_.data(), p_.data());
         precondition(ctx, p_.data(), z_.data());
         tile::launch(ctx, csr(), tile::PlainX<T>{z_.data()}, SpmvDot<T>{q_.data(), shadow_.data(), &s->running, part},
                      "spmv_dot");
-        bi_alpha<<<1, 1024, 0, ctx->stream>>>(s, part,tiles_);
-        launched(ctx, "bi_alpha");
-        bi_s<T><<<pg, 256, 0, ctx->stream>>>(s, n_, r_.data(), q_.data(), z_.data(), s_.data(), x_.data(), part);
-        launched(ctx, "bi_s");
-        bi_snorm<<<1, 1024, 0, ctx->stream>>>(s, part,parts_);
-        launched(ctx, "bi_snorm");
+        launch_kernel(ctx, "bi_alpha", bi_alpha, 1, 1024, 0, s, part, tiles_);
+        launch_kernel(ctx, "bi_s", bi_s<T>, pg, 256, 0, s, n_, r_.data(), q_.data(), z_.data(), s_.data(), x_.data(),
+                      part);
+        launch_kernel(ctx, "bi_snorm", bi_snorm, 1, 1024, 0, s, part, parts_);
         tile::launch(ctx, csr(), tile::PlainX<T>{x_.data()}, ResidualNorm<T>{rhs_.data(), r_.data(), &s->early, part},
                      "residual_norm");
-        bi_early<<<1, 1024, 0, ctx->stream>>>(s, part,tiles_);
-        launched(ctx, "bi_early");
+        launch_kernel(ctx, "bi_early", bi_early, 1, 1024, 0, s, part, tiles_);
         precondition(ctx, s_.data(), sh_.data());
         tile::launch(ctx, csr(), tile::PlainX<T>{sh_.data()}, SpmvDot2<T>{t_.data(), s_.data(), &s->normal, part},
                      "spmv_dot2");
-        bi_omega<<<1, 1024, 0, ctx->stream>>>(s, part,tiles_);
-        launched(ctx, "bi_omega");
-        bi_xr<T><<<pg, 256, 0, ctx->stream>>>(s, n_, sh_.data(), s_.data(), t_.data(), x_.data(), r_.data(), part);
-        launched(ctx, "bi_xr");
-        bi_res<<<1, 1024, 0, ctx->stream>>>(s, part,parts_);
-        launched(ctx, "bi_res");
+        launch_kernel(ctx, "bi_omega", bi_omega, 1, 1024, 0, s, part, tiles_);
+        launch_kernel(ctx, "bi_xr", bi_xr<T>, pg, 256, 0, s, n_, sh_.data(), s_.data(), t_.data(), x_.data(), r_.data(),
+                      part);
+        launch_kernel(ctx, "bi_res", bi_res, 1, 1024, 0, s, part, parts_);
         tile::launch(ctx, csr(), tile::PlainX<T>{x_.data()}, ResidualNorm<T>{rhs_.data(), r_.data(), &s->refresh, part},
                      "residual_norm");
-        bi_end<<<1, 1024, 0, ctx->stream>>>(s, part,tiles_);
-        launched(ctx, "bi_end");
-        k_copy_if<T><<<pg, 256, 0, ctx->stream>>>(&s->copy_shadow, n_, r_.data(), shadow_.data());
-        launched(ctx, "copy_if");
+        launch_kernel(ctx, "bi_end", bi_end, 1, 1024, 0, s, part, tiles_);
+        launch_kernel(ctx, "copy_if", k_copy_if<T>, pg, 256, 0, &s->copy_shadow, n_, r_.data(), shadow_.data());
     }
 
     int kind_;

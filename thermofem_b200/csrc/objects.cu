@@ -340,6 +340,8 @@ tf_amg *tf_solver_amg(tf_solver *s) {
 
 double tf_solver_last_apply_ms(const tf_solver *s) { return s && s->k ? s->k->last_ms : 0.0; }
 
+int tf_solver_last_execution(const tf_solver *s) { return s && s->k ? s->k->last_execution : -1; }
+
 int tf_solver_set_graph_mode(tf_solver *s, int mode) {
     return guard([&] {
         require(s != nullptr && (mode == 0 || mode == 1), "graph mode must be 0 or 1");

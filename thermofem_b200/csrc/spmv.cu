@@ -81,6 +81,7 @@ void launch_tile(tf_ctx *ctx, const Csr<T, I> &a, const XS &xs, const Epi &epi, 
 template <class T>
 __global__ void jacobi_zero_kernel(int64_t n, const T *__restrict__ dinv, const T *__restrict__ b, T *__restrict__ x,
                                    T w, const float *__restrict__ row_w) {
+    pdl_enter();
     for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
          i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
         const T wi = row_w ? static_cast<T>(row_w[i]) : w;
@@ -92,6 +93,7 @@ __global__ void jacobi_zero_kernel(int64_t n, const T *__restrict__ dinv, const 
 template <class T, class I>
 __global__ void inverse_diagonal_kernel(int64_t n, const I *__restrict__ rp, const I *__restrict__ ci,
                                         const T *__restrict__ val, T *__restrict__ dinv, int *bad) {
+    pdl_enter();
     const int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
     if (i >= n) return;
     T d = 0;
@@ -105,6 +107,7 @@ __global__ void inverse_diagonal_kernel(int64_t n, const I *__restrict__ rp, con
 template <class T>
 __global__ void restrict_kernel(int64_t nc, const int32_t *__restrict__ off, const int32_t *__restrict__ mem,
                                 const T *__restrict__ fine, T *__restrict__ coarse) {
+    pdl_enter();
     const int64_t c = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
     if (c >= nc) return;
     T s = 0;
@@ -115,6 +118,7 @@ __global__ void restrict_kernel(int64_t nc, const int32_t *__restrict__ off, con
 template <class T>
 __global__ void prolong_kernel(int64_t nf, const int32_t *__restrict__ map, const T *__restrict__ coarse,
                                T *__restrict__ fine) {
+    pdl_enter();
     for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < nf;
          i += static_cast<int64_t>(gridDim.x) * blockDim.x)
         fine[i] += coarse[map[i]];
@@ -148,6 +152,7 @@ struct DotArgs {
 
 template <class T, int K>
 __global__ void __launch_bounds__(256) dot_partial_kernel(int64_t n, DotArgs args, double *partial) {
+    pdl_enter();
     __shared__ double shm[K * 32];
     double v[K];
 #pragma unroll
@@ -167,6 +172,7 @@ __global__ void __launch_bounds__(256) dot_partial_kernel(int64_t n, DotArgs arg
 
 template <int K>
 __global__ void __launch_bounds__(256) dot_final_kernel(int parts, const double *partial, double *out) {
+    pdl_enter();
     __shared__ double shm[K * 32];
     double v[K];
 #pragma unroll
@@ -182,6 +188,7 @@ __global__ void __launch_bounds__(256) dot_final_kernel(int parts, const double 
 
 template <class T>
 __global__ void axpby_kernel(int64_t n, double a, const T *__restrict__ x, double b, T *__restrict__ y) {
+    pdl_enter();
     for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
          i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
         const T ta = static_cast<T>(a), tb = static_cast<T>(b);
@@ -191,6 +198,7 @@ __global__ void axpby_kernel(int64_t n, double a, const T *__restrict__ x, doubl
 
 template <class S, class D>
 __global__ void convert_kernel(int64_t n, const S *__restrict__ src, D *__restrict__ dst) {
+    pdl_enter();
     for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
          i += static_cast<int64_t>(gridDim.x) * blockDim.x)
         dst[i] = static_cast<D>(src[i]);
@@ -199,6 +207,7 @@ __global__ void convert_kernel(int64_t n, const S *__restrict__ src, D *__restri
 template <class I>
 __global__ void csr_structure_kernel(int64_t rows, int64_t cols, int64_t nnz, const I *__restrict__ rp,
                                      const I *__restrict__ ci, int *bad) {
+    pdl_enter();
     const int64_t r = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
     if (r == 0 && (rp[0] != 0 || static_cast<int64_t>(rp[rows]) != nnz)) atomicExch(bad, 1);
     if (r >= rows) return;
@@ -215,6 +224,7 @@ __global__ void csr_structure_kernel(int64_t rows, int64_t cols, int64_t nnz, co
 template <class T, class I>
 __global__ void canonical_flags_kernel(int64_t n, int64_t nnz, const I *__restrict__ rp, const I *__restrict__ ci,
                                        const T *__restrict__ val, int *flags) {
+    pdl_enter();
     const int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
     if (i >= n) return;
     if (rp[0] != 0 || static_cast<int64_t>(rp[n]) != nnz || rp[i] < 0 || rp[i] > rp[i + 1] ||
@@ -234,6 +244,7 @@ __global__ void canonical_flags_kernel(int64_t n, int64_t nnz, const I *__restri
 // Level validation and row max |offdiag| (GpuAggregation.cu:247-271).
 __global__ void row_stats_kernel(int64_t n, const int32_t *__restrict__ rp, const int32_t *__restrict__ ci,
                                  const double *__restrict__ a, int *bad, double *__restrict__ row_max) {
+    pdl_enter();
     const int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
     if (i >= n) return;
     double diag = 0, mx = 0;
@@ -309,8 +320,7 @@ void jacobi_sweep(tf_ctx *ctx, const Csr<T, I> &a, const T *dinv, const T *b, co
 template <class T>
 void jacobi_zero(tf_ctx *ctx, int64_t n, const T *dinv, const T *b, T *x, T w, const float *row_w) {
     if (!n) return;
-    jacobi_zero_kernel<T><<<stride_grid(ctx, n), kBlock, 0, ctx->stream>>>(n, dinv, b, x, w, row_w);
-    launched(ctx, "jacobi_zero");
+    launch_kernel(ctx, "jacobi_zero", jacobi_zero_kernel<T>, stride_grid(ctx, n), kBlock, 0, n, dinv, b, x, w, row_w);
 }
 
 template <class T, class I>
@@ -318,23 +328,21 @@ void inverse_diagonal(tf_ctx *ctx, const Csr<T, I> &a, T *dinv) {
     require(a.rows > 0 && a.rows == a.cols, "Inverse diagonal requires a nonempty square matrix");
     int *bad = static_cast<int *>(ctx->arena(sizeof(int), 1));
     memset_async(ctx, bad, 0, sizeof(int));
-    inverse_diagonal_kernel<T, I><<<grid_for(a.rows), kBlock, 0, ctx->stream>>>(a.rows, a.rp, a.ci, a.val, dinv, bad);
-    launched(ctx, "inverse_diagonal");
+    launch_kernel(ctx, "inverse_diagonal", inverse_diagonal_kernel<T, I>, grid_for(a.rows), kBlock, 0, a.rows, a.rp,
+                  a.ci, a.val, dinv, bad);
     if (read_scalar(ctx, bad)) fail(TF_ERR_INVALID, "Missing or invalid diagonal");
 }
 
 template <class T>
 void restrict_sum(tf_ctx *ctx, int64_t nc, const int32_t *off, const int32_t *mem, const T *fine, T *coarse) {
     if (!nc) return;
-    restrict_kernel<T><<<grid_for(nc), kBlock, 0, ctx->stream>>>(nc, off, mem, fine, coarse);
-    launched(ctx, "restrict");
+    launch_kernel(ctx, "restrict", restrict_kernel<T>, grid_for(nc), kBlock, 0, nc, off, mem, fine, coarse);
 }
 
 template <class T>
 void prolong_add(tf_ctx *ctx, int64_t nf, const int32_t *map, const T *coarse, T *fine) {
     if (!nf) return;
-    prolong_kernel<T><<<stride_grid(ctx, nf), kBlock, 0, ctx->stream>>>(nf, map, coarse, fine);
-    launched(ctx, "prolong");
+    launch_kernel(ctx, "prolong", prolong_kernel<T>, stride_grid(ctx, nf), kBlock, 0, nf, map, coarse, fine);
 }
 
 template <class T>
@@ -352,33 +360,29 @@ void dot_multi(tf_ctx *ctx, int64_t n, int count, const T *const *xs, const T *c
     const int parts = static_cast<int>(parts64);
     double *partial = static_cast<double *>(ctx->arena(sizeof(double) * 4 * parts));
     switch (count) {
-        case 1: dot_partial_kernel<T, 1><<<parts, 256, 0, ctx->stream>>>(n, args, partial); break;
-        case 2: dot_partial_kernel<T, 2><<<parts, 256, 0, ctx->stream>>>(n, args, partial); break;
-        case 3: dot_partial_kernel<T, 3><<<parts, 256, 0, ctx->stream>>>(n, args, partial); break;
-        default: dot_partial_kernel<T, 4><<<parts, 256, 0, ctx->stream>>>(n, args, partial); break;
+        case 1: launch_kernel(ctx, "dot_partial", dot_partial_kernel<T, 1>, parts, 256, 0, n, args, partial); break;
+        case 2: launch_kernel(ctx, "dot_partial", dot_partial_kernel<T, 2>, parts, 256, 0, n, args, partial); break;
+        case 3: launch_kernel(ctx, "dot_partial", dot_partial_kernel<T, 3>, parts, 256, 0, n, args, partial); break;
+        default: launch_kernel(ctx, "dot_partial", dot_partial_kernel<T, 4>, parts, 256, 0, n, args, partial); break;
     }
-    launched(ctx, "dot_partial");
     switch (count) {
-        case 1: dot_final_kernel<1><<<1, 256, 0, ctx->stream>>>(parts, partial, out); break;
-        case 2: dot_final_kernel<2><<<1, 256, 0, ctx->stream>>>(parts, partial, out); break;
-        case 3: dot_final_kernel<3><<<1, 256, 0, ctx->stream>>>(parts, partial, out); break;
-        default: dot_final_kernel<4><<<1, 256, 0, ctx->stream>>>(parts, partial, out); break;
+        case 1: launch_kernel(ctx, "dot_final", dot_final_kernel<1>, 1, 256, 0, parts, partial, out); break;
+        case 2: launch_kernel(ctx, "dot_final", dot_final_kernel<2>, 1, 256, 0, parts, partial, out); break;
+        case 3: launch_kernel(ctx, "dot_final", dot_final_kernel<3>, 1, 256, 0, parts, partial, out); break;
+        default: launch_kernel(ctx, "dot_final", dot_final_kernel<4>, 1, 256, 0, parts, partial, out); break;
     }
-    launched(ctx, "dot_final");
 }
 
 template <class T>
 void axpby(tf_ctx *ctx, int64_t n, double a, const T *x, double b, T *y) {
     if (!n) return;
-    axpby_kernel<T><<<stride_grid(ctx, n), kBlock, 0, ctx->stream>>>(n, a, x, b, y);
-    launched(ctx, "axpby");
+    launch_kernel(ctx, "axpby", axpby_kernel<T>, stride_grid(ctx, n), kBlock, 0, n, a, x, b, y);
 }
 
 template <class S, class D>
 void convert(tf_ctx *ctx, int64_t n, const S *src, D *dst) {
     if (!n) return;
-    convert_kernel<S, D><<<stride_grid(ctx, n), kBlock, 0, ctx->stream>>>(n, src, dst);
-    launched(ctx, "convert");
+    launch_kernel(ctx, "convert", convert_kernel<S, D>, stride_grid(ctx, n), kBlock, 0, n, src, dst);
 }
 
 template <class T>
@@ -390,8 +394,8 @@ template <class I>
 bool csr_structure_ok(tf_ctx *ctx, int64_t rows, int64_t cols, int64_t nnz, const I *rp, const I *ci) {
     int *bad = static_cast<int *>(ctx->arena(sizeof(int), 1));
     memset_async(ctx, bad, 0, sizeof(int));
-    csr_structure_kernel<I><<<grid_for(rows > 0 ? rows : 1), kBlock, 0, ctx->stream>>>(rows, cols, nnz, rp, ci, bad);
-    launched(ctx, "csr_validate");
+    launch_kernel(ctx, "csr_validate", csr_structure_kernel<I>, grid_for(rows > 0 ? rows : 1), kBlock, 0, rows, cols,
+                  nnz, rp, ci, bad);
     return read_scalar(ctx, bad) == 0;
 }
 
@@ -400,9 +404,8 @@ int csr_canonical_flags(tf_ctx *ctx, const Csr<T, I> &a) {
     int *flags = static_cast<int *>(ctx->arena(sizeof(int), 1));
     memset_async(ctx, flags, 0, sizeof(int));
     if (a.rows) {
-        canonical_flags_kernel<T, I><<<grid_for(a.rows), kBlock, 0, ctx->stream>>>(a.rows, a.nnz, a.rp, a.ci, a.val,
-                                                                                   flags);
-        launched(ctx, "check_canonical");
+        launch_kernel(ctx, "check_canonical", canonical_flags_kernel<T, I>, grid_for(a.rows), kBlock, 0, a.rows, a.nnz,
+                      a.rp, a.ci, a.val, flags);
     }
     return read_scalar(ctx, flags);
 }
@@ -411,8 +414,8 @@ bool row_stats(tf_ctx *ctx, const Csr<double, int32_t> &a, double *row_max) {
     int *bad = static_cast<int *>(ctx->arena(sizeof(int), 1));
     memset_async(ctx, bad, 0, sizeof(int));
     if (a.rows) {
-        row_stats_kernel<<<grid_for(a.rows), kBlock, 0, ctx->stream>>>(a.rows, a.rp, a.ci, a.val, bad, row_max);
-        launched(ctx, "row_stats");
+        launch_kernel(ctx, "row_stats", row_stats_kernel, grid_for(a.rows), kBlock, 0, a.rows, a.rp, a.ci, a.val, bad,
+                      row_max);
     }
     return read_scalar(ctx, bad) == 0;
 }

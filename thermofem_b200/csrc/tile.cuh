@@ -97,6 +97,7 @@ __global__ void __launch_bounds__(kThreads) csr_tile_kernel(int64_t rows, const 
                                                              const I *__restrict__ ci, const T *__restrict__ val,
                                                              int chunk, XS xs, Epi epi) {
     constexpr int K = Epi::kReduce;
+    pdl_enter();
     if (epi.skip()) return;
     extern __shared__ __align__(16) unsigned char smem[];
     T *sval = reinterpret_cast<T *>(smem);
@@ -273,17 +274,22 @@ struct Range {
 // accumulating any (more loads in flight per register).  Partial sums stay
 // per 256-row block in the same warp and lane order, so reductions do not
 // depend on RPT.
+//
+// With early != 0 (the matrix is not written by any kernel still in flight)
+// the producer fills the first `stages` chunks before waiting for the
+// previous kernel of the stream (programmatic dependent launch), so the
+// matrix stream overlaps that kernel's tail; the consumers, which read x and
+// the epilogue operands, always wait first.
 template <class T, class I, int RPT, class XS, class Epi>
 __global__ void __launch_bounds__(kThreads + 32) csr_pipe_kernel(int64_t rows, int64_t nnz, const I *__restrict__ rp,
                                                                   const I *__restrict__ ci,
                                                                   const T *__restrict__ val, int cap, int stages,
-                                                                  XS xs, Epi epi, int *fault) {
+                                                                  int early, XS xs, Epi epi, int *fault) {
     constexpr int K = Epi::kReduce;
     constexpr int KK = K > 0 ? K : 1;
     constexpr int kVT = 16 / sizeof(T), kVI = 16 / sizeof(I);
     constexpr int kTileRows = kThreads * RPT;
     constexpr int kWarps = kThreads / 32;
-    if (epi.skip()) return;
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ uint64_t full_bar[kMaxStages], empty_bar[kMaxStages];
     __shared__ double warp_sums[kMaxStages + 1][RPT][kWarps][KK];
@@ -314,16 +320,29 @@ __global__ void __launch_bounds__(kThreads + 32) csr_pipe_kernel(int64_t rows, i
     if (tid == kThreads) {
         // ---- producer ----
         uint32_t it = 0;
-        for (int64_t tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+        bool entered = false, stop = false;
+        auto enter = [&] {
+            if (!entered) {
+                entered = true;
+                pdl_enter();
+                stop = epi.skip();
+            }
+            return stop;
+        };
+        if (!early) enter();
+        for (int64_t tile = blockIdx.x; tile < ntiles && ok && !stop; tile += gridDim.x) {
             const int64_t r0 = tile * kTileRows;
             const int nr = static_cast<int>(min(static_cast<int64_t>(kTileRows), rows - r0));
             const int64_t s = rp[r0], e = rp[r0 + nr];
             const int64_t nch = e > s ? (e - s + cap - 1) / cap : 1;
             for (int64_t c = 0; c < nch && ok; ++c, ++it) {
                 const int st = static_cast<int>(it % stages);
-                if (it >= static_cast<uint32_t>(stages) && !mbar_wait(&empty_bar[st], ((it / stages) + 1) & 1)) {
-                    ok = false;
-                    break;
+                if (it >= static_cast<uint32_t>(stages)) {
+                    if (enter()) break;
+                    if (!mbar_wait(&empty_bar[st], ((it / stages) + 1) & 1)) {
+                        ok = false;
+                        break;
+                    }
                 }
                 const int64_t cs = s + c * cap, ce = min(e, cs + cap);
                 Range<I> rr;
@@ -343,13 +362,16 @@ __global__ void __launch_bounds__(kThreads + 32) csr_pipe_kernel(int64_t rows, i
                 rc.issue(stage_col(st), ci, &full_bar[st]);
             }
         }
+        enter();
         if (!ok) atomicExch(fault, 1);
     } else if (tid < kThreads) {
         // ---- consumers: RPT rows per thread ----
+        pdl_enter();
         const int lane = tid & 31, warp = tid >> 5;
         uint32_t it = 0, local_tile = 0;
         double red[RPT][KK];
-        for (int64_t tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+        const int64_t first = epi.skip() ? ntiles : blockIdx.x;
+        for (int64_t tile = first; tile < ntiles && ok; tile += gridDim.x) {
             const int64_t r0 = tile * kTileRows;
             const int nr = static_cast<int>(min(static_cast<int64_t>(kTileRows), rows - r0));
             int64_t rs[RPT], re[RPT], s = 0, e = 0, nch = 1;
@@ -590,16 +612,16 @@ void launch(tf_ctx *ctx, const Csr<T, I> &a, const XS &xs, const Epi &epi, const
     if (pipe) {
         const PipeConfig cfg = force ? *force : tuned_config<T, I>(a.rows, a.nnz, ctx->sm_count);
         const PipeShape p = pipe_shape<T, I>(a.rows, a.nnz, ctx->sm_count, cfg);
+        const int early = ctx->stable ? 1 : 0;
         if (p.rpt == 2) {
             allow_smem<csr_pipe_kernel<T, I, 2, XS, Epi>>(p.smem);
-            csr_pipe_kernel<T, I, 2, XS, Epi><<<p.grid, kThreads + 32, p.smem, ctx->stream>>>(
-                a.rows, a.nnz, a.rp, a.ci, a.val, p.cap, p.stages, xs, epi, ctx->fault);
+            launch_kernel(ctx, name, csr_pipe_kernel<T, I, 2, XS, Epi>, p.grid, kThreads + 32, p.smem, a.rows, a.nnz,
+                          a.rp, a.ci, a.val, p.cap, p.stages, early, xs, epi, ctx->fault);
         } else {
             allow_smem<csr_pipe_kernel<T, I, 1, XS, Epi>>(p.smem);
-            csr_pipe_kernel<T, I, 1, XS, Epi><<<p.grid, kThreads + 32, p.smem, ctx->stream>>>(
-                a.rows, a.nnz, a.rp, a.ci, a.val, p.cap, p.stages, xs, epi, ctx->fault);
+            launch_kernel(ctx, name, csr_pipe_kernel<T, I, 1, XS, Epi>, p.grid, kThreads + 32, p.smem, a.rows, a.nnz,
+                          a.rp, a.ci, a.val, p.cap, p.stages, early, xs, epi, ctx->fault);
         }
-        launched(ctx, name);
         return;
     }
     require(Epi::kReduce == 0, "reducing SpMV epilogues need 16-byte aligned CSR arrays");
@@ -609,12 +631,13 @@ void launch(tf_ctx *ctx, const Csr<T, I> &a, const XS &xs, const Epi &epi, const
     const size_t smem = static_cast<size_t>(shape.chunk) * (sizeof(T) + sizeof(I));
     if (shape.rows_per_thread == 2) {
         allow_smem<csr_tile_kernel<T, I, 2, XS, Epi>>(smem);
-        csr_tile_kernel<T, I, 2><<<g, kThreads, smem, ctx->stream>>>(a.rows, a.rp, a.ci, a.val, shape.chunk, xs, epi);
+        launch_kernel(ctx, name, csr_tile_kernel<T, I, 2, XS, Epi>, g, kThreads, smem, a.rows, a.rp, a.ci, a.val,
+                      shape.chunk, xs, epi);
     } else {
         allow_smem<csr_tile_kernel<T, I, 1, XS, Epi>>(smem);
-        csr_tile_kernel<T, I, 1><<<g, kThreads, smem, ctx->stream>>>(a.rows, a.rp, a.ci, a.val, shape.chunk, xs, epi);
+        launch_kernel(ctx, name, csr_tile_kernel<T, I, 1, XS, Epi>, g, kThreads, smem, a.rows, a.rp, a.ci, a.val,
+                      shape.chunk, xs, epi);
     }
-    launched(ctx, name);
 }
 
 // y = b - A x epilogue used to time candidate shapes (the residual and
