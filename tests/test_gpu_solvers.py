@@ -290,3 +290,48 @@ def test_dependent_launch_gives_identical_solves(ctx, kind, monkeypatch):
     assert out[0][0]["status"] == "Converged"
     assert out[0][0] == out[1][0]
     assert torch.equal(out[0][1], out[1][1])
+
+
+@pytest.mark.parametrize("cycle", ["v", "w", "f"])
+@pytest.mark.parametrize("hierarchy", ["f64", "f32"])
+def test_transfer_fusion_is_bit_identical(ctx, cycle, hierarchy, monkeypatch):
+    # Restriction fused into the coarse level's first kernel and
+    # prolongation fused into its last one (THERMOFEM_B200_FUSE=1, the
+    # default, and 2, every level) must reproduce the unfused cycle exactly.
+    m = P.heat3d(56, seed=61)  # 175616 rows: the finest level exceeds the scatter threshold
+    n = len(m[0]) - 1
+    a = to_device(m)
+    b = torch.tensor(P.rhs_uniform(n, 62), device="cuda")
+    outs = []
+    for fuse in ("0", "1", "2"):
+        monkeypatch.setenv("THERMOFEM_B200_FUSE", fuse)
+        amg = tf.Amg(tf.amg_options(cycle=cycle, hierarchy_type=hierarchy, jacobi_weight=2 / 3, post_sweeps=2),
+                     ctx=ctx)
+        amg.setup(a)
+        outs.append(amg.apply(b).clone())
+        amg.apply(b, outs[-1])  # the captured graph replays the same kernels
+        outs.append(outs[-1].clone())
+    assert torch.isfinite(outs[0]).all()
+    for o in outs[1:]:
+        assert torch.equal(outs[0], o)
+
+
+def test_transfer_fusion_solve_and_small_level_program(ctx, monkeypatch):
+    m = P.heat3d(24, seed=71)
+    n = len(m[0]) - 1
+    b = torch.tensor(P.rhs_uniform(n, 72), device="cuda")
+    res = []
+    for fuse, small in (("0", 0), ("1", 0), ("1", 2000)):
+        monkeypatch.setenv("THERMOFEM_B200_FUSE", fuse)
+        s = tf.Cg(tf.solver_options(), "amg",
+                  tf.amg_options(hierarchy_type="f32", jacobi_weight=2 / 3, small_level_rows=small), ctx=ctx)
+        s.setup(to_device(m))
+        x = torch.zeros(n, dtype=torch.float64, device="cuda")
+        rep = s.apply(b, x)
+        res.append((rep, x))
+    assert res[0][0]["status"] == "Converged"
+    assert res[0][0] == res[1][0] and torch.equal(res[0][1], res[1][1])
+    # the cooperative small-level program (transfers never fused into it)
+    # sums in its own order: it must converge in about as many iterations
+    assert res[2][0]["status"] == "Converged"
+    assert abs(res[2][0]["iterations"] - res[0][0]["iterations"]) <= 2

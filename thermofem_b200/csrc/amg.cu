@@ -87,7 +87,13 @@ struct Level {
 template <class S>
 class HierarchyImpl final : public Hierarchy {
   public:
-    HierarchyImpl(const AmgConfig &cfg) : cfg_(cfg), w_(static_cast<S>(cfg.o.jacobi_weight)) {}
+    HierarchyImpl(const AmgConfig &cfg) : cfg_(cfg), w_(static_cast<S>(cfg.o.jacobi_weight)) {
+        // THERMOFEM_B200_FUSE: 0 launches every transfer on its own, 1 fuses
+        // restrictions everywhere and prolongations into fine levels of at
+        // most kScatterRows rows, 2 fuses every prolongation.
+        const char *f = std::getenv("THERMOFEM_B200_FUSE");
+        fuse_ = f ? std::atoi(f) : 1;
+    }
     ~HierarchyImpl() override {
         if (exec_) cudaGraphExecDestroy(exec_);
     }
@@ -258,7 +264,10 @@ class HierarchyImpl final : public Hierarchy {
         std::fill(visits.begin(), visits.end(), 0);
         entry_ = 0;
         rec_.clear();
+        pr_ = {};
+        pw_ = {};
         cycle(ctx, cfg_.o.cycle, 0, true);
+        if (!dry_) flush(ctx);
     }
 
     // ---- level operations: launched, or recorded as a cooperative step ----
@@ -273,6 +282,13 @@ class HierarchyImpl final : public Hierarchy {
             s.xout = l.x();
             rec_.push_back(s);
         } else if (!dry_) {
+            if (fusing() && pr_.coarse == &l) {
+                restrict_jacobi_zero(ctx, l.n, pr_.fine->off.data(), pr_.fine->mem.data(), pr_.src, l.rhs.data(),
+                                     l.dinv.data(), l.x(), w_);
+                pr_ = {};
+                return;
+            }
+            flush(ctx);
             jacobi_zero(ctx, l.n, l.dinv.data(), l.rhs.data(), l.x(), w_, nullptr);
         }
     }
@@ -285,6 +301,7 @@ class HierarchyImpl final : public Hierarchy {
             s.xout = l.x();
             rec_.push_back(s);
         } else if (!dry_) {
+            flush(ctx);
             fill_zero(ctx, l.n, l.x());
         }
     }
@@ -306,7 +323,9 @@ class HierarchyImpl final : public Hierarchy {
             s.e = e;
             rec_.push_back(s);
         } else if (!dry_) {
-            jacobi_sweep(ctx, l.csr(), l.dinv.data(), l.rhs.data(), l.x(), l.other(), w_, nullptr, map, e);
+            flush(ctx);
+            if (fusing() && !map) pw_ = {kWriteSweep, &l, l.x(), l.other(), {}};  // may take a prolongation
+            else jacobi_sweep(ctx, l.csr(), l.dinv.data(), l.rhs.data(), l.x(), l.other(), w_, nullptr, map, e);
         }
         l.cur ^= 1;
     }
@@ -327,8 +346,10 @@ class HierarchyImpl final : public Hierarchy {
             s.coarse_rhs = c.rhs.data();
             rec_.push_back(s);
         } else if (!dry_) {
+            flush(ctx);
             residual(ctx, l.csr(), l.rhs.data(), l.x(), l.r.data());
-            restrict_sum(ctx, l.coarse, l.off.data(), l.mem.data(), l.r.data(), c.rhs.data());
+            if (fusing()) pr_ = {&l, &c, l.r.data()};  // taken by the coarse level's first op
+            else restrict_sum(ctx, l.coarse, l.off.data(), l.mem.data(), l.r.data(), c.rhs.data());
         }
     }
 
@@ -343,7 +364,9 @@ class HierarchyImpl final : public Hierarchy {
             s.coarse_rhs = c.rhs.data();
             rec_.push_back(s);
         } else if (!dry_) {
-            restrict_sum(ctx, l.coarse, l.off.data(), l.mem.data(), l.rhs.data(), c.rhs.data());
+            flush(ctx);
+            if (fusing()) pr_ = {&l, &c, l.rhs.data()};
+            else restrict_sum(ctx, l.coarse, l.off.data(), l.mem.data(), l.rhs.data(), c.rhs.data());
         }
     }
 
@@ -358,6 +381,11 @@ class HierarchyImpl final : public Hierarchy {
             s.e = c.x();
             rec_.push_back(s);
         } else if (!dry_) {
+            if (prolong_fusable(l, c)) {
+                launch_write(ctx, &l);
+                return;
+            }
+            flush(ctx);
             prolong_add(ctx, l.n, l.map.data(), c.x(), l.x());
         }
     }
@@ -372,7 +400,78 @@ class HierarchyImpl final : public Hierarchy {
             s.xout = l.x();
             rec_.push_back(s);
         } else if (!dry_) {
+            if (fusing()) {
+                // restriction into it (if pending) now, prolongation of it later
+                const PendingRestrict r = pr_.coarse == &l ? pr_ : PendingRestrict{};
+                if (r.coarse) pr_ = {};
+                flush(ctx);
+                pw_ = {kWriteDense, &l, nullptr, l.x(), r};
+                return;
+            }
             coarse_dense_apply(ctx, static_cast<int>(l.n), inv_.data(), l.rhs.data(), l.x());
+        }
+    }
+
+    // ---- transfer fusion (launch path) ----
+    // A restriction is held until the coarse level's first op, which takes it
+    // in (restrict_jacobi_zero, dense); a sweep or dense solve is held until
+    // the next op, which is its prolongation when fusable (jacobi_scatter,
+    // dense with scatter).  Anything held is launched before any other op, so
+    // the kernel order and every value are those of the unfused cycle.
+    struct PendingRestrict {
+        Level<S> *fine{nullptr}, *coarse{nullptr};
+        const S *src{nullptr};
+    };
+    static constexpr int kWriteNone = 0, kWriteSweep = 1, kWriteDense = 2;
+    struct PendingWrite {
+        int kind{kWriteNone};
+        Level<S> *l{nullptr};
+        const S *xin{nullptr};
+        S *xout{nullptr};
+        PendingRestrict r;
+    };
+
+    bool fusing() const { return fuse_ > 0 && !recording_ && !dry_; }
+
+    bool prolong_fusable(const Level<S> &l, const Level<S> &c) const {
+        return fusing() && pw_.kind != kWriteNone && pw_.l == &c && pw_.xout == c.x() &&
+               (fuse_ >= 2 || l.n <= kScatterRows);
+    }
+
+    // Launches the held write; with `fine` set, fused with the prolongation
+    // of its result into fine->x().
+    void launch_write(tf_ctx *ctx, Level<S> *fine) {
+        const PendingWrite w = pw_;
+        pw_ = {};
+        const int32_t *off = fine ? fine->off.data() : nullptr;
+        const int32_t *mem = fine ? fine->mem.data() : nullptr;
+        S *fx = fine ? fine->x() : nullptr;
+        Level<S> &l = *w.l;
+        if (w.kind == kWriteSweep) {
+            if (fine)
+                jacobi_sweep_scatter(ctx, l.csr(), l.dinv.data(), l.rhs.data(), w.xin, w.xout, w_, off, mem, fx);
+            else
+                jacobi_sweep(ctx, l.csr(), l.dinv.data(), l.rhs.data(), w.xin, w.xout, w_, nullptr, nullptr,
+                             static_cast<const S *>(nullptr));
+        } else if (w.kind == kWriteDense) {
+            if (!fine && !w.r.coarse) {
+                coarse_dense_apply(ctx, static_cast<int>(l.n), inv_.data(), l.rhs.data(), w.xout);
+                return;
+            }
+            const S *rf = w.r.coarse ? w.r.src : nullptr;
+            const int32_t *roff = w.r.coarse ? w.r.fine->off.data() : nullptr;
+            const int32_t *rmem = w.r.coarse ? w.r.fine->mem.data() : nullptr;
+            coarse_dense_apply_fused(ctx, static_cast<int>(l.n), inv_.data(), l.rhs.data(), w.xout, rf, roff, rmem,
+                                     off, mem, fx);
+        }
+    }
+
+    void flush(tf_ctx *ctx) {
+        if (pw_.kind != kWriteNone) launch_write(ctx, nullptr);
+        if (pr_.coarse) {
+            const PendingRestrict r = pr_;
+            pr_ = {};
+            restrict_sum(ctx, r.fine->coarse, r.fine->off.data(), r.fine->mem.data(), r.src, r.coarse->rhs.data());
         }
     }
 
@@ -396,6 +495,7 @@ class HierarchyImpl final : public Hierarchy {
     // visit counts).
     void cycle(tf_ctx *ctx, int kind, size_t d, bool zero) {
         if (recording_ || d != coop_from_) return cycle_body(ctx, kind, d, zero);
+        if (!dry_) flush(ctx);
         recording_ = true;
         const size_t start = rec_.size();
         cycle_body(ctx, kind, d, zero);
@@ -432,7 +532,11 @@ class HierarchyImpl final : public Hierarchy {
         cycle(ctx, kind, d + 1, true);
         if (kind == TF_CYCLE_W) cycle(ctx, kind, d + 1, false);
         const int post = cfg_.o.post_sweeps;
-        if (post > 0 && l.n <= kFusedProlongRows) {
+        if (prolong_fusable(l, c)) {
+            // x += P e fused into the coarse level's last kernel
+            op_prolong(ctx, l, c);
+            smooth(ctx, l, post, false);
+        } else if (post > 0 && l.n <= kFusedProlongRows) {
             // small level: x + P e read on the fly by the first sweep
             sweep(ctx, l, l.map.data(), c.x());
             smooth(ctx, l, post - 1, false);
@@ -469,6 +573,7 @@ class HierarchyImpl final : public Hierarchy {
     }
 
     static constexpr int64_t kFusedProlongRows = 131072;
+    static constexpr int64_t kScatterRows = 131072;
 
     AmgConfig cfg_;
     S w_;
@@ -484,6 +589,10 @@ class HierarchyImpl final : public Hierarchy {
     // cooperative small-level sub-cycles
     size_t coop_from_{~size_t(0)};
     bool recording_{false}, dry_{false};
+    // transfer fusion
+    int fuse_{1};
+    PendingRestrict pr_;
+    PendingWrite pw_;
     std::vector<CoarseStep<S>> rec_;
     std::vector<std::pair<size_t, size_t>> entries_;
     size_t entry_{0};

@@ -186,6 +186,39 @@ __global__ void dense_apply_kernel(int n, const double *__restrict__ inv, const 
     if (lane == 0) x[warp] = static_cast<T>(s);
 }
 
+// dense_apply_kernel between a restriction and a prolongation.  Every CTA
+// restricts all n (<= 256) coarse values itself (restrict_kernel's order);
+// CTA 0 stores them.
+template <class T>
+__global__ void dense_fused_kernel(int n, const double *__restrict__ inv, T *__restrict__ b, T *__restrict__ x,
+                                   const T *__restrict__ rfine, const int32_t *__restrict__ roff,
+                                   const int32_t *__restrict__ rmem, const int32_t *__restrict__ soff,
+                                   const int32_t *__restrict__ smem, T *__restrict__ fine) {
+    pdl_enter();
+    __shared__ T sb[256];
+    for (int c = threadIdx.x; c < n; c += blockDim.x) {
+        T v;
+        if (rfine) {
+            v = 0;
+            for (int32_t j = roff[c]; j < roff[c + 1]; ++j) v += rfine[rmem[j]];
+            if (blockIdx.x == 0) b[c] = v;
+        } else {
+            v = b[c];
+        }
+        sb[c] = v;
+    }
+    __syncthreads();
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (warp >= n) return;
+    double s = 0;
+    for (int j = lane; j < n; j += 32) s += inv[static_cast<int64_t>(warp) * n + j] * static_cast<double>(sb[j]);
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    const T v = static_cast<T>(__shfl_sync(0xffffffffu, s, 0));
+    if (lane == 0) x[warp] = v;
+    if (fine)
+        for (int32_t k = soff[warp] + lane; k < soff[warp + 1]; k += 32) fine[smem[k]] += v;
+}
+
 }  // namespace
 
 bool coarse_lu_factor(tf_ctx *ctx, const Csr<double, int32_t> &a, double *lu, int32_t *pivots) {
@@ -220,6 +253,20 @@ void coarse_dense_apply(tf_ctx *ctx, int n, const double *inv, const T *b, T *x)
                   b, x);
 }
 
+template <class T>
+void coarse_dense_apply_fused(tf_ctx *ctx, int n, const double *inv, T *b, T *x, const T *rfine, const int32_t *roff,
+                              const int32_t *rmem, const int32_t *soff, const int32_t *smem, T *fine) {
+    require(n >= 1 && n <= 256, "dense coarse solve requires order 1..256");
+    launch_kernel(ctx, "coarse_apply_fused", dense_fused_kernel<T>, grid_for(static_cast<int64_t>(n) * 32), kBlock, 0,
+                  n, inv, b, x, rfine, roff, rmem, soff, smem, fine);
+}
+
+template void coarse_dense_apply_fused<float>(tf_ctx *, int, const double *, float *, float *, const float *,
+                                              const int32_t *, const int32_t *, const int32_t *, const int32_t *,
+                                              float *);
+template void coarse_dense_apply_fused<double>(tf_ctx *, int, const double *, double *, double *, const double *,
+                                               const int32_t *, const int32_t *, const int32_t *, const int32_t *,
+                                               double *);
 template void coarse_lu_solve<float>(tf_ctx *, int, const double *, const int32_t *, const float *, float *);
 template void coarse_lu_solve<double>(tf_ctx *, int, const double *, const int32_t *, const double *, double *);
 template void coarse_dense_apply<float>(tf_ctx *, int, const double *, const float *, float *);

@@ -177,6 +177,9 @@ struct ResidualNorm {
     T *__restrict__ r;
     const int *gate;
     double *partial;
+    // Gated launches (residual refresh, early exit) rarely run: their
+    // kernels do not stream the matrix before the gate is read.
+    bool rarely_runs() const { return gate != nullptr; }
     __device__ __forceinline__ bool skip() const { return gate && !*gate; }
     template <class XS>
     __device__ __forceinline__ Pre pre(int64_t i, const XS &) const {

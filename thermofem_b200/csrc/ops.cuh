@@ -45,6 +45,15 @@ void residual(tf_ctx *ctx, const Csr<T, I> &a, const T *b, const T *x, T *r);
 template <class T, class I>
 void jacobi_sweep(tf_ctx *ctx, const Csr<T, I> &a, const T *dinv, const T *b, const T *x, T *xo, T w,
                   const float *row_w, const int32_t *map, const T *e);
+// xo = x + w Dinv (b - A x), and fine[mem[k]] += xo[c] for k in
+// [off[c], off[c+1]) (the prolongation of the result fused in).
+template <class T, class I>
+void jacobi_sweep_scatter(tf_ctx *ctx, const Csr<T, I> &a, const T *dinv, const T *b, const T *x, T *xo, T w,
+                          const int32_t *off, const int32_t *mem, T *fine);
+// b[c] = sum_k fine[mem[k]] (k in [off[c], off[c+1])), x = w Dinv b.
+template <class T>
+void restrict_jacobi_zero(tf_ctx *ctx, int64_t nc, const int32_t *off, const int32_t *mem, const T *fine, T *b,
+                          const T *dinv, T *x, T w);
 // x = w Dinv b
 template <class T>
 void jacobi_zero(tf_ctx *ctx, int64_t n, const T *dinv, const T *b, T *x, T w, const float *row_w);
@@ -101,6 +110,13 @@ void coarse_lu_solve(tf_ctx *ctx, int n, const double *lu, const int32_t *pivots
 void coarse_inverse(tf_ctx *ctx, int n, const double *lu, const int32_t *pivots, double *inv);
 template <class T>
 void coarse_dense_apply(tf_ctx *ctx, int n, const double *inv, const T *b, T *x);
+// coarse_dense_apply with the transfers around it fused in: when rfine is
+// set, b is first restricted from it (b[c] = sum of rfine over roff/rmem
+// members, stored); when fine is set, x is then prolonged into it
+// (fine[smem[k]] += x[c] over soff/smem members).
+template <class T>
+void coarse_dense_apply_fused(tf_ctx *ctx, int n, const double *inv, T *b, T *x, const T *rfine, const int32_t *roff,
+                              const int32_t *rmem, const int32_t *soff, const int32_t *smem, T *fine);
 
 inline Csr<double, int32_t> csr_of(const tf_dcsr &m) {
     Csr<double, int32_t> c;

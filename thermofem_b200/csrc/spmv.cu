@@ -72,6 +72,38 @@ struct JacobiOut {
     }
 };
 
+// A post-smoothing sweep of a coarse level that also applies the
+// prolongation of its result to the fine level: row c's new value is added
+// to x_fine at every member of aggregate c (fine[m] += coarse[c], the same
+// addition as prolong_kernel; each fine row belongs to one aggregate, so the
+// scatter has no conflicts and no ordering to fix).
+template <class T>
+struct JacobiScatter {
+    static constexpr int kReduce = 0;
+    struct Pre {
+        T x, d, b;
+        int32_t m0, m1;
+    };
+    const T *__restrict__ dinv;
+    const T *__restrict__ b;
+    T *__restrict__ xo;
+    T w;
+    const int32_t *__restrict__ off;  // aggregate -> members (fine rows)
+    const int32_t *__restrict__ mem;
+    T *__restrict__ fine;
+    double *partial{nullptr};
+    __device__ __forceinline__ bool skip() const { return false; }
+    template <class XS>
+    __device__ __forceinline__ Pre pre(int64_t i, const XS &xs) const {
+        return {xs(i), dinv[i], b[i], off[i], off[i + 1]};
+    }
+    __device__ __forceinline__ void operator()(int64_t i, T acc, const Pre &p, double (&)[1]) const {
+        const T v = p.x + w * p.d * (p.b - acc);
+        xo[i] = v;
+        for (int32_t k = p.m0; k < p.m1; ++k) fine[mem[k]] += v;
+    }
+};
+
 template <class T, class I, class XS, class Epi>
 void launch_tile(tf_ctx *ctx, const Csr<T, I> &a, const XS &xs, const Epi &epi, const char *name) {
     tile::launch(ctx, a, xs, epi, name);
@@ -113,6 +145,23 @@ __global__ void restrict_kernel(int64_t nc, const int32_t *__restrict__ off, con
     T s = 0;
     for (int32_t j = off[c]; j < off[c + 1]; ++j) s += fine[mem[j]];
     coarse[c] = s;
+}
+
+// Restriction of a fine vector into the coarse right-hand side fused with
+// the zero-guess sweep that follows it: b[c] = sum of fine[m] over the
+// members of aggregate c (restrict_kernel's order), x[c] = w d[c] b[c]
+// (jacobi_zero_kernel's expression).
+template <class T>
+__global__ void restrict_jacobi_zero_kernel(int64_t nc, const int32_t *__restrict__ off,
+                                            const int32_t *__restrict__ mem, const T *__restrict__ fine,
+                                            T *__restrict__ b, const T *__restrict__ dinv, T *__restrict__ x, T w) {
+    pdl_enter();
+    const int64_t c = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (c >= nc) return;
+    T s = 0;
+    for (int32_t j = off[c]; j < off[c + 1]; ++j) s += fine[mem[j]];
+    b[c] = s;
+    x[c] = w * dinv[c] * s;
 }
 
 template <class T>
@@ -317,6 +366,20 @@ void jacobi_sweep(tf_ctx *ctx, const Csr<T, I> &a, const T *dinv, const T *b, co
         launch_tile(ctx, a, PlainX<T>{x}, epi, "jacobi");
 }
 
+template <class T, class I>
+void jacobi_sweep_scatter(tf_ctx *ctx, const Csr<T, I> &a, const T *dinv, const T *b, const T *x, T *xo, T w,
+                          const int32_t *off, const int32_t *mem, T *fine) {
+    launch_tile(ctx, a, PlainX<T>{x}, JacobiScatter<T>{dinv, b, xo, w, off, mem, fine, nullptr}, "jacobi_scatter");
+}
+
+template <class T>
+void restrict_jacobi_zero(tf_ctx *ctx, int64_t nc, const int32_t *off, const int32_t *mem, const T *fine, T *b,
+                          const T *dinv, T *x, T w) {
+    if (!nc) return;
+    launch_kernel(ctx, "restrict_jacobi_zero", restrict_jacobi_zero_kernel<T>, grid_for(nc), kBlock, 0, nc, off, mem,
+                  fine, b, dinv, x, w);
+}
+
 template <class T>
 void jacobi_zero(tf_ctx *ctx, int64_t n, const T *dinv, const T *b, T *x, T w, const float *row_w) {
     if (!n) return;
@@ -427,6 +490,8 @@ bool row_stats(tf_ctx *ctx, const Csr<double, int32_t> &a, double *row_max) {
     template void residual<T, I>(tf_ctx *, const Csr<T, I> &, const T *, const T *, T *);                      \
     template void jacobi_sweep<T, I>(tf_ctx *, const Csr<T, I> &, const T *, const T *, const T *, T *, T,     \
                                      const float *, const int32_t *, const T *);                               \
+    template void jacobi_sweep_scatter<T, I>(tf_ctx *, const Csr<T, I> &, const T *, const T *, const T *, T *, T, \
+                                             const int32_t *, const int32_t *, T *);                           \
     template void inverse_diagonal<T, I>(tf_ctx *, const Csr<T, I> &, T *);                                    \
     template int csr_canonical_flags<T, I>(tf_ctx *, const Csr<T, I> &);
 TF_SPMV_INST(float, int32_t)
@@ -438,6 +503,8 @@ TF_SPMV_INST(double, int64_t)
 #define TF_VEC_INST(T)                                                                                        \
     template void jacobi_zero<T>(tf_ctx *, int64_t, const T *, const T *, T *, T, const float *);              \
     template void restrict_sum<T>(tf_ctx *, int64_t, const int32_t *, const int32_t *, const T *, T *);        \
+    template void restrict_jacobi_zero<T>(tf_ctx *, int64_t, const int32_t *, const int32_t *, const T *, T *,  \
+                                          const T *, T *, T);                                                  \
     template void prolong_add<T>(tf_ctx *, int64_t, const int32_t *, const T *, T *);                          \
     template void dot_multi<T>(tf_ctx *, int64_t, int, const T *const *, const T *const *, double *);           \
     template void axpby<T>(tf_ctx *, int64_t, double, const T *, double, T *);                                 \

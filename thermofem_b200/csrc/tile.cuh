@@ -600,6 +600,16 @@ void allow_smem(size_t bytes) {
 
 inline bool aligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
+// Epilogues whose launches are usually skipped say so (rarely_runs()).
+template <class E>
+auto rarely_runs(const E &e, int) -> decltype(e.rarely_runs()) {
+    return e.rarely_runs();
+}
+template <class E>
+bool rarely_runs(const E &, long) {
+    return false;
+}
+
 // Launches the pipelined kernel when the three arrays start on 16-byte
 // boundaries (every buffer this library allocates does), the staged kernel
 // otherwise.  Reducing epilogues need the pipelined kernel: it writes their
@@ -612,7 +622,7 @@ void launch(tf_ctx *ctx, const Csr<T, I> &a, const XS &xs, const Epi &epi, const
     if (pipe) {
         const PipeConfig cfg = force ? *force : tuned_config<T, I>(a.rows, a.nnz, ctx->sm_count);
         const PipeShape p = pipe_shape<T, I>(a.rows, a.nnz, ctx->sm_count, cfg);
-        const int early = ctx->stable ? 1 : 0;
+        const int early = ctx->stable && !rarely_runs(epi, 0) ? 1 : 0;
         if (p.rpt == 2) {
             allow_smem<csr_pipe_kernel<T, I, 2, XS, Epi>>(p.smem);
             launch_kernel(ctx, name, csr_pipe_kernel<T, I, 2, XS, Epi>, p.grid, kThreads + 32, p.smem, a.rows, a.nnz,
