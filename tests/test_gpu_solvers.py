@@ -335,3 +335,52 @@ def test_transfer_fusion_solve_and_small_level_program(ctx, monkeypatch):
     # sums in its own order: it must converge in about as many iterations
     assert res[2][0]["status"] == "Converged"
     assert abs(res[2][0]["iterations"] - res[0][0]["iterations"]) <= 2
+
+
+def _far_coupled_poisson(n):
+    # 1-D Poisson plus a symmetric coupling between the first and the last
+    # row: one entry lies n-1 rows from the diagonal, beyond the 2-byte
+    # column offsets, so the operator must keep its 4-byte column stream.
+    rows, cols, vals = [], [], []
+    for i in range(n):
+        d = 2.0 + (0.5 if i in (0, n - 1) else 0.0)
+        ent = {i: d}
+        if i > 0:
+            ent[i - 1] = -1.0
+        if i < n - 1:
+            ent[i + 1] = -1.0
+        if i == 0:
+            ent[n - 1] = -0.5
+        if i == n - 1:
+            ent[0] = -0.5
+        for j in sorted(ent):
+            rows.append(i)
+            cols.append(j)
+            vals.append(ent[j])
+    off = np.zeros(n + 1, np.int32)
+    np.add.at(off, np.array(rows) + 1, 1)
+    return np.cumsum(off).astype(np.int32), np.array(cols, np.int32), np.array(vals)
+
+
+@pytest.mark.parametrize("case", ["heat3d-cg", "heat3d-bicgstab", "far-coupling-cg"])
+def test_two_byte_column_stream_gives_identical_solves(ctx, case, monkeypatch):
+    # Operators whose couplings lie within 32767 rows of the diagonal are
+    # streamed with 2-byte column offsets; THERMOFEM_B200_DELTA16=0 keeps the
+    # 4-byte indices.  Same columns in the same order: the same bits.
+    if case.startswith("heat3d"):
+        m = P.heat3d(24, seed=81)
+    else:
+        m = _far_coupled_poisson(40000)
+    n = len(m[0]) - 1
+    b = torch.tensor(P.rhs_uniform(n, 82), device="cuda")
+    solver = tf.BiCgStab if case.endswith("bicgstab") else tf.Cg
+    out = []
+    for flag in ("1", "0"):
+        monkeypatch.setenv("THERMOFEM_B200_DELTA16", flag)
+        s = solver(tf.solver_options(), "amg", tf.amg_options(hierarchy_type="f32", jacobi_weight=2 / 3), ctx=ctx)
+        s.setup(to_device(m))
+        x = torch.zeros(n, dtype=torch.float64, device="cuda")
+        out.append((s.apply(b, x), x))
+    assert out[0][0]["status"] == "Converged"
+    assert out[0][0] == out[1][0]
+    assert torch.equal(out[0][1], out[1][1])

@@ -69,6 +69,7 @@ struct Level {
     DeviceBuffer<int32_t> rp, ci;
     DeviceBuffer<S> val, dinv, rhs, x0, x1, r;
     DeviceBuffer<int32_t> map, off, mem;
+    DeviceBuffer<int16_t> cd;  // columns as row offsets, when they fit
     int coarse{0};
     int cur{0};
     S *x() const { return cur ? x1.data() : x0.data(); }
@@ -80,6 +81,7 @@ struct Level {
         c.rp = rp.data();
         c.ci = ci.data();
         c.val = val.data();
+        c.cd = cd.data();
         return c;
     }
 };
@@ -122,6 +124,10 @@ class HierarchyImpl final : public Hierarchy {
             for (auto *b : {&l.dinv, &l.rhs, &l.x0, &l.x1, &l.r}) b->allocate(static_cast<size_t>(l.n));
             // The diagonal must also invert in the iteration precision.
             inverse_diagonal(ctx, l.csr(), l.dinv.data());
+            if (delta_columns_enabled() && l.nnz > 0) {
+                l.cd.allocate(static_cast<size_t>(l.nnz));
+                if (!delta_columns(ctx, l.n, l.rp.data(), l.ci.data(), l.cd.data())) l.cd.release();
+            }
             // Launch shape of this level's row-tile kernels (cached by shape).
             fill_zero(ctx, l.n, l.rhs.data());
             autotune_spmv(ctx, l.csr(), static_cast<const S *>(l.rhs.data()), l.r.data(), nullptr, nullptr, nullptr,

@@ -519,6 +519,11 @@ class KrylovImpl final : public Krylov {
         convert(ctx, n_ + 1, nc.rp, rp_.data());
         convert(ctx, nnz_, nc.ci, ci_.data());
         convert(ctx, nnz_, nc.val, val_.data());
+        cd_.release();
+        if (delta_columns_enabled() && nnz_ > 0) {
+            cd_.allocate(static_cast<size_t>(nnz_));
+            if (!delta_columns(ctx, n_, rp_.data(), ci_.data(), cd_.data())) cd_.release();
+        }
         hier_.reset();
         if (precond_ == TF_PRECOND_AMG) {
             const int storage = amg_cfg_->o.hierarchy_type == -1 ? (sizeof(T) == 8 ? TF_F64 : TF_F32)
@@ -611,6 +616,7 @@ class KrylovImpl final : public Krylov {
         c.rp = rp_.data();
         c.ci = ci_.data();
         c.val = val_.data();
+        c.cd = cd_.data();
         return c;
     }
 
@@ -802,6 +808,7 @@ class KrylovImpl final : public Krylov {
     bool ready_{false};
     int64_t n_{0}, nnz_{0};
     DeviceBuffer<I> rp_, ci_;
+    DeviceBuffer<int16_t> cd_;  // columns as row offsets, when they fit
     DeviceBuffer<T> val_;
     DeviceBuffer<T> rhs_, x_, r_, z_, p_, q_, shadow_, s_, t_, sh_;
     DeviceBuffer<double> part_, partb_;

@@ -14,6 +14,10 @@ struct Csr {
     const I *rp{nullptr};
     const I *ci{nullptr};
     const T *val{nullptr};
+    // Optional second copy of the columns as offsets from the row
+    // (ci[j] - row, int16): the pipelined row-tile kernels stream it instead
+    // of ci when set (see delta_columns).
+    const int16_t *cd{nullptr};
 };
 
 // Launch shape of the row-tile SpMV family: rows_per_tile consecutive rows
@@ -60,6 +64,13 @@ void jacobi_zero(tf_ctx *ctx, int64_t n, const T *dinv, const T *b, T *x, T w, c
 // Dinv from summed diagonal entries; throws TF_ERR_INVALID on a bad diagonal.
 template <class T, class I>
 void inverse_diagonal(tf_ctx *ctx, const Csr<T, I> &a, T *dinv);
+// cd[j] = ci[j] - row(j) as int16_t (the pipelined kernels' 2-byte column
+// stream).  False, with cd unusable, when a coupling lies more than 32767
+// rows from the diagonal.  THERMOFEM_B200_DELTA16=0 turns the stream off
+// (delta_columns_enabled() false).
+template <class I>
+bool delta_columns(tf_ctx *ctx, int64_t rows, const I *rp, const I *ci, int16_t *cd);
+bool delta_columns_enabled();
 template <class T>
 void restrict_sum(tf_ctx *ctx, int64_t nc, const int32_t *off, const int32_t *mem, const T *fine, T *coarse);
 template <class T>

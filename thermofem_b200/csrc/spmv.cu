@@ -7,6 +7,8 @@
 // 167-175) and SpMV + update (:26-32,251-269) as separate passes.  Each
 // epilogue's pre() loads the row's own operands (issued at the start of the
 // row's tile so their latency overlaps the gathers).
+#include <cstdlib>
+
 #include "tile.cuh"
 
 namespace tfb {
@@ -162,6 +164,22 @@ __global__ void restrict_jacobi_zero_kernel(int64_t nc, const int32_t *__restric
     for (int32_t j = off[c]; j < off[c + 1]; ++j) s += fine[mem[j]];
     b[c] = s;
     x[c] = w * dinv[c] * s;
+}
+
+template <class I>
+__global__ void delta_columns_kernel(int64_t n, const I *__restrict__ rp, const I *__restrict__ ci,
+                                     int16_t *__restrict__ cd, int *bad) {
+    pdl_enter();
+    const int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (i >= n) return;
+    for (I j = rp[i]; j < rp[i + 1]; ++j) {
+        const int64_t d = static_cast<int64_t>(ci[j]) - i;
+        if (d < -32767 || d > 32767) {
+            atomicExch(bad, 1);
+            return;
+        }
+        cd[j] = static_cast<int16_t>(d);
+    }
 }
 
 template <class T>
@@ -395,6 +413,22 @@ void inverse_diagonal(tf_ctx *ctx, const Csr<T, I> &a, T *dinv) {
                   a.ci, a.val, dinv, bad);
     if (read_scalar(ctx, bad)) fail(TF_ERR_INVALID, "Missing or invalid diagonal");
 }
+
+bool delta_columns_enabled() {
+    const char *v = std::getenv("THERMOFEM_B200_DELTA16");
+    return !(v && v[0] == '0');
+}
+
+template <class I>
+bool delta_columns(tf_ctx *ctx, int64_t rows, const I *rp, const I *ci, int16_t *cd) {
+    if (!rows) return false;
+    int *bad = static_cast<int *>(ctx->arena(sizeof(int), 1));
+    memset_async(ctx, bad, 0, sizeof(int));
+    launch_kernel(ctx, "delta_columns", delta_columns_kernel<I>, grid_for(rows), kBlock, 0, rows, rp, ci, cd, bad);
+    return read_scalar(ctx, bad) == 0;
+}
+template bool delta_columns<int32_t>(tf_ctx *, int64_t, const int32_t *, const int32_t *, int16_t *);
+template bool delta_columns<int64_t>(tf_ctx *, int64_t, const int64_t *, const int64_t *, int16_t *);
 
 template <class T>
 void restrict_sum(tf_ctx *ctx, int64_t nc, const int32_t *off, const int32_t *mem, const T *fine, T *coarse) {

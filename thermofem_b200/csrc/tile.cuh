@@ -16,6 +16,7 @@
 #include <map>
 #include <mutex>
 #include <tuple>
+#include <type_traits>
 
 #include "ops.cuh"
 
@@ -235,15 +236,16 @@ __device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t b
                  : "memory");
 }
 
-// Shared-memory layout of one stage: row offsets, values, column indices.
-template <class T, class I>
+// Shared-memory layout of one stage: row offsets (I), values (T), column
+// entries (C).
+template <class T, class I, class C = I>
 struct StageLayout {
-    static constexpr int kVT = 16 / sizeof(T), kVI = 16 / sizeof(I);
+    static constexpr int kVT = 16 / sizeof(T), kVI = 16 / sizeof(I), kVC = 16 / sizeof(C);
     int rp_bytes, val_bytes, col_bytes, bytes;
     __host__ __device__ StageLayout(int cap, int tile_rows) {
         rp_bytes = ((tile_rows + 1 + kVI) * static_cast<int>(sizeof(I)) + 15) & ~15;
         val_bytes = ((cap + 2 * kVT) * static_cast<int>(sizeof(T)) + 15) & ~15;
-        col_bytes = ((cap + 2 * kVI) * static_cast<int>(sizeof(I)) + 15) & ~15;
+        col_bytes = ((cap + 2 * kVC) * static_cast<int>(sizeof(C)) + 15) & ~15;
         bytes = (rp_bytes + val_bytes + col_bytes + 127) & ~127;
     }
 };
@@ -275,26 +277,37 @@ struct Range {
 // per 256-row block in the same warp and lane order, so reductions do not
 // depend on RPT.
 //
+// Column entries are stored as C: the column itself (C == I) or, for
+// int16_t, its offset from the row (column = row + entry), which cuts the
+// index stream from 4 to 2 bytes per nonzero for operators whose couplings
+// lie within 32767 rows of the diagonal.
+//
 // With early != 0 (the matrix is not written by any kernel still in flight)
 // the producer fills the first `stages` chunks before waiting for the
 // previous kernel of the stream (programmatic dependent launch), so the
 // matrix stream overlaps that kernel's tail; the consumers, which read x and
 // the epilogue operands, always wait first.
-template <class T, class I, int RPT, class XS, class Epi>
+template <class C>
+__device__ __forceinline__ int64_t column_of(int64_t row, C entry) {
+    if constexpr (std::is_same_v<C, int16_t>) return row + entry;
+    else return static_cast<int64_t>(entry);
+}
+
+template <class T, class I, class C, int RPT, class XS, class Epi>
 __global__ void __launch_bounds__(kThreads + 32) csr_pipe_kernel(int64_t rows, int64_t nnz, const I *__restrict__ rp,
-                                                                  const I *__restrict__ ci,
+                                                                  const C *__restrict__ ci,
                                                                   const T *__restrict__ val, int cap, int stages,
                                                                   int early, XS xs, Epi epi, int *fault) {
     constexpr int K = Epi::kReduce;
     constexpr int KK = K > 0 ? K : 1;
-    constexpr int kVT = 16 / sizeof(T), kVI = 16 / sizeof(I);
+    constexpr int kVT = 16 / sizeof(T), kVC = 16 / sizeof(C);
     constexpr int kTileRows = kThreads * RPT;
     constexpr int kWarps = kThreads / 32;
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ uint64_t full_bar[kMaxStages], empty_bar[kMaxStages];
     __shared__ double warp_sums[kMaxStages + 1][RPT][kWarps][KK];
     __shared__ int warp_done[kMaxStages + 1];
-    const StageLayout<T, I> L(cap, kTileRows);
+    const StageLayout<T, I, C> L(cap, kTileRows);
     const int tid = threadIdx.x;
     if (tid == 0) {
         for (int s = 0; s < stages; ++s) {
@@ -310,7 +323,7 @@ __global__ void __launch_bounds__(kThreads + 32) csr_pipe_kernel(int64_t rows, i
         return reinterpret_cast<T *>(smem + static_cast<size_t>(s) * L.bytes + L.rp_bytes);
     };
     auto stage_col = [&](int s) {
-        return reinterpret_cast<I *>(smem + static_cast<size_t>(s) * L.bytes + L.rp_bytes + L.val_bytes);
+        return reinterpret_cast<C *>(smem + static_cast<size_t>(s) * L.bytes + L.rp_bytes + L.val_bytes);
     };
     const int64_t ntiles = (rows + kTileRows - 1) / kTileRows;
     const int64_t nblocks = (rows + kThreads - 1) / kThreads;  // 256-row blocks = partial sums
@@ -350,7 +363,7 @@ __global__ void __launch_bounds__(kThreads + 32) csr_pipe_kernel(int64_t rows, i
                 else rr.plan(r0, r0, rows + 1);
                 Range<T> rv;
                 rv.plan(cs, ce, nnz);
-                Range<I> rc;
+                Range<C> rc;
                 rc.plan(cs, ce, nnz);
                 rr.plain(stage_rp(st), rp);
                 rv.plain(stage_val(st), val);
@@ -410,7 +423,7 @@ __global__ void __launch_bounds__(kThreads + 32) csr_pipe_kernel(int64_t rows, i
                 }
                 const int64_t cs = s + c * cap, ce = min(e, cs + cap);
                 const T *sv = stage_val(st) + (cs % kVT);  // sv[j - cs]
-                const I *sc = stage_col(st) + (cs % kVI);  // sc[j - cs]
+                const C *sc = stage_col(st) + (cs % kVC);  // sc[j - cs]
                 constexpr int kGather = 8;
                 int lo[RPT], hi[RPT];
                 T y[RPT][kGather];
@@ -421,7 +434,7 @@ __global__ void __launch_bounds__(kThreads + 32) csr_pipe_kernel(int64_t rows, i
 #pragma unroll
                     for (int u = 0; u < kGather; ++u) {
                         const int o = lo[k] + u;
-                        y[k][u] = o < hi[k] ? xs(static_cast<int64_t>(sc[o])) : T(0);
+                        y[k][u] = o < hi[k] ? xs(column_of(r0 + tid + k * kThreads, sc[o])) : T(0);
                     }
                 }
 #pragma unroll
@@ -437,7 +450,7 @@ __global__ void __launch_bounds__(kThreads + 32) csr_pipe_kernel(int64_t rows, i
 #pragma unroll
                         for (int u = 0; u < kGather; ++u) {
                             const int o = o0 + u;
-                            z[u] = o < hi[k] ? xs(static_cast<int64_t>(sc[o])) : T(0);
+                            z[u] = o < hi[k] ? xs(column_of(r0 + tid + k * kThreads, sc[o])) : T(0);
                         }
 #pragma unroll
                         for (int u = 0; u < kGather; ++u) {
@@ -517,14 +530,14 @@ struct PipeConfig {
     int stages{2}, ctas_per_sm{4}, cap_pct{125}, rpt{1};
 };
 
-template <class T, class I>
+template <class T, class I, class C = I>
 PipeShape pipe_shape(int64_t rows, int64_t nnz, int sm_count, const PipeConfig &cfg) {
     PipeShape p;
     p.rpt = cfg.rpt == 2 ? 2 : 1;
     const int tile_rows = kThreads * p.rpt;
     const int rp_bytes = ((tile_rows + 1 + 16 / static_cast<int>(sizeof(I))) * static_cast<int>(sizeof(I)) + 15) & ~15;
     const int stage_limit = 32768 * p.rpt;
-    const int max_cap = ((stage_limit - rp_bytes) / static_cast<int>(sizeof(T) + sizeof(I)) - 8) & ~63;
+    const int max_cap = ((stage_limit - rp_bytes) / static_cast<int>(sizeof(T) + sizeof(C)) - 8) & ~63;
     const int64_t mean_tile = rows > 0 ? (nnz * tile_rows + rows - 1) / rows : 0;
     int64_t cap = (mean_tile * cfg.cap_pct / 100 + 63) & ~int64_t(63);
     if (cap < 256) cap = 256;
@@ -532,7 +545,7 @@ PipeShape pipe_shape(int64_t rows, int64_t nnz, int sm_count, const PipeConfig &
     p.cap = static_cast<int>(cap);
     p.stages = cfg.stages;
     p.ctas_per_sm = cfg.ctas_per_sm;
-    p.smem = static_cast<size_t>(StageLayout<T, I>(p.cap, tile_rows).bytes) * p.stages;
+    p.smem = static_cast<size_t>(StageLayout<T, I, C>(p.cap, tile_rows).bytes) * p.stages;
     const int64_t ntiles = (rows + tile_rows - 1) / tile_rows;
     const int64_t g = static_cast<int64_t>(sm_count) * cfg.ctas_per_sm;
     p.grid = static_cast<int>(ntiles < g ? (ntiles < 1 ? 1 : ntiles) : g);
@@ -542,12 +555,14 @@ PipeShape pipe_shape(int64_t rows, int64_t nnz, int sm_count, const PipeConfig &
 // Number of partial sums a reducing launch writes: one per 256-row block.
 inline int partials(int64_t rows) { return static_cast<int>(rows > 0 ? (rows + kThreads - 1) / kThreads : 1); }
 
-// Process-wide cache of tuned configurations, keyed by the operator's shape.
+// Process-wide cache of tuned configurations, keyed by the operator's shape
+// and storage (value, row offset and column entry sizes).
 struct TuneKey {
     int64_t rows, nnz;
-    int vsize, isize, sm_count;
+    int vsize, isize, csize, sm_count;
     bool operator<(const TuneKey &o) const {
-        return std::tie(rows, nnz, vsize, isize, sm_count) < std::tie(o.rows, o.nnz, o.vsize, o.isize, o.sm_count);
+        return std::tie(rows, nnz, vsize, isize, csize, sm_count) <
+               std::tie(o.rows, o.nnz, o.vsize, o.isize, o.csize, o.sm_count);
     }
 };
 inline std::mutex &tune_mutex() {
@@ -558,16 +573,33 @@ inline std::map<TuneKey, PipeConfig> &tune_cache() {
     static std::map<TuneKey, PipeConfig> m;
     return m;
 }
-template <class T, class I>
+template <class T, class I, class C>
+TuneKey tune_key(int64_t rows, int64_t nnz, int sm_count) {
+    return TuneKey{rows, nnz, static_cast<int>(sizeof(T)), static_cast<int>(sizeof(I)), static_cast<int>(sizeof(C)),
+                   sm_count};
+}
+template <class T, class I, class C>
 PipeConfig tuned_config(int64_t rows, int64_t nnz, int sm_count) {
     std::lock_guard<std::mutex> lock(tune_mutex());
-    auto it = tune_cache().find(TuneKey{rows, nnz, static_cast<int>(sizeof(T)), static_cast<int>(sizeof(I)), sm_count});
+    auto it = tune_cache().find(tune_key<T, I, C>(rows, nnz, sm_count));
     return it == tune_cache().end() ? PipeConfig{} : it->second;
 }
-template <class T, class I>
+template <class T, class I, class C>
 void store_config(int64_t rows, int64_t nnz, int sm_count, const PipeConfig &cfg) {
     std::lock_guard<std::mutex> lock(tune_mutex());
-    tune_cache()[TuneKey{rows, nnz, static_cast<int>(sizeof(T)), static_cast<int>(sizeof(I)), sm_count}] = cfg;
+    tune_cache()[tune_key<T, I, C>(rows, nnz, sm_count)] = cfg;
+}
+
+inline bool aligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+// Calls f(cols) with the column stream the pipelined kernel reads for a:
+// the 2-byte row offsets when the operator carries them, else the indices.
+template <class T, class I, class F>
+decltype(auto) with_columns(const Csr<T, I> &a, F &&f) {
+    if constexpr (std::is_same_v<I, int32_t>) {
+        if (a.cd && aligned16(a.cd)) return f(a.cd);
+    }
+    return f(a.ci);
 }
 
 // Validates and caches a launch shape for operators of a's shape.
@@ -577,9 +609,12 @@ void configure(tf_ctx *ctx, const Csr<T, I> &a, const PipeConfig &cfg) {
     require(cfg.stages >= 2 && cfg.stages <= kMaxStages, "stages must be 2..4");
     require(cfg.ctas_per_sm >= 1 && cfg.ctas_per_sm <= 8, "ctas_per_sm must be 1..8");
     require(cfg.cap_pct >= 50 && cfg.cap_pct <= 400, "cap_pct must be 50..400");
-    const PipeShape p = pipe_shape<T, I>(a.rows, a.nnz, ctx->sm_count, cfg);
-    require(p.smem <= 200 * 1024, "stage ring exceeds shared memory");
-    store_config<T, I>(a.rows, a.nnz, ctx->sm_count, cfg);
+    with_columns(a, [&](auto cols) {
+        using C = std::remove_cv_t<std::remove_pointer_t<decltype(cols)>>;
+        const PipeShape p = pipe_shape<T, I, C>(a.rows, a.nnz, ctx->sm_count, cfg);
+        require(p.smem <= 200 * 1024, "stage ring exceeds shared memory");
+        store_config<T, I, C>(a.rows, a.nnz, ctx->sm_count, cfg);
+    });
 }
 
 // Opts the instantiation into the dynamic shared memory it is launched with
@@ -598,8 +633,6 @@ void allow_smem(size_t bytes) {
     configured_bytes = bytes;
 }
 
-inline bool aligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
-
 // Epilogues whose launches are usually skipped say so (rarely_runs()).
 template <class E>
 auto rarely_runs(const E &e, int) -> decltype(e.rarely_runs()) {
@@ -610,28 +643,34 @@ bool rarely_runs(const E &, long) {
     return false;
 }
 
-// Launches the pipelined kernel when the three arrays start on 16-byte
-// boundaries (every buffer this library allocates does), the staged kernel
-// otherwise.  Reducing epilogues need the pipelined kernel: it writes their
-// partial sums per 256-row block (tile::partials).
+template <class T, class I, class C, class XS, class Epi>
+void launch_pipe(tf_ctx *ctx, const Csr<T, I> &a, const C *cols, const XS &xs, const Epi &epi, const char *name,
+                 const PipeConfig *force) {
+    const PipeConfig cfg = force ? *force : tuned_config<T, I, C>(a.rows, a.nnz, ctx->sm_count);
+    const PipeShape p = pipe_shape<T, I, C>(a.rows, a.nnz, ctx->sm_count, cfg);
+    const int early = ctx->stable && !rarely_runs(epi, 0) ? 1 : 0;
+    if (p.rpt == 2) {
+        allow_smem<csr_pipe_kernel<T, I, C, 2, XS, Epi>>(p.smem);
+        launch_kernel(ctx, name, csr_pipe_kernel<T, I, C, 2, XS, Epi>, p.grid, kThreads + 32, p.smem, a.rows, a.nnz,
+                      a.rp, cols, a.val, p.cap, p.stages, early, xs, epi, ctx->fault);
+    } else {
+        allow_smem<csr_pipe_kernel<T, I, C, 1, XS, Epi>>(p.smem);
+        launch_kernel(ctx, name, csr_pipe_kernel<T, I, C, 1, XS, Epi>, p.grid, kThreads + 32, p.smem, a.rows, a.nnz,
+                      a.rp, cols, a.val, p.cap, p.stages, early, xs, epi, ctx->fault);
+    }
+}
+
+// Launches the pipelined kernel when the arrays start on 16-byte boundaries
+// (every buffer this library allocates does), the staged kernel otherwise.
+// Reducing epilogues need the pipelined kernel: it writes their partial sums
+// per 256-row block (tile::partials).
 template <class T, class I, class XS, class Epi>
 void launch(tf_ctx *ctx, const Csr<T, I> &a, const XS &xs, const Epi &epi, const char *name,
             const PipeConfig *force = nullptr) {
     if (a.rows == 0) return;
     const bool pipe = aligned16(a.rp) && (a.nnz == 0 || (aligned16(a.ci) && aligned16(a.val)));
     if (pipe) {
-        const PipeConfig cfg = force ? *force : tuned_config<T, I>(a.rows, a.nnz, ctx->sm_count);
-        const PipeShape p = pipe_shape<T, I>(a.rows, a.nnz, ctx->sm_count, cfg);
-        const int early = ctx->stable && !rarely_runs(epi, 0) ? 1 : 0;
-        if (p.rpt == 2) {
-            allow_smem<csr_pipe_kernel<T, I, 2, XS, Epi>>(p.smem);
-            launch_kernel(ctx, name, csr_pipe_kernel<T, I, 2, XS, Epi>, p.grid, kThreads + 32, p.smem, a.rows, a.nnz,
-                          a.rp, a.ci, a.val, p.cap, p.stages, early, xs, epi, ctx->fault);
-        } else {
-            allow_smem<csr_pipe_kernel<T, I, 1, XS, Epi>>(p.smem);
-            launch_kernel(ctx, name, csr_pipe_kernel<T, I, 1, XS, Epi>, p.grid, kThreads + 32, p.smem, a.rows, a.nnz,
-                          a.rp, a.ci, a.val, p.cap, p.stages, early, xs, epi, ctx->fault);
-        }
+        with_columns(a, [&](auto cols) { launch_pipe(ctx, a, cols, xs, epi, name, force); });
         return;
     }
     require(Epi::kReduce == 0, "reducing SpMV epilogues need 16-byte aligned CSR arrays");
@@ -680,15 +719,10 @@ inline bool tune_log() {
     return on;
 }
 
-// Times the feasible rows per thread, ring depths, CTAs per SM and chunk capacities on this
-// operator (two warm-up and five timed launches each, CUDA events on the
-// context stream) and caches the fastest for every later launch over an
-// operator of the same shape.  y is overwritten.
-template <class T, class I>
-PipeConfig autotune(tf_ctx *ctx, const Csr<T, I> &a, const T *x, T *y, float *best_ms) {
+template <class T, class I, class C>
+PipeConfig autotune_columns(tf_ctx *ctx, const Csr<T, I> &a, const T *x, T *y, float *best_ms) {
     PipeConfig best{};
     float best_t = 0;
-    if (a.rows == 0 || !aligned16(a.rp) || (a.nnz && (!aligned16(a.ci) || !aligned16(a.val)))) return best;
     cudaEvent_t e0, e1;
     cuda_check(cudaEventCreate(&e0), "event");
     cuda_check(cudaEventCreate(&e1), "event");
@@ -698,21 +732,21 @@ PipeConfig autotune(tf_ctx *ctx, const Csr<T, I> &a, const T *x, T *y, float *be
             for (int ctas : {1, 2, 3, 4, 5, 6}) {
                 for (int pct : {100, 125}) {
                     const PipeConfig cfg{stages, ctas, pct, rpt};
-                    const PipeShape p = pipe_shape<T, I>(a.rows, a.nnz, ctx->sm_count, cfg);
+                    const PipeShape p = pipe_shape<T, I, C>(a.rows, a.nnz, ctx->sm_count, cfg);
                     if (p.smem * ctas > 220 * 1024) continue;
                     if ((rpt == 1 && ctas < 2) || (rpt == 2 && ctas > 3)) continue;
                     int resident = 0;
                     if (rpt == 2) {
-                        allow_smem<csr_pipe_kernel<T, I, 2, PlainX<T>, TuneStore<T>>>(p.smem);
+                        allow_smem<csr_pipe_kernel<T, I, C, 2, PlainX<T>, TuneStore<T>>>(p.smem);
                         cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                                       &resident, csr_pipe_kernel<T, I, 2, PlainX<T>, TuneStore<T>>, kThreads + 32,
-                                       p.smem),
+                                       &resident, csr_pipe_kernel<T, I, C, 2, PlainX<T>, TuneStore<T>>,
+                                       kThreads + 32, p.smem),
                                    "occupancy");
                     } else {
-                        allow_smem<csr_pipe_kernel<T, I, 1, PlainX<T>, TuneStore<T>>>(p.smem);
+                        allow_smem<csr_pipe_kernel<T, I, C, 1, PlainX<T>, TuneStore<T>>>(p.smem);
                         cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                                       &resident, csr_pipe_kernel<T, I, 1, PlainX<T>, TuneStore<T>>, kThreads + 32,
-                                       p.smem),
+                                       &resident, csr_pipe_kernel<T, I, C, 1, PlainX<T>, TuneStore<T>>,
+                                       kThreads + 32, p.smem),
                                    "occupancy");
                     }
                     if (resident < ctas) continue;
@@ -727,9 +761,11 @@ PipeConfig autotune(tf_ctx *ctx, const Csr<T, I> &a, const T *x, T *y, float *be
                     cuda_check(cudaEventElapsedTime(&ms, e0, e1), "event");
                     if (tune_log())
                         std::fprintf(stderr,
-                                     "tf_autotune_spmv rows=%lld nnz=%lld T=%d rpt=%d stages=%d ctas=%d cap=%d%% %.2f us\n",
+                                     "tf_autotune_spmv rows=%lld nnz=%lld T=%d C=%d rpt=%d stages=%d ctas=%d cap=%d%% "
+                                     "%.2f us\n",
                                      static_cast<long long>(a.rows), static_cast<long long>(a.nnz),
-                                     static_cast<int>(sizeof(T)), rpt, stages, ctas, pct, ms * 1e3f / 5);
+                                     static_cast<int>(sizeof(T)), static_cast<int>(sizeof(C)), rpt, stages, ctas, pct,
+                                     ms * 1e3f / 5);
                     if (first || ms < best_t) {
                         best_t = ms;
                         best = cfg;
@@ -742,9 +778,22 @@ PipeConfig autotune(tf_ctx *ctx, const Csr<T, I> &a, const T *x, T *y, float *be
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     check_faults(ctx);
-    store_config<T, I>(a.rows, a.nnz, ctx->sm_count, best);
+    store_config<T, I, C>(a.rows, a.nnz, ctx->sm_count, best);
     if (best_ms) *best_ms = best_t / 5.0f;
     return best;
+}
+
+// Times the feasible rows per thread, ring depths, CTAs per SM and chunk
+// capacities on this operator (two warm-up and five timed launches each,
+// CUDA events on the context stream) and caches the fastest for every later
+// launch over an operator of the same shape and storage.  y is overwritten.
+template <class T, class I>
+PipeConfig autotune(tf_ctx *ctx, const Csr<T, I> &a, const T *x, T *y, float *best_ms) {
+    if (a.rows == 0 || !aligned16(a.rp) || (a.nnz && (!aligned16(a.ci) || !aligned16(a.val)))) return PipeConfig{};
+    return with_columns(a, [&](auto cols) {
+        using C = std::remove_cv_t<std::remove_pointer_t<decltype(cols)>>;
+        return autotune_columns<T, I, C>(ctx, a, x, y, best_ms);
+    });
 }
 
 }  // namespace tile
