@@ -152,6 +152,10 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def _small(args):
+    return {} if args.small_level_rows is None else {"small_level_rows": args.small_level_rows}
+
+
 def run_profile(args):
     """The kernels of whole solves, for an ncu launch list: setup and warm-up
     solves first (skip their launches with ncu -s), then args.steps solves."""
@@ -165,7 +169,8 @@ def run_profile(args):
     b = torch.tensor(P.rhs_uniform(n, SEED_RHS), device="cuda")
     x = torch.zeros(n, dtype=torch.float64, device="cuda")
     s = tf.Cg(tf.solver_options(), "amg",
-              tf.amg_options(hierarchy_type="f32" if args.profile == "mixed" else "f64", **AMG), ctx=ctx)
+              tf.amg_options(hierarchy_type="f32" if args.profile == "mixed" else "f64", **AMG, **_small(args)),
+              ctx=ctx)
     s.setup(a)
     s.set_graph_mode(0)  # per-iteration graphs: ncu cannot profile inside conditional graph nodes
     ctx.synchronize()
@@ -192,6 +197,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="thermofem", choices=["thermofem", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    ap.add_argument("--small-level-rows", type=int, default=None,
+                    help="tf_amg_options.small_level_rows (default: the library default)")
     ap.add_argument("--profile", choices=["mixed", "fp64"], default=None,
                     help="profiling run: setup, --warmup solves, then --steps solves of one path; no JSON line")
     args = ap.parse_args()
@@ -226,7 +233,7 @@ def main():
     opts = tf.solver_options(torch.float64)
 
     def make(hier):
-        s = tf.Cg(opts, "amg", tf.amg_options(hierarchy_type=hier, **AMG), ctx=ctx)
+        s = tf.Cg(opts, "amg", tf.amg_options(hierarchy_type=hier, **AMG, **_small(args)), ctx=ctx)
         torch.cuda.synchronize(dev)
         t0 = time.perf_counter()
         s.setup(a)

@@ -276,9 +276,20 @@ class HierarchyImpl final : public Hierarchy {
         if (!dry_) flush(ctx);
     }
 
-    // ---- level operations: launched, or recorded as a cooperative step ----
+    // ---- level operations: launched, or recorded as a small-level program step ----
     void op_jacobi_zero(tf_ctx *ctx, Level<S> &l) {
         if (recording_) {
+            if (rec_.size() > region_start_) {
+                CoarseStep<S> &prev = rec_.back();
+                if ((prev.op == kStepResidualRestrict || prev.op == kStepRestrict) && prev.coarse_rhs == l.rhs.data() &&
+                    !prev.cx) {
+                    // the restriction's pass also does this zero-guess sweep
+                    prev.cdinv = l.dinv.data();
+                    prev.cx = l.x();
+                    prev.cw = w_;
+                    return;
+                }
+            }
             CoarseStep<S> s;
             s.op = kStepJacobiZero;
             s.n = static_cast<int>(l.n);
@@ -428,13 +439,16 @@ class HierarchyImpl final : public Hierarchy {
         Level<S> *fine{nullptr}, *coarse{nullptr};
         const S *src{nullptr};
     };
-    static constexpr int kWriteNone = 0, kWriteSweep = 1, kWriteDense = 2;
+    static constexpr int kWriteNone = 0, kWriteSweep = 1, kWriteDense = 2, kWriteProgram = 3;
     struct PendingWrite {
         int kind{kWriteNone};
         Level<S> *l{nullptr};
         const S *xin{nullptr};
         S *xout{nullptr};
         PendingRestrict r;
+        // kWriteProgram: recorded small-level program and its entry transfer
+        size_t prog_off{0}, prog_count{0};
+        ProgramIO<S> io;
     };
 
     bool fusing() const { return fuse_ > 0 && !recording_ && !dry_; }
@@ -453,6 +467,14 @@ class HierarchyImpl final : public Hierarchy {
         const int32_t *mem = fine ? fine->mem.data() : nullptr;
         S *fx = fine ? fine->x() : nullptr;
         Level<S> &l = *w.l;
+        if (w.kind == kWriteProgram) {
+            ProgramIO<S> io = w.io;
+            io.soff = off;
+            io.smem = mem;
+            io.sfine = fx;
+            launch_coarse_program<S>(ctx, programs_.data() + w.prog_off, static_cast<int>(w.prog_count), io, cluster_);
+            return;
+        }
         if (w.kind == kWriteSweep) {
             if (fine)
                 jacobi_sweep_scatter(ctx, l.csr(), l.dinv.data(), l.rhs.data(), w.xin, w.xout, w_, off, mem, fx);
@@ -496,14 +518,27 @@ class HierarchyImpl final : public Hierarchy {
     }
 
     // Entering the first small level starts a recorded sub-cycle that runs as
-    // one cooperative launch (its program was recorded by the setup dry run;
-    // the recursion here replays the same steps to keep ping-pong state and
-    // visit counts).
+    // one cluster launch (its program was recorded by the setup dry run; the
+    // recursion here replays the same steps to keep ping-pong state and visit
+    // counts).  A restriction into the level that is still held goes into the
+    // launch; the launch itself is held like a sweep, so that the
+    // prolongation of its result can go into it too.
     void cycle(tf_ctx *ctx, int kind, size_t d, bool zero) {
         if (recording_ || d != coop_from_) return cycle_body(ctx, kind, d, zero);
+        Level<S> &l = levels_[d];
+        ProgramIO<S> io;
+        if (!dry_ && fusing() && pr_.coarse == &l) {
+            io.rsrc = pr_.src;
+            io.roff = pr_.fine->off.data();
+            io.rmem = pr_.fine->mem.data();
+            io.rrhs = l.rhs.data();
+            io.rn = static_cast<int>(l.n);
+            pr_ = {};
+        }
         if (!dry_) flush(ctx);
         recording_ = true;
         const size_t start = rec_.size();
+        region_start_ = start;
         cycle_body(ctx, kind, d, zero);
         recording_ = false;
         if (dry_) {
@@ -511,8 +546,21 @@ class HierarchyImpl final : public Hierarchy {
             return;
         }
         const auto [off, count] = entries_.at(entry_++);
+        const CoarseStep<S> last = rec_.back();
         rec_.resize(start);
-        launch_coarse_program<S>(ctx, programs_.data() + off, static_cast<int>(count), barrier_.data(), coop_grid_);
+        PendingWrite w;
+        w.kind = kWriteProgram;
+        w.l = &l;
+        w.prog_off = off;
+        w.prog_count = count;
+        w.io = io;
+        if (fusing() && (last.op == kStepSweep || last.op == kStepDense) && last.xout == l.x()) {
+            w.xout = l.x();
+            pw_ = w;
+        } else {
+            pw_ = w;
+            launch_write(ctx, nullptr);
+        }
     }
 
     void cycle_body(tf_ctx *ctx, int kind, size_t d, bool zero) {
@@ -555,7 +603,7 @@ class HierarchyImpl final : public Hierarchy {
         }
     }
 
-    // Records the cooperative programs of every small-level sub-cycle of one
+    // Records the cluster programs of every small-level sub-cycle of one
     // cycle (a dry run: nothing is launched) and uploads them.
     void plan_small_levels(tf_ctx *ctx) {
         coop_from_ = levels_.size();
@@ -565,7 +613,7 @@ class HierarchyImpl final : public Hierarchy {
                 break;
             }
         if (coop_from_ == levels_.size()) return;
-        coop_grid_ = coarse_grid_size<S>(ctx->sm_count, levels_[coop_from_].n);
+        cluster_ = coarse_cluster_size<S>();
         entries_.clear();
         dry_ = true;
         enqueue(ctx);
@@ -573,8 +621,6 @@ class HierarchyImpl final : public Hierarchy {
         programs_.allocate(rec_.size());
         cuda_check(cudaMemcpy(programs_.data(), rec_.data(), rec_.size() * sizeof(CoarseStep<S>), cudaMemcpyHostToDevice),
                    "coarse program upload");
-        barrier_.allocate(3);
-        cuda_check(cudaMemset(barrier_.data(), 0, 3 * sizeof(unsigned)), "coarse barrier");
         rec_.clear();
     }
 
@@ -592,7 +638,7 @@ class HierarchyImpl final : public Hierarchy {
     int64_t per_cycle_{0};
     std::vector<int> final_cur_;
     std::vector<int64_t> captured_visits_;
-    // cooperative small-level sub-cycles
+    // small-level sub-cycles (one cluster launch each)
     size_t coop_from_{~size_t(0)};
     bool recording_{false}, dry_{false};
     // transfer fusion
@@ -603,8 +649,8 @@ class HierarchyImpl final : public Hierarchy {
     std::vector<std::pair<size_t, size_t>> entries_;
     size_t entry_{0};
     DeviceBuffer<CoarseStep<S>> programs_;
-    DeviceBuffer<unsigned> barrier_;
-    int coop_grid_{0};
+    int cluster_{1};
+    size_t region_start_{0};
 };
 
 }  // namespace

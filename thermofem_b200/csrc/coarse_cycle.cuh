@@ -1,10 +1,10 @@
-// coarse_cycle.cuh -- program steps of the cooperative small-level cycle.
+// coarse_cycle.cuh -- program steps of the small-level cycle (one cluster launch).
 #pragma once
 #include "ops.cuh"
 
 namespace tfb {
 
-constexpr int kCoarseThreads = 512;
+constexpr int kClusterThreads = 1024;
 
 enum CoarseOp : int {
     kStepZero = 0,              // xout = 0
@@ -32,14 +32,36 @@ struct CoarseStep {
     const int32_t *off{nullptr}, *mem{nullptr};
     S *coarse_rhs{nullptr};
     const double *inv{nullptr};
+    // Restrictions only: with cx set, the coarse level's zero-guess sweep is
+    // done in the same pass, cx[c] = cw * cdinv[c] * coarse_rhs[c].
+    const S *cdinv{nullptr};
+    S *cx{nullptr};
+    S cw{0};
 };
 
-// CTAs of the cooperative launch (all resident at once).
+// Transfers around one launch of a program.  With rsrc set, the first
+// step's level first receives rrhs[c] = sum of rsrc over the members
+// roff/rmem of aggregate c (fused into the first step when that is the
+// level's zero-guess sweep).  With sfine set, the last step (a sweep or the
+// dense solve) adds each new value xout[c] to sfine at the members soff/smem
+// of aggregate c.
 template <class S>
-int coarse_grid_size(int sm_count, int64_t max_rows);
+struct ProgramIO {
+    const S *rsrc{nullptr};
+    const int32_t *roff{nullptr}, *rmem{nullptr};
+    S *rrhs{nullptr};
+    int rn{0};
+    const int32_t *soff{nullptr}, *smem{nullptr};
+    S *sfine{nullptr};
+};
 
-// barrier: 3 device words (arrival count, generation, abort), zeroed once.
+// CTAs of the cluster that runs the program: the largest cluster (16, 8, 4,
+// 2 or 1 CTAs of kClusterThreads) the device can schedule.
 template <class S>
-void launch_coarse_program(tf_ctx *ctx, const CoarseStep<S> *program, int steps, unsigned *barrier, int grid);
+int coarse_cluster_size();
+
+template <class S>
+void launch_coarse_program(tf_ctx *ctx, const CoarseStep<S> *program, int steps, const ProgramIO<S> &io,
+                           int cluster);
 
 }  // namespace tfb
