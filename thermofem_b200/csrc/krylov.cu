@@ -5,10 +5,11 @@
 // BiCGStab: include/Solver/BiCgStab.cuh:144-247), including the
 // breakdown/non-finite checks, the true-residual confirmation of a candidate
 // convergence and the periodic refresh with restart.  The difference is
-// where it runs: each scalar decision is a one-CTA kernel that finishes a
-// deterministic reduction and updates a device-resident state record, and
-// the vector kernels are gated on that record, so one iteration is a fixed
-// kernel sequence captured once into a CUDA graph.  Reductions are fused
+// where it runs: each scalar decision runs in the last CTA of the reduction
+// it consumes (a device ticket; tile::finish), which adds the partial sums in
+// a fixed order and updates a device-resident state record, and the vector
+// kernels are gated on that record, so one iteration is a fixed kernel
+// sequence captured once into a CUDA graph.  Reductions are fused
 // into the producing pass (p.Ap into the SpMV that makes Ap, ||r||^2 into the
 // x/r update, t.t and t.s into the SpMV that makes t).  The host reads one
 // word per iteration to stop the loop.
@@ -23,6 +24,7 @@ enum : int { kRunning = -1 };
 struct KState {
     double normB, tol, res, rho, rho_prev, alpha, omega, beta, curv;
     int it, status, running, fresh, pmode, refresh, early, normal, copy_shadow, max_it, interval;
+    unsigned tickets[8];  // last-CTA tickets of the reductions (zero between launches)
 };
 
 constexpr int kParts = 1184;  // upper bound of grid-stride partial sums
@@ -32,13 +34,26 @@ int parts_for(int64_t n) {
     return static_cast<int>(p < 1 ? 1 : (p > kParts ? kParts : p));
 }
 
-// Fixed-order sum of K partial arrays [K][parts]; valid in thread 0.
+// Fixed-order sum of K partial arrays [K][parts]; valid in thread 0.  Each
+// thread adds entries t, t + blockDim, t + 2 blockDim, ... in that order, the
+// loads issued eight at a time (they come from L2, written by other CTAs).
 template <int K>
 __device__ __forceinline__ void sum_partials(const double *part, int parts, double (&v)[K]) {
+    constexpr int kBatch = 8;
+    const int step = static_cast<int>(blockDim.x);
 #pragma unroll
     for (int k = 0; k < K; ++k) {
         v[k] = 0.0;
-        for (int p = threadIdx.x; p < parts; p += blockDim.x) v[k] += part[k * parts + p];
+        for (int p0 = threadIdx.x; p0 < parts; p0 += step * kBatch) {
+            double t[kBatch];
+#pragma unroll
+            for (int u = 0; u < kBatch; ++u) {
+                const int p = p0 + u * step;
+                t[u] = p < parts ? __ldcg(part + k * parts + p) : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < kBatch; ++u) v[k] += t[u];
+        }
     }
     tile::block_reduce<K>(v);
 }
@@ -109,8 +124,8 @@ __global__ void k_set_continue(cudaGraphConditionalHandle handle, const KState *
     cudaGraphSetConditional(handle, (s->running && s->it < s->max_it) ? 1u : 0u);
 }
 
-template <class T>
-__global__ void k_dot(int64_t n, const T *__restrict__ x, const T *__restrict__ y, double *part) {
+template <class T, class Fin = tile::NoFinal>
+__global__ void k_dot(int64_t n, const T *__restrict__ x, const T *__restrict__ y, double *part, Fin fin = {}) {
     pdl_enter();
     double v[1] = {0.0};
     for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
@@ -118,10 +133,11 @@ __global__ void k_dot(int64_t n, const T *__restrict__ x, const T *__restrict__ 
         v[0] += static_cast<double>(x[i]) * static_cast<double>(y[i]);
     tile::block_reduce<1>(v);
     if (threadIdx.x == 0) part[blockIdx.x] = v[0];
+    tile::finish(fin, part, gridDim.x);
 }
 
 // y = A x with sum_i w_i y_i; gated on *gate.
-template <class T>
+template <class T, class Fin = tile::NoFinal>
 struct SpmvDot {
     static constexpr int kReduce = 1;
     struct Pre {
@@ -131,6 +147,7 @@ struct SpmvDot {
     const T *__restrict__ w;
     const int *gate;
     double *partial;
+    Fin fin{};  // scalar step run by the last CTA
     __device__ __forceinline__ bool skip() const { return gate && !*gate; }
     template <class XS>
     __device__ __forceinline__ Pre pre(int64_t i, const XS &) const {
@@ -143,7 +160,7 @@ struct SpmvDot {
 };
 
 // t = A x with sum t_i^2 and sum t_i s_i; gated.
-template <class T>
+template <class T, class Fin = tile::NoFinal>
 struct SpmvDot2 {
     static constexpr int kReduce = 2;
     struct Pre {
@@ -153,6 +170,7 @@ struct SpmvDot2 {
     const T *__restrict__ s;
     const int *gate;
     double *partial;
+    Fin fin{};  // scalar step run by the last CTA
     __device__ __forceinline__ bool skip() const { return gate && !*gate; }
     template <class XS>
     __device__ __forceinline__ Pre pre(int64_t i, const XS &) const {
@@ -167,7 +185,7 @@ struct SpmvDot2 {
 };
 
 // r = b - A x with sum r_i^2; gated (gate may be null).
-template <class T>
+template <class T, class Fin = tile::NoFinal>
 struct ResidualNorm {
     static constexpr int kReduce = 1;
     struct Pre {
@@ -177,6 +195,7 @@ struct ResidualNorm {
     T *__restrict__ r;
     const int *gate;
     double *partial;
+    Fin fin{};  // scalar step run by the last CTA
     // Gated launches (residual refresh, early exit) rarely run: their
     // kernels do not stream the matrix before the gate is read.
     bool rarely_runs() const { return gate != nullptr; }
@@ -194,8 +213,7 @@ struct ResidualNorm {
 
 // ---- PCG -----------------------------------------------------------------
 
-__global__ void cg_rho(KState *s, const double *part, int parts) {
-    pdl_enter();
+__device__ void cg_rho_step(KState *s, const double *part, int parts) {
     if (!s->running) return;
     double v[1];
     sum_partials<1>(part, parts, v);
@@ -227,8 +245,7 @@ __global__ void cg_p(const KState *s, int64_t n, const T *__restrict__ z, T *__r
         p[i] = mode ? z[i] + beta * p[i] : z[i];
 }
 
-__global__ void cg_curv(KState *s, const double *part, int parts) {
-    pdl_enter();
+__device__ void cg_curv_step(KState *s, const double *part, int parts) {
     if (!s->running) return;
     double v[1];
     sum_partials<1>(part, parts, v);
@@ -242,9 +259,9 @@ __global__ void cg_curv(KState *s, const double *part, int parts) {
     s->alpha = alpha;
 }
 
-template <class T>
+template <class T, class Fin>
 __global__ void cg_xr(const KState *s, int64_t n, const T *__restrict__ p, const T *__restrict__ ap, T *__restrict__ x,
-                      T *__restrict__ r, double *part) {
+                      T *__restrict__ r, double *part, Fin fin) {
     pdl_enter();
     if (!s->running) return;
     const T alpha = static_cast<T>(s->alpha);
@@ -258,11 +275,12 @@ __global__ void cg_xr(const KState *s, int64_t n, const T *__restrict__ p, const
     }
     tile::block_reduce<1>(v);
     if (threadIdx.x == 0) part[blockIdx.x] = v[0];
+    tile::finish(fin, part, gridDim.x);
 }
 
-// ||r|| check, refresh decision (Cg.cuh:170-178).
-__global__ void cg_res(KState *s, const double *part, int parts) {
-    pdl_enter();
+// ||r|| check and refresh decision (Cg.cuh:170-178); without a refresh the
+// iteration closes here (Cg.cuh:185-189).
+__device__ void cg_res_step(KState *s, const double *part, int parts) {
     if (!s->running) return;
     double v[1];
     sum_partials<1>(part, parts, v);
@@ -270,32 +288,47 @@ __global__ void cg_res(KState *s, const double *part, int parts) {
     const double res = sqrt(v[0]);
     s->res = res;
     if (!isfinite(res)) return stop(s, TF_NONFINITE);
-    if (res <= s->tol || s->it % s->interval == 0) s->refresh = 1;
-}
-
-// After a gated true residual: confirm or restart (Cg.cuh:178-185), then
-// close the iteration.
-__global__ void cg_end(KState *s, const double *part, int parts) {
-    pdl_enter();
-    if (!s->running) return;
-    double v[1];
-    if (s->refresh) sum_partials<1>(part, parts, v);
-    if (threadIdx.x) return;
-    if (s->refresh) {
-        s->refresh = 0;
-        const double res = sqrt(v[0]);
-        s->res = res;
-        if (!isfinite(res) || res <= s->tol) return stop(s, TF_MAX_ITERATIONS);
-        s->fresh = 1;
+    if (res <= s->tol || s->it % s->interval == 0) {
+        s->refresh = 1;
+        return;
     }
     s->rho_prev = s->rho;
     if (s->it >= s->max_it) stop(s, TF_MAX_ITERATIONS);
 }
 
+// After the gated true residual: confirm or restart (Cg.cuh:178-185), then
+// close the iteration.
+__device__ void cg_refresh_step(KState *s, const double *part, int parts) {
+    if (!s->running) return;
+    double v[1];
+    sum_partials<1>(part, parts, v);
+    if (threadIdx.x) return;
+    s->refresh = 0;
+    const double res = sqrt(v[0]);
+    s->res = res;
+    if (!isfinite(res) || res <= s->tol) return stop(s, TF_MAX_ITERATIONS);
+    s->fresh = 1;
+    s->rho_prev = s->rho;
+    if (s->it >= s->max_it) stop(s, TF_MAX_ITERATIONS);
+}
+
+// Scalar steps as last-CTA handoffs (tile::finish) of the reductions they
+// consume.
+#define TF_KRYLOV_FINAL(Name, step)                                                    \
+    struct Name {                                                                      \
+        static constexpr bool kActive = true;                                          \
+        KState *s;                                                                     \
+        unsigned *ticket;                                                              \
+        __device__ void operator()(const double *p, int n) const { step(s, p, n); }    \
+    };
+TF_KRYLOV_FINAL(CgRho, cg_rho_step)
+TF_KRYLOV_FINAL(CgCurv, cg_curv_step)
+TF_KRYLOV_FINAL(CgRes, cg_res_step)
+TF_KRYLOV_FINAL(CgRefresh, cg_refresh_step)
+
 // ---- BiCGStab ------------------------------------------------------------
 
-__global__ void bi_rho(KState *s, const double *part, int parts) {
-    pdl_enter();
+__device__ void bi_rho_step(KState *s, const double *part, int parts) {
     if (!s->running) return;
     double v[1];
     sum_partials<1>(part, parts, v);
@@ -337,8 +370,7 @@ __global__ void bi_p(const KState *s, int64_t n, const T *__restrict__ r, const 
     }
 }
 
-__global__ void bi_alpha(KState *s, const double *part, int parts) {
-    pdl_enter();
+__device__ void bi_alpha_step(KState *s, const double *part, int parts) {
     if (!s->running) return;
     double v[1];
     sum_partials<1>(part, parts, v);
@@ -352,9 +384,9 @@ __global__ void bi_alpha(KState *s, const double *part, int parts) {
 }
 
 // s = r - alpha v, x += alpha phat, sum s_i^2.
-template <class T>
+template <class T, class Fin>
 __global__ void bi_s(const KState *st, int64_t n, const T *__restrict__ r, const T *__restrict__ v,
-                     const T *__restrict__ ph, T *__restrict__ sv, T *__restrict__ x, double *part) {
+                     const T *__restrict__ ph, T *__restrict__ sv, T *__restrict__ x, double *part, Fin fin) {
     pdl_enter();
     if (!st->running) return;
     const T alpha = static_cast<T>(st->alpha);
@@ -368,11 +400,11 @@ __global__ void bi_s(const KState *st, int64_t n, const T *__restrict__ r, const
     }
     tile::block_reduce<1>(acc);
     if (threadIdx.x == 0) part[blockIdx.x] = acc[0];
+    tile::finish(fin, part, gridDim.x);
 }
 
 // ||s|| check: candidate convergence takes the early path (BiCgStab.cuh:199-211).
-__global__ void bi_snorm(KState *s, const double *part, int parts) {
-    pdl_enter();
+__device__ void bi_snorm_step(KState *s, const double *part, int parts) {
     if (!s->running) return;
     double v[1];
     sum_partials<1>(part, parts, v);
@@ -387,8 +419,7 @@ __global__ void bi_snorm(KState *s, const double *part, int parts) {
 
 // Early path after the gated true residual: confirm or restart, skipping the
 // omega half and the rho_prev update of this iteration.
-__global__ void bi_early(KState *s, const double *part, int parts) {
-    pdl_enter();
+__device__ void bi_early_step(KState *s, const double *part, int parts) {
     if (!s->running || !s->early) return;
     double v[1];
     sum_partials<1>(part, parts, v);
@@ -400,8 +431,7 @@ __global__ void bi_early(KState *s, const double *part, int parts) {
     s->fresh = 1;
 }
 
-__global__ void bi_omega(KState *s, const double *part, int parts) {
-    pdl_enter();
+__device__ void bi_omega_step(KState *s, const double *part, int parts) {
     if (!s->running || !s->normal) return;
     double v[2];
     sum_partials<2>(part, parts, v);
@@ -416,9 +446,9 @@ __global__ void bi_omega(KState *s, const double *part, int parts) {
 }
 
 // x += omega shat, r = s - omega t, sum r_i^2.
-template <class T>
+template <class T, class Fin>
 __global__ void bi_xr(const KState *st, int64_t n, const T *__restrict__ sh, const T *__restrict__ sv,
-                      const T *__restrict__ t, T *__restrict__ x, T *__restrict__ r, double *part) {
+                      const T *__restrict__ t, T *__restrict__ x, T *__restrict__ r, double *part, Fin fin) {
     pdl_enter();
     if (!st->running || !st->normal) return;
     const T omega = static_cast<T>(st->omega);
@@ -432,10 +462,10 @@ __global__ void bi_xr(const KState *st, int64_t n, const T *__restrict__ sh, con
     }
     tile::block_reduce<1>(acc);
     if (threadIdx.x == 0) part[blockIdx.x] = acc[0];
+    tile::finish(fin, part, gridDim.x);
 }
 
-__global__ void bi_res(KState *s, const double *part, int parts) {
-    pdl_enter();
+__device__ void bi_res_step(KState *s, const double *part, int parts) {
     if (!s->running || !s->normal) return;
     double v[1];
     sum_partials<1>(part, parts, v);
@@ -464,6 +494,14 @@ __global__ void bi_end(KState *s, const double *part, int parts) {
     if (s->normal) s->rho_prev = s->rho;
     if (s->it >= s->max_it) stop(s, TF_MAX_ITERATIONS);
 }
+
+TF_KRYLOV_FINAL(BiRho, bi_rho_step)
+TF_KRYLOV_FINAL(BiAlpha, bi_alpha_step)
+TF_KRYLOV_FINAL(BiSnorm, bi_snorm_step)
+TF_KRYLOV_FINAL(BiEarly, bi_early_step)
+TF_KRYLOV_FINAL(BiOmega, bi_omega_step)
+TF_KRYLOV_FINAL(BiRes, bi_res_step)
+#undef TF_KRYLOV_FINAL
 
 // ---- solver object --------------------------------------------------------
 
@@ -627,7 +665,8 @@ class KrylovImpl final : public Krylov {
 
     // ||b||^2, r = b - A x with ||r||^2, initial decisions.
     void enqueue_prefix(tf_ctx *ctx) {
-        launch_kernel(ctx, "dot", k_dot<T>, parts_, 256, 0, n_, rhs_.data(), rhs_.data(), partb_.data());
+        launch_kernel(ctx, "dot", k_dot<T>, parts_, 256, 0, n_, rhs_.data(), rhs_.data(), partb_.data(),
+                      tile::NoFinal{});
         tile::launch(ctx, csr(), tile::PlainX<T>{x_.data()},
                      ResidualNorm<T>{rhs_.data(), r_.data(), nullptr, part_.data()}, "residual_norm");
         launch_kernel(ctx, "k_init", k_init, 1, 1024, 0, state_.data(), partb_.data(), parts_, part_.data(), tiles_,
@@ -757,43 +796,42 @@ class KrylovImpl final : public Krylov {
     void enqueue_iteration(tf_ctx *ctx) {
         KState *s = state_.data();
         double *part = part_.data();
+        unsigned *tk = s->tickets;
         const unsigned pg = static_cast<unsigned>(parts_);
         if (kind_ == TF_SOLVER_CG) {
             precondition(ctx, r_.data(), z_.data());
-            launch_kernel(ctx, "dot", k_dot<T>, pg, 256, 0, n_, r_.data(), z_.data(), part);
-            launch_kernel(ctx, "cg_rho", cg_rho, 1, 1024, 0, s, part, parts_);
+            launch_kernel(ctx, "dot_rho", k_dot<T, CgRho>, pg, 256, 0, n_, r_.data(), z_.data(), part,
+                          CgRho{s, tk + 0});
             launch_kernel(ctx, "cg_p", cg_p<T>, pg, 256, 0, s, n_, z_.data(), p_.data());
-            tile::launch(ctx, csr(), tile::PlainX<T>{p_.data()}, SpmvDot<T>{q_.data(), p_.data(), &s->running, part},
-                         "spmv_dot");
-            launch_kernel(ctx, "cg_curv", cg_curv, 1, 1024, 0, s, part, tiles_);
-            launch_kernel(ctx, "cg_xr", cg_xr<T>, pg, 256, 0, s, n_, p_.data(), q_.data(), x_.data(), r_.data(), part);
-            launch_kernel(ctx, "cg_res", cg_res, 1, 1024, 0, s, part, parts_);
+            tile::launch(ctx, csr(), tile::PlainX<T>{p_.data()},
+                         SpmvDot<T, CgCurv>{q_.data(), p_.data(), &s->running, part, CgCurv{s, tk + 1}},
+                         "spmv_dot_curv");
+            launch_kernel(ctx, "cg_xr_res", cg_xr<T, CgRes>, pg, 256, 0, s, n_, p_.data(), q_.data(), x_.data(),
+                          r_.data(), part, CgRes{s, tk + 2});
             tile::launch(ctx, csr(), tile::PlainX<T>{x_.data()},
-                         ResidualNorm<T>{rhs_.data(), r_.data(), &s->refresh, part}, "residual_norm");
-            launch_kernel(ctx, "cg_end", cg_end, 1, 1024, 0, s, part, tiles_);
+                         ResidualNorm<T, CgRefresh>{rhs_.data(), r_.data(), &s->refresh, part, CgRefresh{s, tk + 3}},
+                         "residual_refresh");
             return;
         }
         // BiCGStab: v = q_, phat = z_
-        launch_kernel(ctx, "dot", k_dot<T>, pg, 256, 0, n_, shadow_.data(), r_.data(), part);
-        launch_kernel(ctx, "bi_rho", bi_rho, 1, 1024, 0, s, part, parts_);
+        launch_kernel(ctx, "dot_rho", k_dot<T, BiRho>, pg, 256, 0, n_, shadow_.data(), r_.data(), part,
+                      BiRho{s, tk + 0});
         launch_kernel(ctx, "bi_p", bi_p<T>, pg, 256, 0, s, n_, r_.data(), q_.data(), p_.data());
         precondition(ctx, p_.data(), z_.data());
-        tile::launch(ctx, csr(), tile::PlainX<T>{z_.data()}, SpmvDot<T>{q_.data(), shadow_.data(), &s->running, part},
-                     "spmv_dot");
-        launch_kernel(ctx, "bi_alpha", bi_alpha, 1, 1024, 0, s, part, tiles_);
-        launch_kernel(ctx, "bi_s", bi_s<T>, pg, 256, 0, s, n_, r_.data(), q_.data(), z_.data(), s_.data(), x_.data(),
-                      part);
-        launch_kernel(ctx, "bi_snorm", bi_snorm, 1, 1024, 0, s, part, parts_);
-        tile::launch(ctx, csr(), tile::PlainX<T>{x_.data()}, ResidualNorm<T>{rhs_.data(), r_.data(), &s->early, part},
-                     "residual_norm");
-        launch_kernel(ctx, "bi_early", bi_early, 1, 1024, 0, s, part, tiles_);
+        tile::launch(ctx, csr(), tile::PlainX<T>{z_.data()},
+                     SpmvDot<T, BiAlpha>{q_.data(), shadow_.data(), &s->running, part, BiAlpha{s, tk + 1}},
+                     "spmv_dot_alpha");
+        launch_kernel(ctx, "bi_s_norm", bi_s<T, BiSnorm>, pg, 256, 0, s, n_, r_.data(), q_.data(), z_.data(),
+                      s_.data(), x_.data(), part, BiSnorm{s, tk + 2});
+        tile::launch(ctx, csr(), tile::PlainX<T>{x_.data()},
+                     ResidualNorm<T, BiEarly>{rhs_.data(), r_.data(), &s->early, part, BiEarly{s, tk + 3}},
+                     "residual_early");
         precondition(ctx, s_.data(), sh_.data());
-        tile::launch(ctx, csr(), tile::PlainX<T>{sh_.data()}, SpmvDot2<T>{t_.data(), s_.data(), &s->normal, part},
-                     "spmv_dot2");
-        launch_kernel(ctx, "bi_omega", bi_omega, 1, 1024, 0, s, part, tiles_);
-        launch_kernel(ctx, "bi_xr", bi_xr<T>, pg, 256, 0, s, n_, sh_.data(), s_.data(), t_.data(), x_.data(), r_.data(),
-                      part);
-        launch_kernel(ctx, "bi_res", bi_res, 1, 1024, 0, s, part, parts_);
+        tile::launch(ctx, csr(), tile::PlainX<T>{sh_.data()},
+                     SpmvDot2<T, BiOmega>{t_.data(), s_.data(), &s->normal, part, BiOmega{s, tk + 4}},
+                     "spmv_dot2_omega");
+        launch_kernel(ctx, "bi_xr_res", bi_xr<T, BiRes>, pg, 256, 0, s, n_, sh_.data(), s_.data(), t_.data(),
+                      x_.data(), r_.data(), part, BiRes{s, tk + 5});
         tile::launch(ctx, csr(), tile::PlainX<T>{x_.data()}, ResidualNorm<T>{rhs_.data(), r_.data(), &s->refresh, part},
                      "residual_norm");
         launch_kernel(ctx, "bi_end", bi_end, 1, 1024, 0, s, part, tiles_);

@@ -88,11 +88,48 @@ __device__ __forceinline__ void block_reduce(double (&v)[K]) {
     }
 }
 
+// Last-CTA handoff.  Every CTA of a reducing launch calls last_cta() once,
+// after its partial sums are written; it returns true in the CTA that comes
+// last (a device-wide ticket), which then sees every partial sum and runs the
+// scalar step that consumes them, in place of a separate one-CTA launch.  The
+// ticket is reset for the next launch.  All threads of the CTA must call it.
+__device__ __forceinline__ bool last_cta(unsigned *ticket) {
+    __shared__ unsigned is_last;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();  // this CTA's partial sums before its ticket
+        const unsigned t = atomicAdd(ticket, 1u);
+        is_last = t == gridDim.x - 1 ? 1u : 0u;
+        if (is_last) {
+            atomicExch(ticket, 0u);
+            __threadfence();
+        }
+    }
+    __syncthreads();
+    return is_last != 0;
+}
+
+// No scalar step after the reduction.
+struct NoFinal {
+    static constexpr bool kActive = false;
+    unsigned *ticket{nullptr};
+    __device__ void operator()(const double *, int) const {}
+};
+
+// Runs fin (when active) in the last CTA over `parts` partial sums.
+template <class Fin>
+__device__ __forceinline__ void finish(const Fin &fin, const double *part, int parts) {
+    if constexpr (Fin::kActive) {
+        if (last_cta(fin.ticket)) fin(part, parts);
+    }
+}
+
 // Epilogue requirements:
 //   static constexpr int kReduce;           number of reduced products (0..4)
 //   __device__ bool skip() const;           true: the whole launch is gated off
 //   __device__ void operator()(int64_t i, T acc, const XS &xs, double (&red)[kReduce or 1]) const;
 //   double *partial;                        [kReduce][gridDim.x] when kReduce > 0
+// (the pipelined kernel also needs `fin`, a tile::finish step, when kReduce > 0)
 template <class T, class I, int RPT, class XS, class Epi>
 __global__ void __launch_bounds__(kThreads) csr_tile_kernel(int64_t rows, const I *__restrict__ rp,
                                                              const I *__restrict__ ci, const T *__restrict__ val,
@@ -307,6 +344,7 @@ __global__ void __launch_bounds__(kThreads + 32) csr_pipe_kernel(int64_t rows, i
     __shared__ uint64_t full_bar[kMaxStages], empty_bar[kMaxStages];
     __shared__ double warp_sums[kMaxStages + 1][RPT][kWarps][KK];
     __shared__ int warp_done[kMaxStages + 1];
+    __shared__ int skipped_cta;
     const StageLayout<T, I, C> L(cap, kTileRows);
     const int tid = threadIdx.x;
     if (tid == 0) {
@@ -383,7 +421,9 @@ __global__ void __launch_bounds__(kThreads + 32) csr_pipe_kernel(int64_t rows, i
         const int lane = tid & 31, warp = tid >> 5;
         uint32_t it = 0, local_tile = 0;
         double red[RPT][KK];
-        const int64_t first = epi.skip() ? ntiles : blockIdx.x;
+        const bool skipped = epi.skip();
+        if (tid == 0) skipped_cta = skipped ? 1 : 0;
+        const int64_t first = skipped ? ntiles : blockIdx.x;
         for (int64_t tile = first; tile < ntiles && ok; tile += gridDim.x) {
             const int64_t r0 = tile * kTileRows;
             const int nr = static_cast<int>(min(static_cast<int64_t>(kTileRows), rows - r0));
@@ -511,6 +551,12 @@ __global__ void __launch_bounds__(kThreads + 32) csr_pipe_kernel(int64_t rows, i
         // last phase armed on every stage.
         for (int st = 0; st < stages; ++st)
             if (armed[st]) mbar_wait(&full_bar[st], (armed[st] - 1) & 1);
+    }
+    if constexpr (K > 0) {
+        // the scalar step that consumes the partial sums, in the last CTA
+        // (the gate is the same in every CTA: all count or none does)
+        __syncthreads();
+        if (!skipped_cta) finish(epi.fin, epi.partial, static_cast<int>(nblocks));
     }
 }
 
