@@ -241,7 +241,8 @@ typedef struct {
     int hierarchy_type;      /* TF_F64 or TF_F32 storage/arithmetic of the cycle; -1 = same as vectors */
     int coarse_lu_rows;      /* LU when the last level has <= this many rows; default 64, max 256 */
     int small_level_rows;    /* levels (below the finest) with <= this many rows run each sub-cycle as one
-                                thread-block-cluster launch; 0 launches every level step separately */
+                                launch out of shared memory (one CTA when they fit, else a thread-block
+                                cluster); default 1200, 0 launches every level step separately */
 } tf_amg_options;
 void tf_amg_options_default(tf_amg_options *o);
 

@@ -18,15 +18,16 @@ pytestmark = pytest.mark.gpu
 @pytest.mark.parametrize("cycle", ["v", "w", "f"])
 @pytest.mark.parametrize("post", [1, 0, 2])
 @pytest.mark.parametrize("fuse", ["1", "0"])
-def test_cluster_levels_match_launched_levels(ctx, cycle, post, fuse, monkeypatch):
+@pytest.mark.parametrize("rows", [700, 5000])  # one CTA; a cluster (levels too big for one)
+def test_cluster_levels_match_launched_levels(ctx, cycle, post, fuse, rows, monkeypatch):
     monkeypatch.setenv("THERMOFEM_B200_FUSE", fuse)
     m = P.heat3d(24, seed=41)
     n = len(m[0]) - 1
     b = P.rhs_uniform(n, 42)
     a = to_device(m)
     opts = dict(coarse_rows=32, cycle=cycle, post_sweeps=post, jacobi_weight=2 / 3)
-    plain = tf.Amg(tf.amg_options(**opts), ctx=ctx)
-    coop = tf.Amg(tf.amg_options(small_level_rows=3000, **opts), ctx=ctx)
+    plain = tf.Amg(tf.amg_options(small_level_rows=0, **opts), ctx=ctx)
+    coop = tf.Amg(tf.amg_options(small_level_rows=rows, **opts), ctx=ctx)
     plain.setup(a)
     coop.setup(a)
     assert plain.level_count() >= 4

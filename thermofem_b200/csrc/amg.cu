@@ -446,8 +446,9 @@ class HierarchyImpl final : public Hierarchy {
         const S *xin{nullptr};
         S *xout{nullptr};
         PendingRestrict r;
-        // kWriteProgram: recorded small-level program and its entry transfer
-        size_t prog_off{0}, prog_count{0};
+        // kWriteProgram: small-level region entry, its entry transfer and the
+        // root buffer that holds its result
+        int entry{0}, root_cur{0};
         ProgramIO<S> io;
     };
 
@@ -472,7 +473,7 @@ class HierarchyImpl final : public Hierarchy {
             io.soff = off;
             io.smem = mem;
             io.sfine = fx;
-            launch_coarse_program<S>(ctx, programs_.data() + w.prog_off, static_cast<int>(w.prog_count), io, cluster_);
+            tail_.launch(ctx, w.entry, io, w.root_cur);
             return;
         }
         if (w.kind == kWriteSweep) {
@@ -545,14 +546,13 @@ class HierarchyImpl final : public Hierarchy {
             entries_.emplace_back(start, rec_.size() - start);
             return;
         }
-        const auto [off, count] = entries_.at(entry_++);
         const CoarseStep<S> last = rec_.back();
         rec_.resize(start);
         PendingWrite w;
         w.kind = kWriteProgram;
         w.l = &l;
-        w.prog_off = off;
-        w.prog_count = count;
+        w.entry = static_cast<int>(entry_++);
+        w.root_cur = l.cur;
         w.io = io;
         if (fusing() && (last.op == kStepSweep || last.op == kStepDense) && last.xout == l.x()) {
             w.xout = l.x();
@@ -603,25 +603,66 @@ class HierarchyImpl final : public Hierarchy {
         }
     }
 
-    // Records the cluster programs of every small-level sub-cycle of one
-    // cycle (a dry run: nothing is launched) and uploads them.
+    // The small-level region: the first level (below the finest) with at
+    // most small_level_rows rows, or the first one below it whose levels fit
+    // in the cluster's shared memory.  Its sub-cycles are recorded by a dry
+    // run of the cycle (nothing is launched) and translated into region
+    // steps; without a fitting region every level is launched.
     void plan_small_levels(tf_ctx *ctx) {
-        coop_from_ = levels_.size();
-        for (size_t d = 1; d < levels_.size() && cfg_.o.small_level_rows > 0; ++d)
+        const size_t none = levels_.size();
+        coop_from_ = none;
+        if (cfg_.o.small_level_rows <= 0) return;
+        size_t root = none;
+        for (size_t d = 1; d < levels_.size(); ++d)
             if (levels_[d].n <= cfg_.o.small_level_rows) {
-                coop_from_ = d;
+                root = d;
                 break;
             }
-        if (coop_from_ == levels_.size()) return;
-        cluster_ = coarse_cluster_size<S>();
-        entries_.clear();
-        dry_ = true;
-        enqueue(ctx);
-        dry_ = false;
-        programs_.allocate(rec_.size());
-        cuda_check(cudaMemcpy(programs_.data(), rec_.data(), rec_.size() * sizeof(CoarseStep<S>), cudaMemcpyHostToDevice),
-                   "coarse program upload");
-        rec_.clear();
+        for (; root < levels_.size(); ++root) {
+            // record this root's sub-cycles first: their length sizes the plan
+            coop_from_ = root;
+            entries_.clear();
+            dry_ = true;
+            enqueue(ctx);
+            dry_ = false;
+            size_t max_steps = 1;
+            for (const auto &e : entries_) max_steps = std::max(max_steps, e.second);
+            std::vector<TailLevel<S>> tl;
+            for (size_t d = root; d < levels_.size(); ++d) {
+                const Level<S> &l = levels_[d];
+                TailLevel<S> t;
+                t.n = l.n;
+                t.rp = l.rp.data();
+                t.ci = l.ci.data();
+                t.cd = l.cd.data();
+                t.val = l.val.data();
+                t.dinv = l.dinv.data();
+                t.rhs = l.rhs.data();
+                t.x0 = l.x0.data();
+                t.x1 = l.x1.data();
+                if (d + 1 < levels_.size()) {
+                    t.map = l.map.data();
+                    t.off = l.off.data();
+                    t.mem = l.mem.data();
+                }
+                tl.push_back(t);
+            }
+            const int dense_n = factored_ ? static_cast<int>(levels_.back().n) : 0;
+            TailParent parent;
+            parent.n = levels_[root - 1].n;
+            parent.off = levels_[root - 1].off.data();
+            parent.mem = levels_[root - 1].mem.data();
+            bool ok = tail_.plan(ctx, tl, parent, factored_ ? inv_.data() : nullptr, dense_n, w_,
+                                 static_cast<int>(max_steps));
+            for (const auto &[first, count] : entries_) ok = ok && tail_.add_entry(rec_, first, count);
+            rec_.clear();
+            entries_.clear();
+            if (ok) {
+                tail_.upload();
+                return;
+            }
+            coop_from_ = none;
+        }
     }
 
     static constexpr int64_t kFusedProlongRows = 131072;
@@ -648,8 +689,7 @@ class HierarchyImpl final : public Hierarchy {
     std::vector<CoarseStep<S>> rec_;
     std::vector<std::pair<size_t, size_t>> entries_;
     size_t entry_{0};
-    DeviceBuffer<CoarseStep<S>> programs_;
-    int cluster_{1};
+    TailRegion<S> tail_;
     size_t region_start_{0};
 };
 
