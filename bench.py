@@ -34,13 +34,18 @@ SIZE = 128
 SEED_MATRIX, SEED_RHS = 1001, 1002
 AMG = dict(jacobi_weight=2.0 / 3.0, pre_sweeps=1, post_sweeps=1, cycle="v", coarse_rows=64)
 METRIC = "time-to-1e-8 FP64 relative residual (s), AMG-PCG V-cycle, FP32 hierarchy / FP64 outer"
+# DRAM bytes (read + write) of one launch of the FP64 operator SpMV on the
+# 128^3 problem, from the ncu capture summarised in
+# profiles/csr_pipe_kernel_heat3d_128_fp64_operator.md
+SPMV_TRAFFIC = 171013632 + 13778176
 WORKLOAD = f"heat3d {SIZE}^3 7-point FV, log-normal k (seed {SEED_MATRIX}), Dirichlet x=0, rhs U[-1,1] (seed {SEED_RHS})"
 
 
-def spmv_bytes(n, nnz, vsize=8, isize=4):
-    """Algorithmic bytes of one CSR SpMV: values + column indices, row
-    offsets, x and y each once."""
-    return nnz * (vsize + isize) + n * (isize + 2 * vsize) + isize
+def spmv_bytes(n, nnz, vsize=8, isize=4, csize=None):
+    """Algorithmic bytes of one CSR SpMV: values + column entries (csize
+    bytes each, default the index size), row offsets, x and y each once."""
+    csize = isize if csize is None else csize
+    return nnz * (vsize + csize) + n * (isize + 2 * vsize) + isize
 
 
 def measured_peaks():
@@ -158,7 +163,8 @@ def _small(args):
 
 def run_profile(args):
     """The kernels of whole solves, for an ncu launch list: setup and warm-up
-    solves first (skip their launches with ncu -s), then args.steps solves."""
+    solves first (skip their launches with ncu -s), then args.steps solves.
+    --profile spmv: the FP64 operator SpMV instead (NVTX range "spmv")."""
     import torch
     import thermofem_b200 as tf
     from thermofem_b200 import problems as P
@@ -168,6 +174,19 @@ def run_profile(args):
     a = tf.DeviceCsr.from_host(off, idx, val)
     b = torch.tensor(P.rhs_uniform(n, SEED_RHS), device="cuda")
     x = torch.zeros(n, dtype=torch.float64, device="cuda")
+    if args.profile == "spmv":
+        s = tf.Cg(tf.solver_options(), "identity", ctx=ctx)
+        s.setup(a)
+        for _ in range(args.warmup):
+            s.spmv(b, x)
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_push("spmv")  # ncu --nvtx --nvtx-include "spmv/"
+        for _ in range(args.steps):
+            s.spmv(b, x)
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_pop()
+        print(json.dumps({"profile": "spmv", "rows": n, "nnz": len(idx)}), flush=True)
+        return
     s = tf.Cg(tf.solver_options(), "amg",
               tf.amg_options(hierarchy_type="f32" if args.profile == "mixed" else "f64", **AMG, **_small(args)),
               ctx=ctx)
@@ -199,7 +218,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--small-level-rows", type=int, default=None,
                     help="tf_amg_options.small_level_rows (default: the library default)")
-    ap.add_argument("--profile", choices=["mixed", "fp64"], default=None,
+    ap.add_argument("--profile", choices=["mixed", "fp64", "spmv"], default=None,
                     help="profiling run: setup, --warmup solves, then --steps solves of one path; no JSON line")
     args = ap.parse_args()
     if args.impl == "reference":
@@ -299,33 +318,32 @@ def main():
     e2e_s = maxover((time.perf_counter() - t0) / args.steps)
     assert rep_e2e["status"] == "Converged"
 
-    # roofline of the dominant kernel family: the row-tile SpMV on the FP64 operator
+    # roofline of the dominant kernel family, the pipelined row-tile SpMV, as
+    # the solves stream it: the FP64 Krylov operator and the FP32 finest
+    # level, both with 2-byte column offsets (and, for reference, the FP64
+    # SpMV of a caller's int32 CSR)
+    def time_launch(fn, reps=50):
+        for _ in range(5):
+            fn()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(ctx.stream)
+        for _ in range(reps):
+            fn()
+        e1.record(ctx.stream)
+        torch.cuda.synchronize(dev)
+        return e0.elapsed_time(e1) / reps
+
     y = torch.empty_like(b)
-    for _ in range(5):
-        tf.spmv(a, b, y, ctx=ctx)
-    reps = 50
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(ctx.stream)
-    for _ in range(reps):
-        tf.spmv(a, b, y, ctx=ctx)
-    e1.record(ctx.stream)
-    torch.cuda.synchronize(dev)
-    spmv_ms = e0.elapsed_time(e1) / reps
-    peak, peak_kind = measured_peaks()
-    algo = spmv_bytes(n, nnz)
-    achieved = algo / (spmv_ms * 1e-3) / 1e9
-    a32 = a.to(torch.float32)
     b32 = b.float()
     y32 = torch.empty_like(b32)
-    for _ in range(5):
-        tf.spmv(a32, b32, y32, ctx=ctx)
-    e0.record(ctx.stream)
-    for _ in range(reps):
-        tf.spmv(a32, b32, y32, ctx=ctx)
-    e1.record(ctx.stream)
-    torch.cuda.synchronize(dev)
-    spmv32_ms = e0.elapsed_time(e1) / reps
-    achieved32 = spmv_bytes(n, nnz, 4, 4) / (spmv32_ms * 1e-3) / 1e9
+    spmv_ms = time_launch(lambda: plain.spmv(b, y))
+    spmv32_ms = time_launch(lambda: mixed.level_spmv(0, b32, y32))
+    csr_ms = time_launch(lambda: tf.spmv(a, b, y, ctx=ctx))
+    peak, peak_kind = measured_peaks()
+    algo = spmv_bytes(n, nnz, 8, 4, 2)
+    achieved = algo / (spmv_ms * 1e-3) / 1e9
+    achieved32 = spmv_bytes(n, nnz, 4, 4, 2) / (spmv32_ms * 1e-3) / 1e9
+    achieved_csr = spmv_bytes(n, nnz) / (csr_ms * 1e-3) / 1e9
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -354,10 +372,11 @@ def main():
             "plain_fp64": {"value": ms_plain / 1e3, "unit": "s", "iterations": rep_plain["iterations"],
                            "setup_s": setup_plain},
             "speedup_mixed_vs_fp64": ms_plain / ms_mixed,
-            "spmv_gbs": {"f64": achieved, "f32": achieved32},
+            "spmv_gbs": {"f64_operator": achieved, "f32_level0": achieved32, "f64_int32_csr": achieved_csr},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None,
-                         "kernel": "csr_tile_kernel (SpMV, FP64 operator)", "peak_source": peak_kind,
+                         "frac": achieved / peak, "traffic": SPMV_TRAFFIC,
+                         "kernel": "csr_pipe_kernel<double,int,short> (SpMV, FP64 Krylov operator, "
+                                   "2-byte column offsets)", "peak_source": peak_kind,
                          "algorithmic_bytes": algo, "launch_ms": spmv_ms},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": 2 * n * 8, "d2h_bytes_per_step": n * 8},

@@ -265,6 +265,10 @@ const char *tf_amg_coarse_solver(const tf_amg *m);
 int tf_amg_last_visits(const tf_amg *m, int64_t *visits, int capacity);
 /* Level operator and transfer of the hierarchy (read-only device views). */
 int tf_amg_level_matrix(const tf_amg *m, int level, tf_csr *out);
+/* y = A_level x with the level's operator as the cycle streams it (its
+ * storage type and column stream); x, y device vectors of the hierarchy's
+ * storage type, not aliased. */
+int tf_amg_level_spmv(const tf_amg *amg, int level, const void *x, void *y);
 int tf_amg_level_transfer(const tf_amg *m, int level, const int32_t **map, const int32_t **offsets,
                           const int32_t **members, int *coarse_rows);
 
@@ -314,6 +318,11 @@ int tf_solver_apply(tf_solver *s, const void *rhs, void *x, int host_buffers, tf
  * reads a 4-byte running flag.  Same kernels, same results; mode 0 exists for
  * profilers that cannot look inside conditional graph nodes. */
 int tf_solver_set_graph_mode(tf_solver *s, int mode);
+/* y = A x with the solver's own copy of the operator, as its iterations
+ * stream it (IterationContext::multiply, IterationContext.cu:140-159, on the
+ * snapshot taken by setup); x, y device vectors of the solver's value type,
+ * not aliased.  TF_ERR_LOGIC before setup. */
+int tf_solver_spmv(tf_solver *s, const void *x, void *y);
 /* How the last apply ran: 2 as one whole-solve graph, 1 as one graph per
  * iteration, 0 as uncaptured launches (a step the driver refused to
  * capture), -1 before the first apply or for a NULL solver.  No reference

@@ -382,3 +382,22 @@ def test_two_byte_column_stream_gives_identical_solves(ctx, case, monkeypatch):
     assert out[0][0]["status"] == "Converged"
     assert out[0][0] == out[1][0]
     assert torch.equal(out[0][1], out[1][1])
+
+
+def test_operator_spmv_entry_points(ctx):
+    # The solver's and the hierarchy's own operators (2-byte column stream)
+    # give the same product as the plain CSR SpMV.
+    m = P.heat3d(24, seed=91)
+    n = len(m[0]) - 1
+    a = to_device(m)
+    x = torch.tensor(np.random.default_rng(92).standard_normal(n), device="cuda")
+    s = tf.Cg(tf.solver_options(), "amg", tf.amg_options(hierarchy_type="f32"), ctx=ctx)
+    with pytest.raises(tf.LogicError):
+        s.spmv(x)
+    s.setup(a)
+    assert torch.equal(s.spmv(x), tf.spmv(a, x, ctx=ctx))
+    h = s  # the solver is a view of its hierarchy
+    for d in range(h.level_count()):
+        lm = h.level_matrix(d)
+        xd = torch.tensor(np.random.default_rng(d).standard_normal(lm.rows), dtype=torch.float32, device="cuda")
+        assert torch.equal(h.level_spmv(d, xd), tf.spmv(lm, xd, ctx=ctx))

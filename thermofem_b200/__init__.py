@@ -169,6 +169,8 @@ SIGNATURES = {
     "tf_solver_set_graph_mode": ([_P, _I], _I),
     "tf_solver_last_apply_ms": ([_P], _D),
     "tf_solver_last_execution": ([_P], _I),
+    "tf_solver_spmv": ([_P, _P, _P], _I),
+    "tf_amg_level_spmv": ([_P, _I, _P, _P], _I),
     "tf_read_matrix_market": ([C.c_char_p, _S, C.POINTER(HostCsr)], _I),
     "tf_read_matrix_market_file": ([C.c_char_p, C.POINTER(HostCsr)], _I),
     "tf_host_csr_free": ([C.POINTER(HostCsr)], None),

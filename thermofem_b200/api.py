@@ -503,6 +503,15 @@ class _AmgView:
         val = raw.view(dt).clone() if raw is not None else torch.empty(0, dtype=dt, device=dev)
         return DeviceCsr(off, idx, val)
 
+    def level_spmv(self, d, x, y=None):
+        """y = A_d x with level d's operator as the cycle streams it (x, y of
+        the hierarchy's storage type)."""
+        y = torch.empty_like(x) if y is None else y
+        ctx = getattr(self, "ctx", None) or default_context()
+        with ctx:
+            check(lib().tf_amg_level_spmv(self._h(), int(d), _p(x), _p(y)))
+        return y
+
     def level_transfer(self, d, device="cuda"):
         pm, po, pe = C.c_void_p(), C.c_void_p(), C.c_void_p()
         cr = C.c_int()
@@ -622,6 +631,13 @@ class _Solver(_AmgView):
         """1: one graph per solve with a device-side loop (default); 0: one
         graph per iteration and a host loop (for kernel profilers)."""
         check(lib().tf_solver_set_graph_mode(self.h, int(mode)))
+
+    def spmv(self, x, y=None):
+        """y = A x with the solver's own operator (as its iterations stream it)."""
+        y = torch.empty_like(x) if y is None else y
+        with self.ctx:
+            check(lib().tf_solver_spmv(self.h, _p(x), _p(y)))
+        return y
 
     @property
     def last_execution(self) -> int:

@@ -192,6 +192,11 @@ class HierarchyImpl final : public Hierarchy {
         tf_csr c{l.n, l.n, l.nnz, TF_I32, storage_type(), l.rp.data(), l.ci.data(), l.val.data()};
         return c;
     }
+    void level_spmv(tf_ctx *ctx, int d, const void *x, void *y) const override {
+        const auto &l = levels_.at(static_cast<size_t>(d));
+        StableScope stable(ctx);
+        spmv(ctx, l.csr(), static_cast<const S *>(x), static_cast<S *>(y));
+    }
     void level_transfer(int d, const int32_t **map, const int32_t **off, const int32_t **mem,
                         int *coarse) const override {
         const auto &l = levels_.at(static_cast<size_t>(d));

@@ -37,6 +37,9 @@ class Hierarchy {
     virtual int64_t rows() const = 0;
     virtual int level_count() const = 0;
     virtual tf_csr level_matrix(int d) const = 0;
+    // y = A_d x with level d's operator as the cycle streams it (its column
+    // storage included); x, y of the level's storage type.
+    virtual void level_spmv(tf_ctx *ctx, int d, const void *x, void *y) const = 0;
     virtual void level_transfer(int d, const int32_t **map, const int32_t **off, const int32_t **mem,
                                 int *coarse) const = 0;
     // Kernels launched by one cycle (graph replay counts them too).
@@ -60,6 +63,8 @@ class Krylov {
     virtual void setup(tf_ctx *ctx, const tf_csr &a) = 0;
     // rhs/x are device pointers of T; x holds the initial guess.
     virtual tf_solve_result solve(tf_ctx *ctx, const void *rhs, void *x) = 0;
+    // y = A x with the solver's operator as the solve streams it.
+    virtual void spmv(tf_ctx *ctx, const void *x, void *y) = 0;
     virtual Hierarchy *amg() = 0;
     virtual int64_t rows() const = 0;
     // 1: the whole solve is one graph with a device-side loop (default);

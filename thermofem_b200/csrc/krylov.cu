@@ -644,6 +644,11 @@ class KrylovImpl final : public Krylov {
     }
 
     Hierarchy *amg() override { return hier_.get(); }
+    void spmv(tf_ctx *ctx, const void *x, void *y) override {
+        if (!ready_) fail(TF_ERR_LOGIC, "solver requires setup");
+        StableScope stable(ctx);
+        tfb::spmv(ctx, csr(), static_cast<const T *>(x), static_cast<T *>(y));
+    }
     int64_t rows() const override { return n_; }
 
   private:

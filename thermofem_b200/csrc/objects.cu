@@ -160,6 +160,16 @@ int tf_amg_level_matrix(const tf_amg *m, int level, tf_csr *out) {
     });
 }
 
+int tf_amg_level_spmv(const tf_amg *m, int level, const void *x, void *y) {
+    return guard([&] {
+        require(m != nullptr && x != nullptr && y != nullptr && x != y, "null or aliased argument");
+        if (!m->h) fail(TF_ERR_LOGIC, "AMG requires setup");
+        require(level >= 0 && level < m->h->level_count(), "level out of range");
+        DeviceScope scope(m->ctx->device);
+        m->h->level_spmv(m->ctx, level, x, y);
+    });
+}
+
 int tf_amg_level_transfer(const tf_amg *m, int level, const int32_t **map, const int32_t **offsets,
                           const int32_t **members, int *coarse_rows) {
     return guard([&] {
@@ -341,6 +351,14 @@ tf_amg *tf_solver_amg(tf_solver *s) {
 double tf_solver_last_apply_ms(const tf_solver *s) { return s && s->k ? s->k->last_ms : 0.0; }
 
 int tf_solver_last_execution(const tf_solver *s) { return s && s->k ? s->k->last_execution : -1; }
+
+int tf_solver_spmv(tf_solver *s, const void *x, void *y) {
+    return guard([&] {
+        require(s != nullptr && x != nullptr && y != nullptr && x != y, "null or aliased argument");
+        DeviceScope scope(s->ctx->device);
+        s->k->spmv(s->ctx, x, y);
+    });
+}
 
 int tf_solver_set_graph_mode(tf_solver *s, int mode) {
     return guard([&] {
