@@ -324,7 +324,7 @@ int tf_solver_set_graph_mode(tf_solver *s, int mode);
  * not aliased.  TF_ERR_LOGIC before setup. */
 int tf_solver_spmv(tf_solver *s, const void *x, void *y);
 /* How the last apply ran: 2 as one whole-solve graph, 1 as one graph per
- * iteration, 0 as uncaptured launches (a step the driver refused to
+ * iteration, 0 as uncaptured launches (a step CUDA refused to
  * capture), -1 before the first apply or for a NULL solver.  No reference
  * counterpart (the reference launches from the host). */
 int tf_solver_last_execution(const tf_solver *s);

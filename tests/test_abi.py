@@ -94,3 +94,40 @@ def test_problem_generators_match_baseline_sizes():
     assert np.array_equal(P.uniform(5, 10), P.uniform(5, 10))  # pure function of (seed, index)
     assert not np.array_equal(P.uniform(5, 10), P.uniform(6, 10))
     del a
+
+
+def test_solve_matrix_driver_input_errors(tmp_path):
+    # Argument and input errors exit 1 with error=... before touching a GPU
+    # (example/solve-matrix.cu:59-78).
+    import subprocess
+    from thermofem_b200 import build as B
+    from thermofem_b200 import problems as P
+    B.build_driver()
+
+    def run(*args):
+        r = subprocess.run([B.DRIVER, *args], capture_output=True, text=True, timeout=60)
+        return r.returncode, r.stderr.strip()
+
+    assert run() == (1, "error=Usage: solve-matrix path [amg|identity] [v|w|f]")
+    assert run("a", "b", "c", "d") == (1, "error=Usage: solve-matrix path [amg|identity] [v|w|f]")
+    assert run("x.mtx", "amg", "z") == (1, "error=Unknown cycle")
+    assert run("x.mtx", "jacobi") == (1, "error=Unknown preconditioner")
+    assert run(str(tmp_path / "missing.mtx")) == (1, "error=Cannot open matrix file")
+    rect = tmp_path / "rect.mtx"
+    rect.write_text("%%MatrixMarket matrix coordinate real general\n2 3 1\n1 1 1.0\n")
+    assert run(str(rect)) == (1, "error=Expected nonempty square matrix")
+    bad = tmp_path / "bad.mtx"
+    bad.write_text("%%MatrixMarket matrix coordinate complex general\n2 2 1\n1 1 1.0 0.0\n")
+    rc, err = run(str(bad))
+    assert rc == 1 and err.startswith("error=")
+    # the synthetic writer round-trips through the library's reader
+    off, idx, val = P.laplace2d(5)
+    path = tmp_path / "lap.mtx"
+    P.write_matrix_market(str(path), off, idx, val, symmetric=True)
+    back = tf.read_matrix_market_file(str(path))
+
+    def triplets(o, i, v):
+        r = np.repeat(np.arange(len(o) - 1), np.diff(o))
+        return sorted(zip(r.tolist(), np.asarray(i).tolist(), np.asarray(v).tolist()))
+
+    assert triplets(back["offsets"], back["indices"], back["values"]) == triplets(off, idx, val)

@@ -80,7 +80,27 @@ def build(jobs: int | None = None, verbose: bool = False, force: bool = False) -
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError("link failed:\n" + r.stdout + r.stderr)
+    build_driver()
     return LIB
+
+
+DRIVER_SRC = os.path.join(PKG, "driver", "solve_matrix.cpp")
+DRIVER = os.path.join(PKG, "bin", "solve-matrix")
+
+
+def build_driver() -> str:
+    """The solve-matrix executable (host C++ over the C ABI, linked against
+    the library with an rpath to thermofem_b200/lib)."""
+    os.makedirs(os.path.dirname(DRIVER), exist_ok=True)
+    deps = [DRIVER_SRC, LIB] + glob.glob(os.path.join(ROOT, "include", "*.h"))
+    if os.path.exists(DRIVER) and os.path.getmtime(DRIVER) >= max(os.path.getmtime(d) for d in deps):
+        return DRIVER
+    cmd = [NVCC, "-O2", "-std=c++20", "-ccbin", "g++", "-I", os.path.join(ROOT, "include"), DRIVER_SRC, "-o", DRIVER,
+           "-L", LIBDIR, "-lthermofem_b200", "-Xlinker", "-rpath=$ORIGIN/../lib"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("solve-matrix build failed:\n" + r.stdout + r.stderr)
+    return DRIVER
 
 
 if __name__ == "__main__":

@@ -158,3 +158,21 @@ def manufactured_solution(n: int) -> np.ndarray:
     manufactured solution."""
     i = np.arange(n, dtype=np.float64)
     return 1.0 + 0.25 * np.sin(i * 0.013) + 0.125 * np.cos(i * 0.007)
+
+
+def write_matrix_market(path: str, offsets, indices, values, symmetric: bool = False) -> None:
+    """Writes a CSR matrix as Matrix Market coordinate real text (1-based;
+    with symmetric=True only the lower triangle, as `general` otherwise) --
+    the synthetic stand-in for the reference's real `.mtx` inputs."""
+    offsets = np.asarray(offsets)
+    indices = np.asarray(indices)
+    values = np.asarray(values, dtype=np.float64)
+    n = len(offsets) - 1
+    rows = np.repeat(np.arange(n), np.diff(offsets))
+    keep = indices <= rows if symmetric else np.ones(len(indices), bool)
+    r, c, v = rows[keep] + 1, indices[keep] + 1, values[keep]
+    with open(path, "w") as f:
+        f.write(f"%%MatrixMarket matrix coordinate real {'symmetric' if symmetric else 'general'}\n")
+        f.write(f"{n} {n} {len(v)}\n")
+        for a, b, x in zip(r.tolist(), c.tolist(), v.tolist()):
+            f.write(f"{a} {b} {x!r}\n")
