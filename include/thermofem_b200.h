@@ -333,6 +333,22 @@ tf_amg *tf_solver_amg(tf_solver *s);
 /* Device time of the last apply in milliseconds (CUDA events on the ctx stream). */
 double tf_solver_last_apply_ms(const tf_solver *s);
 
+/* ---- Batched solves (no reference counterpart) ---------------------------
+ * Many independent systems solved together: every solver's whole solve
+ * (its own hierarchy, Krylov loop and convergence test) becomes one branch
+ * of a single CUDA graph, so one apply is one graph launch in which the
+ * systems run concurrently -- the transient use case of many small problems
+ * per time step.  The batch borrows set-up solvers that share its context
+ * (they must outlive it); a solver set up again after the graph was built
+ * makes the next apply rebuild it.  rhs[k] / x[k] are device vectors of
+ * solver k (x[k] is its initial guess and receives its solution);
+ * results[k] is its report.  Each system's iterations and results are those
+ * of tf_solver_apply on it alone. */
+typedef struct tf_batch tf_batch;
+int tf_batch_create(tf_ctx *ctx, int count, tf_solver *const *solvers, tf_batch **out);
+int tf_batch_destroy(tf_batch *b);
+int tf_batch_apply(tf_batch *b, const void *const *rhs, void *const *x, tf_solve_result *results);
+
 /* ---- Matrix Market input (include/IO/MatrixMarket.cuh:14-31) ----------- */
 typedef struct {
     int rows, cols;

@@ -170,6 +170,9 @@ SIGNATURES = {
     "tf_solver_last_apply_ms": ([_P], _D),
     "tf_solver_last_execution": ([_P], _I),
     "tf_solver_spmv": ([_P, _P, _P], _I),
+    "tf_batch_create": ([_P, _I, _PP, _PP], _I),
+    "tf_batch_destroy": ([_P], _I),
+    "tf_batch_apply": ([_P, _PP, _PP, C.POINTER(SolveResult)], _I),
     "tf_amg_level_spmv": ([_P, _I, _P, _P], _I),
     "tf_read_matrix_market": ([C.c_char_p, _S, C.POINTER(HostCsr)], _I),
     "tf_read_matrix_market_file": ([C.c_char_p, C.POINTER(HostCsr)], _I),

@@ -12,7 +12,7 @@ import torch
 from . import (AmgOptions, Csr, HostCsr, SolveResult, SolverOptions, F32, F64, I32, I64, CYCLE, SOLVER_CG,
                SOLVER_BICGSTAB, PRECOND_AMG, PRECOND_IDENTITY, check, lib)
 
-__all__ = ["Context", "DeviceCsr", "Transfer", "Amg", "Jacobi", "Cg", "BiCgStab", "amg_options", "solver_options",
+__all__ = ["Context", "DeviceCsr", "Transfer", "Amg", "Jacobi", "Cg", "BiCgStab", "Batch", "amg_options", "solver_options",
            "read_matrix_market", "read_matrix_market_file", "spmv", "autotune_spmv", "set_spmv_config", "residual", "jacobi_sweep", "jacobi_zero",
            "inverse_diagonal", "restrict_aggregates", "prolong_aggregates", "dot_multi", "axpby", "convert",
            "csr_validate", "check_canonical", "canonicalize", "row_stats", "strength", "match", "contract",
@@ -678,3 +678,33 @@ def read_matrix_market_file(path: str):
     h = HostCsr()
     check(lib().tf_read_matrix_market_file(path.encode(), C.byref(h)))
     return _take_host(h)
+
+
+class Batch:
+    """Independent set-up solvers (sharing one Context) solved together: one
+    CUDA graph launch per apply, the systems' solves as concurrent branches
+    (tf_batch_*).  apply(rhs_list, x_list) -> list of reports."""
+
+    def __init__(self, solvers, ctx=None):
+        self.ctx = _ctx(ctx)
+        self.solvers = list(solvers)  # keep them alive as long as the batch
+        arr = (C.c_void_p * len(self.solvers))(*[s.h.value for s in self.solvers])
+        h = C.c_void_p()
+        check(lib().tf_batch_create(self.ctx.h, len(self.solvers), arr, C.byref(h)))
+        self.h = h
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            _release("tf_batch_destroy", self.h)
+            self.h = None
+
+    def apply(self, rhs, xs):
+        n = len(self.solvers)
+        if len(rhs) != n or len(xs) != n:
+            raise ValueError("one rhs and one x per solver")
+        r = (C.c_void_p * n)(*[t.data_ptr() for t in rhs])
+        x = (C.c_void_p * n)(*[t.data_ptr() for t in xs])
+        res = (SolveResult * n)()
+        with self.ctx:
+            check(lib().tf_batch_apply(self.h, r, x, res))
+        return [res[k].as_dict() for k in range(n)]

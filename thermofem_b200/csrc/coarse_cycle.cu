@@ -38,6 +38,8 @@
 
 #include <algorithm>
 #include <cstring>
+#include <map>
+#include <mutex>
 
 #include "coarse_cycle.cuh"
 #include "tile.cuh"
@@ -386,6 +388,23 @@ __global__ void __launch_bounds__(kTailThreads, 1)
 
 unsigned align16(size_t v) { return static_cast<unsigned>((v + 15) & ~size_t(15)); }
 
+// The dynamic shared memory a kernel may use is one attribute per function
+// and device: raise it to what a region needs, never lower it (other
+// regions of the process may need more).
+template <auto Kernel>
+void allow_region_smem(size_t bytes) {
+    static std::mutex m;
+    static std::map<int, size_t> granted;
+    int dev = 0;
+    cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+    std::lock_guard<std::mutex> lock(m);
+    auto it = granted.find(dev);
+    if (bytes <= 48 * 1024 || (it != granted.end() && bytes <= it->second)) return;
+    cuda_check(cudaFuncSetAttribute(Kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes)),
+               "region shared memory");
+    granted[dev] = bytes;
+}
+
 unsigned reciprocal(int64_t R) { return R > 1 ? static_cast<unsigned>(((uint64_t(1) << 32) + R - 1) / R) : 0u; }
 
 }  // namespace
@@ -549,13 +568,9 @@ bool TailRegion<S>::plan(tf_ctx *ctx, const std::vector<TailLevel<S>> &levels, c
         for (int k = 0; k < C; ++k) tx_ok = tx_ok && tx[static_cast<size_t>(k)] < (1u << 20);
         if (!tx_ok) continue;
         if (C == 1) {
-            cuda_check(cudaFuncSetAttribute(tail_kernel<S, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            static_cast<int>(bytes)),
-                       "region shared memory");
+            allow_region_smem<tail_kernel<S, true>>(bytes);
         } else {
-            cuda_check(cudaFuncSetAttribute(tail_kernel<S, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            static_cast<int>(bytes)),
-                       "region shared memory");
+            allow_region_smem<tail_kernel<S, false>>(bytes);
             cudaLaunchConfig_t cfg = {};
             cfg.gridDim = dim3(static_cast<unsigned>(C));
             cfg.blockDim = dim3(kTailThreads);
@@ -711,6 +726,8 @@ void TailRegion<S>::launch(tf_ctx *ctx, int entry, const ProgramIO<S> &io, int r
     }
     cfg.attrs = attr;
     cfg.numAttrs = na;
+    if (cluster_ > 1) allow_region_smem<tail_kernel<S, false>>(smem_);
+    else allow_region_smem<tail_kernel<S, true>>(smem_);
     auto kernel = cluster_ > 1 ? tail_kernel<S, false> : tail_kernel<S, true>;
     cuda_check(cudaLaunchKernelEx(&cfg, kernel, static_cast<const TailHeader<S> *>(dev_->header.data()),
                                   static_cast<const TailStepDev *>(dev_->steps.data()),

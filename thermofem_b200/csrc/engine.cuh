@@ -67,6 +67,17 @@ class Krylov {
     virtual void spmv(tf_ctx *ctx, const void *x, void *y) = 0;
     virtual Hierarchy *amg() = 0;
     virtual int64_t rows() const = 0;
+    // Batches (tf_batch): the whole solve added to graph g as an independent
+    // branch that loads its own initial state; inputs staged into and the
+    // result copied out of the solver's buffers around the graph launch.
+    virtual void batch_nodes(tf_ctx *ctx, cudaGraph_t g) = 0;
+    virtual int64_t batch_launches(int iterations) const = 0;
+    virtual void batch_stage(tf_ctx *ctx, const void *rhs, const void *x) = 0;
+    virtual void batch_finish(tf_ctx *ctx, void *x, void *state_host) = 0;
+    virtual size_t state_bytes() const = 0;
+    virtual tf_solve_result batch_result(const void *state_host) const = 0;
+    // Incremented by every setup (a batch graph built before is stale).
+    virtual int64_t generation() const = 0;
     // 1: the whole solve is one graph with a device-side loop (default);
     // 0: one graph per iteration and a host loop (same kernels; profilers
     // that cannot see inside conditional graph nodes need this).

@@ -117,6 +117,12 @@ __global__ void k_copy_if(const int *flag, int64_t n, const T *__restrict__ src,
         dst[i] = src[i];
 }
 
+// Loads the initial state of a solve (batched graphs carry it as a parameter).
+__global__ void k_reset(KState *s, KState init) {
+    pdl_enter();
+    *s = init;
+}
+
 // Re-arms the WHILE node of the solve graph: one more iteration while the
 // recurrence is running and below the iteration limit.
 __global__ void k_set_continue(cudaGraphConditionalHandle handle, const KState *s) {
@@ -584,6 +590,7 @@ class KrylovImpl final : public Krylov {
         }
         cuda_check(cudaStreamSynchronize(ctx->stream), "solver setup");
         ready_ = true;
+        ++generation_;
     }
 
     tf_solve_result solve(tf_ctx *ctx, const void *rhs, void *x) override {
@@ -592,12 +599,7 @@ class KrylovImpl final : public Krylov {
         cuda_check(cudaEventRecord(ev0_, ctx->stream), "event");
         copy_async(ctx, rhs_.data(), rhs, n_ * sizeof(T));
         copy_async(ctx, x_.data(), x, n_ * sizeof(T));
-        KState init{};
-        init.tol = opt_.absolute_tolerance;
-        init.res = opt_.relative_tolerance;
-        init.max_it = opt_.max_iterations;
-        init.interval = opt_.residual_refresh_interval;
-        init.status = TF_MAX_ITERATIONS;
+        const KState init = initial_state();
         cuda_check(cudaMemcpyAsync(state_.data(), &init, sizeof(KState), cudaMemcpyHostToDevice, ctx->stream),
                    "state upload");
         if (graph_mode == 1 && !solve_exec_ && !solve_graph_failed_) build_solve_graph(ctx);
@@ -644,6 +646,37 @@ class KrylovImpl final : public Krylov {
     }
 
     Hierarchy *amg() override { return hier_.get(); }
+
+    // ---- batches: many solvers' whole solves as branches of one graph ----
+    void batch_nodes(tf_ctx *ctx, cudaGraph_t g) override {
+        if (!ready_) fail(TF_ERR_LOGIC, kind_ == TF_SOLVER_CG ? "CG requires setup" : "BiCGStab requires setup");
+        StableScope stable(ctx);
+        add_solve_nodes(ctx, g, true);
+    }
+    int64_t batch_launches(int iterations) const override {
+        return prefix_launches_ + suffix_launches_ + per_iteration_ * iterations;
+    }
+    void batch_stage(tf_ctx *ctx, const void *rhs, const void *x) override {
+        copy_async(ctx, rhs_.data(), rhs, n_ * sizeof(T));
+        copy_async(ctx, x_.data(), x, n_ * sizeof(T));
+    }
+    void batch_finish(tf_ctx *ctx, void *x, void *state_host) override {
+        copy_async(ctx, x, x_.data(), n_ * sizeof(T));
+        cuda_check(cudaMemcpyAsync(state_host, state_.data(), sizeof(KState), cudaMemcpyDeviceToHost, ctx->stream),
+                   "state readback");
+    }
+    size_t state_bytes() const override { return sizeof(KState); }
+    tf_solve_result batch_result(const void *state_host) const override {
+        KState fin;
+        std::memcpy(&fin, state_host, sizeof(KState));
+        tf_solve_result out;
+        out.status = fin.status;
+        out.iterations = fin.it;
+        out.residual_norm = fin.res;
+        out.relative_residual = fin.normB > 0 ? fin.res / fin.normB : fin.res;
+        return out;
+    }
+    int64_t generation() const override { return generation_; }
     void spmv(tf_ctx *ctx, const void *x, void *y) override {
         if (!ready_) fail(TF_ERR_LOGIC, "solver requires setup");
         StableScope stable(ctx);
@@ -693,68 +726,85 @@ class KrylovImpl final : public Krylov {
     // whose body is one iteration (it re-arms the condition from the device
     // state at its end), then the suffix.  Falls back to the host loop when
     // the driver refuses any step.
+    // Adds the whole solve to graph g as one independent branch: (with
+    // reset, a kernel that loads the initial state) prefix, a conditional
+    // WHILE node whose body is one iteration (it re-arms the condition from
+    // the device state at its end), suffix.  Throws when CUDA refuses a
+    // step; the caller ends any capture left open.
+    void add_solve_nodes(tf_ctx *ctx, cudaGraph_t g, bool reset) {
+        const int64_t before = ctx->launches;
+        cudaGraphConditionalHandle handle;
+        cuda_check(cudaGraphConditionalHandleCreate(&handle, g, 0, cudaGraphCondAssignDefault), "condition");
+        cuda_check(cudaStreamBeginCaptureToGraph(ctx->stream, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal),
+                   "capture prefix");
+        if (reset) launch_kernel(ctx, "k_reset", k_reset, 1, 1, 0, state_.data(), initial_state());
+        enqueue_prefix(ctx);
+        launch_kernel(ctx, "set_continue", k_set_continue, 1, 1, 0, handle, state_.data());
+        cudaStreamCaptureStatus st;
+        const cudaGraphNode_t *deps = nullptr;
+        size_t ndeps = 0;
+        cuda_check(cudaStreamGetCaptureInfo(ctx->stream, &st, nullptr, nullptr, &deps, &ndeps), "capture info");
+        std::vector<cudaGraphNode_t> last(deps, deps + ndeps);
+        cudaGraph_t out = nullptr;
+        cuda_check(cudaStreamEndCapture(ctx->stream, &out), "capture prefix end");
+        prefix_launches_ = ctx->launches - before;
+        cudaGraphNodeParams cp = {};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = handle;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t loop;
+        cuda_check(cudaGraphAddNode(&loop, g, last.data(), last.size(), &cp), "while node");
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        const int64_t b0 = ctx->launches;
+        cuda_check(cudaStreamBeginCaptureToGraph(ctx->stream, body, nullptr, nullptr, 0,
+                                                 cudaStreamCaptureModeThreadLocal),
+                   "capture body");
+        enqueue_iteration(ctx);
+        launch_kernel(ctx, "set_continue", k_set_continue, 1, 1, 0, handle, state_.data());
+        cuda_check(cudaStreamEndCapture(ctx->stream, &out), "capture body end");
+        per_iteration_ = ctx->launches - b0;
+        const int64_t s0 = ctx->launches;
+        cuda_check(cudaStreamBeginCaptureToGraph(ctx->stream, g, &loop, nullptr, 1, cudaStreamCaptureModeThreadLocal),
+                   "capture suffix");
+        enqueue_suffix(ctx);
+        cuda_check(cudaStreamEndCapture(ctx->stream, &out), "capture suffix end");
+        suffix_launches_ = ctx->launches - s0;
+        ctx->launches = before;
+    }
+
     void build_solve_graph(tf_ctx *ctx) {
         cudaGraph_t g = nullptr;
-        bool capturing = false;
-        const int64_t before = ctx->launches;
         try {
             cuda_check(cudaGraphCreate(&g, 0), "graph create");
-            cudaGraphConditionalHandle handle;
-            cuda_check(cudaGraphConditionalHandleCreate(&handle, g, 0, cudaGraphCondAssignDefault), "condition");
-            cuda_check(cudaStreamBeginCaptureToGraph(ctx->stream, g, nullptr, nullptr, 0,
-                                                     cudaStreamCaptureModeThreadLocal),
-                       "capture prefix");
-            capturing = true;
-            enqueue_prefix(ctx);
-            launch_kernel(ctx, "set_continue", k_set_continue, 1, 1, 0, handle, state_.data());
-            cudaStreamCaptureStatus st;
-            const cudaGraphNode_t *deps = nullptr;
-            size_t ndeps = 0;
-            cuda_check(cudaStreamGetCaptureInfo(ctx->stream, &st, nullptr, nullptr, &deps, &ndeps), "capture info");
-            std::vector<cudaGraphNode_t> last(deps, deps + ndeps);
-            cudaGraph_t out = nullptr;
-            capturing = false;
-            cuda_check(cudaStreamEndCapture(ctx->stream, &out), "capture prefix end");
-            prefix_launches_ = ctx->launches - before;
-            cudaGraphNodeParams cp = {};
-            cp.type = cudaGraphNodeTypeConditional;
-            cp.conditional.handle = handle;
-            cp.conditional.type = cudaGraphCondTypeWhile;
-            cp.conditional.size = 1;
-            cudaGraphNode_t loop;
-            cuda_check(cudaGraphAddNode(&loop, g, last.data(), last.size(), &cp), "while node");
-            cudaGraph_t body = cp.conditional.phGraph_out[0];
-            const int64_t b0 = ctx->launches;
-            cuda_check(cudaStreamBeginCaptureToGraph(ctx->stream, body, nullptr, nullptr, 0,
-                                                     cudaStreamCaptureModeThreadLocal),
-                       "capture body");
-            capturing = true;
-            enqueue_iteration(ctx);
-            launch_kernel(ctx, "set_continue", k_set_continue, 1, 1, 0, handle, state_.data());
-            capturing = false;
-            cuda_check(cudaStreamEndCapture(ctx->stream, &out), "capture body end");
-            per_iteration_ = ctx->launches - b0;
-            const int64_t s0 = ctx->launches;
-            cuda_check(cudaStreamBeginCaptureToGraph(ctx->stream, g, &loop, nullptr, 1,
-                                                     cudaStreamCaptureModeThreadLocal),
-                       "capture suffix");
-            capturing = true;
-            enqueue_suffix(ctx);
-            capturing = false;
-            cuda_check(cudaStreamEndCapture(ctx->stream, &out), "capture suffix end");
-            suffix_launches_ = ctx->launches - s0;
+            add_solve_nodes(ctx, g, false);
             cuda_check(cudaGraphInstantiate(&solve_exec_, g, 0), "solve graph instantiate");
         } catch (const Failure &) {
-            if (capturing) {
-                cudaGraph_t junk = nullptr;
-                cudaStreamEndCapture(ctx->stream, &junk);
-            }
-            cudaGetLastError();
+            end_open_capture(ctx);
             solve_exec_ = nullptr;
             solve_graph_failed_ = true;
         }
         if (g) cudaGraphDestroy(g);
-        ctx->launches = before;
+    }
+
+    static void end_open_capture(tf_ctx *ctx) {
+        cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+        if (cudaStreamIsCapturing(ctx->stream, &st) == cudaSuccess && st != cudaStreamCaptureStatusNone) {
+            cudaGraph_t junk = nullptr;
+            cudaStreamEndCapture(ctx->stream, &junk);
+            if (junk) cudaGraphDestroy(junk);
+        }
+        cudaGetLastError();
+    }
+
+    KState initial_state() const {
+        KState init{};
+        init.tol = opt_.absolute_tolerance;
+        init.res = opt_.relative_tolerance;
+        init.max_it = opt_.max_iterations;
+        init.interval = opt_.residual_refresh_interval;
+        init.status = TF_MAX_ITERATIONS;
+        return init;
     }
 
     void run_iteration(tf_ctx *ctx) {
@@ -861,6 +911,7 @@ class KrylovImpl final : public Krylov {
     cudaGraphExec_t solve_exec_{nullptr};
     bool solve_graph_failed_{false};
     int64_t prefix_launches_{0}, suffix_launches_{0};
+    int64_t generation_{0};
     bool capture_failed_{false};
     int64_t per_iteration_{0};
     cudaEvent_t ev0_{nullptr}, ev1_{nullptr};

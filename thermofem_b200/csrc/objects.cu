@@ -35,6 +35,20 @@ struct tf_solver {
     std::unique_ptr<tf_amg> view;        // borrowed view of the AMG preconditioner
 };
 
+struct tf_batch {
+    tf_ctx *ctx{nullptr};
+    std::vector<tf_solver *> solvers;
+    std::vector<int64_t> generations;  // of the solvers when the graph was built
+    cudaGraphExec_t exec{nullptr};
+    bool graph_failed{false};
+    void *pinned{nullptr};  // one state record per solver, read back after a launch
+    size_t state_bytes{0};
+    ~tf_batch() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (pinned) cudaFreeHost(pinned);
+    }
+};
+
 namespace {
 
 void check_types(int value_type, int index_type) {
@@ -364,6 +378,89 @@ int tf_solver_set_graph_mode(tf_solver *s, int mode) {
     return guard([&] {
         require(s != nullptr && (mode == 0 || mode == 1), "graph mode must be 0 or 1");
         s->k->graph_mode = mode;
+    });
+}
+
+int tf_batch_create(tf_ctx *ctx, int count, tf_solver *const *solvers, tf_batch **out) {
+    return guard([&] {
+        require(out != nullptr, "null argument");
+        *out = nullptr;
+        check_ctx(ctx);
+        require(count >= 1 && solvers != nullptr, "a batch needs at least one solver");
+        auto b = std::make_unique<tf_batch>();
+        b->ctx = ctx;
+        for (int k = 0; k < count; ++k) {
+            require(solvers[k] != nullptr && solvers[k]->ctx == ctx, "batched solvers must share the batch context");
+            for (int j = 0; j < k; ++j) require(solvers[j] != solvers[k], "a solver appears twice in the batch");
+            b->solvers.push_back(solvers[k]);
+        }
+        DeviceScope scope(ctx->device);
+        b->state_bytes = (b->solvers.front()->k->state_bytes() + 15) & ~size_t(15);
+        cuda_check(cudaMallocHost(&b->pinned, b->state_bytes * static_cast<size_t>(count)), "cudaMallocHost");
+        *out = b.release();
+    });
+}
+
+int tf_batch_destroy(tf_batch *b) {
+    return guard([&] {
+        if (!b) return;
+        DeviceScope scope(b->ctx->device);
+        delete b;
+    });
+}
+
+int tf_batch_apply(tf_batch *b, const void *const *rhs, void *const *x, tf_solve_result *results) {
+    return guard([&] {
+        require(b != nullptr && rhs != nullptr && x != nullptr && results != nullptr, "null argument");
+        tf_ctx *ctx = b->ctx;
+        DeviceScope scope(ctx->device);
+        const size_t count = b->solvers.size();
+        bool stale = b->exec == nullptr;
+        for (size_t k = 0; k < count; ++k) {
+            require(rhs[k] != nullptr && x[k] != nullptr, "null vector");
+            const int64_t g = b->solvers[k]->k->generation();
+            if (g == 0) fail(TF_ERR_LOGIC, "batched solver requires setup");
+            if (b->generations.size() != count || b->generations[k] != g) stale = true;
+        }
+        if (stale && !b->graph_failed) {
+            // every solve as an independent branch of one graph
+            if (b->exec) cudaGraphExecDestroy(b->exec);
+            b->exec = nullptr;
+            cudaGraph_t g = nullptr;
+            try {
+                cuda_check(cudaGraphCreate(&g, 0), "graph create");
+                for (auto *s : b->solvers) s->k->batch_nodes(ctx, g);
+                cuda_check(cudaGraphInstantiate(&b->exec, g, 0), "batch graph instantiate");
+            } catch (const Failure &) {
+                cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+                if (cudaStreamIsCapturing(ctx->stream, &st) == cudaSuccess && st != cudaStreamCaptureStatusNone) {
+                    cudaGraph_t junk = nullptr;
+                    cudaStreamEndCapture(ctx->stream, &junk);
+                    if (junk) cudaGraphDestroy(junk);
+                }
+                cudaGetLastError();
+                b->exec = nullptr;
+                b->graph_failed = true;
+            }
+            if (g) cudaGraphDestroy(g);
+            b->generations.clear();
+            for (auto *s : b->solvers) b->generations.push_back(s->k->generation());
+        }
+        if (!b->exec) {
+            // CUDA refused the batch graph: the same solves one by one
+            for (size_t k = 0; k < count; ++k) results[k] = b->solvers[k]->k->solve(ctx, rhs[k], x[k]);
+            return;
+        }
+        for (size_t k = 0; k < count; ++k) b->solvers[k]->k->batch_stage(ctx, rhs[k], x[k]);
+        cuda_check(cudaGraphLaunch(b->exec, ctx->stream), "batch graph launch");
+        unsigned char *host = static_cast<unsigned char *>(b->pinned);
+        for (size_t k = 0; k < count; ++k) b->solvers[k]->k->batch_finish(ctx, x[k], host + k * b->state_bytes);
+        cuda_check(cudaStreamSynchronize(ctx->stream), "batch");
+        for (size_t k = 0; k < count; ++k) {
+            results[k] = b->solvers[k]->k->batch_result(host + k * b->state_bytes);
+            ctx->launches += b->solvers[k]->k->batch_launches(results[k].iterations);
+        }
+        check_faults(ctx);
     });
 }
 

@@ -176,3 +176,38 @@ def write_matrix_market(path: str, offsets, indices, values, symmetric: bool = F
         f.write(f"{n} {n} {len(v)}\n")
         for a, b, x in zip(r.tolist(), c.tolist(), v.tolist()):
             f.write(f"{a} {b} {x!r}\n")
+
+
+def transient3d(m: int, r: float):
+    """Backward-Euler step operator of 3-D heat conduction on m^3 cells,
+    scaled by 1/(k h): A = (1/r) I + K7, K7 the 7-point stencil (6 on the
+    diagonal, -1 per interior neighbour; Dirichlet walls), r = dt k / h^2."""
+    n, i, ix, iy, iz = _grid3(m)
+    mm = m * m
+    steps = [-mm, -m, -1, 1, m, mm]
+    valid = [iz > 0, iy > 0, ix > 0, ix < m - 1, iy < m - 1, iz < m - 1]
+    cols = np.empty((n, 7), np.int64)
+    vals = np.empty((n, 7), np.float64)
+    mask = np.empty((n, 7), bool)
+    for s, step, ok in zip([0, 1, 2, 4, 5, 6], steps, valid):
+        cols[:, s] = np.where(ok, i + step, i)
+        vals[:, s] = -1.0
+        mask[:, s] = ok
+    cols[:, 3] = i
+    vals[:, 3] = 6.0 + 1.0 / r
+    mask[:, 3] = True
+    return _csr_from_stencil(cols, vals, mask)
+
+
+def batched_transient(count: int = 48, seed: int = 1004, side_min: int = 16, side_max: int = 96):
+    """The batched transient workload: `count` independent problems with
+    sides uniform in [side_min, side_max], r = dt k / h^2 uniform in
+    [0.1, 10] and initial temperatures uniform in [0, 1] (problem k uses
+    streams of seed + k).  Returns [(m, r, (offsets, indices, values), T0)]."""
+    out = []
+    for k in range(count):
+        u = uniform(seed + k, 2, 7)
+        m = side_min + min(int(u[0] * (side_max - side_min + 1)), side_max - side_min)
+        r = 0.1 + 9.9 * float(u[1])
+        out.append((m, r, transient3d(m, r), uniform(seed + k, m * m * m, 8)))
+    return out
