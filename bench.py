@@ -157,6 +157,102 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_workload(args):
+    """Single-GPU measurements of the other BASELINE configs (synthetic
+    inputs of the stated shapes; device times from CUDA events)."""
+    import torch
+    import thermofem_b200 as tf
+    from thermofem_b200 import problems as P
+    ctx = tf.Context(0)
+
+    def events():
+        return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    if args.workload == "batched":
+        probs = P.batched_transient(48, seed=1004)
+        solvers = []
+        t0 = time.perf_counter()
+        for m, r, mat, _ in probs:
+            s = tf.Cg(tf.solver_options(), "amg", tf.amg_options(hierarchy_type="f32", **AMG, **_small(args)),
+                      ctx=ctx)
+            s.setup(tf.DeviceCsr.from_host(*mat))
+            solvers.append(s)
+        setup_s = time.perf_counter() - t0
+        batch = tf.Batch(solvers, ctx=ctx)
+        t_init = [torch.tensor(p[3], device="cuda") for p in probs]
+        steps = 20
+        out = {}
+        for mode in ("batched", "one_by_one", "batched"):
+            temps = [t.clone() for t in t_init]
+            its = 0
+            ok = True
+            e0, e1 = events()
+            e0.record(ctx.stream)
+            for _ in range(steps):
+                rhs = [t / p[1] for t, p in zip(temps, probs)]
+                xs = [t.clone() for t in temps]
+                if mode == "batched":
+                    reps = batch.apply(rhs, xs)
+                else:
+                    reps = [s.apply(b, x) for s, b, x in zip(solvers, rhs, xs)]
+                its += sum(r["iterations"] for r in reps)
+                ok = ok and all(r["status"] == "Converged" for r in reps)
+                temps = xs
+            e1.record(ctx.stream)
+            torch.cuda.synchronize()
+            out[mode] = {"s_per_step": e0.elapsed_time(e1) / 1e3 / steps, "iterations": its, "converged": ok}
+        rows = sum(p[0] ** 3 for p in probs)
+        print(json.dumps({
+            "workload": "batched transient: 48 backward-Euler 3-D 7-point problems, sides U{16..96} "
+                        f"({rows} rows in all), r = dt k/h^2 U[0.1,10], 20 steps, AMG-PCG V FP32 / FP64 outer, rtol 1e-8",
+            "metric": "seconds per time step (all 48 systems)", "unit": "s",
+            "batched": out["batched"], "one_by_one": out["one_by_one"],
+            "speedup_batched": out["one_by_one"]["s_per_step"] / out["batched"]["s_per_step"],
+            "setup_s": setup_s, "data": "synthetic (seeded generator)"}), flush=True)
+        return
+    if args.workload == "convdiff":
+        m = args.size or 192
+        off, idx, val = P.convdiff3d(m, 1003)
+        kind, label, cycle = tf.BiCgStab, "BiCGStab + AMG W-cycle", "w"
+    else:
+        m = args.size or 256
+        off, idx, val = P.heat3d(m, SEED_MATRIX)
+        kind, label, cycle = tf.Cg, "PCG + AMG V-cycle", "v"
+    n = len(off) - 1
+    a = tf.DeviceCsr.from_host(off, idx, val)
+    del off, idx, val
+    b = torch.tensor(P.rhs_uniform(n, SEED_RHS), device="cuda")
+    res = {}
+    for hier in ("f32", "f64"):
+        opts = dict(AMG, cycle=cycle)
+        s = kind(tf.solver_options(), "amg", tf.amg_options(hierarchy_type=hier, **opts, **_small(args)), ctx=ctx)
+        t0 = time.perf_counter()
+        s.setup(a)
+        torch.cuda.synchronize()
+        setup_s = time.perf_counter() - t0
+        times = []
+        for k in range(1 + args.steps):
+            x = torch.zeros(n, dtype=torch.float64, device="cuda")
+            e0, e1 = events()
+            e0.record(ctx.stream)
+            rep = s.apply(b, x)
+            e1.record(ctx.stream)
+            torch.cuda.synchronize()
+            if k:
+                times.append(e0.elapsed_time(e1) / 1e3)
+        r = tf.residual(a, b, x, ctx=ctx)
+        true_rel = float(torch.linalg.norm(r) / torch.linalg.norm(b))
+        res[hier] = {"s": sorted(times)[len(times) // 2], "iterations": rep["iterations"], "status": rep["status"],
+                     "true_relative_residual": true_rel, "setup_s": setup_s}
+        del s
+    print(json.dumps({
+        "workload": f"{args.workload} {m}^3 ({n} rows, {a.nnz} nnz), {label}, Jacobi w=2/3 V/W(1,1), rtol 1e-8",
+        "metric": "time-to-1e-8 FP64 relative residual (s), median", "unit": "s",
+        "mixed_f32_hierarchy": res["f32"], "plain_fp64": res["f64"],
+        "speedup_mixed_vs_fp64": res["f64"]["s"] / res["f32"]["s"], "data": "synthetic (seeded generator)"}),
+        flush=True)
+
+
 def _small(args):
     return {} if args.small_level_rows is None else {"small_level_rows": args.small_level_rows}
 
@@ -220,11 +316,17 @@ def main():
                     help="tf_amg_options.small_level_rows (default: the library default)")
     ap.add_argument("--profile", choices=["mixed", "fp64", "spmv"], default=None,
                     help="profiling run: setup, --warmup solves, then --steps solves of one path; no JSON line")
+    ap.add_argument("--workload", choices=["batched", "convdiff", "heat"], default=None,
+                    help="the other BASELINE configs (one JSON line each, not the headline): batched = 48 "
+                         "transient systems x 20 steps; convdiff = 192^3 BiCGStab W-cycle; heat = --size^3 heat")
+    ap.add_argument("--size", type=int, default=None, help="grid side of --workload convdiff/heat")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
     if args.profile:
         return run_profile(args)
+    if args.workload:
+        return run_workload(args)
 
     import torch
     import thermofem_b200 as tf
