@@ -227,6 +227,9 @@ int tf_coarse_lu_solve(tf_ctx *ctx, int rows, const double *lu, const int32_t *p
 /* ---- components (include/Smoother/Jacobi.cuh, include/Preconditioner/
  *      Amg.cuh, include/Solver/{Cg,BiCgStab}.cuh) ------------------------ */
 /* AmgOptions (Amg.cuh:14-25) plus the precision extension. */
+/* A learned per-row Jacobi damping model (tf_mlp_*, below). */
+typedef struct tf_mlp tf_mlp;
+
 typedef struct {
     int max_levels;          /* 1..20, default 20 */
     int coarse_rows;         /* 1..256, default 64 */
@@ -243,6 +246,9 @@ typedef struct {
     int small_level_rows;    /* levels (below the finest) with <= this many rows run each sub-cycle as one
                                 launch out of shared memory (one CTA when they fit, else a thread-block
                                 cluster); default 1200, 0 launches every level step separately */
+    const tf_mlp *damping_model; /* NULL (default): every smoother sweeps with jacobi_weight; else each row
+                                    of each level is damped by the model's omega_i (weights copied at
+                                    create time) -- no reference counterpart */
 } tf_amg_options;
 void tf_amg_options_default(tf_amg_options *o);
 
@@ -348,6 +354,36 @@ typedef struct tf_batch tf_batch;
 int tf_batch_create(tf_ctx *ctx, int count, tf_solver *const *solvers, tf_batch **out);
 int tf_batch_destroy(tf_batch *b);
 int tf_batch_apply(tf_batch *b, const void *const *rhs, void *const *x, tf_solve_result *results);
+
+/* ---- Learned per-row damping (no reference counterpart) -----------------
+ * A 2-layer MLP (4 row features -> 32 ReLU units -> 1, BF16 weights, FP32
+ * accumulation) maps each row of a level operator to a Jacobi damping
+ * omega_i = omega_min + (omega_max - omega_min) * sigmoid(z).  Features
+ * (tf_row_features, n x 4 floats, row-major): log(|a_ii| / mean_j |a_jj|),
+ * sum_j!=i |a_ij| / |a_ii|, row nonzeros / 8, level index / 10.  Training is
+ * on the GPU with the library's own kernels: tf_mlp_backward accumulates the
+ * gradient of the mean squared error to per-row targets (deterministic,
+ * fixed reduction order), tf_mlp_sgd takes a momentum step on the FP32
+ * master weights with the mean gradient and clears it.  A new model starts
+ * near omega = 2/3 (the fixed-weight smoother) for every row.  Parameters
+ * (TF_MLP_PARAMS floats): W1[32][4], b1[32], w2[32], b2. */
+#define TF_MLP_FEATURES 4
+#define TF_MLP_HIDDEN 32
+#define TF_MLP_PARAMS (TF_MLP_HIDDEN * TF_MLP_FEATURES + 2 * TF_MLP_HIDDEN + 1)
+int tf_mlp_create(tf_ctx *ctx, uint64_t seed, double omega_min, double omega_max, tf_mlp **out);
+int tf_mlp_destroy(tf_mlp *m);
+int tf_mlp_get_params(const tf_mlp *m, float *host_params);
+int tf_mlp_set_params(tf_mlp *m, const float *host_params);
+int tf_mlp_bounds(const tf_mlp *m, double *omega_min, double *omega_max);
+int tf_row_features(tf_ctx *ctx, const tf_csr *a, int level, float *features);
+/* omega (n floats, device) from features (n x 4, device); BF16 weights. */
+int tf_mlp_forward(tf_mlp *m, int64_t n, const float *features, float *omega);
+/* Adds the gradient of sum_i (omega_i - target_i)^2 over the batch to the
+ * model's accumulator; *loss (nullable) = the batch's mean squared error. */
+int tf_mlp_backward(tf_mlp *m, int64_t n, const float *features, const float *target, double *loss);
+/* The accumulated gradient sums (TF_MLP_PARAMS doubles, host). */
+int tf_mlp_get_gradient(const tf_mlp *m, double *host_gradient);
+int tf_mlp_sgd(tf_mlp *m, double lr, double momentum);
 
 /* ---- Matrix Market input (include/IO/MatrixMarket.cuh:14-31) ----------- */
 typedef struct {

@@ -412,3 +412,65 @@ def ref_std_mt19937(seed, count):
     out = np.zeros(count, np.uint32)
     ref().ref_std_mt19937(seed, count, _ptr(out))
     return out
+
+
+# ---- learned damping: a NumPy restatement of the row features and the MLP
+# (thermofem_b200/csrc/mlp.cu), FP64 arithmetic on the BF16-rounded weights.
+
+MLP_F, MLP_H = 4, 32
+MLP_P = MLP_H * MLP_F + 2 * MLP_H + 1
+
+
+def bf16_round(p):
+    """float32 values rounded to BF16 (nearest, ties to even), as float32."""
+    u = np.ascontiguousarray(p, dtype=np.float32).view(np.uint32).astype(np.uint64)
+    u = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16) << 16
+    return (u & 0xFFFFFFFF).astype(np.uint32).view(np.float32)
+
+
+def mlp_features(off, idx, val, level):
+    off = np.asarray(off, np.int64)
+    n = len(off) - 1
+    rows = np.repeat(np.arange(n), np.diff(off))
+    val = np.asarray(val, np.float64)
+    on = np.asarray(idx) == rows
+    d = np.zeros(n)
+    np.add.at(d, rows[on], val[on])
+    offs = np.zeros(n)
+    np.add.at(offs, rows[~on], np.abs(val[~on]))
+    ad = np.abs(d)
+    mean = ad.sum() / n
+    f = np.zeros((n, MLP_F))
+    ok = (ad > 0) & (mean > 0)
+    f[ok, 0] = np.log(ad[ok] / mean)
+    f[ad > 0, 1] = offs[ad > 0] / ad[ad > 0]
+    f[:, 2] = np.diff(off) * 0.125
+    f[:, 3] = level * 0.1
+    return f.astype(np.float32)
+
+
+def _mlp_parts(params):
+    w = bf16_round(params).astype(np.float64)
+    k = MLP_H * MLP_F
+    return w[:k].reshape(MLP_H, MLP_F), w[k:k + MLP_H], w[k + MLP_H:k + 2 * MLP_H], w[-1]
+
+
+def mlp_forward(params, x, lo, hi):
+    W1, b1, w2, b2 = _mlp_parts(params)
+    a = np.asarray(x, np.float64) @ W1.T + b1
+    z = np.maximum(a, 0.0) @ w2 + b2
+    return lo + (hi - lo) / (1.0 + np.exp(-z))
+
+
+def mlp_gradient(params, x, target, lo, hi):
+    """Sum over rows of the gradient of (omega - target)^2, and the loss sum."""
+    W1, b1, w2, b2 = _mlp_parts(params)
+    x = np.asarray(x, np.float64)
+    a = x @ W1.T + b1
+    h = np.maximum(a, 0.0)
+    s = 1.0 / (1.0 + np.exp(-(h @ w2 + b2)))
+    e = lo + (hi - lo) * s - np.asarray(target, np.float64)
+    dz = 2.0 * e * (hi - lo) * s * (1.0 - s)
+    dh = np.where(a > 0, dz[:, None] * w2[None, :], 0.0)
+    g = np.concatenate([(dh.T @ x).ravel(), dh.sum(0), (dz[:, None] * h).sum(0), [dz.sum()]])
+    return g, float((e * e).sum())

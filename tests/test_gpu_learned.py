@@ -1,0 +1,88 @@
+"""Learned per-row damping (tf_mlp_*, tf_row_features): features, forward
+and gradient against the NumPy oracle, training with the library's kernels,
+the hierarchy using the model, and what the trained model gains."""
+import numpy as np
+import pytest
+import torch
+
+import thermofem_b200 as tf
+from conftest import to_device
+from oracle import oracle as O
+from thermofem_b200 import learned as L
+from thermofem_b200 import problems as P
+
+pytestmark = pytest.mark.gpu
+
+
+def test_row_features_match_oracle(ctx):
+    off, idx, val = P.heat3d(12, seed=3)
+    for dtype in (torch.float64, torch.float32):
+        f = tf.row_features(to_device((off, idx, val), dtype=dtype), level=2, ctx=ctx).cpu().numpy()
+        ref = O.mlp_features(off, idx, val.astype(np.float32) if dtype == torch.float32 else val, 2)
+        assert np.allclose(f, ref, rtol=1e-6, atol=1e-6)
+
+
+def test_forward_and_gradient_match_oracle(ctx):
+    rng = np.random.default_rng(4)
+    m = tf.Mlp(seed=11, omega_min=0.3, omega_max=1.2, ctx=ctx)
+    p = rng.standard_normal(tf.MLP_PARAMS).astype(np.float32) * 0.5
+    m.set_params(p)
+    assert np.array_equal(m.params(), p)
+    x = rng.standard_normal((1000, 4)).astype(np.float32)
+    t = rng.uniform(0.5, 1.0, 1000).astype(np.float32)
+    xd, td = torch.tensor(x, device="cuda"), torch.tensor(t, device="cuda")
+    om = m.forward(xd).cpu().numpy()
+    assert np.allclose(om, O.mlp_forward(p, x, 0.3, 1.2), rtol=1e-5, atol=1e-6)
+    loss = m.backward(xd, td)
+    g = m.gradient()
+    gref, lref = O.mlp_gradient(p, x, t, 0.3, 1.2)
+    assert abs(loss - lref / 1000) <= 1e-5 * lref / 1000
+    assert np.allclose(g, gref, rtol=1e-4, atol=1e-4 * np.abs(gref).max())
+    # deterministic: the same batch gives the same sums
+    m2 = tf.Mlp(seed=11, ctx=ctx, params=p)
+    m2.backward(xd, td)
+    assert np.array_equal(m2.gradient(), g)
+    # one SGD step moves the master weights by -lr * mean gradient
+    m.sgd(0.1, momentum=0.0)
+    assert np.allclose(m.params(), p - 0.1 * (gref / 1000), rtol=1e-4, atol=1e-5)
+
+
+def test_new_model_starts_at_fixed_damping(ctx):
+    m = tf.Mlp(seed=5, ctx=ctx)
+    f = tf.row_features(to_device(P.heat3d(10, seed=1)), 0, ctx=ctx)
+    om = m.forward(f)
+    assert torch.allclose(om, torch.full_like(om, 2 / 3), atol=0.05)
+
+
+def test_training_reduces_error_and_hierarchy_uses_model(ctx):
+    x, y = L.training_set(count=3, side_min=12, side_max=16, seed=5000, rows_per_level=512, ctx=ctx)
+    assert x.shape[0] == y.shape[0] > 0 and set(np.unique(y.cpu().numpy())) <= set(np.float32(L.CANDIDATES))
+    model, hist = L.train(x, y, epochs=30, batch=2048, ctx=ctx)
+    assert hist[-1] < hist[0]
+    # a hierarchy built with the model: dinv scaled by the model's omega
+    m = P.heat3d(14, seed=9)
+    a = to_device(m)
+    plain = tf.Amg(tf.amg_options(jacobi_weight=1.0, hierarchy_type="f64", small_level_rows=0), ctx=ctx)
+    learned = tf.Amg(tf.amg_options(damping_model=model, hierarchy_type="f64", small_level_rows=0), ctx=ctx)
+    plain.setup(a)
+    learned.setup(a)
+    b = torch.tensor(P.rhs_uniform(len(m[0]) - 1, 3), device="cuda")
+    assert not torch.equal(plain.apply(b), learned.apply(b))
+    s = tf.Cg(tf.solver_options(), "amg", tf.amg_options(damping_model=model, hierarchy_type="f32"), ctx=ctx)
+    s.setup(a)
+    x0 = torch.zeros_like(b)
+    assert s.apply(b, x0)["status"] == "Converged"
+    r = tf.residual(a, b, x0, ctx=ctx)
+    assert float(torch.linalg.norm(r) / torch.linalg.norm(b)) <= 1.0001e-8
+
+
+def test_shipped_model_is_no_worse_than_fixed_damping(ctx):
+    # The committed model (trained by `python -m thermofem_b200.learned
+    # train`) on a held-out problem: F-cycle PCG and BiCGStab iterations
+    # with learned damping against fixed w = 2/3.
+    model = L.load(ctx=ctx)
+    res = L.evaluate(model, m=40, seed=9000, ctx=ctx)
+    for kind in ("pcg", "bicgstab"):
+        assert res[f"{kind}_learned"]["status"] == "Converged"
+        assert res[f"{kind}_learned"]["true_relative_residual"] <= 1.0001e-8
+        assert res[f"{kind}_learned"]["iterations"] <= res[f"{kind}_fixed_2_3"]["iterations"]

@@ -73,7 +73,8 @@ class AmgOptions(C.Structure):
                 ("pre_sweeps", C.c_int), ("post_sweeps", C.c_int), ("coarse_sweeps", C.c_int),
                 ("jacobi_weight", C.c_double), ("strength_threshold", C.c_double),
                 ("absorb_singletons", C.c_int), ("compact_sort_keys", C.c_int), ("cycle", C.c_int),
-                ("hierarchy_type", C.c_int), ("coarse_lu_rows", C.c_int), ("small_level_rows", C.c_int)]
+                ("hierarchy_type", C.c_int), ("coarse_lu_rows", C.c_int), ("small_level_rows", C.c_int),
+                ("damping_model", C.c_void_p)]
 
 
 class SolverOptions(C.Structure):
@@ -174,6 +175,16 @@ SIGNATURES = {
     "tf_batch_destroy": ([_P], _I),
     "tf_batch_apply": ([_P, _PP, _PP, C.POINTER(SolveResult)], _I),
     "tf_amg_level_spmv": ([_P, _I, _P, _P], _I),
+    "tf_mlp_create": ([_P, C.c_uint64, _D, _D, _PP], _I),
+    "tf_mlp_destroy": ([_P], _I),
+    "tf_mlp_get_params": ([_P, C.POINTER(C.c_float)], _I),
+    "tf_mlp_set_params": ([_P, C.POINTER(C.c_float)], _I),
+    "tf_mlp_bounds": ([_P, C.POINTER(C.c_double), C.POINTER(C.c_double)], _I),
+    "tf_row_features": ([_P, C.POINTER(Csr), _I, _P], _I),
+    "tf_mlp_forward": ([_P, _L, _P, _P], _I),
+    "tf_mlp_backward": ([_P, _L, _P, _P, C.POINTER(C.c_double)], _I),
+    "tf_mlp_get_gradient": ([_P, C.POINTER(C.c_double)], _I),
+    "tf_mlp_sgd": ([_P, _D, _D], _I),
     "tf_read_matrix_market": ([C.c_char_p, _S, C.POINTER(HostCsr)], _I),
     "tf_read_matrix_market_file": ([C.c_char_p, C.POINTER(HostCsr)], _I),
     "tf_host_csr_free": ([C.POINTER(HostCsr)], None),

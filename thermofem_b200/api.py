@@ -12,7 +12,8 @@ import torch
 from . import (AmgOptions, Csr, HostCsr, SolveResult, SolverOptions, F32, F64, I32, I64, CYCLE, SOLVER_CG,
                SOLVER_BICGSTAB, PRECOND_AMG, PRECOND_IDENTITY, check, lib)
 
-__all__ = ["Context", "DeviceCsr", "Transfer", "Amg", "Jacobi", "Cg", "BiCgStab", "Batch", "amg_options", "solver_options",
+__all__ = ["Context", "DeviceCsr", "Transfer", "Amg", "Jacobi", "Cg", "BiCgStab", "Batch", "Mlp", "row_features", "MLP_PARAMS",
+           "MLP_FEATURES", "MLP_HIDDEN", "amg_options", "solver_options",
            "read_matrix_market", "read_matrix_market_file", "spmv", "autotune_spmv", "set_spmv_config", "residual", "jacobi_sweep", "jacobi_zero",
            "inverse_diagonal", "restrict_aggregates", "prolong_aggregates", "dot_multi", "axpby", "convert",
            "csr_validate", "check_canonical", "canonicalize", "row_stats", "strength", "match", "contract",
@@ -443,6 +444,9 @@ def amg_options(**kw) -> AmgOptions:
     for k, v in kw.items():
         if k == "cycle" and isinstance(v, str):
             v = CYCLE[v.lower()]
+        if k == "damping_model":
+            o._damping_model_ref = v  # the model must live until the options are used
+            v = v.h.value if v is not None else None
         if k == "hierarchy_type" and not isinstance(v, int):
             v = {torch.float32: F32, torch.float64: F64, "f32": F32, "f64": F64, None: -1}[v]
         if not hasattr(o, k):
@@ -708,3 +712,69 @@ class Batch:
         with self.ctx:
             check(lib().tf_batch_apply(self.h, r, x, res))
         return [res[k].as_dict() for k in range(n)]
+
+
+MLP_FEATURES, MLP_HIDDEN = 4, 32
+MLP_PARAMS = MLP_HIDDEN * MLP_FEATURES + 2 * MLP_HIDDEN + 1
+
+
+class Mlp:
+    """Learned per-row Jacobi damping (tf_mlp_*): 4 row features -> 32 ReLU
+    units -> omega in [omega_min, omega_max]; BF16 weights, FP32 master
+    copy, trained with the library's forward/backward/SGD kernels."""
+
+    def __init__(self, seed=0, omega_min=0.3, omega_max=1.2, ctx=None, params=None):
+        self.ctx = _ctx(ctx)
+        h = C.c_void_p()
+        check(lib().tf_mlp_create(self.ctx.h, int(seed), float(omega_min), float(omega_max), C.byref(h)))
+        self.h = h
+        self.omega_min, self.omega_max = float(omega_min), float(omega_max)
+        if params is not None:
+            self.set_params(params)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            _release("tf_mlp_destroy", self.h)
+            self.h = None
+
+    def params(self) -> np.ndarray:
+        p = np.zeros(MLP_PARAMS, np.float32)
+        check(lib().tf_mlp_get_params(self.h, p.ctypes.data_as(C.POINTER(C.c_float))))
+        return p
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        if p.size != MLP_PARAMS:
+            raise ValueError(f"expected {MLP_PARAMS} parameters")
+        check(lib().tf_mlp_set_params(self.h, p.ctypes.data_as(C.POINTER(C.c_float))))
+
+    def forward(self, features):
+        out = torch.empty(features.shape[0], dtype=torch.float32, device=features.device)
+        with self.ctx:
+            check(lib().tf_mlp_forward(self.h, features.shape[0], _p(features), _p(out)))
+        return out
+
+    def backward(self, features, target) -> float:
+        loss = C.c_double()
+        with self.ctx:
+            check(lib().tf_mlp_backward(self.h, features.shape[0], _p(features), _p(target), C.byref(loss)))
+        return loss.value
+
+    def gradient(self) -> np.ndarray:
+        g = np.zeros(MLP_PARAMS, np.float64)
+        check(lib().tf_mlp_get_gradient(self.h, g.ctypes.data_as(C.POINTER(C.c_double))))
+        return g
+
+    def sgd(self, lr, momentum=0.9):
+        with self.ctx:
+            check(lib().tf_mlp_sgd(self.h, float(lr), float(momentum)))
+
+
+def row_features(a: DeviceCsr, level=0, ctx=None):
+    """n x 4 row features of a level operator (tf_row_features)."""
+    ctx = _ctx(ctx)
+    out = torch.empty((a.rows, MLP_FEATURES), dtype=torch.float32, device=a.values.device)
+    d = a.desc()
+    with ctx:
+        check(lib().tf_row_features(ctx.h, C.byref(d), int(level), _p(out)))
+    return out

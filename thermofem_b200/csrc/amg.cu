@@ -18,6 +18,7 @@
 
 #include "coarse_cycle.cuh"
 #include "engine.cuh"
+#include "mlp.cuh"
 
 namespace tfb {
 
@@ -31,6 +32,7 @@ AmgConfig::AmgConfig(const tf_amg_options &opt) : o(opt) {
         (p.hierarchy_type != -1 && p.hierarchy_type != TF_F32 && p.hierarchy_type != TF_F64) ||
         p.coarse_lu_rows < 1 || p.coarse_lu_rows > 256 || p.small_level_rows < 0)
         fail(TF_ERR_INVALID, "Invalid AMG options");
+    model = damping_model_of(p.damping_model);
 }
 
 std::unique_ptr<tf_dcsr> to_native(tf_ctx *ctx, const tf_csr &a) {
@@ -89,7 +91,7 @@ struct Level {
 template <class S>
 class HierarchyImpl final : public Hierarchy {
   public:
-    HierarchyImpl(const AmgConfig &cfg) : cfg_(cfg), w_(static_cast<S>(cfg.o.jacobi_weight)) {
+    HierarchyImpl(const AmgConfig &cfg) : cfg_(cfg), w_(static_cast<S>(cfg.model ? 1.0 : cfg.o.jacobi_weight)) {
         // THERMOFEM_B200_FUSE: 0 launches every transfer on its own, 1 fuses
         // restrictions everywhere and prolongations into fine levels of at
         // most kScatterRows rows, 2 fuses every prolongation.
@@ -124,6 +126,8 @@ class HierarchyImpl final : public Hierarchy {
             for (auto *b : {&l.dinv, &l.rhs, &l.x0, &l.x1, &l.r}) b->allocate(static_cast<size_t>(l.n));
             // The diagonal must also invert in the iteration precision.
             inverse_diagonal(ctx, l.csr(), l.dinv.data());
+            // learned damping: dinv_i scaled by omega_i, sweeps with weight 1
+            if (cfg_.model) learned_damping(ctx, *cfg_.model, l.csr(), depth, l.dinv.data());
             if (delta_columns_enabled() && l.nnz > 0) {
                 l.cd.allocate(static_cast<size_t>(l.nnz));
                 if (!delta_columns(ctx, l.n, l.rp.data(), l.ci.data(), l.cd.data())) l.cd.release();

@@ -2,6 +2,7 @@
 // component API (include/Preconditioner/Amg.cuh, include/Solver/Cg.cuh,
 // include/Solver/BiCgStab.cuh of the reference).
 #pragma once
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -15,8 +16,11 @@ struct LevelStats {
 };
 
 // Validated copy of tf_amg_options.
+struct DampingModel;
+
 struct AmgConfig {
     tf_amg_options o;
+    std::shared_ptr<const DampingModel> model;  // per-row damping (snapshot of o.damping_model)
     explicit AmgConfig(const tf_amg_options &opt);
 };
 

@@ -81,6 +81,7 @@ void tf_amg_options_default(tf_amg_options *o) {
     o->hierarchy_type = -1;
     o->coarse_lu_rows = 64;
     o->small_level_rows = 1200;
+    o->damping_model = nullptr;
 }
 
 void tf_solver_options_default(int value_type, tf_solver_options *o) {
