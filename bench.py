@@ -158,57 +158,121 @@ def run_reference(args):
 
 
 def run_workload(args):
-    """Single-GPU measurements of the other BASELINE configs (synthetic
-    inputs of the stated shapes; device times from CUDA events)."""
+    """Measurements of the other BASELINE configs (synthetic inputs of the
+    stated shapes; device times from CUDA events).  The batched workload
+    shards its systems over the ranks of a torchrun launch (longest first to
+    the least loaded rank, no data-path collective; the time is the max over
+    ranks); the single-system workloads run on one GPU."""
     import torch
     import thermofem_b200 as tf
     from thermofem_b200 import problems as P
-    ctx = tf.Context(0)
+    from thermofem_b200 import shard
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if args.workload == "batched" and world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    elif rank != 0:
+        return
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    ctx = tf.Context(local)
 
     def events():
         return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
 
     if args.workload == "batched":
-        probs = P.batched_transient(48, seed=1004)
+        count, steps = 48, 20
+        params = P.batched_transient_params(count, seed=1004)
+        weights = [P.transient3d_nnz(m) for m, _ in params]
+        mine = shard.assign(weights, world)[rank]
+        probs = P.batched_transient(count, seed=1004, only=mine)
         solvers = []
         t0 = time.perf_counter()
         for m, r, mat, _ in probs:
             s = tf.Cg(tf.solver_options(), "amg", tf.amg_options(hierarchy_type="f32", **AMG, **_small(args)),
                       ctx=ctx)
-            s.setup(tf.DeviceCsr.from_host(*mat))
+            s.setup(tf.DeviceCsr.from_host(*mat, device=dev))
             solvers.append(s)
         setup_s = time.perf_counter() - t0
-        batch = tf.Batch(solvers, ctx=ctx)
-        t_init = [torch.tensor(p[3], device="cuda") for p in probs]
-        steps = 20
+        batch = tf.Batch(solvers, ctx=ctx) if solvers else None
+        t_init = [torch.tensor(p[3], device=dev) for p in probs]
+
+        def maxover(v):
+            if dist is None:
+                return v
+            t = torch.tensor([v], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            return float(t.item())
+
         out = {}
+        reports = []
         for mode in ("batched", "one_by_one", "batched"):
             temps = [t.clone() for t in t_init]
-            its = 0
-            ok = True
+            its = [0] * len(probs)
+            ok = [True] * len(probs)
+            if dist is not None:
+                dist.barrier()
+            torch.cuda.synchronize(dev)
             e0, e1 = events()
             e0.record(ctx.stream)
             for _ in range(steps):
                 rhs = [t / p[1] for t, p in zip(temps, probs)]
                 xs = [t.clone() for t in temps]
-                if mode == "batched":
+                if not solvers:
+                    reps = []
+                elif mode == "batched":
                     reps = batch.apply(rhs, xs)
                 else:
                     reps = [s.apply(b, x) for s, b, x in zip(solvers, rhs, xs)]
-                its += sum(r["iterations"] for r in reps)
-                ok = ok and all(r["status"] == "Converged" for r in reps)
+                for i, rep in enumerate(reps):
+                    its[i] += rep["iterations"]
+                    ok[i] = ok[i] and rep["status"] == "Converged"
                 temps = xs
             e1.record(ctx.stream)
-            torch.cuda.synchronize()
-            out[mode] = {"s_per_step": e0.elapsed_time(e1) / 1e3 / steps, "iterations": its, "converged": ok}
-        rows = sum(p[0] ** 3 for p in probs)
+            torch.cuda.synchronize(dev)
+            if dist is not None:
+                dist.barrier()
+            s_step = maxover(e0.elapsed_time(e1) / 1e3 / steps)
+            reports = [{"iterations": it, "converged": c} for it, c in zip(its, ok)]
+            out[mode] = {"s_per_step": s_step}
+        everything = shard.gather_reports(reports, mine, count)
+        setup_s = maxover(setup_s)
+        for mode in out:
+            out[mode]["iterations"] = sum(r["iterations"] for r in everything)
+            out[mode]["converged"] = all(r["converged"] for r in everything)
+        if rank == 0:
+            rows = sum(m ** 3 for m, _ in params)
+            print(json.dumps({
+                "workload": f"batched transient: {count} backward-Euler 3-D 7-point problems, sides U{{16..96}} "
+                            f"({rows} rows in all), r = dt k/h^2 U[0.1,10], {steps} steps, AMG-PCG V FP32 / FP64 "
+                            "outer, rtol 1e-8",
+                "metric": f"seconds per time step (all {count} systems)", "unit": "s", "n_gpus": world,
+                "scaling": "strong",
+                "parallelism": "systems sharded over ranks by nonzeros (longest first), no data-path collective"
+                               if world > 1 else "single GPU",
+                "imbalance": shard.imbalance(weights, shard.assign(weights, world)),
+                "batched": out["batched"], "one_by_one": out["one_by_one"],
+                "speedup_batched": out["one_by_one"]["s_per_step"] / out["batched"]["s_per_step"],
+                "setup_s": setup_s, "data": "synthetic (seeded generator)"}), flush=True)
+        del batch, solvers
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+    if args.workload == "learned":
+        from thermofem_b200 import learned as L
+        m = args.size or 256
+        res = L.evaluate(L.load(ctx=ctx), m, ctx=ctx)
         print(json.dumps({
-            "workload": "batched transient: 48 backward-Euler 3-D 7-point problems, sides U{16..96} "
-                        f"({rows} rows in all), r = dt k/h^2 U[0.1,10], 20 steps, AMG-PCG V FP32 / FP64 outer, rtol 1e-8",
-            "metric": "seconds per time step (all 48 systems)", "unit": "s",
-            "batched": out["batched"], "one_by_one": out["one_by_one"],
-            "speedup_batched": out["one_by_one"]["s_per_step"] / out["batched"]["s_per_step"],
-            "setup_s": setup_s, "data": "synthetic (seeded generator)"}), flush=True)
+            "workload": f"heat3d {m}^3 (seed 9000, held out), AMG F(1,1) FP32 hierarchy / FP64 outer, rtol 1e-8; "
+                        "learned per-row Jacobi damping (trained on 200 problems of sides 32..64) vs fixed w=2/3",
+            "metric": "time-to-1e-8 FP64 relative residual (ms) and iterations", "unit": "ms",
+            **res, "data": "synthetic (seeded generator)"}), flush=True)
         return
     if args.workload == "convdiff":
         m = args.size or 192
@@ -316,9 +380,10 @@ def main():
                     help="tf_amg_options.small_level_rows (default: the library default)")
     ap.add_argument("--profile", choices=["mixed", "fp64", "spmv"], default=None,
                     help="profiling run: setup, --warmup solves, then --steps solves of one path; no JSON line")
-    ap.add_argument("--workload", choices=["batched", "convdiff", "heat"], default=None,
+    ap.add_argument("--workload", choices=["batched", "convdiff", "heat", "learned"], default=None,
                     help="the other BASELINE configs (one JSON line each, not the headline): batched = 48 "
-                         "transient systems x 20 steps; convdiff = 192^3 BiCGStab W-cycle; heat = --size^3 heat")
+                         "transient systems x 20 steps; convdiff = 192^3 BiCGStab W-cycle; heat = --size^3 heat; "
+                         "learned = shipped damping model vs w=2/3 on --size^3 (default 256), F-cycle")
     ap.add_argument("--size", type=int, default=None, help="grid side of --workload convdiff/heat")
     args = ap.parse_args()
     if args.impl == "reference":

@@ -1,0 +1,83 @@
+"""Sharding of independent systems over ranks (CPU; world size 2 over gloo)."""
+import json
+import os
+import socket
+
+import pytest
+import torch.multiprocessing as mp
+
+from thermofem_b200 import problems as P
+from thermofem_b200 import shard
+
+
+def _weights():
+    return [P.transient3d_nnz(m) for m, _ in P.batched_transient_params(48, seed=1004)]
+
+
+@pytest.mark.parametrize("world", [1, 2, 3, 4, 8])
+def test_assign_covers_every_system_once_and_balances(world):
+    w = _weights()
+    parts = shard.assign(w, world)
+    assert len(parts) == world
+    flat = sorted(k for ks in parts for k in ks)
+    assert flat == list(range(len(w)))
+    assert all(ks == sorted(ks) for ks in parts)
+    # LPT: the largest load is within 4/3 of the lower bound max(mean, largest)
+    loads = [sum(w[k] for k in ks) for ks in parts]
+    bound = max(sum(w) / world, max(w))
+    assert max(loads) <= 4 / 3 * bound
+    assert shard.assign(w, world) == parts  # deterministic
+
+
+def test_assign_edge_cases():
+    assert shard.assign([], 2) == [[], []]
+    assert shard.assign([5], 3) == [[0], [], []]
+    assert shard.assign([1, 1, 1, 1], 2) == [[0, 2], [1, 3]]
+    with pytest.raises(ValueError):
+        shard.assign([1], 0)
+    with pytest.raises(ValueError):
+        shard.assign([-1], 1)
+
+
+def test_gather_without_process_group():
+    assert shard.gather_reports(["b", "a"], [1, 0], 2) == ["a", "b"]
+    with pytest.raises(ValueError):
+        shard.gather_reports(["a"], [0], 2)
+    with pytest.raises(ValueError):
+        shard.gather_reports(["a", "b"], [0, 0], 2)
+
+
+def _worker(rank, world, port, out):
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    import datetime
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        w = _weights()
+        mine = shard.assign(w, world)[rank]
+        reps = [{"system": k, "rank": rank, "nnz": w[k]} for k in mine]
+        allr = shard.gather_reports(reps, mine, len(w))
+        if rank == 0:
+            with open(out, "w") as f:
+                json.dump(allr, f)
+    finally:
+        dist.destroy_process_group()
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def test_gather_reports_over_two_gloo_ranks(tmp_path):
+    out = str(tmp_path / "reports.json")
+    mp.start_processes(_worker, args=(2, _free_port(), out), nprocs=2, join=True, start_method="spawn")
+    with open(out) as f:
+        reps = json.load(f)
+    w = _weights()
+    parts = shard.assign(w, 2)
+    assert [r["system"] for r in reps] == list(range(48))
+    for k, r in enumerate(reps):
+        assert r["rank"] == (0 if k in parts[0] else 1)
+        assert r["nnz"] == w[k]

@@ -199,15 +199,32 @@ def transient3d(m: int, r: float):
     return _csr_from_stencil(cols, vals, mask)
 
 
-def batched_transient(count: int = 48, seed: int = 1004, side_min: int = 16, side_max: int = 96):
-    """The batched transient workload: `count` independent problems with
-    sides uniform in [side_min, side_max], r = dt k / h^2 uniform in
-    [0.1, 10] and initial temperatures uniform in [0, 1] (problem k uses
-    streams of seed + k).  Returns [(m, r, (offsets, indices, values), T0)]."""
+def batched_transient_params(count: int = 48, seed: int = 1004, side_min: int = 16, side_max: int = 96):
+    """(side m, r = dt k / h^2) of each problem of the batched transient
+    workload: m uniform in [side_min, side_max], r uniform in [0.1, 10]
+    (problem k uses streams of seed + k)."""
     out = []
     for k in range(count):
         u = uniform(seed + k, 2, 7)
         m = side_min + min(int(u[0] * (side_max - side_min + 1)), side_max - side_min)
-        r = 0.1 + 9.9 * float(u[1])
+        out.append((m, 0.1 + 9.9 * float(u[1])))
+    return out
+
+
+def transient3d_nnz(m: int) -> int:
+    """Nonzeros of transient3d(m, r): the diagonal plus two per interior
+    face of the m^3 grid."""
+    return m ** 3 + 6 * m * m * (m - 1)
+
+
+def batched_transient(count: int = 48, seed: int = 1004, side_min: int = 16, side_max: int = 96, only=None):
+    """The batched transient workload: the problems of
+    batched_transient_params with initial temperatures uniform in [0, 1].
+    Returns [(m, r, (offsets, indices, values), T0)]; with `only` (problem
+    indices) just those problems, in that order."""
+    params = batched_transient_params(count, seed, side_min, side_max)
+    out = []
+    for k in (range(count) if only is None else only):
+        m, r = params[k]
         out.append((m, r, transient3d(m, r), uniform(seed + k, m * m * m, 8)))
     return out
