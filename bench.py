@@ -35,9 +35,10 @@ SEED_MATRIX, SEED_RHS = 1001, 1002
 AMG = dict(jacobi_weight=2.0 / 3.0, pre_sweeps=1, post_sweeps=1, cycle="v", coarse_rows=64)
 METRIC = "time-to-1e-8 FP64 relative residual (s), AMG-PCG V-cycle, FP32 hierarchy / FP64 outer"
 # DRAM bytes (read + write) of one launch of the FP64 operator SpMV on the
-# 128^3 problem, from the ncu capture summarised in
-# profiles/csr_pipe_kernel_heat3d_128_fp64_operator.md
-SPMV_TRAFFIC = 171013632 + 13778176
+# 128^3 problem, from the ncu captures summarised in
+# profiles/sliced_kernel_heat3d_128_fp64_operator.md (sliced copy) and
+# profiles/csr_pipe_kernel_heat3d_128_fp64_operator.md (CSR row tiles)
+SPMV_TRAFFIC = {"sliced": 163200256 + 5292288, "csr": 171013632 + 13778176}
 WORKLOAD = f"heat3d {SIZE}^3 7-point FV, log-normal k (seed {SEED_MATRIX}), Dirichlet x=0, rhs U[-1,1] (seed {SEED_RHS})"
 
 
@@ -46,6 +47,15 @@ def spmv_bytes(n, nnz, vsize=8, isize=4, csize=None):
     bytes each, default the index size), row offsets, x and y each once."""
     csize = isize if csize is None else csize
     return nnz * (vsize + csize) + n * (isize + 2 * vsize) + isize
+
+
+def layout_bytes(layout, n, entries, vsize):
+    """Algorithmic bytes of one SpMV over the storage it streams: the sliced
+    copy (entries incl. padding x (value + 2-byte column), one 4-byte start
+    per 32-row slice, x and y once) or the CSR with 2-byte columns."""
+    if layout == "sliced":
+        return entries * (vsize + 2) + ((n + 31) // 32 + 1) * 4 + 2 * n * vsize
+    return spmv_bytes(n, entries, vsize, 4, 2)
 
 
 def measured_peaks():
@@ -507,9 +517,11 @@ def main():
     spmv32_ms = time_launch(lambda: mixed.level_spmv(0, b32, y32))
     csr_ms = time_launch(lambda: tf.spmv(a, b, y, ctx=ctx))
     peak, peak_kind = measured_peaks()
-    algo = spmv_bytes(n, nnz, 8, 4, 2)
+    layout, entries = plain.spmv_layout()
+    layout32, entries32 = mixed.level_spmv_layout(0)
+    algo = layout_bytes(layout, n, entries, 8)
     achieved = algo / (spmv_ms * 1e-3) / 1e9
-    achieved32 = spmv_bytes(n, nnz, 4, 4, 2) / (spmv32_ms * 1e-3) / 1e9
+    achieved32 = layout_bytes(layout32, n, entries32, 4) / (spmv32_ms * 1e-3) / 1e9
     achieved_csr = spmv_bytes(n, nnz) / (csr_ms * 1e-3) / 1e9
 
     cpu = None
@@ -541,8 +553,10 @@ def main():
             "speedup_mixed_vs_fp64": ms_plain / ms_mixed,
             "spmv_gbs": {"f64_operator": achieved, "f32_level0": achieved32, "f64_int32_csr": achieved_csr},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": SPMV_TRAFFIC,
-                         "kernel": "csr_pipe_kernel<double,int,short> (SpMV, FP64 Krylov operator, "
+                         "frac": achieved / peak, "traffic": SPMV_TRAFFIC[layout],
+                         "kernel": ("sliced_kernel<double> (SpMV, FP64 Krylov operator, 32-row slices, "
+                                    f"2-byte column offsets, {entries} entries)") if layout == "sliced" else
+                                   "csr_pipe_kernel<double,int,short> (SpMV, FP64 Krylov operator, "
                                    "2-byte column offsets)", "peak_source": peak_kind,
                          "algorithmic_bytes": algo, "launch_ms": spmv_ms},
             "cpu_baseline": cpu,

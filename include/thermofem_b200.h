@@ -113,12 +113,15 @@ int tf_spmv_f32(tf_ctx *ctx, int64_t rows, int64_t cols, int64_t nnz, const int3
                 const int32_t *indices, const float *values, const float *x, float *y);
 /* SpMV autotuner (replaces the fixed library algorithm choice of
  * cusparseSpMV ALG_DEFAULT, IterationContext.cu:140-159): times the feasible
- * pipelined launch shapes (1 or 2 rows per thread, ring depth 2-4, 1-6
+ * pipelined launch shapes (1 or 2 rows per thread, ring depth 2-3, 1-6
  * resident CTAs per SM, chunk capacity 100% or 125% of the mean tile) on this
  * operator and caches the fastest for every later row-tile launch over an
- * operator of the same shape (rows, nnz, types).  y is overwritten.  Outputs
- * may be NULL; *ms is the best time per launch.  Results never depend on the
- * shape chosen. */
+ * operator of the same shape (rows, nnz, types).  A solver's or hierarchy's
+ * own operators that carry a sliced copy also time the sliced kernel (next
+ * tile prefetched or not, 2-6 resident CTAs per SM).  Operators larger than
+ * half the L2 cache are timed with the cache flushed before every launch, as
+ * a solve meets them.  y is overwritten.  Outputs may be NULL; *ms is the
+ * best time per launch.  Results never depend on the shape chosen. */
 int tf_autotune_spmv(tf_ctx *ctx, const tf_csr *a, const void *x, void *y, int *stages, int *ctas_per_sm,
                      int *cap_pct, int *rows_per_thread, float *ms);
 /* Sets the cached launch shape for operators of a's shape without timing
@@ -275,6 +278,11 @@ int tf_amg_level_matrix(const tf_amg *m, int level, tf_csr *out);
  * storage type and column stream); x, y device vectors of the hierarchy's
  * storage type, not aliased. */
 int tf_amg_level_spmv(const tf_amg *amg, int level, const void *x, void *y);
+/* The storage that SpMV streams (no reference counterpart): *sliced = 1
+ * for the operator's sliced copy (32-row slices, entries column-major,
+ * 2-byte column offsets; *entries counts its padding too), 0 for the CSR
+ * arrays (*entries = nnz). */
+int tf_amg_level_spmv_layout(const tf_amg *m, int level, int *sliced, int64_t *entries);
 int tf_amg_level_transfer(const tf_amg *m, int level, const int32_t **map, const int32_t **offsets,
                           const int32_t **members, int *coarse_rows);
 
@@ -329,6 +337,9 @@ int tf_solver_set_graph_mode(tf_solver *s, int mode);
  * snapshot taken by setup); x, y device vectors of the solver's value type,
  * not aliased.  TF_ERR_LOGIC before setup. */
 int tf_solver_spmv(tf_solver *s, const void *x, void *y);
+/* The storage tf_solver_spmv streams, as tf_amg_level_spmv_layout says;
+ * TF_ERR_LOGIC before setup. */
+int tf_solver_spmv_layout(const tf_solver *s, int *sliced, int64_t *entries);
 /* How the last apply ran: 2 as one whole-solve graph, 1 as one graph per
  * iteration, 0 as uncaptured launches (a step CUDA refused to
  * capture), -1 before the first apply or for a NULL solver.  No reference

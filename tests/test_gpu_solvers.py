@@ -384,9 +384,50 @@ def test_two_byte_column_stream_gives_identical_solves(ctx, case, monkeypatch):
     assert torch.equal(out[0][1], out[1][1])
 
 
-def test_operator_spmv_entry_points(ctx):
-    # The solver's and the hierarchy's own operators (2-byte column stream)
-    # give the same product as the plain CSR SpMV.
+@pytest.mark.parametrize("shape", ["0,2", "1,3", "1,8", "0,5"])
+@pytest.mark.parametrize("case", ["heat3d-cg-f32", "heat3d-cg-f64", "heat3d-bicgstab-f32"])
+def test_sliced_layout_gives_identical_solves(ctx, case, shape, monkeypatch):
+    # Operators with 2-byte column offsets also carry a sliced copy (32-row
+    # slices, entries column-major) that the SpMV family streams when it is
+    # faster.  THERMOFEM_B200_SLICED_SHAPE="prefetch,ctas" forces it with
+    # that launch shape, THERMOFEM_B200_SLICED=0 turns the copy off.  Same
+    # per-row order and the same 256-row-block partial sums: the same bits,
+    # on every level (coarse levels have rows longer than one 8-entry group)
+    # and on a row count that is no multiple of 32.
+    m = P.heat3d(25, seed=83)
+    n = len(m[0]) - 1
+    b = torch.tensor(P.rhs_uniform(n, 84), device="cuda")
+    solver = tf.BiCgStab if "bicgstab" in case else tf.Cg
+    out = []
+    for flag in ("0", "1"):
+        monkeypatch.setenv("THERMOFEM_B200_SLICED", flag)
+        monkeypatch.setenv("THERMOFEM_B200_SLICED_SHAPE", shape)
+        s = solver(tf.solver_options(), "amg",
+                   tf.amg_options(hierarchy_type=case[-3:], jacobi_weight=2 / 3, cycle="w"), ctx=ctx)
+        s.setup(to_device(m))
+        x = torch.zeros(n, dtype=torch.float64, device="cuda")
+        rep = s.apply(b, x)
+        xs = torch.randn(n, dtype=torch.float64, device="cuda", generator=torch.Generator("cuda").manual_seed(5))
+        out.append((rep, x, s.spmv(xs)))
+        layout, entries = s.spmv_layout()
+        if flag == "1":
+            assert layout == "sliced" and len(m[1]) <= entries <= len(m[1]) * 1.25
+            assert s.level_spmv_layout(0)[0] == "sliced"
+        else:
+            assert (layout, entries) == ("csr", len(m[1]))
+    assert out[0][0]["status"] == "Converged"
+    assert out[0][0] == out[1][0]
+    assert torch.equal(out[0][1], out[1][1])
+    assert torch.equal(out[0][2], out[1][2])
+
+
+@pytest.mark.parametrize("shape", [None, "1,4", "0,3"])
+def test_operator_spmv_entry_points(ctx, shape, monkeypatch):
+    # The solver's and the hierarchy's own operators (2-byte column stream,
+    # sliced copy when the tuner picks it or a shape forces it) give the same
+    # product as the plain CSR SpMV.
+    if shape:
+        monkeypatch.setenv("THERMOFEM_B200_SLICED_SHAPE", shape)
     m = P.heat3d(24, seed=91)
     n = len(m[0]) - 1
     a = to_device(m)

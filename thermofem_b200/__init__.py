@@ -171,10 +171,12 @@ SIGNATURES = {
     "tf_solver_last_apply_ms": ([_P], _D),
     "tf_solver_last_execution": ([_P], _I),
     "tf_solver_spmv": ([_P, _P, _P], _I),
+    "tf_solver_spmv_layout": ([_P, C.POINTER(C.c_int), C.POINTER(C.c_int64)], _I),
     "tf_batch_create": ([_P, _I, _PP, _PP], _I),
     "tf_batch_destroy": ([_P], _I),
     "tf_batch_apply": ([_P, _PP, _PP, C.POINTER(SolveResult)], _I),
     "tf_amg_level_spmv": ([_P, _I, _P, _P], _I),
+    "tf_amg_level_spmv_layout": ([_P, _I, C.POINTER(C.c_int), C.POINTER(C.c_int64)], _I),
     "tf_mlp_create": ([_P, C.c_uint64, _D, _D, _PP], _I),
     "tf_mlp_destroy": ([_P], _I),
     "tf_mlp_get_params": ([_P, C.POINTER(C.c_float)], _I),

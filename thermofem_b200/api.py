@@ -516,6 +516,12 @@ class _AmgView:
             check(lib().tf_amg_level_spmv(self._h(), int(d), _p(x), _p(y)))
         return y
 
+    def level_spmv_layout(self, d):
+        """("sliced" | "csr", entries streamed) of level d's SpMV."""
+        sl, n = C.c_int(), C.c_int64()
+        check(lib().tf_amg_level_spmv_layout(self._h(), int(d), C.byref(sl), C.byref(n)))
+        return ("sliced" if sl.value else "csr"), n.value
+
     def level_transfer(self, d, device="cuda"):
         pm, po, pe = C.c_void_p(), C.c_void_p(), C.c_void_p()
         cr = C.c_int()
@@ -642,6 +648,12 @@ class _Solver(_AmgView):
         with self.ctx:
             check(lib().tf_solver_spmv(self.h, _p(x), _p(y)))
         return y
+
+    def spmv_layout(self):
+        """("sliced" | "csr", entries streamed) of the solver's operator SpMV."""
+        sl, n = C.c_int(), C.c_int64()
+        check(lib().tf_solver_spmv_layout(self.h, C.byref(sl), C.byref(n)))
+        return ("sliced" if sl.value else "csr"), n.value
 
     @property
     def last_execution(self) -> int:

@@ -72,6 +72,7 @@ struct Level {
     DeviceBuffer<S> val, dinv, rhs, x0, x1, r;
     DeviceBuffer<int32_t> map, off, mem;
     DeviceBuffer<int16_t> cd;  // columns as row offsets, when they fit
+    SlicedCopy<S> sl;          // sliced copy for the SpMV family, when built
     int coarse{0};
     int cur{0};
     S *x() const { return cur ? x1.data() : x0.data(); }
@@ -84,6 +85,7 @@ struct Level {
         c.ci = ci.data();
         c.val = val.data();
         c.cd = cd.data();
+        sl.attach(c);
         return c;
     }
 };
@@ -132,10 +134,10 @@ class HierarchyImpl final : public Hierarchy {
                 l.cd.allocate(static_cast<size_t>(l.nnz));
                 if (!delta_columns(ctx, l.n, l.rp.data(), l.ci.data(), l.cd.data())) l.cd.release();
             }
+            if (l.cd.data() && sliced_enabled()) build_sliced(ctx, l.csr(), l.sl);
             // Launch shape of this level's row-tile kernels (cached by shape).
             fill_zero(ctx, l.n, l.rhs.data());
-            autotune_spmv(ctx, l.csr(), static_cast<const S *>(l.rhs.data()), l.r.data(), nullptr, nullptr, nullptr,
-                          nullptr, nullptr);
+            tune_spmv(ctx, l.csr(), static_cast<const S *>(l.rhs.data()), l.r.data());
             LevelStats st;
             st.rows = l.n;
             st.nnz = l.nnz;
@@ -200,6 +202,10 @@ class HierarchyImpl final : public Hierarchy {
         const auto &l = levels_.at(static_cast<size_t>(d));
         StableScope stable(ctx);
         spmv(ctx, l.csr(), static_cast<const S *>(x), static_cast<S *>(y));
+    }
+    int level_spmv_layout(tf_ctx *ctx, int d, int64_t *entries) const override {
+        const auto &l = levels_.at(static_cast<size_t>(d));
+        return streams_sliced(ctx, l.csr(), l.sl.entries, entries) ? 1 : 0;
     }
     void level_transfer(int d, const int32_t **map, const int32_t **off, const int32_t **mem,
                         int *coarse) const override {

@@ -44,6 +44,8 @@ class Hierarchy {
     // y = A_d x with level d's operator as the cycle streams it (its column
     // storage included); x, y of the level's storage type.
     virtual void level_spmv(tf_ctx *ctx, int d, const void *x, void *y) const = 0;
+    // 1 when level d's SpMV streams its sliced copy (entries incl. padding), 0 for CSR.
+    virtual int level_spmv_layout(tf_ctx *ctx, int d, int64_t *entries) const = 0;
     virtual void level_transfer(int d, const int32_t **map, const int32_t **off, const int32_t **mem,
                                 int *coarse) const = 0;
     // Kernels launched by one cycle (graph replay counts them too).
@@ -69,6 +71,8 @@ class Krylov {
     virtual tf_solve_result solve(tf_ctx *ctx, const void *rhs, void *x) = 0;
     // y = A x with the solver's operator as the solve streams it.
     virtual void spmv(tf_ctx *ctx, const void *x, void *y) = 0;
+    // 1 when that SpMV streams the sliced copy (entries incl. padding), 0 for CSR.
+    virtual int spmv_layout(tf_ctx *ctx, int64_t *entries) const = 0;
     virtual Hierarchy *amg() = 0;
     virtual int64_t rows() const = 0;
     // Batches (tf_batch): the whole solve added to graph g as an independent

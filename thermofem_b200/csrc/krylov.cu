@@ -568,6 +568,10 @@ class KrylovImpl final : public Krylov {
             cd_.allocate(static_cast<size_t>(nnz_));
             if (!delta_columns(ctx, n_, rp_.data(), ci_.data(), cd_.data())) cd_.release();
         }
+        sl_.release();
+        if constexpr (std::is_same_v<I, int32_t>) {
+            if (cd_.data() && sliced_enabled()) build_sliced(ctx, csr(), sl_);
+        }
         hier_.reset();
         if (precond_ == TF_PRECOND_AMG) {
             const int storage = amg_cfg_->o.hierarchy_type == -1 ? (sizeof(T) == 8 ? TF_F64 : TF_F32)
@@ -578,8 +582,7 @@ class KrylovImpl final : public Krylov {
             b->allocate(static_cast<size_t>(n_));
         tiles_ = tile::partials(n_);
         fill_zero(ctx, n_, x_.data());
-        autotune_spmv(ctx, csr(), static_cast<const T *>(x_.data()), q_.data(), nullptr, nullptr, nullptr, nullptr,
-                      nullptr);
+        tune_spmv(ctx, csr(), static_cast<const T *>(x_.data()), q_.data());
         parts_ = parts_for(n_);
         part_.allocate(static_cast<size_t>(2 * std::max(tiles_, parts_)));
         partb_.allocate(static_cast<size_t>(std::max(tiles_, parts_)));
@@ -682,6 +685,10 @@ class KrylovImpl final : public Krylov {
         StableScope stable(ctx);
         tfb::spmv(ctx, csr(), static_cast<const T *>(x), static_cast<T *>(y));
     }
+    int spmv_layout(tf_ctx *ctx, int64_t *entries) const override {
+        if (!ready_) fail(TF_ERR_LOGIC, "solver requires setup");
+        return streams_sliced(ctx, csr(), sl_.entries, entries) ? 1 : 0;
+    }
     int64_t rows() const override { return n_; }
 
   private:
@@ -693,6 +700,7 @@ class KrylovImpl final : public Krylov {
         c.ci = ci_.data();
         c.val = val_.data();
         c.cd = cd_.data();
+        sl_.attach(c);
         return c;
     }
 
@@ -902,6 +910,7 @@ class KrylovImpl final : public Krylov {
     int64_t n_{0}, nnz_{0};
     DeviceBuffer<I> rp_, ci_;
     DeviceBuffer<int16_t> cd_;  // columns as row offsets, when they fit
+    SlicedCopy<T> sl_;          // sliced copy for the SpMV family, when built
     DeviceBuffer<T> val_;
     DeviceBuffer<T> rhs_, x_, r_, z_, p_, q_, shadow_, s_, t_, sh_;
     DeviceBuffer<double> part_, partb_;

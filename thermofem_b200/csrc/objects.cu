@@ -185,6 +185,15 @@ int tf_amg_level_spmv(const tf_amg *m, int level, const void *x, void *y) {
     });
 }
 
+int tf_amg_level_spmv_layout(const tf_amg *m, int level, int *sliced, int64_t *entries) {
+    return guard([&] {
+        require(m != nullptr && sliced != nullptr && entries != nullptr, "null argument");
+        if (!m->h) fail(TF_ERR_LOGIC, "AMG requires setup");
+        require(level >= 0 && level < m->h->level_count(), "level out of range");
+        *sliced = m->h->level_spmv_layout(m->ctx, level, entries);
+    });
+}
+
 int tf_amg_level_transfer(const tf_amg *m, int level, const int32_t **map, const int32_t **offsets,
                           const int32_t **members, int *coarse_rows) {
     return guard([&] {
@@ -372,6 +381,13 @@ int tf_solver_spmv(tf_solver *s, const void *x, void *y) {
         require(s != nullptr && x != nullptr && y != nullptr && x != y, "null or aliased argument");
         DeviceScope scope(s->ctx->device);
         s->k->spmv(s->ctx, x, y);
+    });
+}
+
+int tf_solver_spmv_layout(const tf_solver *s, int *sliced, int64_t *entries) {
+    return guard([&] {
+        require(s != nullptr && sliced != nullptr && entries != nullptr, "null argument");
+        *sliced = s->k->spmv_layout(s->ctx, entries);
     });
 }
 

@@ -18,6 +18,40 @@ struct Csr {
     // (ci[j] - row, int16): the pipelined row-tile kernels stream it instead
     // of ci when set (see delta_columns).
     const int16_t *cd{nullptr};
+    // Optional sliced copy (SlicedCopy below): slices of 32 consecutive
+    // rows, entry j of row 32 s + l at sp[s] + 32 j + l (values sv, column
+    // offsets from the row sc, padding kSlicePad with value 0).  The SpMV
+    // family may stream it instead of the CSR arrays; results are the same
+    // bits either way.
+    const int32_t *sp{nullptr};
+    const T *sv{nullptr};
+    const int16_t *sc{nullptr};
+};
+
+// Column offset of a padding entry of the sliced layout.
+constexpr int16_t kSlicePad = -32768;
+
+// Owner of an operator's sliced copy.
+template <class T>
+struct SlicedCopy {
+    DeviceBuffer<int32_t> sp;
+    DeviceBuffer<T> val;
+    DeviceBuffer<int16_t> col;
+    int64_t entries{0};
+    void release() {
+        sp.release();
+        val.release();
+        col.release();
+        entries = 0;
+    }
+    template <class I>
+    void attach(Csr<T, I> &c) const {
+        if (sp.data()) {
+            c.sp = sp.data();
+            c.sv = val.data();
+            c.sc = col.data();
+        }
+    }
 };
 
 // Launch shape of the row-tile SpMV family: rows_per_tile consecutive rows
@@ -39,6 +73,15 @@ void spmv(tf_ctx *ctx, const Csr<T, I> &a, const T *x, T *y);
 template <class T, class I>
 void autotune_spmv(tf_ctx *ctx, const Csr<T, I> &a, const T *x, T *y, int *stages, int *ctas_per_sm, int *cap_pct,
                    int *rows_per_thread, float *ms);
+// autotune_spmv the first time an operator of a's shape and storage is set
+// up in the process; later setups reuse the cached shape
+// (THERMOFEM_B200_SLICED_SHAPE forces the timing, and with it that shape).
+template <class T, class I>
+void tune_spmv(tf_ctx *ctx, const Csr<T, I> &a, const T *x, T *y);
+// The storage the SpMV family streams for a under its cached shape: true
+// (sliced copy, *entries its padded entry count) or false (CSR, *entries = nnz).
+template <class T, class I>
+bool streams_sliced(tf_ctx *ctx, const Csr<T, I> &a, int64_t entries_if_sliced, int64_t *entries);
 // Stores a launch shape for operators of a's shape (validated, not timed).
 template <class T, class I>
 void set_spmv_config(tf_ctx *ctx, const Csr<T, I> &a, int stages, int ctas_per_sm, int cap_pct, int rows_per_thread);
@@ -71,6 +114,13 @@ void inverse_diagonal(tf_ctx *ctx, const Csr<T, I> &a, T *dinv);
 template <class I>
 bool delta_columns(tf_ctx *ctx, int64_t rows, const I *rp, const I *ci, int16_t *cd);
 bool delta_columns_enabled();
+// Builds the sliced copy of a (which must carry its 2-byte column offsets
+// cd): slice width = its longest row.  False, with out released, when the
+// padding would exceed a quarter of nnz or the entries do not fit int32.
+// THERMOFEM_B200_SLICED=0 turns the copy off (sliced_enabled() false).
+template <class T>
+bool build_sliced(tf_ctx *ctx, const Csr<T, int32_t> &a, SlicedCopy<T> &out);
+bool sliced_enabled();
 template <class T>
 void restrict_sum(tf_ctx *ctx, int64_t nc, const int32_t *off, const int32_t *mem, const T *fine, T *coarse);
 template <class T>

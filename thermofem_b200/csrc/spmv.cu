@@ -182,6 +182,54 @@ __global__ void delta_columns_kernel(int64_t n, const I *__restrict__ rp, const 
     }
 }
 
+// Entries of each 32-row slice of the sliced layout (32 x its longest row),
+// one warp per slice, and their total.
+template <class I>
+__global__ void slice_entries_kernel(int64_t rows, int64_t nslices, const I *__restrict__ rp,
+                                     int32_t *__restrict__ entries, unsigned long long *total) {
+    pdl_enter();
+    const int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    const int64_t s = t >> 5;  // uniform across the warp
+    if (s >= nslices) return;
+    const int lane = static_cast<int>(t & 31);
+    int64_t len = t < rows ? static_cast<int64_t>(rp[t + 1] - rp[t]) : 0;
+    for (int o = 16; o > 0; o >>= 1) len = max(len, static_cast<int64_t>(__shfl_xor_sync(0xffffffffu, len, o)));
+    if (lane == 0) {
+        const int64_t e = len * 32;
+        entries[s] = e > INT32_MAX ? INT32_MAX : static_cast<int32_t>(e);
+        atomicAdd(total, static_cast<unsigned long long>(e));
+    }
+}
+
+// Row t's entries into its slice (column-major, padding after its last entry).
+template <class T, class I>
+__global__ void slice_fill_kernel(int64_t rows, int64_t nslices, const I *__restrict__ rp,
+                                  const T *__restrict__ val, const int16_t *__restrict__ cd,
+                                  const int32_t *__restrict__ sp, T *__restrict__ sv, int16_t *__restrict__ sc) {
+    pdl_enter();
+    const int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    const int64_t s = t >> 5;
+    if (s >= nslices) return;
+    const int lane = static_cast<int>(t & 31);
+    const int64_t base = sp[s];
+    const int64_t width = (static_cast<int64_t>(sp[s + 1]) - base) >> 5;
+    int64_t j0 = 0, len = 0;
+    if (t < rows) {
+        j0 = rp[t];
+        len = static_cast<int64_t>(rp[t + 1]) - j0;
+    }
+    for (int64_t j = 0; j < width; ++j) {
+        const int64_t k = base + j * 32 + lane;
+        if (j < len) {
+            sv[k] = val[j0 + j];
+            sc[k] = cd[j0 + j];
+        } else {
+            sv[k] = T(0);
+            sc[k] = kSlicePad;
+        }
+    }
+}
+
 template <class T>
 __global__ void prolong_kernel(int64_t nf, const int32_t *__restrict__ map, const T *__restrict__ coarse,
                                T *__restrict__ fine) {
@@ -365,6 +413,22 @@ void autotune_spmv(tf_ctx *ctx, const Csr<T, I> &a, const T *x, T *y, int *stage
 }
 
 template <class T, class I>
+void tune_spmv(tf_ctx *ctx, const Csr<T, I> &a, const T *x, T *y) {
+    if (!std::getenv("THERMOFEM_B200_SLICED_SHAPE") && tile::tuned(ctx, a)) return;
+    tile::autotune(ctx, a, x, y, nullptr);
+}
+
+template <class T, class I>
+bool streams_sliced(tf_ctx *ctx, const Csr<T, I> &a, int64_t entries_if_sliced, int64_t *entries) {
+    bool sliced = false;
+    if constexpr (std::is_same_v<I, int32_t>) {
+        if (a.sp && a.cd) sliced = tile::tuned_config<T, I, int16_t>(a.rows, a.nnz, ctx->sm_count).sliced != 0;
+    }
+    *entries = sliced ? entries_if_sliced : a.nnz;
+    return sliced;
+}
+
+template <class T, class I>
 void set_spmv_config(tf_ctx *ctx, const Csr<T, I> &a, int stages, int ctas_per_sm, int cap_pct, int rows_per_thread) {
     tile::configure(ctx, a, tile::PipeConfig{stages, ctas_per_sm, cap_pct, rows_per_thread});
 }
@@ -429,6 +493,37 @@ bool delta_columns(tf_ctx *ctx, int64_t rows, const I *rp, const I *ci, int16_t 
 }
 template bool delta_columns<int32_t>(tf_ctx *, int64_t, const int32_t *, const int32_t *, int16_t *);
 template bool delta_columns<int64_t>(tf_ctx *, int64_t, const int64_t *, const int64_t *, int16_t *);
+
+bool sliced_enabled() {
+    const char *v = std::getenv("THERMOFEM_B200_SLICED");
+    return !(v && v[0] == '0');
+}
+
+template <class T>
+bool build_sliced(tf_ctx *ctx, const Csr<T, int32_t> &a, SlicedCopy<T> &out) {
+    out.release();
+    if (!a.rows || !a.nnz || !a.cd) return false;
+    const int64_t nslices = (a.rows + 31) / 32;
+    DeviceBuffer<int32_t> entries(static_cast<size_t>(nslices) + 1);
+    DeviceBuffer<unsigned long long> total(1);
+    memset_async(ctx, entries.data(), 0, (nslices + 1) * sizeof(int32_t));
+    memset_async(ctx, total.data(), 0, sizeof(unsigned long long));
+    launch_kernel(ctx, "slice_entries", slice_entries_kernel<int32_t>, grid_for(nslices * 32), kBlock, 0, a.rows,
+                  nslices, a.rp, entries.data(), total.data());
+    const int64_t n = static_cast<int64_t>(read_scalar(ctx, total.data()));
+    // padding of at most a quarter of nnz (tiny operators excepted); int32 entry starts
+    if (n >= INT32_MAX || (n > a.nnz + a.nnz / 4 && n > 4096)) return false;
+    out.sp.allocate(static_cast<size_t>(nslices) + 1);
+    scan_exclusive(ctx, nslices + 1, entries.data(), out.sp.data());
+    out.val.allocate(static_cast<size_t>(n));
+    out.col.allocate(static_cast<size_t>(n));
+    launch_kernel(ctx, "slice_fill", slice_fill_kernel<T, int32_t>, grid_for(nslices * 32), kBlock, 0, a.rows,
+                  nslices, a.rp, a.val, a.cd, out.sp.data(), out.val.data(), out.col.data());
+    out.entries = n;
+    return true;
+}
+template bool build_sliced<float>(tf_ctx *, const Csr<float, int32_t> &, SlicedCopy<float> &);
+template bool build_sliced<double>(tf_ctx *, const Csr<double, int32_t> &, SlicedCopy<double> &);
 
 template <class T>
 void restrict_sum(tf_ctx *ctx, int64_t nc, const int32_t *off, const int32_t *mem, const T *fine, T *coarse) {
@@ -521,6 +616,8 @@ bool row_stats(tf_ctx *ctx, const Csr<double, int32_t> &a, double *row_max) {
     template void spmv<T, I>(tf_ctx *, const Csr<T, I> &, const T *, T *);                                     \
     template void autotune_spmv<T, I>(tf_ctx *, const Csr<T, I> &, const T *, T *, int *, int *, int *, int *, float *); \
     template void set_spmv_config<T, I>(tf_ctx *, const Csr<T, I> &, int, int, int, int); \
+    template void tune_spmv<T, I>(tf_ctx *, const Csr<T, I> &, const T *, T *);                                \
+    template bool streams_sliced<T, I>(tf_ctx *, const Csr<T, I> &, int64_t, int64_t *);                      \
     template void residual<T, I>(tf_ctx *, const Csr<T, I> &, const T *, const T *, T *);                      \
     template void jacobi_sweep<T, I>(tf_ctx *, const Csr<T, I> &, const T *, const T *, const T *, T *, T,     \
                                      const float *, const int32_t *, const T *);                               \
