@@ -316,15 +316,19 @@ def test_transfer_fusion_is_bit_identical(ctx, cycle, hierarchy, monkeypatch):
         assert torch.equal(outs[0], o)
 
 
-def test_transfer_fusion_solve_and_small_level_program(ctx, monkeypatch):
+@pytest.mark.parametrize("kind,hierarchy", [("cg", "f32"), ("cg", "f64"), ("bicgstab", "f32"), ("bicgstab", "f64")])
+def test_transfer_fusion_solve_and_small_level_program(ctx, kind, hierarchy, monkeypatch):
+    # THERMOFEM_B200_FUSE=0 also keeps the preconditioner's final conversion
+    # apart from the PCG dot / BiCGStab SpMVs that follow it.
     m = P.heat3d(24, seed=71)
     n = len(m[0]) - 1
     b = torch.tensor(P.rhs_uniform(n, 72), device="cuda")
     res = []
+    solver = tf.BiCgStab if kind == "bicgstab" else tf.Cg
     for fuse, small in (("0", 0), ("1", 0), ("1", 2000)):
         monkeypatch.setenv("THERMOFEM_B200_FUSE", fuse)
-        s = tf.Cg(tf.solver_options(), "amg",
-                  tf.amg_options(hierarchy_type="f32", jacobi_weight=2 / 3, small_level_rows=small), ctx=ctx)
+        s = solver(tf.solver_options(), "amg",
+                   tf.amg_options(hierarchy_type=hierarchy, jacobi_weight=2 / 3, small_level_rows=small), ctx=ctx)
         s.setup(to_device(m))
         x = torch.zeros(n, dtype=torch.float64, device="cuda")
         rep = s.apply(b, x)
@@ -399,7 +403,7 @@ def test_sliced_layout_gives_identical_solves(ctx, case, shape, monkeypatch):
     b = torch.tensor(P.rhs_uniform(n, 84), device="cuda")
     solver = tf.BiCgStab if "bicgstab" in case else tf.Cg
     out = []
-    for flag in ("0", "1"):
+    for flag in ("0", "1", "sorted"):
         monkeypatch.setenv("THERMOFEM_B200_SLICED", flag)
         monkeypatch.setenv("THERMOFEM_B200_SLICED_SHAPE", shape)
         s = solver(tf.solver_options(), "amg",
@@ -410,15 +414,19 @@ def test_sliced_layout_gives_identical_solves(ctx, case, shape, monkeypatch):
         xs = torch.randn(n, dtype=torch.float64, device="cuda", generator=torch.Generator("cuda").manual_seed(5))
         out.append((rep, x, s.spmv(xs)))
         layout, entries = s.spmv_layout()
-        if flag == "1":
+        if flag == "0":
+            assert (layout, entries) == ("csr", len(m[1]))
+        else:
             assert layout == "sliced" and len(m[1]) <= entries <= len(m[1]) * 1.25
             assert s.level_spmv_layout(0)[0] == "sliced"
-        else:
-            assert (layout, entries) == ("csr", len(m[1]))
+            # coarse aggregated levels: with "sorted", rows ordered longest first within their tiles
+            kinds = [s.level_spmv_layout(d)[0] for d in range(1, s.level_count())]
+            assert ("sorted" in kinds) == (flag == "sorted"), kinds
     assert out[0][0]["status"] == "Converged"
-    assert out[0][0] == out[1][0]
-    assert torch.equal(out[0][1], out[1][1])
-    assert torch.equal(out[0][2], out[1][2])
+    for other in out[1:]:
+        assert out[0][0] == other[0]
+        assert torch.equal(out[0][1], other[1])
+        assert torch.equal(out[0][2], other[2])
 
 
 @pytest.mark.parametrize("shape", [None, "1,4", "0,3"])

@@ -517,10 +517,10 @@ class _AmgView:
         return y
 
     def level_spmv_layout(self, d):
-        """("sliced" | "csr", entries streamed) of level d's SpMV."""
+        """("sliced" | "sorted" | "csr", entries streamed) of level d's SpMV."""
         sl, n = C.c_int(), C.c_int64()
         check(lib().tf_amg_level_spmv_layout(self._h(), int(d), C.byref(sl), C.byref(n)))
-        return ("sliced" if sl.value else "csr"), n.value
+        return ("csr", "sliced", "sorted")[sl.value], n.value
 
     def level_transfer(self, d, device="cuda"):
         pm, po, pe = C.c_void_p(), C.c_void_p(), C.c_void_p()

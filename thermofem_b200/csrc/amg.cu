@@ -134,7 +134,7 @@ class HierarchyImpl final : public Hierarchy {
                 l.cd.allocate(static_cast<size_t>(l.nnz));
                 if (!delta_columns(ctx, l.n, l.rp.data(), l.ci.data(), l.cd.data())) l.cd.release();
             }
-            if (l.cd.data() && sliced_enabled()) build_sliced(ctx, l.csr(), l.sl);
+            if (l.cd.data() && sliced_enabled()) build_sliced(ctx, l.csr(), l.sl, true);
             // Launch shape of this level's row-tile kernels (cached by shape).
             fill_zero(ctx, l.n, l.rhs.data());
             tune_spmv(ctx, l.csr(), static_cast<const S *>(l.rhs.data()), l.r.data());
@@ -205,7 +205,8 @@ class HierarchyImpl final : public Hierarchy {
     }
     int level_spmv_layout(tf_ctx *ctx, int d, int64_t *entries) const override {
         const auto &l = levels_.at(static_cast<size_t>(d));
-        return streams_sliced(ctx, l.csr(), l.sl.entries, entries) ? 1 : 0;
+        if (!streams_sliced(ctx, l.csr(), l.sl.entries, entries)) return 0;
+        return l.sl.perm.data() ? 2 : 1;
     }
     void level_transfer(int d, const int32_t **map, const int32_t **off, const int32_t **mem,
                         int *coarse) const override {
@@ -225,6 +226,16 @@ class HierarchyImpl final : public Hierarchy {
         convert(ctx, f.n, rhs, f.rhs.data());
         run_cycle(ctx);
         convert(ctx, f.n, levels_.front().x(), x);
+    }
+    const void *apply_open(tf_ctx *ctx, const double *rhs) override { return open_t(ctx, rhs); }
+    const void *apply_open(tf_ctx *ctx, const float *rhs) override { return open_t(ctx, rhs); }
+    template <class T>
+    const void *open_t(tf_ctx *ctx, const T *rhs) {
+        StableScope stable(ctx);
+        Level<S> &f = levels_.front();
+        convert(ctx, f.n, rhs, f.rhs.data());
+        run_cycle(ctx);
+        return levels_.front().x();
     }
 
     void run_cycle(tf_ctx *ctx) {

@@ -37,6 +37,11 @@ class Hierarchy {
     // rhs may alias x.  Vector type T is the caller's (float or double).
     virtual void apply(tf_ctx *ctx, const double *rhs, double *x) = 0;
     virtual void apply(tf_ctx *ctx, const float *rhs, float *x) = 0;
+    // apply without its last step: x = M^-1 rhs is left in the finest
+    // level's own storage (storage_type()) and returned, for a caller that
+    // converts it inside its next kernel.
+    virtual const void *apply_open(tf_ctx *ctx, const double *rhs) = 0;
+    virtual const void *apply_open(tf_ctx *ctx, const float *rhs) = 0;
     virtual int storage_type() const = 0;
     virtual int64_t rows() const = 0;
     virtual int level_count() const = 0;
@@ -44,7 +49,8 @@ class Hierarchy {
     // y = A_d x with level d's operator as the cycle streams it (its column
     // storage included); x, y of the level's storage type.
     virtual void level_spmv(tf_ctx *ctx, int d, const void *x, void *y) const = 0;
-    // 1 when level d's SpMV streams its sliced copy (entries incl. padding), 0 for CSR.
+    // 1 (2: rows sorted within tiles) when level d's SpMV streams its sliced
+    // copy (entries incl. padding), 0 for CSR.
     virtual int level_spmv_layout(tf_ctx *ctx, int d, int64_t *entries) const = 0;
     virtual void level_transfer(int d, const int32_t **map, const int32_t **off, const int32_t **mem,
                                 int *coarse) const = 0;

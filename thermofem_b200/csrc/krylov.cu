@@ -142,6 +142,63 @@ __global__ void k_dot(int64_t n, const T *__restrict__ x, const T *__restrict__ 
     tile::finish(fin, part, gridDim.x);
 }
 
+// z = T(xs) (the preconditioner's output in its own storage) and
+// sum_i r_i z_i, in the grid and order of k_dot: the conversion that ends
+// the preconditioner fused into the dot that follows it (same bits).
+template <class T, class S, class Fin>
+__global__ void k_dot_from(int64_t n, const T *__restrict__ r, const S *__restrict__ xs, T *__restrict__ z,
+                           double *part, Fin fin) {
+    pdl_enter();
+    double v[1] = {0.0};
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const T zi = static_cast<T>(xs[i]);
+        z[i] = zi;
+        v[0] += static_cast<double>(r[i]) * static_cast<double>(zi);
+    }
+    tile::block_reduce<1>(v);
+    if (threadIdx.x == 0) part[blockIdx.x] = v[0];
+    tile::finish(fin, part, gridDim.x);
+}
+
+// x_j read from the preconditioner's output in its own storage S.
+template <class T, class S>
+struct ConvertX {
+    const S *__restrict__ x;
+    __device__ __forceinline__ T operator()(int64_t j) const { return static_cast<T>(__ldg(x + j)); }
+};
+
+// Epi that also stores each row's own converted x_i into z: the SpMV that
+// follows the preconditioner writes the converted vector the later steps
+// read (in place of a separate conversion kernel).
+template <class T, class Epi>
+struct StoreOwnX {
+    static constexpr int kReduce = Epi::kReduce;
+    struct Pre {
+        typename Epi::Pre inner;
+        T xi;
+    };
+    Epi inner;
+    T *__restrict__ z;
+    double *partial;
+    decltype(Epi::fin) fin;
+    bool rarely_runs() const { return tile::rarely_runs(inner, 0); }
+    __device__ __forceinline__ bool skip() const { return inner.skip(); }
+    template <class XS>
+    __device__ __forceinline__ Pre pre(int64_t i, const XS &xs) const {
+        return {inner.pre(i, xs), xs(i)};
+    }
+    __device__ __forceinline__ void operator()(int64_t i, T acc, const Pre &p,
+                                               double (&red)[kReduce > 0 ? kReduce : 1]) const {
+        z[i] = p.xi;
+        inner(i, acc, p.inner, red);
+    }
+};
+template <class T, class Epi>
+StoreOwnX<T, Epi> store_own_x(const Epi &e, T *z) {
+    return StoreOwnX<T, Epi>{e, z, e.partial, e.fin};
+}
+
 // y = A x with sum_i w_i y_i; gated on *gate.
 template <class T, class Fin = tile::NoFinal>
 struct SpmvDot {
@@ -533,6 +590,9 @@ class KrylovImpl final : public Krylov {
 
     void setup(tf_ctx *ctx, const tf_csr &a) override {
         ready_ = false;
+        const char *f = std::getenv("THERMOFEM_B200_FUSE");
+        const char *fo = std::getenv("THERMOFEM_B200_FUSE_OUTER");
+        fuse_ = (f ? std::atoi(f) : 1) != 0 && !(fo && fo[0] == '0') ? 1 : 0;
         if (exec_) {
             cudaGraphExecDestroy(exec_);
             exec_ = nullptr;
@@ -570,7 +630,7 @@ class KrylovImpl final : public Krylov {
         }
         sl_.release();
         if constexpr (std::is_same_v<I, int32_t>) {
-            if (cd_.data() && sliced_enabled()) build_sliced(ctx, csr(), sl_);
+            if (cd_.data() && sliced_enabled()) build_sliced(ctx, csr(), sl_, false);
         }
         hier_.reset();
         if (precond_ == TF_PRECOND_AMG) {
@@ -702,6 +762,24 @@ class KrylovImpl final : public Krylov {
         c.cd = cd_.data();
         sl_.attach(c);
         return c;
+    }
+
+    // The preconditioner's last conversion fused into the kernel after it
+    // (THERMOFEM_B200_FUSE=0 or THERMOFEM_B200_FUSE_OUTER=0 keep them apart;
+    // the same bits either way).
+    bool fuse_outer() const { return hier_ && fuse_ != 0; }
+
+    // out = M^-1 in, then the operator SpMV of out with epi: the gathers read
+    // the preconditioner's output in its own storage and every row also
+    // stores its converted value into out.
+    template <class Epi>
+    void preconditioned_spmv(tf_ctx *ctx, const T *in, T *out, const Epi &epi, const char *name) {
+        const void *zs = hier_->apply_open(ctx, in);
+        if (hier_->storage_type() == TF_F32)
+            tile::launch(ctx, csr(), ConvertX<T, float>{static_cast<const float *>(zs)}, store_own_x(epi, out), name);
+        else
+            tile::launch(ctx, csr(), ConvertX<T, double>{static_cast<const double *>(zs)}, store_own_x(epi, out),
+                         name);
     }
 
     void precondition(tf_ctx *ctx, const T *in, T *out) {
@@ -862,9 +940,19 @@ class KrylovImpl final : public Krylov {
         unsigned *tk = s->tickets;
         const unsigned pg = static_cast<unsigned>(parts_);
         if (kind_ == TF_SOLVER_CG) {
-            precondition(ctx, r_.data(), z_.data());
-            launch_kernel(ctx, "dot_rho", k_dot<T, CgRho>, pg, 256, 0, n_, r_.data(), z_.data(), part,
-                          CgRho{s, tk + 0});
+            if (fuse_outer()) {
+                const void *zs = hier_->apply_open(ctx, static_cast<const T *>(r_.data()));
+                if (hier_->storage_type() == TF_F32)
+                    launch_kernel(ctx, "dot_rho_from", k_dot_from<T, float, CgRho>, pg, 256, 0, n_, r_.data(),
+                                  static_cast<const float *>(zs), z_.data(), part, CgRho{s, tk + 0});
+                else
+                    launch_kernel(ctx, "dot_rho_from", k_dot_from<T, double, CgRho>, pg, 256, 0, n_, r_.data(),
+                                  static_cast<const double *>(zs), z_.data(), part, CgRho{s, tk + 0});
+            } else {
+                precondition(ctx, r_.data(), z_.data());
+                launch_kernel(ctx, "dot_rho", k_dot<T, CgRho>, pg, 256, 0, n_, r_.data(), z_.data(), part,
+                              CgRho{s, tk + 0});
+            }
             launch_kernel(ctx, "cg_p", cg_p<T>, pg, 256, 0, s, n_, z_.data(), p_.data());
             tile::launch(ctx, csr(), tile::PlainX<T>{p_.data()},
                          SpmvDot<T, CgCurv>{q_.data(), p_.data(), &s->running, part, CgCurv{s, tk + 1}},
@@ -880,19 +968,25 @@ class KrylovImpl final : public Krylov {
         launch_kernel(ctx, "dot_rho", k_dot<T, BiRho>, pg, 256, 0, n_, shadow_.data(), r_.data(), part,
                       BiRho{s, tk + 0});
         launch_kernel(ctx, "bi_p", bi_p<T>, pg, 256, 0, s, n_, r_.data(), q_.data(), p_.data());
-        precondition(ctx, p_.data(), z_.data());
-        tile::launch(ctx, csr(), tile::PlainX<T>{z_.data()},
-                     SpmvDot<T, BiAlpha>{q_.data(), shadow_.data(), &s->running, part, BiAlpha{s, tk + 1}},
-                     "spmv_dot_alpha");
+        const SpmvDot<T, BiAlpha> alpha_epi{q_.data(), shadow_.data(), &s->running, part, BiAlpha{s, tk + 1}};
+        if (fuse_outer())
+            preconditioned_spmv(ctx, p_.data(), z_.data(), alpha_epi, "spmv_dot_alpha_from");
+        else {
+            precondition(ctx, p_.data(), z_.data());
+            tile::launch(ctx, csr(), tile::PlainX<T>{z_.data()}, alpha_epi, "spmv_dot_alpha");
+        }
         launch_kernel(ctx, "bi_s_norm", bi_s<T, BiSnorm>, pg, 256, 0, s, n_, r_.data(), q_.data(), z_.data(),
                       s_.data(), x_.data(), part, BiSnorm{s, tk + 2});
         tile::launch(ctx, csr(), tile::PlainX<T>{x_.data()},
                      ResidualNorm<T, BiEarly>{rhs_.data(), r_.data(), &s->early, part, BiEarly{s, tk + 3}},
                      "residual_early");
-        precondition(ctx, s_.data(), sh_.data());
-        tile::launch(ctx, csr(), tile::PlainX<T>{sh_.data()},
-                     SpmvDot2<T, BiOmega>{t_.data(), s_.data(), &s->normal, part, BiOmega{s, tk + 4}},
-                     "spmv_dot2_omega");
+        const SpmvDot2<T, BiOmega> omega_epi{t_.data(), s_.data(), &s->normal, part, BiOmega{s, tk + 4}};
+        if (fuse_outer())
+            preconditioned_spmv(ctx, s_.data(), sh_.data(), omega_epi, "spmv_dot2_omega_from");
+        else {
+            precondition(ctx, s_.data(), sh_.data());
+            tile::launch(ctx, csr(), tile::PlainX<T>{sh_.data()}, omega_epi, "spmv_dot2_omega");
+        }
         launch_kernel(ctx, "bi_xr_res", bi_xr<T, BiRes>, pg, 256, 0, s, n_, sh_.data(), s_.data(), t_.data(),
                       x_.data(), r_.data(), part, BiRes{s, tk + 5});
         tile::launch(ctx, csr(), tile::PlainX<T>{x_.data()}, ResidualNorm<T>{rhs_.data(), r_.data(), &s->refresh, part},
@@ -902,6 +996,7 @@ class KrylovImpl final : public Krylov {
     }
 
     int kind_;
+    int fuse_{1};
     tf_solver_options opt_;
     int precond_;
     std::unique_ptr<AmgConfig> amg_cfg_;

@@ -26,6 +26,10 @@ struct Csr {
     const int32_t *sp{nullptr};
     const T *sv{nullptr};
     const int16_t *sc{nullptr};
+    // With sorted slices: the row at position t of the sliced order (rows
+    // permuted within their 256-row tile, longest first).  Only epilogues
+    // without partial sums stream a sorted copy.
+    const int32_t *perm{nullptr};
 };
 
 // Column offset of a padding entry of the sliced layout.
@@ -37,11 +41,13 @@ struct SlicedCopy {
     DeviceBuffer<int32_t> sp;
     DeviceBuffer<T> val;
     DeviceBuffer<int16_t> col;
+    DeviceBuffer<int32_t> perm;  // sorted slices only
     int64_t entries{0};
     void release() {
         sp.release();
         val.release();
         col.release();
+        perm.release();
         entries = 0;
     }
     template <class I>
@@ -50,6 +56,7 @@ struct SlicedCopy {
             c.sp = sp.data();
             c.sv = val.data();
             c.sc = col.data();
+            c.perm = perm.data();
         }
     }
 };
@@ -115,11 +122,16 @@ template <class I>
 bool delta_columns(tf_ctx *ctx, int64_t rows, const I *rp, const I *ci, int16_t *cd);
 bool delta_columns_enabled();
 // Builds the sliced copy of a (which must carry its 2-byte column offsets
-// cd): slice width = its longest row.  False, with out released, when the
-// padding would exceed a quarter of nnz or the entries do not fit int32.
-// THERMOFEM_B200_SLICED=0 turns the copy off (sliced_enabled() false).
+// cd): slice width = its longest row.  When the rows in their own order
+// would pad by more than a quarter of nnz, allow_sort is set and
+// THERMOFEM_B200_SLICED=sorted, the rows of every 256-row tile are ordered
+// longest first (ties by row) and the copy carries that permutation (off by
+// default: on the aggregated levels the permuted row loads and stores cost
+// more in a cycle than the even slices save).  False, with out released,
+// when the padding still exceeds a quarter of nnz or the entries do not fit
+// int32.  THERMOFEM_B200_SLICED=0 turns the copy off (sliced_enabled() false).
 template <class T>
-bool build_sliced(tf_ctx *ctx, const Csr<T, int32_t> &a, SlicedCopy<T> &out);
+bool build_sliced(tf_ctx *ctx, const Csr<T, int32_t> &a, SlicedCopy<T> &out, bool allow_sort);
 bool sliced_enabled();
 template <class T>
 void restrict_sum(tf_ctx *ctx, int64_t nc, const int32_t *off, const int32_t *mem, const T *fine, T *coarse);

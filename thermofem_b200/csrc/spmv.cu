@@ -8,6 +8,7 @@
 // epilogue's pre() loads the row's own operands (issued at the start of the
 // row's tile so their latency overlaps the gathers).
 #include <cstdlib>
+#include <cstring>
 
 #include "tile.cuh"
 
@@ -182,17 +183,40 @@ __global__ void delta_columns_kernel(int64_t n, const I *__restrict__ rp, const 
     }
 }
 
+// Row order of the sorted sliced layout: within each 256-row tile, rows by
+// decreasing length, ties by row (a rank by counting; one CTA per tile).
+template <class I>
+__global__ void slice_sort_kernel(int64_t rows, const I *__restrict__ rp, int32_t *__restrict__ perm) {
+    pdl_enter();
+    __shared__ int64_t len[256];
+    const int64_t r0 = static_cast<int64_t>(blockIdx.x) * 256;
+    const int nr = static_cast<int>(rows - r0 < 256 ? rows - r0 : 256);
+    const int t = threadIdx.x;
+    if (t < nr) len[t] = static_cast<int64_t>(rp[r0 + t + 1] - rp[r0 + t]);
+    __syncthreads();
+    if (t >= nr) return;
+    const int64_t mine = len[t];
+    int rank = 0;
+    for (int k = 0; k < nr; ++k) rank += (len[k] > mine || (len[k] == mine && k < t)) ? 1 : 0;
+    perm[r0 + rank] = static_cast<int32_t>(r0 + t);
+}
+
 // Entries of each 32-row slice of the sliced layout (32 x its longest row),
-// one warp per slice, and their total.
+// one warp per slice, and their total.  Position t holds row perm[t] (or t).
 template <class I>
 __global__ void slice_entries_kernel(int64_t rows, int64_t nslices, const I *__restrict__ rp,
-                                     int32_t *__restrict__ entries, unsigned long long *total) {
+                                     const int32_t *__restrict__ perm, int32_t *__restrict__ entries,
+                                     unsigned long long *total) {
     pdl_enter();
     const int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
     const int64_t s = t >> 5;  // uniform across the warp
     if (s >= nslices) return;
     const int lane = static_cast<int>(t & 31);
-    int64_t len = t < rows ? static_cast<int64_t>(rp[t + 1] - rp[t]) : 0;
+    int64_t len = 0;
+    if (t < rows) {
+        const int64_t row = perm ? perm[t] : t;
+        len = static_cast<int64_t>(rp[row + 1] - rp[row]);
+    }
     for (int o = 16; o > 0; o >>= 1) len = max(len, static_cast<int64_t>(__shfl_xor_sync(0xffffffffu, len, o)));
     if (lane == 0) {
         const int64_t e = len * 32;
@@ -201,11 +225,13 @@ __global__ void slice_entries_kernel(int64_t rows, int64_t nslices, const I *__r
     }
 }
 
-// Row t's entries into its slice (column-major, padding after its last entry).
+// The entries of the row at position t into its slice (column-major,
+// padding after its last entry).
 template <class T, class I>
 __global__ void slice_fill_kernel(int64_t rows, int64_t nslices, const I *__restrict__ rp,
                                   const T *__restrict__ val, const int16_t *__restrict__ cd,
-                                  const int32_t *__restrict__ sp, T *__restrict__ sv, int16_t *__restrict__ sc) {
+                                  const int32_t *__restrict__ perm, const int32_t *__restrict__ sp,
+                                  T *__restrict__ sv, int16_t *__restrict__ sc) {
     pdl_enter();
     const int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
     const int64_t s = t >> 5;
@@ -215,8 +241,9 @@ __global__ void slice_fill_kernel(int64_t rows, int64_t nslices, const I *__rest
     const int64_t width = (static_cast<int64_t>(sp[s + 1]) - base) >> 5;
     int64_t j0 = 0, len = 0;
     if (t < rows) {
-        j0 = rp[t];
-        len = static_cast<int64_t>(rp[t + 1]) - j0;
+        const int64_t row = perm ? perm[t] : t;
+        j0 = rp[row];
+        len = static_cast<int64_t>(rp[row + 1]) - j0;
     }
     for (int64_t j = 0; j < width; ++j) {
         const int64_t k = base + j * 32 + lane;
@@ -499,31 +526,53 @@ bool sliced_enabled() {
     return !(v && v[0] == '0');
 }
 
+static bool sorted_slices_enabled() {
+    const char *v = std::getenv("THERMOFEM_B200_SLICED");
+    return v && std::strcmp(v, "sorted") == 0;
+}
+
+// Slice entry counts for the given row order; returns their total.
+static int64_t slice_entries(tf_ctx *ctx, int64_t rows, int64_t nslices, const int32_t *rp, const int32_t *perm,
+                             int32_t *entries) {
+    DeviceBuffer<unsigned long long> total(1);
+    memset_async(ctx, entries, 0, (nslices + 1) * sizeof(int32_t));
+    memset_async(ctx, total.data(), 0, sizeof(unsigned long long));
+    launch_kernel(ctx, "slice_entries", slice_entries_kernel<int32_t>, grid_for(nslices * 32), kBlock, 0, rows,
+                  nslices, rp, perm, entries, total.data());
+    return static_cast<int64_t>(read_scalar(ctx, total.data()));
+}
+
 template <class T>
-bool build_sliced(tf_ctx *ctx, const Csr<T, int32_t> &a, SlicedCopy<T> &out) {
+bool build_sliced(tf_ctx *ctx, const Csr<T, int32_t> &a, SlicedCopy<T> &out, bool allow_sort) {
     out.release();
     if (!a.rows || !a.nnz || !a.cd) return false;
     const int64_t nslices = (a.rows + 31) / 32;
-    DeviceBuffer<int32_t> entries(static_cast<size_t>(nslices) + 1);
-    DeviceBuffer<unsigned long long> total(1);
-    memset_async(ctx, entries.data(), 0, (nslices + 1) * sizeof(int32_t));
-    memset_async(ctx, total.data(), 0, sizeof(unsigned long long));
-    launch_kernel(ctx, "slice_entries", slice_entries_kernel<int32_t>, grid_for(nslices * 32), kBlock, 0, a.rows,
-                  nslices, a.rp, entries.data(), total.data());
-    const int64_t n = static_cast<int64_t>(read_scalar(ctx, total.data()));
     // padding of at most a quarter of nnz (tiny operators excepted); int32 entry starts
-    if (n >= INT32_MAX || (n > a.nnz + a.nnz / 4 && n > 4096)) return false;
+    auto fits = [&](int64_t n) { return n < INT32_MAX && (n <= a.nnz + a.nnz / 4 || n <= 4096); };
+    DeviceBuffer<int32_t> entries(static_cast<size_t>(nslices) + 1);
+    int64_t n = slice_entries(ctx, a.rows, nslices, a.rp, nullptr, entries.data());
+    if (!fits(n)) {
+        if (!allow_sort || !sorted_slices_enabled()) return false;
+        out.perm.allocate(static_cast<size_t>(a.rows));
+        launch_kernel(ctx, "slice_sort", slice_sort_kernel<int32_t>, grid_for(a.rows, 256), 256, 0, a.rows, a.rp,
+                      out.perm.data());
+        n = slice_entries(ctx, a.rows, nslices, a.rp, out.perm.data(), entries.data());
+        if (!fits(n)) {
+            out.release();
+            return false;
+        }
+    }
     out.sp.allocate(static_cast<size_t>(nslices) + 1);
     scan_exclusive(ctx, nslices + 1, entries.data(), out.sp.data());
     out.val.allocate(static_cast<size_t>(n));
     out.col.allocate(static_cast<size_t>(n));
     launch_kernel(ctx, "slice_fill", slice_fill_kernel<T, int32_t>, grid_for(nslices * 32), kBlock, 0, a.rows,
-                  nslices, a.rp, a.val, a.cd, out.sp.data(), out.val.data(), out.col.data());
+                  nslices, a.rp, a.val, a.cd, out.perm.data(), out.sp.data(), out.val.data(), out.col.data());
     out.entries = n;
     return true;
 }
-template bool build_sliced<float>(tf_ctx *, const Csr<float, int32_t> &, SlicedCopy<float> &);
-template bool build_sliced<double>(tf_ctx *, const Csr<double, int32_t> &, SlicedCopy<double> &);
+template bool build_sliced<float>(tf_ctx *, const Csr<float, int32_t> &, SlicedCopy<float> &, bool);
+template bool build_sliced<double>(tf_ctx *, const Csr<double, int32_t> &, SlicedCopy<double> &, bool);
 
 template <class T>
 void restrict_sum(tf_ctx *ctx, int64_t nc, const int32_t *off, const int32_t *mem, const T *fine, T *coarse) {

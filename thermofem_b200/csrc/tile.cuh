@@ -576,6 +576,10 @@ __global__ void __launch_bounds__(kThreads + 32) csr_pipe_kernel(int64_t rows, i
 // row accumulates its entries left to right from +0 exactly as the
 // row-per-thread kernels do (padding adds 0 * 0, which leaves any sum that
 // starts at +0 unchanged), so every output and partial sum is bit-identical.
+// A sorted copy (perm) orders the rows of each tile longest first, so a
+// slice's rows have similar lengths; lane l then computes row perm[slot]
+// (every output is still the same bits; only epilogues without partial sums
+// are launched on it).
 // ---------------------------------------------------------------------------
 template <class T, int G>
 struct SliceHead {
@@ -610,7 +614,8 @@ __device__ __forceinline__ void load_slice_head(SliceHead<T, G> &h, int64_t slic
 template <class T, int G, bool PF, class XS, class Epi>
 __global__ void __launch_bounds__(kThreads) sliced_kernel(int64_t rows, const int32_t *__restrict__ sp,
                                                           const T *__restrict__ sv, const int16_t *__restrict__ sc,
-                                                          int early, XS xs, Epi epi) {
+                                                          const int32_t *__restrict__ perm, int early, XS xs,
+                                                          Epi epi) {
     constexpr int K = Epi::kReduce;
     constexpr int KK = K > 0 ? K : 1;
     constexpr int kWarps = kThreads / 32;
@@ -625,8 +630,9 @@ __global__ void __launch_bounds__(kThreads) sliced_kernel(int64_t rows, const in
     if (epi.skip()) return;  // the gate reads the same device word in every CTA
     if (!early) load_slice_head(h, tile * kWarps + warp, nslices, sp, sv, sc, lane);
     for (; tile < ntiles; tile += gridDim.x) {
-        const int64_t row = tile * kThreads + threadIdx.x;
-        const bool live = row < rows;
+        const int64_t slot = tile * kThreads + threadIdx.x;  // position in the sliced order
+        const bool live = slot < rows;
+        const int64_t row = live && perm ? static_cast<int64_t>(__ldg(perm + slot)) : slot;
         typename Epi::Pre pre{};
         if (live) pre = epi.pre(row, xs);
         SliceHead<T, G> next;
@@ -878,11 +884,11 @@ void launch_sliced(tf_ctx *ctx, const Csr<T, I> &a, const XS &xs, const Epi &epi
     if (cfg.prefetch)
         launch_kernel(ctx, name, sliced_kernel<T, 8, true, XS, Epi>,
                       grid(resident_ctas<sliced_kernel<T, 8, true, XS, Epi>>(kThreads, 0)), kThreads, 0, a.rows, a.sp,
-                      a.sv, a.sc, early, xs, epi);
+                      a.sv, a.sc, a.perm, early, xs, epi);
     else
         launch_kernel(ctx, name, sliced_kernel<T, 8, false, XS, Epi>,
                       grid(resident_ctas<sliced_kernel<T, 8, false, XS, Epi>>(kThreads, 0)), kThreads, 0, a.rows,
-                      a.sp, a.sv, a.sc, early, xs, epi);
+                      a.sp, a.sv, a.sc, a.perm, early, xs, epi);
 }
 
 // Launches the sliced kernel when the operator carries a sliced copy and its
@@ -895,7 +901,9 @@ void launch(tf_ctx *ctx, const Csr<T, I> &a, const XS &xs, const Epi &epi, const
             const PipeConfig *force = nullptr) {
     if (a.rows == 0) return;
     if constexpr (std::is_same_v<I, int32_t>) {
-        if (a.sp && a.cd) {
+        // a sorted copy permutes rows within their tile, which would change
+        // the order of a reducing epilogue's partial sums: row tiles then
+        if (a.sp && a.cd && (!a.perm || Epi::kReduce == 0)) {
             const PipeConfig cfg = force ? *force : tuned_config<T, I, int16_t>(a.rows, a.nnz, ctx->sm_count);
             if (cfg.sliced) {
                 launch_sliced(ctx, a, xs, epi, name, cfg);
