@@ -233,6 +233,16 @@ class HierarchyImpl final : public Hierarchy {
     const void *open_t(tf_ctx *ctx, const T *rhs) {
         StableScope stable(ctx);
         Level<S> &f = levels_.front();
+        cudaStreamCaptureStatus capturing;
+        cuda_check(cudaStreamIsCapturing(ctx->stream, &capturing), "capture status");
+        if (capturing != cudaStreamCaptureStatusNone && fuse_ > 0) {
+            // inside the caller's capture the cycle is recorded inline (as
+            // run_cycle does), so its first kernel may read rhs itself: the
+            // conversion is held for the finest level's first op
+            pin_ = {rhs, std::is_same_v<T, double>};
+            enqueue(ctx);
+            return levels_.front().x();
+        }
         convert(ctx, f.n, rhs, f.rhs.data());
         run_cycle(ctx);
         return levels_.front().x();
@@ -325,6 +335,17 @@ class HierarchyImpl final : public Hierarchy {
             s.xout = l.x();
             rec_.push_back(s);
         } else if (!dry_) {
+            if (fusing() && pin_.src && &l == &levels_.front()) {
+                const PendingInput in = pin_;
+                pin_ = {};
+                if (in.f64)
+                    jacobi_zero_convert(ctx, l.n, l.dinv.data(), static_cast<const double *>(in.src), l.rhs.data(),
+                                        l.x(), w_);
+                else
+                    jacobi_zero_convert(ctx, l.n, l.dinv.data(), static_cast<const float *>(in.src), l.rhs.data(),
+                                        l.x(), w_);
+                return;
+            }
             if (fusing() && pr_.coarse == &l) {
                 restrict_jacobi_zero(ctx, l.n, pr_.fine->off.data(), pr_.fine->mem.data(), pr_.src, l.rhs.data(),
                                      l.dinv.data(), l.x(), w_);
@@ -522,6 +543,13 @@ class HierarchyImpl final : public Hierarchy {
     }
 
     void flush(tf_ctx *ctx) {
+        if (pin_.src) {
+            const PendingInput in = pin_;
+            pin_ = {};
+            Level<S> &f = levels_.front();
+            if (in.f64) convert(ctx, f.n, static_cast<const double *>(in.src), f.rhs.data());
+            else convert(ctx, f.n, static_cast<const float *>(in.src), f.rhs.data());
+        }
         if (pw_.kind != kWriteNone) launch_write(ctx, nullptr);
         if (pr_.coarse) {
             const PendingRestrict r = pr_;
@@ -712,6 +740,12 @@ class HierarchyImpl final : public Hierarchy {
     int fuse_{1};
     PendingRestrict pr_;
     PendingWrite pw_;
+    // The cycle input still to be converted into the finest level's rhs
+    // (taken by that level's zero-guess sweep, else launched by flush).
+    struct PendingInput {
+        const void *src{nullptr};
+        bool f64{false};
+    } pin_;
     std::vector<CoarseStep<S>> rec_;
     std::vector<std::pair<size_t, size_t>> entries_;
     size_t entry_{0};

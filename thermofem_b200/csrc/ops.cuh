@@ -111,6 +111,9 @@ void restrict_jacobi_zero(tf_ctx *ctx, int64_t nc, const int32_t *off, const int
 // x = w Dinv b
 template <class T>
 void jacobi_zero(tf_ctx *ctx, int64_t n, const T *dinv, const T *b, T *x, T w, const float *row_w);
+// b = S(in), x = w Dinv b (a cycle's input conversion fused with its first sweep)
+template <class S, class T>
+void jacobi_zero_convert(tf_ctx *ctx, int64_t n, const S *dinv, const T *in, S *b, S *x, S w);
 // Dinv from summed diagonal entries; throws TF_ERR_INVALID on a bad diagonal.
 template <class T, class I>
 void inverse_diagonal(tf_ctx *ctx, const Csr<T, I> &a, T *dinv);

@@ -495,6 +495,36 @@ void jacobi_zero(tf_ctx *ctx, int64_t n, const T *dinv, const T *b, T *x, T w, c
     launch_kernel(ctx, "jacobi_zero", jacobi_zero_kernel<T>, stride_grid(ctx, n), kBlock, 0, n, dinv, b, x, w, row_w);
 }
 
+// b = S(in), x = w Dinv b: the conversion of a cycle's right-hand side into
+// the finest level's storage fused with its zero-guess sweep (the same
+// values as convert followed by jacobi_zero).
+template <class S, class T>
+__global__ void jacobi_zero_convert_kernel(int64_t n, const S *__restrict__ dinv, const T *__restrict__ in,
+                                           S *__restrict__ b, S *__restrict__ x, S w) {
+    pdl_enter();
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const S bi = static_cast<S>(in[i]);
+        b[i] = bi;
+        x[i] = w * dinv[i] * bi;
+    }
+}
+
+template <class S, class T>
+void jacobi_zero_convert(tf_ctx *ctx, int64_t n, const S *dinv, const T *in, S *b, S *x, S w) {
+    if (!n) return;
+    launch_kernel(ctx, "jacobi_zero_convert", jacobi_zero_convert_kernel<S, T>, stride_grid(ctx, n), kBlock, 0, n,
+                  dinv, in, b, x, w);
+}
+template void jacobi_zero_convert<float, double>(tf_ctx *, int64_t, const float *, const double *, float *, float *,
+                                                 float);
+template void jacobi_zero_convert<float, float>(tf_ctx *, int64_t, const float *, const float *, float *, float *,
+                                                float);
+template void jacobi_zero_convert<double, double>(tf_ctx *, int64_t, const double *, const double *, double *,
+                                                  double *, double);
+template void jacobi_zero_convert<double, float>(tf_ctx *, int64_t, const double *, const float *, double *,
+                                                 double *, double);
+
 template <class T, class I>
 void inverse_diagonal(tf_ctx *ctx, const Csr<T, I> &a, T *dinv) {
     require(a.rows > 0 && a.rows == a.cols, "Inverse diagonal requires a nonempty square matrix");
