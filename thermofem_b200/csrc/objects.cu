@@ -31,7 +31,6 @@ struct tf_solver {
     tf_ctx *ctx;
     int value_type, index_type;
     std::unique_ptr<Krylov> k;
-    DeviceBuffer<unsigned char> hb, hx;  // staging for host-buffer applies
     std::unique_ptr<tf_amg> view;        // borrowed view of the AMG preconditioner
 };
 
@@ -343,21 +342,11 @@ int tf_solver_apply(tf_solver *s, const void *rhs, void *x, int host_buffers, tf
         require(s != nullptr && result != nullptr, "null argument");
         require(rhs && x, "null vector");
         DeviceScope scope(s->ctx->device);
-        if (!host_buffers) {
-            *result = s->k->solve(s->ctx, rhs, x);
-            return;
-        }
-        const int64_t n = s->k->rows();
-        if (n == 0) fail(TF_ERR_LOGIC, "solver requires setup");
-        const size_t bytes = static_cast<size_t>(n) * type_size(s->value_type);
-        s->hb.reserve(bytes);
-        s->hx.reserve(bytes);
-        tf_ctx *ctx = s->ctx;
-        cuda_check(cudaMemcpyAsync(s->hb.data(), rhs, bytes, cudaMemcpyHostToDevice, ctx->stream), "rhs upload");
-        cuda_check(cudaMemcpyAsync(s->hx.data(), x, bytes, cudaMemcpyHostToDevice, ctx->stream), "x upload");
-        *result = s->k->solve(ctx, s->hb.data(), s->hx.data());
-        cuda_check(cudaMemcpyAsync(x, s->hx.data(), bytes, cudaMemcpyDeviceToHost, ctx->stream), "x download");
-        cuda_check(cudaStreamSynchronize(ctx->stream), "solve download");
+        // Host buffers: the solve's own input and output copies (unified
+        // addressing, cudaMemcpyDefault) move rhs and x between the host and
+        // the solver's vectors directly; the solve ends with a stream sync.
+        if (host_buffers && s->k->rows() == 0) fail(TF_ERR_LOGIC, "solver requires setup");
+        *result = s->k->solve(s->ctx, rhs, x);
     });
 }
 
