@@ -388,13 +388,15 @@ def test_two_byte_column_stream_gives_identical_solves(ctx, case, monkeypatch):
     assert torch.equal(out[0][1], out[1][1])
 
 
-@pytest.mark.parametrize("shape", ["0,2", "1,3", "1,8", "0,5"])
+@pytest.mark.parametrize("shape", ["0,2", "1,3", "1,8", "0,5", "2,2,3", "2,3,5", "2,4,1"])
 @pytest.mark.parametrize("case", ["heat3d-cg-f32", "heat3d-cg-f64", "heat3d-bicgstab-f32"])
 def test_sliced_layout_gives_identical_solves(ctx, case, shape, monkeypatch):
     # Operators with 2-byte column offsets also carry a sliced copy (32-row
     # slices, entries column-major) that the SpMV family streams when it is
-    # faster.  THERMOFEM_B200_SLICED_SHAPE="prefetch,ctas" forces it with
-    # that launch shape, THERMOFEM_B200_SLICED=0 turns the copy off.  Same
+    # faster.  THERMOFEM_B200_SLICED_SHAPE="prefetch,ctas" forces the direct
+    # kernel with that launch shape, "2,stages,ctas" the staged one (tiles
+    # bulk-copied into a shared-memory ring), THERMOFEM_B200_SLICED=0 turns
+    # the copy off.  Same
     # per-row order and the same 256-row-block partial sums: the same bits,
     # on every level (coarse levels have rows longer than one 8-entry group)
     # and on a row count that is no multiple of 32.
@@ -429,7 +431,7 @@ def test_sliced_layout_gives_identical_solves(ctx, case, shape, monkeypatch):
         assert torch.equal(out[0][2], other[2])
 
 
-@pytest.mark.parametrize("shape", [None, "1,4", "0,3"])
+@pytest.mark.parametrize("shape", [None, "1,4", "0,3", "2,2,4", "2,3,2"])
 def test_operator_spmv_entry_points(ctx, shape, monkeypatch):
     # The solver's and the hierarchy's own operators (2-byte column stream,
     # sliced copy when the tuner picks it or a shape forces it) give the same

@@ -30,6 +30,8 @@ struct Csr {
     // permuted within their 256-row tile, longest first).  Only epilogues
     // without partial sums stream a sorted copy.
     const int32_t *perm{nullptr};
+    // Most entries of any 256-row tile (8 slices) of the sliced copy.
+    int64_t sl_tile_max{0};
 };
 
 // Column offset of a padding entry of the sliced layout.
@@ -43,12 +45,14 @@ struct SlicedCopy {
     DeviceBuffer<int16_t> col;
     DeviceBuffer<int32_t> perm;  // sorted slices only
     int64_t entries{0};
+    int64_t tile_max{0};  // most entries of any 256-row tile
     void release() {
         sp.release();
         val.release();
         col.release();
         perm.release();
         entries = 0;
+        tile_max = 0;
     }
     template <class I>
     void attach(Csr<T, I> &c) const {
@@ -57,6 +61,7 @@ struct SlicedCopy {
             c.sv = val.data();
             c.sc = col.data();
             c.perm = perm.data();
+            c.sl_tile_max = tile_max;
         }
     }
 };

@@ -572,6 +572,17 @@ static int64_t slice_entries(tf_ctx *ctx, int64_t rows, int64_t nslices, const i
     return static_cast<int64_t>(read_scalar(ctx, total.data()));
 }
 
+// Most entries of any 256-row tile (8 consecutive slices) of a sliced copy.
+__global__ void slice_tile_max_kernel(int64_t nslices, const int32_t *__restrict__ sp,
+                                      unsigned long long *tile_max) {
+    pdl_enter();
+    const int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    const int64_t s0 = t * 8;
+    if (s0 >= nslices) return;
+    const int64_t s1 = s0 + 8 < nslices ? s0 + 8 : nslices;
+    atomicMax(tile_max, static_cast<unsigned long long>(sp[s1] - sp[s0]));
+}
+
 template <class T>
 bool build_sliced(tf_ctx *ctx, const Csr<T, int32_t> &a, SlicedCopy<T> &out, bool allow_sort) {
     out.release();
@@ -598,6 +609,11 @@ bool build_sliced(tf_ctx *ctx, const Csr<T, int32_t> &a, SlicedCopy<T> &out, boo
     out.col.allocate(static_cast<size_t>(n));
     launch_kernel(ctx, "slice_fill", slice_fill_kernel<T, int32_t>, grid_for(nslices * 32), kBlock, 0, a.rows,
                   nslices, a.rp, a.val, a.cd, out.perm.data(), out.sp.data(), out.val.data(), out.col.data());
+    DeviceBuffer<unsigned long long> tmax(1);
+    memset_async(ctx, tmax.data(), 0, sizeof(unsigned long long));
+    launch_kernel(ctx, "slice_tile_max", slice_tile_max_kernel, grid_for((nslices + 7) / 8), kBlock, 0, nslices,
+                  out.sp.data(), tmax.data());
+    out.tile_max = static_cast<int64_t>(read_scalar(ctx, tmax.data()));
     out.entries = n;
     return true;
 }

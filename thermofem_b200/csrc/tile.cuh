@@ -688,6 +688,196 @@ __global__ void __launch_bounds__(kThreads) sliced_kernel(int64_t rows, const in
     if constexpr (K > 0) finish(epi.fin, epi.partial, static_cast<int>(ntiles));
 }
 
+// ---------------------------------------------------------------------------
+// Staged sliced kernel: the sliced copy streamed through shared memory.
+//
+// A tile's 8 slices are contiguous in the copy (entries [sp[8t], sp[8t+8])
+// of the values and of the column offsets), so the producer thread (warp 8,
+// lane 0) moves a whole tile with two bulk copies into a ring stage.  Slice
+// starts are multiples of 32 entries, so both copies start and end on
+// 16-byte boundaries (no ragged edges).  The producer also writes the
+// tile's 9 slice starts into the stage header before arming the stage.
+// Each consumer warp then reads its slice from shared memory lane by lane
+// (consecutive addresses: no bank conflicts) and only the x gathers leave
+// the SM.  Row sums, epilogues and the per-256-row-block partial sums are
+// those of the kernels above: the same bits.  Every wait is bounded as in
+// csr_pipe_kernel (fault word, drain of the CTA's own copies).
+// ---------------------------------------------------------------------------
+template <class T>
+struct SlicedStage {
+    static constexpr int kHeader = 64;  // 9 int32 slice starts, padded
+    int val_bytes, col_bytes, bytes;
+    __host__ __device__ explicit SlicedStage(int cap) {
+        val_bytes = (cap * static_cast<int>(sizeof(T)) + 127) & ~127;
+        col_bytes = (cap * 2 + 127) & ~127;
+        bytes = (kHeader + val_bytes + col_bytes + 127) & ~127;
+    }
+};
+
+template <class T, class XS, class Epi>
+__global__ void __launch_bounds__(kThreads + 32)
+    sliced_pipe_kernel(int64_t rows, const int32_t *__restrict__ sp, const T *__restrict__ sv,
+                       const int16_t *__restrict__ sc, int cap, int stages, int early, XS xs, Epi epi, int *fault) {
+    constexpr int K = Epi::kReduce;
+    constexpr int KK = K > 0 ? K : 1;
+    constexpr int kWarps = kThreads / 32;
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ uint64_t full_bar[kMaxStages], empty_bar[kMaxStages];
+    __shared__ double warp_sums[kMaxStages + 1][kWarps][KK];
+    __shared__ int warp_done[kMaxStages + 1];
+    __shared__ int skipped_cta;
+    const SlicedStage<T> L(cap);
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        for (int st = 0; st < stages; ++st) {
+            mbar_init(&full_bar[st], 1);
+            mbar_init(&empty_bar[st], kWarps);
+        }
+        for (int st = 0; st < kMaxStages + 1; ++st) warp_done[st] = 0;
+        mbar_fence_init();
+    }
+    __syncthreads();
+    auto stage_hdr = [&](int st) { return reinterpret_cast<int32_t *>(smem + static_cast<size_t>(st) * L.bytes); };
+    auto stage_val = [&](int st) {
+        return reinterpret_cast<T *>(smem + static_cast<size_t>(st) * L.bytes + SlicedStage<T>::kHeader);
+    };
+    auto stage_col = [&](int st) {
+        return reinterpret_cast<int16_t *>(smem + static_cast<size_t>(st) * L.bytes + SlicedStage<T>::kHeader +
+                                           L.val_bytes);
+    };
+    const int64_t ntiles = (rows + kThreads - 1) / kThreads;  // = 256-row blocks of partial sums
+    const int64_t nslices = (rows + 31) / 32;
+    bool ok = true;
+    uint32_t armed[kMaxStages] = {0, 0, 0, 0};  // producer: completions requested per stage
+
+    if (tid == kThreads) {
+        // ---- producer ----
+        uint32_t it = 0;
+        bool entered = false, stop = false;
+        auto enter = [&] {
+            if (!entered) {
+                entered = true;
+                pdl_enter();
+                stop = epi.skip();
+            }
+            return stop;
+        };
+        if (!early) enter();
+        // the slice starts of the CTA's next tile are loaded one tile ahead,
+        // so their latency overlaps the wait for a free stage
+        int32_t starts[kWarps + 1];
+        auto load_starts = [&](int64_t tile) {
+            const int64_t s0 = tile * kWarps;
+#pragma unroll
+            for (int k = 0; k <= kWarps; ++k) starts[k] = __ldg(sp + (s0 + k < nslices ? s0 + k : nslices));
+        };
+        if (static_cast<int64_t>(blockIdx.x) < ntiles) load_starts(blockIdx.x);
+        for (int64_t tile = blockIdx.x; tile < ntiles && ok && !stop; tile += gridDim.x, ++it) {
+            int32_t cur[kWarps + 1];
+#pragma unroll
+            for (int k = 0; k <= kWarps; ++k) cur[k] = starts[k];
+            if (tile + gridDim.x < ntiles) load_starts(tile + gridDim.x);
+            const int st = static_cast<int>(it % stages);
+            if (it >= static_cast<uint32_t>(stages)) {
+                if (enter()) break;
+                if (!mbar_wait(&empty_bar[st], ((it / stages) + 1) & 1)) {
+                    ok = false;
+                    break;
+                }
+            }
+            int32_t *hdr = stage_hdr(st);
+#pragma unroll
+            for (int k = 0; k <= kWarps; ++k) hdr[k] = cur[k];
+            const int64_t e0 = cur[0], e1 = cur[kWarps];
+            const uint32_t nv = static_cast<uint32_t>((e1 - e0) * static_cast<int64_t>(sizeof(T)));
+            const uint32_t nc = static_cast<uint32_t>((e1 - e0) * 2);
+            mbar_arrive_expect_tx(&full_bar[st], nv + nc);
+            ++armed[st];
+            if (e1 > e0) {
+                bulk_load(stage_val(st), sv + e0, nv, &full_bar[st]);
+                bulk_load(stage_col(st), sc + e0, nc, &full_bar[st]);
+            }
+        }
+        enter();
+        if (!ok) atomicExch(fault, 1);
+    } else if (tid < kThreads) {
+        // ---- consumers: warp w owns slice 8 tile + w, lane l its row ----
+        pdl_enter();
+        const int lane = tid & 31, warp = tid >> 5;
+        uint32_t it = 0, local_tile = 0;
+        const bool skipped = epi.skip();
+        if (tid == 0) skipped_cta = skipped ? 1 : 0;
+        const int64_t first = skipped ? ntiles : blockIdx.x;
+        for (int64_t tile = first; tile < ntiles && ok; tile += gridDim.x, ++it) {
+            const int64_t row = tile * kThreads + tid;
+            const bool live = row < rows;
+            typename Epi::Pre pre{};
+            if (live) pre = epi.pre(row, xs);
+            const int st = static_cast<int>(it % stages);
+            if (__any_sync(0xffffffffu, !mbar_wait(&full_bar[st], (it / stages) & 1))) {
+                ok = false;
+                if (lane == 0) atomicExch(fault, 1);
+                break;
+            }
+            const int32_t *hdr = stage_hdr(st);
+            const int base = hdr[warp] - hdr[0];
+            const int width = (hdr[warp + 1] - hdr[warp]) >> 5;
+            const T *vs = stage_val(st) + base + lane;
+            const int16_t *cs = stage_col(st) + base + lane;
+            T acc = T(0);
+            for (int j0 = 0; j0 < width; j0 += 8) {
+                int16_t c[8];
+                T y[8];
+#pragma unroll
+                for (int g = 0; g < 8; ++g) c[g] = j0 + g < width ? cs[(j0 + g) * 32] : kSlicePad;
+#pragma unroll
+                for (int g = 0; g < 8; ++g) y[g] = c[g] != kSlicePad ? xs(row + c[g]) : T(0);
+#pragma unroll
+                for (int g = 0; g < 8; ++g) acc += (j0 + g < width ? vs[(j0 + g) * 32] : T(0)) * y[g];
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty_bar[st]);
+            double red[KK];
+#pragma unroll
+            for (int q = 0; q < KK; ++q) red[q] = 0.0;
+            if (live) epi(row, acc, pre, red);
+            if constexpr (K > 0) {
+                // as in csr_pipe_kernel: the last warp of the tile adds the
+                // eight warp sums in warp order (ring of kMaxStages + 1 slots)
+                const int slot = static_cast<int>(local_tile % (kMaxStages + 1));
+#pragma unroll
+                for (int q = 0; q < K; ++q)
+                    for (int o = 16; o > 0; o >>= 1) red[q] += __shfl_down_sync(0xffffffffu, red[q], o);
+                if (lane == 0) {
+#pragma unroll
+                    for (int q = 0; q < K; ++q) warp_sums[slot][warp][q] = red[q];
+                    __threadfence_block();
+                    if (atomicAdd(&warp_done[slot], 1) == kWarps - 1) {
+                        __threadfence_block();
+#pragma unroll
+                        for (int q = 0; q < K; ++q) {
+                            double v = 0.0;
+                            for (int w = 0; w < kWarps; ++w) v += warp_sums[slot][w][q];
+                            epi.partial[q * ntiles + tile] = v;
+                        }
+                        warp_done[slot] = 0;
+                    }
+                }
+            }
+            ++local_tile;
+        }
+    }
+    __syncthreads();
+    if (tid == kThreads) {
+        for (int st = 0; st < stages; ++st)
+            if (armed[st]) mbar_wait(&full_bar[st], (armed[st] - 1) & 1);
+    }
+    if constexpr (K > 0) {
+        __syncthreads();
+        if (!skipped_cta) finish(epi.fin, epi.partial, static_cast<int>(ntiles));
+    }
+}
+
 // Pipelined launch shape: rows per thread, entries per chunk, stages in the
 // ring, resident CTAs per SM (the persistent grid is ctas_per_sm x SMs, at
 // most one CTA per tile).
@@ -702,10 +892,21 @@ struct PipeShape {
 // partial sums are per 256-row block), only the speed does.
 struct PipeConfig {
     int stages{2}, ctas_per_sm{4}, cap_pct{125}, rpt{1};
-    // Operators with a sliced copy: stream it (sliced_kernel) with
-    // sliced_ctas resident CTAs per SM and next-tile prefetch when set.
-    int sliced{0}, sliced_ctas{4}, prefetch{1};
+    // Operators with a sliced copy: stream it with sliced_ctas resident CTAs
+    // per SM, sliced = 1 directly (sliced_kernel, next-tile prefetch when
+    // set), sliced = 2 through a ring of sliced_stages shared-memory stages
+    // (sliced_pipe_kernel).
+    int sliced{0}, sliced_ctas{4}, prefetch{1}, sliced_stages{2};
 };
+
+// Stage capacity (entries) of the staged sliced kernel for a's copy: its
+// largest tile, or 0 when a stage would exceed 64 KB.
+template <class T, class I>
+int sliced_stage_cap(const Csr<T, I> &a) {
+    const int64_t cap = (a.sl_tile_max + 255) & ~int64_t(255);
+    if (cap <= 0 || cap > (int64_t(64) << 10)) return 0;
+    return SlicedStage<T>(static_cast<int>(cap)).bytes <= (64 << 10) ? static_cast<int>(cap) : 0;
+}
 
 template <class T, class I, class C = I>
 PipeShape pipe_shape(int64_t rows, int64_t nnz, int sm_count, const PipeConfig &cfg) {
@@ -876,6 +1077,20 @@ void launch_sliced(tf_ctx *ctx, const Csr<T, I> &a, const XS &xs, const Epi &epi
                    const PipeConfig &cfg) {
     const int64_t ntiles = (a.rows + kThreads - 1) / kThreads;
     const int early = ctx->stable && !rarely_runs(epi, 0) ? 1 : 0;
+    if (cfg.sliced == 2 && !a.perm) {
+        const int cap = sliced_stage_cap(a);
+        if (cap > 0) {
+            const size_t smem = static_cast<size_t>(SlicedStage<T>(cap).bytes) * cfg.sliced_stages;
+            allow_smem<sliced_pipe_kernel<T, XS, Epi>>(smem);
+            const int resident = resident_ctas<sliced_pipe_kernel<T, XS, Epi>>(kThreads + 32, smem);
+            const int per_sm = cfg.sliced_ctas < resident || resident < 1 ? cfg.sliced_ctas : resident;
+            const int64_t g = static_cast<int64_t>(ctx->sm_count) * per_sm;
+            launch_kernel(ctx, name, sliced_pipe_kernel<T, XS, Epi>, static_cast<int>(ntiles < g ? ntiles : g),
+                          kThreads + 32, smem, a.rows, a.sp, a.sv, a.sc, cap, cfg.sliced_stages, early, xs, epi,
+                          ctx->fault);
+            return;
+        }
+    }
     auto grid = [&](int resident) {
         const int per_sm = cfg.sliced_ctas < resident || resident < 1 ? cfg.sliced_ctas : resident;
         const int64_t g = static_cast<int64_t>(ctx->sm_count) * per_sm;
@@ -1052,27 +1267,50 @@ PipeConfig autotune_columns(tf_ctx *ctx, const Csr<T, I> &a, const T *x, T *y, f
             PipeConfig sbest = best;
             float sbest_t = 0;
             bool sfirst = true;
-            std::vector<std::pair<int, int>> shapes;
-            if (forced_pf >= 0) shapes.emplace_back(forced_pf ? 1 : 0, forced_ctas < 1 ? 1 : forced_ctas);
-            else
+            // shapes: (kind, prefetch or stages, ctas); kind 1 direct, 2 staged
+            std::vector<std::tuple<int, int, int>> shapes;
+            const int cap = sliced_stage_cap(a);
+            if (forced_pf >= 0) {
+                // "prefetch,ctas" forces the direct kernel, "2,stages,ctas" the staged one
+                int a3 = 0;
+                const char *v = std::getenv("THERMOFEM_B200_SLICED_SHAPE");
+                if (v && std::sscanf(v, "%d,%d,%d", &forced_pf, &forced_ctas, &a3) == 3 && forced_pf == 2 && cap)
+                    shapes.emplace_back(2, forced_ctas < 2 ? 2 : (forced_ctas > kMaxStages ? kMaxStages : forced_ctas),
+                                        a3 < 1 ? 1 : a3);
+                else
+                    shapes.emplace_back(1, forced_pf ? 1 : 0, forced_ctas < 1 ? 1 : forced_ctas);
+            } else {
                 for (int pf : {0, 1})
-                    for (int ctas : {2, 3, 4, 5, 6}) shapes.emplace_back(pf, ctas);
-            for (const auto &[pf, ctas] : shapes) {
+                    for (int ctas : {2, 3, 4, 5, 6}) shapes.emplace_back(1, pf, ctas);
+                if (cap)
+                    for (int stg : {2, 3})
+                        for (int ctas : {2, 3, 4, 5}) shapes.emplace_back(2, stg, ctas);
+            }
+            for (const auto &[kind, knob, ctas] : shapes) {
                 {
                     PipeConfig cfg = best;
-                    cfg.sliced = 1;
-                    cfg.prefetch = pf;
+                    cfg.sliced = kind;
                     cfg.sliced_ctas = ctas;
-                    const int resident =
-                        pf ? resident_ctas<sliced_kernel<T, 8, true, PlainX<T>, TuneStore<T>>>(kThreads, 0)
-                           : resident_ctas<sliced_kernel<T, 8, false, PlainX<T>, TuneStore<T>>>(kThreads, 0);
+                    int resident = 0;
+                    if (kind == 2) {
+                        cfg.sliced_stages = knob;
+                        const size_t smem = static_cast<size_t>(SlicedStage<T>(cap).bytes) * knob;
+                        if (smem * ctas > 220 * 1024 && forced_pf < 0) continue;
+                        allow_smem<sliced_pipe_kernel<T, PlainX<T>, TuneStore<T>>>(smem);
+                        resident = resident_ctas<sliced_pipe_kernel<T, PlainX<T>, TuneStore<T>>>(kThreads + 32, smem);
+                    } else {
+                        cfg.prefetch = knob;
+                        resident = knob ? resident_ctas<sliced_kernel<T, 8, true, PlainX<T>, TuneStore<T>>>(kThreads, 0)
+                                        : resident_ctas<sliced_kernel<T, 8, false, PlainX<T>, TuneStore<T>>>(kThreads, 0);
+                    }
                     if (resident < ctas && forced_pf < 0) continue;
                     const float ms = time_cfg(cfg);
                     if (tune_log())
                         std::fprintf(stderr,
-                                     "tf_autotune_spmv rows=%lld nnz=%lld T=%d sliced prefetch=%d ctas=%d %.2f us\n",
+                                     "tf_autotune_spmv rows=%lld nnz=%lld T=%d sliced %s=%d ctas=%d %.2f us\n",
                                      static_cast<long long>(a.rows), static_cast<long long>(a.nnz),
-                                     static_cast<int>(sizeof(T)), pf, ctas, ms * 1e3f);
+                                     static_cast<int>(sizeof(T)), kind == 2 ? "staged stages" : "prefetch", knob,
+                                     ctas, ms * 1e3f);
                     if (sfirst || ms < sbest_t) {
                         sbest_t = ms;
                         sbest = cfg;
