@@ -405,8 +405,11 @@ def test_sliced_layout_gives_identical_solves(ctx, case, shape, monkeypatch):
     b = torch.tensor(P.rhs_uniform(n, 84), device="cuda")
     solver = tf.BiCgStab if "bicgstab" in case else tf.Cg
     out = []
-    for flag in ("0", "1", "sorted"):
+    # padding bound 10 %: the aggregated levels (30-50 % in row order) keep
+    # CSR unless sorted; 50 % (the default): they take row-order slices too
+    for flag, pad in (("0", "10"), ("1", "10"), ("sorted", "10"), ("1", "50")):
         monkeypatch.setenv("THERMOFEM_B200_SLICED", flag)
+        monkeypatch.setenv("THERMOFEM_B200_SLICED_PAD", pad)
         monkeypatch.setenv("THERMOFEM_B200_SLICED_SHAPE", shape)
         s = solver(tf.solver_options(), "amg",
                    tf.amg_options(hierarchy_type=case[-3:], jacobi_weight=2 / 3, cycle="w"), ctx=ctx)
@@ -419,11 +422,12 @@ def test_sliced_layout_gives_identical_solves(ctx, case, shape, monkeypatch):
         if flag == "0":
             assert (layout, entries) == ("csr", len(m[1]))
         else:
-            assert layout == "sliced" and len(m[1]) <= entries <= len(m[1]) * 1.25
+            assert layout == "sliced" and len(m[1]) <= entries <= len(m[1]) * 1.5
             assert s.level_spmv_layout(0)[0] == "sliced"
             # coarse aggregated levels: with "sorted", rows ordered longest first within their tiles
             kinds = [s.level_spmv_layout(d)[0] for d in range(1, s.level_count())]
             assert ("sorted" in kinds) == (flag == "sorted"), kinds
+            assert (kinds[0] == "sliced") == (pad == "50"), kinds
     assert out[0][0]["status"] == "Converged"
     for other in out[1:]:
         assert out[0][0] == other[0]

@@ -73,6 +73,7 @@ struct Level {
     DeviceBuffer<int32_t> map, off, mem;
     DeviceBuffer<int16_t> cd;  // columns as row offsets, when they fit
     SlicedCopy<S> sl;          // sliced copy for the SpMV family, when built
+    bool sliced_on{true};      // the cycle streams sl (chosen at setup, select_layouts)
     int coarse{0};
     int cur{0};
     S *x() const { return cur ? x1.data() : x0.data(); }
@@ -85,7 +86,7 @@ struct Level {
         c.ci = ci.data();
         c.val = val.data();
         c.cd = cd.data();
-        sl.attach(c);
+        if (sliced_on) sl.attach(c);
         return c;
     }
 };
@@ -185,7 +186,76 @@ class HierarchyImpl final : public Hierarchy {
         coarse_solver = factored_ ? "pivoted GPU LU" : (singular ? "Jacobi (singular LU)" : "Jacobi (coarsening stopped)");
         visits.assign(levels_.size(), 0);
         plan_small_levels(ctx);
+        select_layouts(ctx);
         cuda_check(cudaStreamSynchronize(ctx->stream), "AMG setup");
+    }
+
+    // Which levels the cycle streams through their sliced copy, decided in
+    // the cycle itself: a kernel timed alone (tile::autotune) meets its
+    // operator either cold or warm in L2, while inside a cycle a mid-size
+    // level is partly resident and its neighbours' epilogues and
+    // programmatic launch overlap change the balance.  For every launched
+    // level with a sliced copy, finest first, the captured cycle is timed
+    // (CUDA events, 2 warm-up and 8 timed replays, each after the L2 cache
+    // is flushed) with the copy streamed and without, and the faster is kept.  Either choice gives the same
+    // bits.  Skipped when THERMOFEM_B200_SLICED_SHAPE forces a shape or
+    // THERMOFEM_B200_SLICED_SELECT=0.
+    void select_layouts(tf_ctx *ctx) {
+        if (std::getenv("THERMOFEM_B200_SLICED_SHAPE")) return;
+        if (const char *v = std::getenv("THERMOFEM_B200_SLICED_SELECT"); v && v[0] == '0') return;
+        std::vector<size_t> cand;
+        for (size_t d = 0; d < levels_.size() && d < coop_from_; ++d)
+            if (levels_[d].sl.sp.data()) cand.push_back(d);
+        if (cand.empty()) return;
+        StableScope stable(ctx);
+        fill_zero(ctx, levels_.front().n, levels_.front().rhs.data());
+        cudaEvent_t e0, e1;
+        cuda_check(cudaEventCreate(&e0), "event");
+        cuda_check(cudaEventCreate(&e1), "event");
+        // a solve runs its outer loop (an operator stream larger than the L2
+        // cache) between cycles: every timed replay starts after a write of
+        // more than the L2 size
+        void *flush = ctx->arena(tile::kTuneFlushBytes, 1);
+        auto time_cycle = [&](float *ms) {
+            capture(ctx);
+            if (!exec_) return false;
+            bool ok = true;
+            for (int r = 0; r < 2 && ok; ++r) ok = cudaGraphLaunch(exec_, ctx->stream) == cudaSuccess;
+            *ms = 0;
+            for (int r = 0; r < 8 && ok; ++r) {
+                float t = 0;
+                ok = cudaMemsetAsync(flush, r, tile::kTuneFlushBytes, ctx->stream) == cudaSuccess &&
+                     cudaEventRecord(e0, ctx->stream) == cudaSuccess &&
+                     cudaGraphLaunch(exec_, ctx->stream) == cudaSuccess &&
+                     cudaEventRecord(e1, ctx->stream) == cudaSuccess && cudaEventSynchronize(e1) == cudaSuccess &&
+                     cudaEventElapsedTime(&t, e0, e1) == cudaSuccess;
+                *ms += t;
+            }
+            cudaGraphExecDestroy(exec_);
+            exec_ = nullptr;
+            return ok;
+        };
+        bool ok = true;
+        for (size_t d : cand) {
+            float on = 0, off = 0;
+            levels_[d].sliced_on = true;
+            ok = time_cycle(&on);
+            levels_[d].sliced_on = false;
+            ok = ok && time_cycle(&off);
+            levels_[d].sliced_on = ok && on <= off;
+            if (tile::tune_log())
+                std::fprintf(stderr, "select_layouts level %zu rows=%lld cycle %.2f us sliced, %.2f us csr\n", d,
+                             static_cast<long long>(levels_[d].n), on * 1e3f / 8, off * 1e3f / 8);
+            if (!ok) break;
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        // the cycle graph of the first apply is captured with the kept layouts
+        cudaGetLastError();
+        capture_failed_ = false;
+        for (auto &l : levels_) l.cur = 0;
+        std::fill(visits.begin(), visits.end(), 0);
+        check_faults(ctx);
     }
 
     void apply(tf_ctx *ctx, const double *rhs, double *x) override { apply_t(ctx, rhs, x); }

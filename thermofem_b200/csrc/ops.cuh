@@ -131,12 +131,13 @@ bool delta_columns(tf_ctx *ctx, int64_t rows, const I *rp, const I *ci, int16_t 
 bool delta_columns_enabled();
 // Builds the sliced copy of a (which must carry its 2-byte column offsets
 // cd): slice width = its longest row.  When the rows in their own order
-// would pad by more than a quarter of nnz, allow_sort is set and
+// would pad by more than THERMOFEM_B200_SLICED_PAD percent of nnz (default
+// 50 for FP64 values, 25 for FP32), allow_sort is set and
 // THERMOFEM_B200_SLICED=sorted, the rows of every 256-row tile are ordered
 // longest first (ties by row) and the copy carries that permutation (off by
 // default: on the aggregated levels the permuted row loads and stores cost
 // more in a cycle than the even slices save).  False, with out released,
-// when the padding still exceeds a quarter of nnz or the entries do not fit
+// when the padding still exceeds that bound or the entries do not fit
 // int32.  THERMOFEM_B200_SLICED=0 turns the copy off (sliced_enabled() false).
 template <class T>
 bool build_sliced(tf_ctx *ctx, const Csr<T, int32_t> &a, SlicedCopy<T> &out, bool allow_sort);

@@ -588,8 +588,15 @@ bool build_sliced(tf_ctx *ctx, const Csr<T, int32_t> &a, SlicedCopy<T> &out, boo
     out.release();
     if (!a.rows || !a.nnz || !a.cd) return false;
     const int64_t nslices = (a.rows + 31) / 32;
-    // padding of at most a quarter of nnz (tiny operators excepted); int32 entry starts
-    auto fits = [&](int64_t n) { return n < INT32_MAX && (n <= a.nnz + a.nnz / 4 || n <= 4096); };
+    // padding of at most THERMOFEM_B200_SLICED_PAD percent of nnz (tiny
+    // operators excepted; int32 entry starts).  Default 50 for FP64 values,
+    // where the row-tile kernel's per-row work outweighs the padded bytes on
+    // the aggregated levels (30-45 % padding), 25 for FP32, where it does not
+    // (128^3 PCG, one B200: FP64 36.1-36.8 vs 37.9-38.5 ms with 50 vs 25;
+    // mixed 30.6 vs 29.4-29.8 ms).
+    int pad_pct = sizeof(T) == 8 ? 50 : 25;
+    if (const char *v = std::getenv("THERMOFEM_B200_SLICED_PAD")) pad_pct = std::atoi(v);
+    auto fits = [&](int64_t n) { return n < INT32_MAX && (n <= a.nnz + a.nnz * pad_pct / 100 || n <= 4096); };
     DeviceBuffer<int32_t> entries(static_cast<size_t>(nslices) + 1);
     int64_t n = slice_entries(ctx, a.rows, nslices, a.rp, nullptr, entries.data());
     if (!fits(n)) {

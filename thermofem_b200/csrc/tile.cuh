@@ -1192,7 +1192,8 @@ PipeConfig autotune_columns(tf_ctx *ctx, const Csr<T, I> &a, const T *x, T *y, f
     const bool cold = static_cast<double>(a.nnz) * (sizeof(T) + sizeof(C)) +
                           static_cast<double>(a.rows) * (sizeof(I) + 2 * sizeof(T)) >
                       static_cast<double>(kTuneFlushBytes) / 3;
-    DeviceBuffer<unsigned char> flush(cold ? kTuneFlushBytes : 0);
+    // (the context's second scratch arena: allocated once, kept for later setups)
+    unsigned char *flush = cold ? static_cast<unsigned char *>(ctx->arena(kTuneFlushBytes, 1)) : nullptr;
     auto time_cfg = [&](const PipeConfig &cfg) {
         for (int w = 0; w < 2; ++w) launch(ctx, a, PlainX<T>{x}, TuneStore<T>{x, y, nullptr}, "autotune", &cfg);
         if (!cold) {
@@ -1206,7 +1207,7 @@ PipeConfig autotune_columns(tf_ctx *ctx, const Csr<T, I> &a, const T *x, T *y, f
         }
         float total = 0;
         for (int r = 0; r < 5; ++r) {
-            cuda_check(cudaMemsetAsync(flush.data(), r, kTuneFlushBytes, ctx->stream), "tune flush");
+            cuda_check(cudaMemsetAsync(flush, r, kTuneFlushBytes, ctx->stream), "tune flush");
             cuda_check(cudaMemcpyAsync(y, x, static_cast<size_t>(a.rows) * sizeof(T), cudaMemcpyDeviceToDevice,
                                        ctx->stream),
                        "tune copy");
