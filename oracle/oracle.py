@@ -474,3 +474,44 @@ def mlp_gradient(params, x, target, lo, hi):
     dh = np.where(a > 0, dz[:, None] * w2[None, :], 0.0)
     g = np.concatenate([(dh.T @ x).ravel(), dh.sum(0), (dz[:, None] * h).sum(0), [dz.sum()]])
     return g, float((e * e).sum())
+
+
+# --------------------------------------------------------------------------
+# The reference's own GPU solve path (oracle/_ref/libref_gpu.so, built by
+# `make -C oracle refgpu` from the reference sources): Cg / BiCgStab with its
+# aggregation Amg in FP64 (ref_gpu_shim.cu).  A checker for the GPU tests.
+# --------------------------------------------------------------------------
+REF_GPU_LIB = os.path.join(HERE, "_ref", "libref_gpu.so")
+_ref_gpu = None
+
+
+def ref_gpu_available():
+    return os.path.exists(REF_GPU_LIB)
+
+
+def ref_gpu_solve(a: Csr, b, x0=None, kind="cg", cycle="v", jacobi_weight=2.0 / 3.0, coarse_rows=64, repeats=1):
+    """The reference's FP64 AMG-preconditioned solve of a x = b (from x0,
+    default zero).  Returns (x, report) with iterations, status (0 Converged,
+    1 MaxIterations, 2 Breakdown, 3 NonFinite), relative_residual, setup_s
+    and solve_s (the fastest of `repeats` solves, host clock around
+    device-synchronised calls)."""
+    global _ref_gpu
+    if _ref_gpu is None:
+        r = C.CDLL(REF_GPU_LIB)
+        P, I, D = C.c_void_p, C.c_int, C.c_double
+        r.ref_gpu_solve.argtypes = [I, P, P, P, C.c_int64, P, P, I, D, I, I, P, P, P, P, P]
+        r.ref_gpu_solve.restype = I
+        _ref_gpu = r
+    rp, ci, val = _arrs(a)
+    n = a.rows
+    b = np.ascontiguousarray(b, np.float64)
+    x = np.zeros(n) if x0 is None else np.array(x0, np.float64)
+    it, st = np.zeros(1, np.int32), np.zeros(1, np.int32)
+    rel, ts, tv = np.zeros(1), np.zeros(1), np.zeros(1)
+    rc = _ref_gpu.ref_gpu_solve({"cg": 0, "bicgstab": 1}[kind], _ptr(rp), _ptr(ci), _ptr(val), n, _ptr(b), _ptr(x),
+                                {"v": 0, "w": 1, "f": 2}[cycle], float(jacobi_weight), int(coarse_rows),
+                                int(repeats), _ptr(it), _ptr(st), _ptr(rel), _ptr(ts), _ptr(tv))
+    if rc != 0:
+        raise OracleError("reference GPU solve failed")
+    return x, {"iterations": int(it[0]), "status": int(st[0]), "relative_residual": float(rel[0]),
+               "setup_s": float(ts[0]), "solve_s": float(tv[0])}

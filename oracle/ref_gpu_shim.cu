@@ -1,0 +1,95 @@
+// ref_gpu_shim.cu -- test infrastructure, never linked by the product.
+//
+// A C entry point over the reference's own GPU solve path (its Cg / BiCgStab
+// with its aggregation Amg, cuSPARSE/cuBLAS/CUB underneath), compiled by
+// oracle/Makefile from the reference sources where they lie into
+// oracle/_ref/libref_gpu.so.  The tests call it to compare this library's
+// solves with the reference's on the same inputs, and report its time.
+//
+// Reference API used: CsrMatrix(rows, cols, offsets, columns, values)
+// (include/DataStructure/CsrMatrix.cuh:81-87), Vector(span)
+// (include/DataStructure/Vector.cuh:34), copyToHost (Vector.cuh:65),
+// AmgOptions (include/Preconditioner/Amg.cuh:14-25), Amg(options)
+// (Amg.cuh:64), Cg(options, preconditioner) (include/Solver/Cg.cuh:44),
+// BiCgStab(options, preconditioner) (include/Solver/BiCgStab.cuh:50),
+// setup / apply and SolveResult (include/Solver/Interfaces.cuh).
+#include <Preconditioner/Amg.cuh>
+#include <Solver/BiCgStab.cuh>
+#include <Solver/Cg.cuh>
+
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cstdio>
+#include <exception>
+#include <memory>
+#include <span>
+
+namespace {
+
+using namespace thermofem;
+
+template <class S, class O>
+int run(const int32_t *rp, const int32_t *ci, const double *val, int64_t n, const double *b, double *x, int cycle,
+        double jacobi_weight, int coarse_rows, int repeats, int *iterations, int *status, double *rel_residual,
+        double *setup_seconds, double *solve_seconds) {
+    const int64_t nnz = rp[n];
+    CsrMatrix<double> a(static_cast<std::size_t>(n), static_cast<std::size_t>(n),
+                        std::span<const int>(rp, static_cast<std::size_t>(n + 1)),
+                        std::span<const int>(ci, static_cast<std::size_t>(nnz)),
+                        std::span<const double>(val, static_cast<std::size_t>(nnz)));
+    AmgOptions<double> ao;
+    ao.jacobiWeight_ = jacobi_weight;
+    ao.coarseRows_ = coarse_rows;
+    ao.cycle_ = cycle == 1 ? multigrid::Cycle::W : (cycle == 2 ? multigrid::Cycle::F : multigrid::Cycle::V);
+    O so;
+    S solver(so, std::make_unique<Amg<double>>(ao));
+    cudaDeviceSynchronize();
+    auto t0 = std::chrono::steady_clock::now();
+    solver.setup(a);
+    cudaDeviceSynchronize();
+    *setup_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    Vector<double> rhs(std::span<const double>(b, static_cast<std::size_t>(n)));
+    double best = 0;
+    for (int r = 0; r < (repeats < 1 ? 1 : repeats); ++r) {
+        Vector<double> xv(std::span<const double>(x, static_cast<std::size_t>(n)));
+        cudaDeviceSynchronize();
+        t0 = std::chrono::steady_clock::now();
+        const auto res = solver.apply(rhs, xv);
+        cudaDeviceSynchronize();
+        const double t = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        if (r == 0 || t < best) best = t;
+        if (r + 1 == (repeats < 1 ? 1 : repeats)) {
+            xv.copyToHost(std::span<double>(x, static_cast<std::size_t>(n)));
+            *iterations = res.iterations_;
+            *status = static_cast<int>(res.status_);
+            *rel_residual = res.relativeResidual_;
+        }
+    }
+    *solve_seconds = best;
+    return 0;
+}
+
+}  // namespace
+
+// Solves A x = b with the reference's FP64 AMG-preconditioned solver (kind 0
+// PCG, 1 BiCGStab; cycle 0 V, 1 W, 2 F) from the initial guess in x, `repeats`
+// times from that guess; x receives the last solution.  Times are host wall
+// clock around device-synchronised calls (setup once, the fastest solve).
+// Returns 0, or -1 after printing the exception the reference raised.
+extern "C" int ref_gpu_solve(int kind, const int32_t *rp, const int32_t *ci, const double *val, int64_t n,
+                             const double *b, double *x, int cycle, double jacobi_weight, int coarse_rows,
+                             int repeats, int *iterations, int *status, double *rel_residual, double *setup_seconds,
+                             double *solve_seconds) {
+    try {
+        if (kind == 1)
+            return run<BiCgStab<double>, BiCgStabOptions<double>>(rp, ci, val, n, b, x, cycle, jacobi_weight,
+                                                                  coarse_rows, repeats, iterations, status,
+                                                                  rel_residual, setup_seconds, solve_seconds);
+        return run<Cg<double>, CgOptions<double>>(rp, ci, val, n, b, x, cycle, jacobi_weight, coarse_rows, repeats,
+                                                  iterations, status, rel_residual, setup_seconds, solve_seconds);
+    } catch (const std::exception &e) {
+        std::fprintf(stderr, "reference solve failed: %s\n", e.what());
+        return -1;
+    }
+}

@@ -1,0 +1,77 @@
+"""This library's solves against the reference's own GPU solve path.
+
+The reference library (its Cg / BiCgStab with its aggregation Amg on
+cuSPARSE, cuBLAS and CUB) is compiled for sm_100a from its sources by
+`make -C oracle refgpu` into oracle/_ref/libref_gpu.so; these tests skip
+where that build is absent.  Same inputs, same options (FP64 hierarchy,
+Jacobi w = 2/3, coarse LU <= 64 rows, tolerance 1e-8): the iteration
+counts agree within one and the solutions within 1e-6, as the CPU-oracle
+parity tests require.  The last test also reports both solve times on the
+128^3 benchmark problem.
+"""
+import json
+
+import numpy as np
+import pytest
+import torch
+
+import thermofem_b200 as tf
+from oracle import oracle as O
+from thermofem_b200 import problems as P
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not O.ref_gpu_available(), reason="reference GPU build absent (make -C oracle refgpu)")]
+
+
+def _ours(m, b, kind, cycle, hierarchy="f64"):
+    solver = tf.BiCgStab if kind == "bicgstab" else tf.Cg
+    s = solver(tf.solver_options(), "amg",
+               tf.amg_options(hierarchy_type=hierarchy, jacobi_weight=2 / 3, coarse_rows=64, cycle=cycle))
+    s.setup(tf.DeviceCsr.from_host(*m))
+    x = torch.zeros(len(b), dtype=torch.float64, device="cuda")
+    bd = torch.tensor(b, device="cuda")
+    rep = s.apply(bd, x)
+    return s, x, bd, rep
+
+
+@pytest.mark.parametrize("problem,kind,cycle", [("heat", "cg", "v"), ("heat", "cg", "w"), ("heat", "cg", "f"),
+                                                ("heat", "bicgstab", "v"), ("convdiff", "bicgstab", "w")])
+def test_solves_match_the_reference_gpu_build(problem, kind, cycle):
+    m = P.heat3d(24, seed=41) if problem == "heat" else P.convdiff3d(20, seed=43)
+    n = len(m[0]) - 1
+    b = P.rhs_uniform(n, 42)
+    xr, rr = O.ref_gpu_solve(O.Csr(n, *m), b, kind=kind, cycle=cycle)
+    _, x, _, rep = _ours(m, b, kind, cycle)
+    assert rr["status"] == 0 and rep["status"] == "Converged"
+    assert abs(rep["iterations"] - rr["iterations"]) <= 1, (rep["iterations"], rr["iterations"])
+    xo = x.cpu().numpy()
+    assert np.linalg.norm(xo - xr) / np.linalg.norm(xr) < 1e-6
+
+
+def test_reference_gpu_build_on_the_benchmark_problem(capsys):
+    # 128^3 log-normal heat, PCG + AMG V(1,1): the reference's FP64 solve and
+    # this library's FP64 and mixed solves, device-synchronised wall times.
+    m = P.heat3d(128, 1001)
+    n = len(m[0]) - 1
+    b = P.rhs_uniform(n, 1002)
+    xr, rr = O.ref_gpu_solve(O.Csr(n, *m), b, kind="cg", cycle="v", repeats=2)
+    out = {"reference_fp64": rr}
+    for hierarchy in ("f64", "f32"):
+        s, x, bd, rep = _ours(m, b, "cg", "v", hierarchy)
+        times = []
+        for _ in range(3):
+            x.zero_()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            rep = s.apply(bd, x)
+            e1.record()
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1) / 1e3)
+        out[f"ours_{hierarchy}"] = {"iterations": rep["iterations"], "solve_s": min(times)}
+        if hierarchy == "f64":
+            assert abs(rep["iterations"] - rr["iterations"]) <= 1
+            assert np.linalg.norm(x.cpu().numpy() - xr) / np.linalg.norm(xr) < 1e-6
+            assert min(times) < rr["solve_s"]
+    with capsys.disabled():
+        print("\nreference GPU build vs this library, heat3d 128^3 PCG V(1,1): " + json.dumps(out))

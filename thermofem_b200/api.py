@@ -52,7 +52,7 @@ class Context:
         check(lib().tf_ctx_create(device, C.c_void_p(self.stream.cuda_stream), C.byref(h)))
         self.h = h
 
-    def close(self):
+    def close(self, _release=_release):  # bound now: module globals are cleared at interpreter shutdown
         if getattr(self, "h", None):
             _release("tf_ctx_destroy", self.h)
             self.h = None
@@ -358,7 +358,7 @@ class Transfer:
     histogram: np.ndarray
     _handle: object = None
 
-    def __del__(self):
+    def __del__(self, _release=_release):  # bound now: globals are cleared at shutdown
         if self._handle is not None:
             _release("tf_transfer_free", self._handle)
             self._handle = None
@@ -548,7 +548,7 @@ class Amg(_AmgView):
     def _h(self):
         return self.h
 
-    def __del__(self):
+    def __del__(self, _release=_release):  # bound now: globals are cleared at shutdown
         if getattr(self, "h", None):
             _release("tf_amg_destroy", self.h)
             self.h = None
@@ -575,7 +575,7 @@ class Jacobi:
                                      C.byref(h)))
         self.h = h
 
-    def __del__(self):
+    def __del__(self, _release=_release):  # bound now: globals are cleared at shutdown
         if getattr(self, "h", None):
             _release("tf_jacobi_destroy", self.h)
             self.h = None
@@ -611,7 +611,7 @@ class _Solver(_AmgView):
             raise ValueError("solver has no AMG preconditioner")
         return p
 
-    def __del__(self):
+    def __del__(self, _release=_release):  # bound now: globals are cleared at shutdown
         if getattr(self, "h", None):
             _release("tf_solver_destroy", self.h)
             self.h = None
@@ -709,7 +709,7 @@ class Batch:
         check(lib().tf_batch_create(self.ctx.h, len(self.solvers), arr, C.byref(h)))
         self.h = h
 
-    def __del__(self):
+    def __del__(self, _release=_release):  # bound now: globals are cleared at shutdown
         if getattr(self, "h", None):
             _release("tf_batch_destroy", self.h)
             self.h = None
@@ -744,7 +744,7 @@ class Mlp:
         if params is not None:
             self.set_params(params)
 
-    def __del__(self):
+    def __del__(self, _release=_release):  # bound now: globals are cleared at shutdown
         if getattr(self, "h", None):
             _release("tf_mlp_destroy", self.h)
             self.h = None
