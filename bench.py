@@ -355,7 +355,23 @@ def run_profile(args):
             s.spmv(b, x)
         torch.cuda.synchronize()
         torch.cuda.nvtx.range_pop()
-        print(json.dumps({"profile": "spmv", "rows": n, "nnz": len(idx)}), flush=True)
+        print(json.dumps({"profile": "spmv", "rows": n, "nnz": len(idx), "layout": s.spmv_layout()}), flush=True)
+        return
+    if args.profile == "spmv32":
+        # the FP32 finest level of the mixed hierarchy, as level_spmv streams it
+        s = tf.Cg(tf.solver_options(), "amg", tf.amg_options(hierarchy_type="f32", **AMG, **_small(args)), ctx=ctx)
+        s.setup(a)
+        x32, y32 = b.float(), torch.empty(n, dtype=torch.float32, device="cuda")
+        for _ in range(args.warmup):
+            s.level_spmv(0, x32, y32)
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_push("spmv")  # ncu --nvtx --nvtx-include "spmv/"
+        for _ in range(args.steps):
+            s.level_spmv(0, x32, y32)
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_pop()
+        print(json.dumps({"profile": "spmv32", "rows": n, "nnz": len(idx), "layout": s.level_spmv_layout(0)}),
+              flush=True)
         return
     s = tf.Cg(tf.solver_options(), "amg",
               tf.amg_options(hierarchy_type="f32" if args.profile == "mixed" else "f64", **AMG, **_small(args)),
@@ -388,8 +404,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--small-level-rows", type=int, default=None,
                     help="tf_amg_options.small_level_rows (default: the library default)")
-    ap.add_argument("--profile", choices=["mixed", "fp64", "spmv"], default=None,
-                    help="profiling run: setup, --warmup solves, then --steps solves of one path; no JSON line")
+    ap.add_argument("--profile", choices=["mixed", "fp64", "spmv", "spmv32"], default=None,
+                    help="profiling run: setup, --warmup solves, then --steps solves of one path (spmv: the FP64 "
+                         "operator SpMV; spmv32: the FP32 finest level's)")
     ap.add_argument("--workload", choices=["batched", "convdiff", "heat", "learned"], default=None,
                     help="the other BASELINE configs (one JSON line each, not the headline): batched = 48 "
                          "transient systems x 20 steps; convdiff = 192^3 BiCGStab W-cycle; heat = --size^3 heat; "

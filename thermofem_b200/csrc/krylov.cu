@@ -166,6 +166,11 @@ template <class T, class S>
 struct ConvertX {
     const S *__restrict__ x;
     __device__ __forceinline__ T operator()(int64_t j) const { return static_cast<T>(__ldg(x + j)); }
+    struct View {
+        const S *__restrict__ p;
+        __device__ __forceinline__ T operator()(int c) const { return static_cast<T>(__ldg(p + c)); }
+    };
+    __device__ __forceinline__ View row(int64_t i) const { return {x + i}; }
 };
 
 // Epi that also stores each row's own converted x_i into z: the SpMV that

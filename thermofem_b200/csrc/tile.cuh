@@ -53,10 +53,18 @@ __device__ __forceinline__ void stage(E *dst, const E *__restrict__ src, int n) 
     if (tail + static_cast<int>(threadIdx.x) < n) dst[tail + threadIdx.x] = src[tail + threadIdx.x];
 }
 
+// Gather functors: xs(j) is x~_j; xs.row(i) is a view of x~ around row i,
+// view(c) = x~_{i+c}, for kernels that gather by column offsets (one 32-bit
+// offset per entry instead of a 64-bit index).
 template <class T>
 struct PlainX {
     const T *__restrict__ x;
     __device__ __forceinline__ T operator()(int64_t j) const { return __ldg(x + j); }
+    struct View {
+        const T *__restrict__ p;
+        __device__ __forceinline__ T operator()(int c) const { return __ldg(p + c); }
+    };
+    __device__ __forceinline__ View row(int64_t i) const { return {x + i}; }
 };
 
 // x~_j = x_j + e[map_j]: the prolongation x += P e read on the fly.
@@ -66,6 +74,13 @@ struct ProlongX {
     const int32_t *__restrict__ map;
     const T *__restrict__ e;
     __device__ __forceinline__ T operator()(int64_t j) const { return __ldg(x + j) + __ldg(e + __ldg(map + j)); }
+    struct View {
+        const T *__restrict__ p;
+        const int32_t *__restrict__ m;
+        const T *__restrict__ e;
+        __device__ __forceinline__ T operator()(int c) const { return __ldg(p + c) + __ldg(e + __ldg(m + c)); }
+    };
+    __device__ __forceinline__ View row(int64_t i) const { return {x + i, map + i, e}; }
 };
 
 // Deterministic block reduction of K doubles; thread 0 holds the result.
@@ -469,6 +484,12 @@ __global__ void __launch_bounds__(kThreads + 32) csr_pipe_kernel(int64_t rows, i
                 constexpr int kGather = 8;
                 int lo[RPT], hi[RPT];
                 T y[RPT][kGather];
+                // x~_j of entry o of row k: through the row's view when the
+                // entries are column offsets (a 32-bit offset per gather)
+                auto gather = [&](int k, int o) {
+                    if constexpr (std::is_same_v<C, int16_t>) return xs.row(r0 + tid + k * kThreads)(sc[o]);
+                    else return xs(column_of(r0 + tid + k * kThreads, sc[o]));
+                };
 #pragma unroll
                 for (int k = 0; k < RPT; ++k) {
                     lo[k] = static_cast<int>(max(rs[k], cs) - cs);
@@ -476,7 +497,7 @@ __global__ void __launch_bounds__(kThreads + 32) csr_pipe_kernel(int64_t rows, i
 #pragma unroll
                     for (int u = 0; u < kGather; ++u) {
                         const int o = lo[k] + u;
-                        y[k][u] = o < hi[k] ? xs(column_of(r0 + tid + k * kThreads, sc[o])) : T(0);
+                        y[k][u] = o < hi[k] ? gather(k, o) : T(0);
                     }
                 }
 #pragma unroll
@@ -492,7 +513,7 @@ __global__ void __launch_bounds__(kThreads + 32) csr_pipe_kernel(int64_t rows, i
 #pragma unroll
                         for (int u = 0; u < kGather; ++u) {
                             const int o = o0 + u;
-                            z[u] = o < hi[k] ? xs(column_of(r0 + tid + k * kThreads, sc[o])) : T(0);
+                            z[u] = o < hi[k] ? gather(k, o) : T(0);
                         }
 #pragma unroll
                         for (int u = 0; u < kGather; ++u) {
@@ -598,12 +619,13 @@ __device__ __forceinline__ void load_slice_head(SliceHead<T, G> &h, int64_t slic
         h.base = __ldg(sp + slice);
         h.width = (__ldg(sp + slice + 1) - h.base) >> 5;
     }
+    const T *pv = sv + h.base + lane;  // entry g of this lane's row at pv[32 g]
+    const int16_t *pc = sc + h.base + lane;
 #pragma unroll
     for (int g = 0; g < G; ++g) {
         if (g < h.width) {
-            const int64_t k = static_cast<int64_t>(h.base) + g * 32 + lane;
-            h.v[g] = __ldcs(sv + k);
-            h.c[g] = __ldcs(sc + k);
+            h.v[g] = __ldcs(pv + g * 32);
+            h.c[g] = __ldcs(pc + g * 32);
         } else {
             h.v[g] = T(0);
             h.c[g] = kSlicePad;
@@ -637,28 +659,30 @@ __global__ void __launch_bounds__(kThreads) sliced_kernel(int64_t rows, const in
         if (live) pre = epi.pre(row, xs);
         SliceHead<T, G> next;
         if constexpr (PF) load_slice_head(next, (tile + gridDim.x) * kWarps + warp, nslices, sp, sv, sc, lane);
+        const auto xr = xs.row(row);  // x~ around this lane's row, indexed by column offset
         T y[G];
 #pragma unroll
-        for (int g = 0; g < G; ++g) y[g] = h.c[g] != kSlicePad ? xs(row + h.c[g]) : T(0);
+        for (int g = 0; g < G; ++g) y[g] = h.c[g] != kSlicePad ? xr(h.c[g]) : T(0);
         T acc = T(0);
 #pragma unroll
         for (int g = 0; g < G; ++g) acc += h.v[g] * y[g];
         for (int j0 = G; j0 < h.width; j0 += G) {
             T v[G];
             int16_t c[G];
+            const T *pv = sv + h.base + lane + j0 * 32;
+            const int16_t *pc = sc + h.base + lane + j0 * 32;
 #pragma unroll
             for (int g = 0; g < G; ++g) {
                 if (j0 + g < h.width) {
-                    const int64_t k = static_cast<int64_t>(h.base) + (j0 + g) * 32 + lane;
-                    v[g] = __ldcs(sv + k);
-                    c[g] = __ldcs(sc + k);
+                    v[g] = __ldcs(pv + g * 32);
+                    c[g] = __ldcs(pc + g * 32);
                 } else {
                     v[g] = T(0);
                     c[g] = kSlicePad;
                 }
             }
 #pragma unroll
-            for (int g = 0; g < G; ++g) y[g] = c[g] != kSlicePad ? xs(row + c[g]) : T(0);
+            for (int g = 0; g < G; ++g) y[g] = c[g] != kSlicePad ? xr(c[g]) : T(0);
 #pragma unroll
             for (int g = 0; g < G; ++g) acc += v[g] * y[g];
         }
@@ -825,13 +849,14 @@ __global__ void __launch_bounds__(kThreads + 32)
             const T *vs = stage_val(st) + base + lane;
             const int16_t *cs = stage_col(st) + base + lane;
             T acc = T(0);
+            const auto xr = xs.row(row);
             for (int j0 = 0; j0 < width; j0 += 8) {
                 int16_t c[8];
                 T y[8];
 #pragma unroll
                 for (int g = 0; g < 8; ++g) c[g] = j0 + g < width ? cs[(j0 + g) * 32] : kSlicePad;
 #pragma unroll
-                for (int g = 0; g < 8; ++g) y[g] = c[g] != kSlicePad ? xs(row + c[g]) : T(0);
+                for (int g = 0; g < 8; ++g) y[g] = c[g] != kSlicePad ? xr(c[g]) : T(0);
 #pragma unroll
                 for (int g = 0; g < 8; ++g) acc += (j0 + g < width ? vs[(j0 + g) * 32] : T(0)) * y[g];
             }
