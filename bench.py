@@ -38,7 +38,7 @@ METRIC = "time-to-1e-8 FP64 relative residual (s), AMG-PCG V-cycle, FP32 hierarc
 # 128^3 problem, from the ncu captures summarised in
 # profiles/sliced_kernel_heat3d_128_fp64_operator.md (sliced copy) and
 # profiles/csr_pipe_kernel_heat3d_128_fp64_operator.md (CSR row tiles)
-SPMV_TRAFFIC = {"sliced": 163200256 + 5292288, "csr": 171013632 + 13778176}
+SPMV_TRAFFIC = {"sliced": 163197184 + 4258048, "csr": 171013632 + 13778176}
 WORKLOAD = f"heat3d {SIZE}^3 7-point FV, log-normal k (seed {SEED_MATRIX}), Dirichlet x=0, rhs U[-1,1] (seed {SEED_RHS})"
 
 

@@ -641,20 +641,23 @@ __global__ void __launch_bounds__(kThreads) sliced_kernel(int64_t rows, const in
     constexpr int K = Epi::kReduce;
     constexpr int KK = K > 0 ? K : 1;
     constexpr int kWarps = kThreads / 32;
-    __shared__ double warp_sums[kWarps][KK];
+    // warp sums, double-buffered by tile parity: one barrier per tile suffices
+    __shared__ double warp_sums[2][kWarps][KK];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int64_t ntiles = (rows + kThreads - 1) / kThreads;  // = 256-row blocks of partial sums
-    const int64_t nslices = (rows + 31) / 32;
-    int64_t tile = blockIdx.x;
+    // sliced copies exist for int32 operators only: 32-bit row arithmetic
+    const int nrows = static_cast<int>(rows);
+    const int ntiles = (nrows + kThreads - 1) / kThreads;  // = 256-row blocks of partial sums
+    const int nslices = (nrows + 31) / 32;
+    int tile = blockIdx.x;
     SliceHead<T, G> h;
     if (early) load_slice_head(h, tile * kWarps + warp, nslices, sp, sv, sc, lane);
     pdl_enter();
     if (epi.skip()) return;  // the gate reads the same device word in every CTA
     if (!early) load_slice_head(h, tile * kWarps + warp, nslices, sp, sv, sc, lane);
-    for (; tile < ntiles; tile += gridDim.x) {
-        const int64_t slot = tile * kThreads + threadIdx.x;  // position in the sliced order
-        const bool live = slot < rows;
-        const int64_t row = live && perm ? static_cast<int64_t>(__ldg(perm + slot)) : slot;
+    for (int parity = 0; tile < ntiles; tile += gridDim.x, parity ^= 1) {
+        const int slot = tile * kThreads + threadIdx.x;  // position in the sliced order
+        const bool live = slot < nrows;
+        const int row = live && perm ? __ldg(perm + slot) : slot;
         typename Epi::Pre pre{};
         if (live) pre = epi.pre(row, xs);
         SliceHead<T, G> next;
@@ -696,20 +699,21 @@ __global__ void __launch_bounds__(kThreads) sliced_kernel(int64_t rows, const in
                 for (int o = 16; o > 0; o >>= 1) red[q] += __shfl_down_sync(0xffffffffu, red[q], o);
             if (lane == 0)
 #pragma unroll
-                for (int q = 0; q < K; ++q) warp_sums[warp][q] = red[q];
+                for (int q = 0; q < K; ++q) warp_sums[parity][warp][q] = red[q];
+            // a warp writes this parity's slots again two tiles later, past
+            // the next barrier, which thread q reaches only after this read
             __syncthreads();
             if (threadIdx.x < K) {
                 double v = 0.0;
-                for (int w = 0; w < kWarps; ++w) v += warp_sums[w][threadIdx.x];
-                epi.partial[threadIdx.x * ntiles + tile] = v;
+                for (int w = 0; w < kWarps; ++w) v += warp_sums[parity][w][threadIdx.x];
+                epi.partial[threadIdx.x * static_cast<int64_t>(ntiles) + tile] = v;
             }
-            __syncthreads();
         }
         if constexpr (PF) h = next;
-        else if (tile + gridDim.x < ntiles)
+        else if (tile + static_cast<int>(gridDim.x) < ntiles)
             load_slice_head(h, (tile + gridDim.x) * kWarps + warp, nslices, sp, sv, sc, lane);
     }
-    if constexpr (K > 0) finish(epi.fin, epi.partial, static_cast<int>(ntiles));
+    if constexpr (K > 0) finish(epi.fin, epi.partial, ntiles);
 }
 
 // ---------------------------------------------------------------------------
