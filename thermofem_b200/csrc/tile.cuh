@@ -441,11 +441,18 @@ __global__ void __launch_bounds__(kThreads + 32) csr_pipe_kernel(int64_t rows, i
         const bool skipped = epi.skip();
         if (tid == 0) skipped_cta = skipped ? 1 : 0;
         const int64_t first = skipped ? ntiles : blockIdx.x;
+        // entry offsets in the index type's width (32-bit arithmetic for int32 CSR)
+        using Off = std::conditional_t<sizeof(I) == 4, int32_t, int64_t>;
         for (int64_t tile = first; tile < ntiles && ok; tile += gridDim.x) {
             const int64_t r0 = tile * kTileRows;
             const int nr = static_cast<int>(min(static_cast<int64_t>(kTileRows), rows - r0));
-            int64_t rs[RPT], re[RPT], s = 0, e = 0, nch = 1;
+            Off rs[RPT], re[RPT], s = 0, e = 0;
+            int nch = 1;
             T acc[RPT];
+            // x~ around each of this thread's rows (gathers by column offset)
+            decltype(xs.row(0)) xv[RPT];
+#pragma unroll
+            for (int k = 0; k < RPT; ++k) xv[k] = xs.row(r0 + tid + k * kThreads);
             // The rows' own epilogue operands (b, D^-1, x_i, ...) are loaded
             // now, so their latency overlaps the stage wait and the gathers.
             typename Epi::Pre pre[RPT];
@@ -458,7 +465,7 @@ __global__ void __launch_bounds__(kThreads + 32) csr_pipe_kernel(int64_t rows, i
 #pragma unroll
                 for (int q = 0; q < KK; ++q) red[k][q] = 0.0;
             }
-            for (int64_t c = 0; c < nch; ++c, ++it) {
+            for (int c = 0; c < nch; ++c, ++it) {
                 const int st = static_cast<int>(it % stages);
                 // warp-uniform decision, so __syncwarp below never waits on a lane that left
                 if (__any_sync(0xffffffffu, !mbar_wait(&full_bar[st], (it / stages) & 1))) {
@@ -468,9 +475,9 @@ __global__ void __launch_bounds__(kThreads + 32) csr_pipe_kernel(int64_t rows, i
                 }
                 if (c == 0) {
                     const I *srp = stage_rp(st);
-                    s = srp[0];
-                    e = srp[nr];
-                    nch = e > s ? (e - s + cap - 1) / cap : 1;
+                    s = static_cast<Off>(srp[0]);
+                    e = static_cast<Off>(srp[nr]);
+                    nch = e > s ? static_cast<int>((static_cast<int64_t>(e) - s + cap - 1) / cap) : 1;
 #pragma unroll
                     for (int k = 0; k < RPT; ++k)
                         if (tid + k * kThreads < nr) {
@@ -478,7 +485,7 @@ __global__ void __launch_bounds__(kThreads + 32) csr_pipe_kernel(int64_t rows, i
                             re[k] = srp[tid + k * kThreads + 1];
                         }
                 }
-                const int64_t cs = s + c * cap, ce = min(e, cs + cap);
+                const Off cs = s + static_cast<Off>(c) * cap, ce = min(e, cs + static_cast<Off>(cap));
                 const T *sv = stage_val(st) + (cs % kVT);  // sv[j - cs]
                 const C *sc = stage_col(st) + (cs % kVC);  // sc[j - cs]
                 constexpr int kGather = 8;
@@ -487,13 +494,13 @@ __global__ void __launch_bounds__(kThreads + 32) csr_pipe_kernel(int64_t rows, i
                 // x~_j of entry o of row k: through the row's view when the
                 // entries are column offsets (a 32-bit offset per gather)
                 auto gather = [&](int k, int o) {
-                    if constexpr (std::is_same_v<C, int16_t>) return xs.row(r0 + tid + k * kThreads)(sc[o]);
+                    if constexpr (std::is_same_v<C, int16_t>) return xv[k](sc[o]);
                     else return xs(column_of(r0 + tid + k * kThreads, sc[o]));
                 };
 #pragma unroll
                 for (int k = 0; k < RPT; ++k) {
                     lo[k] = static_cast<int>(max(rs[k], cs) - cs);
-                    hi[k] = static_cast<int>(max(min(re[k], ce) - cs, int64_t(0)));
+                    hi[k] = static_cast<int>(max(min(re[k], ce) - cs, Off(0)));
 #pragma unroll
                     for (int u = 0; u < kGather; ++u) {
                         const int o = lo[k] + u;
