@@ -1,7 +1,14 @@
-// tile.cuh -- the row-tile CSR kernel shared by the SpMV family (spmv.cu)
-// and the fused Krylov steps (krylov.cu).
+// tile.cuh -- the SpMV kernels shared by the SpMV family (spmv.cu) and the
+// fused Krylov steps (krylov.cu): the staged row-tile kernel (unaligned
+// arrays), the pipelined row-tile kernel (csr_pipe_kernel: CSR chunks
+// bulk-copied into a shared-memory ring), and the two kernels over an
+// operator's sliced copy (sliced_kernel: coalesced loads per 32-row slice;
+// sliced_pipe_kernel: whole tiles bulk-copied into a ring).  All of them take
+// the same epilogues and gather functors, reduce every row left to right and
+// write partial sums per 256-row block, so they give the same bits;
+// tile::launch picks one by the operator's storage and its tuned shape.
 //
-// One CTA owns 256 * RPT consecutive rows.  Their nonzeros form one
+// Staged row-tile kernel: one CTA owns 256 * RPT consecutive rows.  Their nonzeros form one
 // contiguous range of values and column indices, which is staged into
 // shared memory with 16-byte vector loads (every HBM sector read once and
 // fully); each thread then reduces its rows from shared memory left to right
