@@ -118,10 +118,13 @@ class Clocks:
                 "power_w_max": max(r[2] for r in rows), "samples": len(rows), "reasons": reasons}
 
 
-def cpu_solve_once(A, amg, b, O):
+def cpu_solve_once(A, amg, b, O, keep=None):
     t0 = time.perf_counter()
     x, rep = O.cg(A, amg, b, np.zeros(A.rows))
-    return time.perf_counter() - t0, rep
+    t = time.perf_counter() - t0
+    if keep is not None:
+        keep.append(x)
+    return t, rep
 
 
 def run_reference(args):
@@ -492,11 +495,13 @@ def main():
     with Clocks(local) as clk:
         ms_mixed, rep_mixed, launches_mixed = timed(mixed, args.steps)
     clocks = clk.summary()
+    x_mixed_dev = x.clone()  # the last mixed solve (the plain solves reuse x)
     ms_plain, rep_plain, launches_plain = timed(plain, args.steps)
 
     # true FP64 residual of the last mixed solve
-    r = tf.residual(a, b, x, ctx=ctx)
+    r = tf.residual(a, b, x_mixed_dev, ctx=ctx)
     true_rel = float(torch.linalg.norm(r) / torch.linalg.norm(b))
+    x_mixed = x_mixed_dev.cpu().numpy()
 
     # e2e: public C ABI call with pinned host buffers, copies inside the timed region
     # (a zeroed pinned initial guess per step, prepared outside the timed region)
@@ -542,15 +547,20 @@ def main():
     achieved_csr = spmv_bytes(n, nnz) / (csr_ms * 1e-3) / 1e9
 
     cpu = None
+    err_vs_oracle = None
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
             subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle")], check=True)
             from oracle import oracle as O
             A = O.Csr(n, off, idx, val)
             amg = O.Amg(A, jacobi_weight=AMG["jacobi_weight"], coarse_rows=AMG["coarse_rows"])
-            t_cpu, rep_cpu = cpu_solve_once(A, amg, b_host.numpy(), O)
+            xs_cpu = []
+            t_cpu, rep_cpu = cpu_solve_once(A, amg, b_host.numpy(), O, keep=xs_cpu)
             cpu = {"value": t_cpu, "unit": "s", "cores": O.num_threads(), "kind": "port",
                    "sample": f"one full FP64 AMG-PCG solve of the same 128^3 problem ({rep_cpu['iterations']} iterations)"}
+            # the mixed solve's error against the oracle's FP64 solve
+            xo = xs_cpu[0]
+            err_vs_oracle = float(np.linalg.norm(x_mixed - xo) / np.linalg.norm(xo))
         except Exception as e:  # the baseline is reported, never required
             cpu = {"value": None, "unit": "s", "cores": None, "kind": "port", "sample": f"failed: {e}"}
 
@@ -564,6 +574,7 @@ def main():
                        "parallelism": "replicas" if world > 1 else "single GPU",
                        "l2": "inputs larger than L2 (217 MB FP64 operator), no flush"},
             "iterations": rep_mixed["iterations"], "true_relative_residual": true_rel,
+            "relative_error_vs_oracle": err_vs_oracle,
             "setup_s": setup_mixed,
             "plain_fp64": {"value": ms_plain / 1e3, "unit": "s", "iterations": rep_plain["iterations"],
                            "setup_s": setup_plain},
