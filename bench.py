@@ -23,6 +23,7 @@ import json
 import os
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -73,7 +74,7 @@ class Clocks:
     def __init__(self, index):
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+        self.path = os.path.join(tempfile.gettempdir(), f"thermofem_b200_clocks_{os.getpid()}.csv")
 
     def __enter__(self):
         try:
@@ -171,7 +172,7 @@ def run_reference(args):
 
 
 def run_workload(args):
-    """Measurements of the other BASELINE configs (synthetic inputs of the
+    """Measurements of the other benchmark configurations (synthetic inputs of the
     stated shapes; device times from CUDA events).  The batched workload
     shards its systems over the ranks of a torchrun launch (longest first to
     the least loaded rank, no data-path collective; the time is the max over
@@ -411,7 +412,7 @@ def main():
                     help="profiling run: setup, --warmup solves, then --steps solves of one path (spmv: the FP64 "
                          "operator SpMV; spmv32: the FP32 finest level's)")
     ap.add_argument("--workload", choices=["batched", "convdiff", "heat", "learned"], default=None,
-                    help="the other BASELINE configs (one JSON line each, not the headline): batched = 48 "
+                    help="the other benchmark configurations (one JSON line each, not the headline): batched = 48 "
                          "transient systems x 20 steps; convdiff = 192^3 BiCGStab W-cycle; heat = --size^3 heat; "
                          "learned = shipped damping model vs w=2/3 on --size^3 (default 256), F-cycle")
     ap.add_argument("--size", type=int, default=None, help="grid side of --workload convdiff/heat")
