@@ -204,8 +204,9 @@ class HierarchyImpl final : public Hierarchy {
         if (std::getenv("THERMOFEM_B200_SLICED_SHAPE")) return;
         if (const char *v = std::getenv("THERMOFEM_B200_SLICED_SELECT"); v && v[0] == '0') return;
         std::vector<size_t> cand;
+        // (levels under 16,384 rows are launch-latency bound: their layout is left as built)
         for (size_t d = 0; d < levels_.size() && d < coop_from_; ++d)
-            if (levels_[d].sl.sp.data()) cand.push_back(d);
+            if (levels_[d].sl.sp.data() && levels_[d].n >= 16384) cand.push_back(d);
         if (cand.empty()) return;
         StableScope stable(ctx);
         fill_zero(ctx, levels_.front().n, levels_.front().rhs.data());
