@@ -10,10 +10,12 @@
 // (include/DataStructure/CsrMatrix.cuh:81-87), Vector(span)
 // (include/DataStructure/Vector.cuh:34), copyToHost (Vector.cuh:65),
 // AmgOptions (include/Preconditioner/Amg.cuh:14-25), Amg(options)
-// (Amg.cuh:64), Cg(options, preconditioner) (include/Solver/Cg.cuh:44),
+// (Amg.cuh:64), Identity (include/Preconditioner/Identity.cuh:17-36),
+// Cg(options, preconditioner) (include/Solver/Cg.cuh:44),
 // BiCgStab(options, preconditioner) (include/Solver/BiCgStab.cuh:50),
 // setup / apply and SolveResult (include/Solver/Interfaces.cuh).
 #include <Preconditioner/Amg.cuh>
+#include <Preconditioner/Identity.cuh>
 #include <Solver/BiCgStab.cuh>
 #include <Solver/Cg.cuh>
 
@@ -30,9 +32,9 @@ namespace {
 using namespace thermofem;
 
 template <class S, class O>
-int run(const int32_t *rp, const int32_t *ci, const double *val, int64_t n, const double *b, double *x, int cycle,
-        double jacobi_weight, int coarse_rows, int repeats, int *iterations, int *status, double *rel_residual,
-        double *setup_seconds, double *solve_seconds) {
+int run(const int32_t *rp, const int32_t *ci, const double *val, int64_t n, const double *b, double *x, int precond,
+        int cycle, double jacobi_weight, int coarse_rows, int repeats, int *iterations, int *status,
+        double *rel_residual, double *setup_seconds, double *solve_seconds) {
     const int64_t nnz = rp[n];
     CsrMatrix<double> a(static_cast<std::size_t>(n), static_cast<std::size_t>(n),
                         std::span<const int>(rp, static_cast<std::size_t>(n + 1)),
@@ -43,7 +45,9 @@ int run(const int32_t *rp, const int32_t *ci, const double *val, int64_t n, cons
     ao.coarseRows_ = coarse_rows;
     ao.cycle_ = cycle == 1 ? multigrid::Cycle::W : (cycle == 2 ? multigrid::Cycle::F : multigrid::Cycle::V);
     O so;
-    S solver(so, std::make_unique<Amg<double>>(ao));
+    // precond 0: Identity, passed explicitly (BiCgStab builds an Amg when given none)
+    S solver(so, precond ? std::unique_ptr<Preconditioner<double>>(std::make_unique<Amg<double>>(ao))
+                         : std::unique_ptr<Preconditioner<double>>(std::make_unique<Identity<double>>()));
     cudaDeviceSynchronize();
     auto t0 = std::chrono::steady_clock::now();
     solver.setup(a);
@@ -72,21 +76,22 @@ int run(const int32_t *rp, const int32_t *ci, const double *val, int64_t n, cons
 
 }  // namespace
 
-// Solves A x = b with the reference's FP64 AMG-preconditioned solver (kind 0
-// PCG, 1 BiCGStab; cycle 0 V, 1 W, 2 F) from the initial guess in x, `repeats`
+// Solves A x = b with the reference's FP64 solver (kind 0 PCG, 1 BiCGStab;
+// precond 1 its aggregation AMG, cycle 0 V, 1 W, 2 F; precond 0 identity)
+// from the initial guess in x, `repeats`
 // times from that guess; x receives the last solution.  Times are host wall
 // clock around device-synchronised calls (setup once, the fastest solve).
 // Returns 0, or -1 after printing the exception the reference raised.
 extern "C" int ref_gpu_solve(int kind, const int32_t *rp, const int32_t *ci, const double *val, int64_t n,
-                             const double *b, double *x, int cycle, double jacobi_weight, int coarse_rows,
+                             const double *b, double *x, int precond, int cycle, double jacobi_weight, int coarse_rows,
                              int repeats, int *iterations, int *status, double *rel_residual, double *setup_seconds,
                              double *solve_seconds) {
     try {
         if (kind == 1)
-            return run<BiCgStab<double>, BiCgStabOptions<double>>(rp, ci, val, n, b, x, cycle, jacobi_weight,
+            return run<BiCgStab<double>, BiCgStabOptions<double>>(rp, ci, val, n, b, x, precond, cycle, jacobi_weight,
                                                                   coarse_rows, repeats, iterations, status,
                                                                   rel_residual, setup_seconds, solve_seconds);
-        return run<Cg<double>, CgOptions<double>>(rp, ci, val, n, b, x, cycle, jacobi_weight, coarse_rows, repeats,
+        return run<Cg<double>, CgOptions<double>>(rp, ci, val, n, b, x, precond, cycle, jacobi_weight, coarse_rows, repeats,
                                                   iterations, status, rel_residual, setup_seconds, solve_seconds);
     } catch (const std::exception &e) {
         std::fprintf(stderr, "reference solve failed: %s\n", e.what());

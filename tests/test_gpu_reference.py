@@ -23,10 +23,14 @@ pytestmark = [pytest.mark.gpu,
               pytest.mark.skipif(not O.ref_gpu_available(), reason="reference GPU build absent (make -C oracle refgpu)")]
 
 
-def _ours(m, b, kind, cycle, hierarchy="f64"):
+def _ours(m, b, kind, cycle, hierarchy="f64", jacobi_weight=2 / 3, coarse_rows=64, precond="amg"):
     solver = tf.BiCgStab if kind == "bicgstab" else tf.Cg
-    s = solver(tf.solver_options(), "amg",
-               tf.amg_options(hierarchy_type=hierarchy, jacobi_weight=2 / 3, coarse_rows=64, cycle=cycle))
+    if precond == "identity":
+        s = solver(tf.solver_options(), "identity")
+    else:
+        s = solver(tf.solver_options(), "amg",
+                   tf.amg_options(hierarchy_type=hierarchy, jacobi_weight=jacobi_weight, coarse_rows=coarse_rows,
+                                  cycle=cycle))
     s.setup(tf.DeviceCsr.from_host(*m))
     x = torch.zeros(len(b), dtype=torch.float64, device="cuda")
     bd = torch.tensor(b, device="cuda")
@@ -46,6 +50,42 @@ def test_solves_match_the_reference_gpu_build(problem, kind, cycle):
     assert abs(rep["iterations"] - rr["iterations"]) <= 1, (rep["iterations"], rr["iterations"])
     xo = x.cpu().numpy()
     assert np.linalg.norm(xo - xr) / np.linalg.norm(xr) < 1e-6
+
+
+@pytest.mark.parametrize("case", ["laplace2d-128", "w-0.75", "coarse-16", "identity-cg", "identity-bicgstab"])
+def test_more_solves_match_the_reference_gpu_build(case):
+    # the 2-D 128^2 Laplacian of the small benchmark configuration; the
+    # reference's default Jacobi weight 0.75; a 16-row coarse level; and the
+    # solvers without a preconditioner (the reference's default identity)
+    if case == "laplace2d-128":
+        m, kw = P.laplace2d(128), {}
+    elif case.startswith("identity"):
+        m, kw = P.laplace2d(48), {}  # converges without a preconditioner within the default 1000 iterations
+    else:
+        m, kw = P.heat3d(20, seed=47), {}
+    if case == "w-0.75":
+        kw = {"jacobi_weight": 0.75}
+    elif case == "coarse-16":
+        kw = {"coarse_rows": 16}
+    kind = "bicgstab" if case.endswith("bicgstab") else "cg"
+    precond = "identity" if case.startswith("identity") else "amg"
+    n = len(m[0]) - 1
+    b = P.rhs_uniform(n, 48)
+    xr, rr = O.ref_gpu_solve(O.Csr(n, *m), b, kind=kind, precond=precond, **kw)
+    _, x, _, rep = _ours(m, b, kind, "v", precond=precond, **kw)
+    assert rr["status"] == 0 and rep["status"] == "Converged"
+    # without a preconditioner hundreds of iterations accumulate the two
+    # implementations' different reduction orders (BiCGStab's iteration count
+    # is erratic under them: a textbook restatement takes 107 here, the CPU
+    # oracle 124), and a 1e-8 residual bounds the solution only to about
+    # cond(A) * 1e-8
+    if precond == "identity":
+        slack = max(1, rr["iterations"] // (50 if kind == "cg" else 4))
+        tol = 1e-4
+    else:
+        slack, tol = 1, 1e-6
+    assert abs(rep["iterations"] - rr["iterations"]) <= slack, (rep["iterations"], rr["iterations"])
+    assert np.linalg.norm(x.cpu().numpy() - xr) / np.linalg.norm(xr) < tol
 
 
 def test_reference_gpu_build_on_the_benchmark_problem(capsys):
