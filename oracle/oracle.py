@@ -490,9 +490,10 @@ def ref_gpu_available():
 
 
 def ref_gpu_solve(a: Csr, b, x0=None, kind="cg", cycle="v", jacobi_weight=2.0 / 3.0, coarse_rows=64, repeats=1,
-                  precond="amg"):
-    """The reference's FP64 solve of a x = b (from x0, default zero) with its
-    aggregation AMG (precond "amg") or its identity preconditioner.  Returns (x, report) with iterations, status (0 Converged,
+                  precond="amg", single=False):
+    """The reference's solve of a x = b (from x0, default zero) with its
+    aggregation AMG (precond "amg") or its identity preconditioner, in FP64
+    or (single) with its float components and their default tolerance.  Returns (x, report) with iterations, status (0 Converged,
     1 MaxIterations, 2 Breakdown, 3 NonFinite), relative_residual, setup_s
     and solve_s (the fastest of `repeats` solves, host clock around
     device-synchronised calls)."""
@@ -500,7 +501,7 @@ def ref_gpu_solve(a: Csr, b, x0=None, kind="cg", cycle="v", jacobi_weight=2.0 / 
     if _ref_gpu is None:
         r = C.CDLL(REF_GPU_LIB)
         P, I, D = C.c_void_p, C.c_int, C.c_double
-        r.ref_gpu_solve.argtypes = [I, P, P, P, C.c_int64, P, P, I, I, D, I, I, P, P, P, P, P]
+        r.ref_gpu_solve.argtypes = [I, P, P, P, C.c_int64, P, P, I, I, D, I, I, I, P, P, P, P, P]
         r.ref_gpu_solve.restype = I
         _ref_gpu = r
     rp, ci, val = _arrs(a)
@@ -511,7 +512,7 @@ def ref_gpu_solve(a: Csr, b, x0=None, kind="cg", cycle="v", jacobi_weight=2.0 / 
     rel, ts, tv = np.zeros(1), np.zeros(1), np.zeros(1)
     rc = _ref_gpu.ref_gpu_solve({"cg": 0, "bicgstab": 1}[kind], _ptr(rp), _ptr(ci), _ptr(val), n, _ptr(b), _ptr(x),
                                 {"identity": 0, "amg": 1}[precond], {"v": 0, "w": 1, "f": 2}[cycle], float(jacobi_weight), int(coarse_rows),
-                                int(repeats), _ptr(it), _ptr(st), _ptr(rel), _ptr(ts), _ptr(tv))
+                                int(repeats), int(bool(single)), _ptr(it), _ptr(st), _ptr(rel), _ptr(ts), _ptr(tv))
     if rc != 0:
         raise OracleError("reference GPU solve failed")
     return x, {"iterations": int(it[0]), "status": int(st[0]), "relative_residual": float(rel[0]),

@@ -26,37 +26,42 @@
 #include <exception>
 #include <memory>
 #include <span>
+#include <vector>
 
 namespace {
 
 using namespace thermofem;
 
-template <class S, class O>
-int run(const int32_t *rp, const int32_t *ci, const double *val, int64_t n, const double *b, double *x, int precond,
-        int cycle, double jacobi_weight, int coarse_rows, int repeats, int *iterations, int *status,
+// T: the reference components' value type (double or float; float inputs
+// are the double ones rounded, float results are widened back).
+template <class T, class S, class O>
+int run(const int32_t *rp, const int32_t *ci, const double *val64, int64_t n, const double *b64, double *x64,
+        int precond, int cycle, double jacobi_weight, int coarse_rows, int repeats, int *iterations, int *status,
         double *rel_residual, double *setup_seconds, double *solve_seconds) {
     const int64_t nnz = rp[n];
-    CsrMatrix<double> a(static_cast<std::size_t>(n), static_cast<std::size_t>(n),
-                        std::span<const int>(rp, static_cast<std::size_t>(n + 1)),
-                        std::span<const int>(ci, static_cast<std::size_t>(nnz)),
-                        std::span<const double>(val, static_cast<std::size_t>(nnz)));
-    AmgOptions<double> ao;
-    ao.jacobiWeight_ = jacobi_weight;
+    const std::vector<T> val(val64, val64 + nnz), b(b64, b64 + n);
+    std::vector<T> x(x64, x64 + n);
+    CsrMatrix<T> a(static_cast<std::size_t>(n), static_cast<std::size_t>(n),
+                   std::span<const int>(rp, static_cast<std::size_t>(n + 1)),
+                   std::span<const int>(ci, static_cast<std::size_t>(nnz)),
+                   std::span<const T>(val.data(), static_cast<std::size_t>(nnz)));
+    AmgOptions<T> ao;
+    ao.jacobiWeight_ = static_cast<T>(jacobi_weight);
     ao.coarseRows_ = coarse_rows;
     ao.cycle_ = cycle == 1 ? multigrid::Cycle::W : (cycle == 2 ? multigrid::Cycle::F : multigrid::Cycle::V);
     O so;
     // precond 0: Identity, passed explicitly (BiCgStab builds an Amg when given none)
-    S solver(so, precond ? std::unique_ptr<Preconditioner<double>>(std::make_unique<Amg<double>>(ao))
-                         : std::unique_ptr<Preconditioner<double>>(std::make_unique<Identity<double>>()));
+    S solver(so, precond ? std::unique_ptr<Preconditioner<T>>(std::make_unique<Amg<T>>(ao))
+                         : std::unique_ptr<Preconditioner<T>>(std::make_unique<Identity<T>>()));
     cudaDeviceSynchronize();
     auto t0 = std::chrono::steady_clock::now();
     solver.setup(a);
     cudaDeviceSynchronize();
     *setup_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-    Vector<double> rhs(std::span<const double>(b, static_cast<std::size_t>(n)));
+    Vector<T> rhs(std::span<const T>(b.data(), static_cast<std::size_t>(n)));
     double best = 0;
     for (int r = 0; r < (repeats < 1 ? 1 : repeats); ++r) {
-        Vector<double> xv(std::span<const double>(x, static_cast<std::size_t>(n)));
+        Vector<T> xv(std::span<const T>(x.data(), static_cast<std::size_t>(n)));
         cudaDeviceSynchronize();
         t0 = std::chrono::steady_clock::now();
         const auto res = solver.apply(rhs, xv);
@@ -64,10 +69,12 @@ int run(const int32_t *rp, const int32_t *ci, const double *val, int64_t n, cons
         const double t = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         if (r == 0 || t < best) best = t;
         if (r + 1 == (repeats < 1 ? 1 : repeats)) {
-            xv.copyToHost(std::span<double>(x, static_cast<std::size_t>(n)));
+            std::vector<T> out(static_cast<std::size_t>(n));
+            xv.copyToHost(std::span<T>(out.data(), out.size()));
+            for (int64_t i = 0; i < n; ++i) x64[i] = static_cast<double>(out[static_cast<std::size_t>(i)]);
             *iterations = res.iterations_;
             *status = static_cast<int>(res.status_);
-            *rel_residual = res.relativeResidual_;
+            *rel_residual = static_cast<double>(res.relativeResidual_);
         }
     }
     *solve_seconds = best;
@@ -76,7 +83,8 @@ int run(const int32_t *rp, const int32_t *ci, const double *val, int64_t n, cons
 
 }  // namespace
 
-// Solves A x = b with the reference's FP64 solver (kind 0 PCG, 1 BiCGStab;
+// Solves A x = b with the reference's solver (FP64, or FP32 with single;
+// kind 0 PCG, 1 BiCGStab;
 // precond 1 its aggregation AMG, cycle 0 V, 1 W, 2 F; precond 0 identity)
 // from the initial guess in x, `repeats`
 // times from that guess; x receives the last solution.  Times are host wall
@@ -84,15 +92,19 @@ int run(const int32_t *rp, const int32_t *ci, const double *val, int64_t n, cons
 // Returns 0, or -1 after printing the exception the reference raised.
 extern "C" int ref_gpu_solve(int kind, const int32_t *rp, const int32_t *ci, const double *val, int64_t n,
                              const double *b, double *x, int precond, int cycle, double jacobi_weight, int coarse_rows,
-                             int repeats, int *iterations, int *status, double *rel_residual, double *setup_seconds,
-                             double *solve_seconds) {
+                             int repeats, int single, int *iterations, int *status, double *rel_residual,
+                             double *setup_seconds, double *solve_seconds) {
     try {
-        if (kind == 1)
-            return run<BiCgStab<double>, BiCgStabOptions<double>>(rp, ci, val, n, b, x, precond, cycle, jacobi_weight,
-                                                                  coarse_rows, repeats, iterations, status,
-                                                                  rel_residual, setup_seconds, solve_seconds);
-        return run<Cg<double>, CgOptions<double>>(rp, ci, val, n, b, x, precond, cycle, jacobi_weight, coarse_rows, repeats,
-                                                  iterations, status, rel_residual, setup_seconds, solve_seconds);
+#define TF_REF_RUN(T, S, O)                                                                                      \
+    return run<T, S, O>(rp, ci, val, n, b, x, precond, cycle, jacobi_weight, coarse_rows, repeats, iterations, \
+                        status, rel_residual, setup_seconds, solve_seconds)
+        if (single) {
+            if (kind == 1) TF_REF_RUN(float, BiCgStab<float>, BiCgStabOptions<float>);
+            TF_REF_RUN(float, Cg<float>, CgOptions<float>);
+        }
+        if (kind == 1) TF_REF_RUN(double, BiCgStab<double>, BiCgStabOptions<double>);
+        TF_REF_RUN(double, Cg<double>, CgOptions<double>);
+#undef TF_REF_RUN
     } catch (const std::exception &e) {
         std::fprintf(stderr, "reference solve failed: %s\n", e.what());
         return -1;

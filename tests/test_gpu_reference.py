@@ -205,3 +205,26 @@ def test_reference_gpu_build_at_256(kind, capsys):
         del s
     with capsys.disabled():
         print(f"\nreference GPU build vs this library, heat3d 256^3 {kind} V(1,1): " + json.dumps(out))
+
+
+@pytest.mark.parametrize("kind", ["cg", "bicgstab"])
+def test_float_solves_match_the_reference_gpu_build(kind):
+    # the float components on both sides (FP32 operator, vectors and
+    # hierarchy, the float default tolerance 1e-5), heat 20^3, AMG V(1,1)
+    m = P.heat3d(20, seed=53)
+    n = len(m[0]) - 1
+    b = P.rhs_uniform(n, 54)
+    # both sides see the same FP32 values: round them once here
+    m32 = (m[0], m[1], m[2].astype(np.float32).astype(np.float64))
+    b32 = b.astype(np.float32).astype(np.float64)
+    xr, rr = O.ref_gpu_solve(O.Csr(n, *m32), b32, kind=kind, single=True)
+    solver = tf.BiCgStab if kind == "bicgstab" else tf.Cg
+    s = solver(tf.solver_options(torch.float32), "amg",
+               tf.amg_options(jacobi_weight=2 / 3, coarse_rows=64, cycle="v"), dtype=torch.float32)
+    s.setup(tf.DeviceCsr.from_host(*m32, dtype=torch.float32))
+    x = torch.zeros(n, dtype=torch.float32, device="cuda")
+    rep = s.apply(torch.tensor(b32, dtype=torch.float32, device="cuda"), x)
+    assert rr["status"] == 0 and rep["status"] == "Converged"
+    assert abs(rep["iterations"] - rr["iterations"]) <= 1, (rep["iterations"], rr["iterations"])
+    xo = x.cpu().numpy().astype(np.float64)
+    assert np.linalg.norm(xo - xr) / np.linalg.norm(xr) < 1e-3
