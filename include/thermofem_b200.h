@@ -65,6 +65,14 @@ typedef struct tf_ctx tf_ctx;
 int tf_ctx_create(int device, void *stream /* cudaStream_t or NULL */, tf_ctx **out);
 int tf_ctx_destroy(tf_ctx *ctx);
 int tf_ctx_synchronize(tf_ctx *ctx);
+/* Self-check of the failure path of the bounded device waits (no reference
+ * counterpart): one CTA waits, with the wait every pipelined kernel uses, on a
+ * barrier that nothing completes, gives up after `polls` polls (1..2^20) and
+ * raises the context's fault word as a stalled kernel would.  Returns
+ * TF_ERR_TIMEOUT, having cleared the word; the context stays usable.  A
+ * monitoring caller can run it to check that a stalled wait surfaces as an
+ * error instead of a hang. */
+int tf_ctx_check_bounded_wait(tf_ctx *ctx, int64_t polls);
 void *tf_ctx_stream(tf_ctx *ctx);
 int tf_ctx_device(tf_ctx *ctx);
 /* Number of kernels this context has launched (all entry points). */

@@ -106,6 +106,7 @@ SIGNATURES = {
     "tf_ctx_create": ([_I, _P, _PP], _I),
     "tf_ctx_destroy": ([_P], _I),
     "tf_ctx_synchronize": ([_P], _I),
+    "tf_ctx_check_bounded_wait": ([_P, _L], _I),
     "tf_ctx_stream": ([_P], _P),
     "tf_ctx_device": ([_P], _I),
     "tf_ctx_launch_count": ([_P], _L),

@@ -129,6 +129,14 @@ int tf_ctx_synchronize(tf_ctx *ctx) {
     });
 }
 
+int tf_ctx_check_bounded_wait(tf_ctx *ctx, int64_t polls) {
+    return guard([&] {
+        check_ctx(ctx);
+        DeviceScope scope(ctx->device);
+        bounded_wait_check(ctx, polls);
+    });
+}
+
 void *tf_ctx_stream(tf_ctx *ctx) { return ctx ? static_cast<void *>(ctx->stream) : nullptr; }
 int tf_ctx_device(tf_ctx *ctx) { return ctx ? ctx->device : -1; }
 int64_t tf_ctx_launch_count(tf_ctx *ctx) { return ctx ? ctx->launches : -1; }

@@ -142,6 +142,10 @@ bool delta_columns_enabled();
 template <class T>
 bool build_sliced(tf_ctx *ctx, const Csr<T, int32_t> &a, SlicedCopy<T> &out, bool allow_sort);
 bool sliced_enabled();
+// Self-check of the bounded device waits: a kernel whose wait nothing ends
+// gives up after `polls` polls and raises the context's fault word; throws
+// TF_ERR_TIMEOUT from check_faults (the word is cleared).
+void bounded_wait_check(tf_ctx *ctx, int64_t polls);
 template <class T>
 void restrict_sum(tf_ctx *ctx, int64_t nc, const int32_t *off, const int32_t *mem, const T *fine, T *coarse);
 template <class T>

@@ -551,6 +551,26 @@ bool delta_columns(tf_ctx *ctx, int64_t rows, const I *rp, const I *ci, int16_t 
 template bool delta_columns<int32_t>(tf_ctx *, int64_t, const int32_t *, const int32_t *, int16_t *);
 template bool delta_columns<int64_t>(tf_ctx *, int64_t, const int64_t *, const int64_t *, int16_t *);
 
+// One CTA waits, with the pipelined kernels' bounded wait, on an mbarrier
+// that nothing completes, and raises the fault word as they do when a wait
+// expires (no copy is in flight, so there is nothing to drain).
+__global__ void wait_check_kernel(long long polls, int *fault) {
+    __shared__ uint64_t bar;
+    if (threadIdx.x == 0) {
+        tile::mbar_init(&bar, 1);
+        tile::mbar_fence_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && !tile::mbar_wait(&bar, 0, polls)) atomicExch(fault, 1);
+}
+
+void bounded_wait_check(tf_ctx *ctx, int64_t polls) {
+    require(polls >= 1 && polls <= tile::kWaitLimit, "polls must be 1..2^20");
+    launch_kernel(ctx, "wait_check", wait_check_kernel, 1, 32, 0, static_cast<long long>(polls), ctx->fault);
+    cuda_check(cudaStreamSynchronize(ctx->stream), "wait check");
+    check_faults(ctx);  // TF_ERR_TIMEOUT, fault word cleared
+}
+
 bool sliced_enabled() {
     const char *v = std::getenv("THERMOFEM_B200_SLICED");
     return !(v && v[0] == '0');
