@@ -81,3 +81,40 @@ def test_gather_reports_over_two_gloo_ranks(tmp_path):
     for k, r in enumerate(reps):
         assert r["rank"] == (0 if k in parts[0] else 1)
         assert r["nnz"] == w[k]
+
+
+def _failing_worker(rank, world, port, out):
+    import datetime
+
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=10))
+    if rank == 1:
+        # a rank that fails between steps, with nothing in flight
+        raise RuntimeError("rank 1 failed before reporting")
+    w = _weights()
+    mine = shard.assign(w, world)[rank]
+    try:
+        shard.gather_reports([{"system": k} for k in mine], mine, len(w))
+        outcome = "gathered"
+    except Exception as e:  # the peer is gone: the collective ends with an error
+        outcome = f"error: {type(e).__name__}"
+    with open(out, "w") as f:
+        f.write(outcome)
+    dist.destroy_process_group()
+
+
+def test_gather_fails_instead_of_hanging_when_a_rank_dies(tmp_path):
+    out = str(tmp_path / "outcome.txt")
+    pc = mp.start_processes(_failing_worker, args=(2, _free_port(), out), nprocs=2, join=False,
+                            start_method="spawn")
+    for p in pc.processes:  # each on its own: a failed rank must not take the other down
+        p.join(timeout=120)
+    codes = [p.exitcode for p in pc.processes]
+    for p in pc.processes:
+        if p.is_alive():
+            p.kill()
+    assert codes[1] not in (0, None)  # rank 1 failed
+    assert codes[0] == 0  # rank 0 did not hang: its collective ended with an error
+    with open(out) as f:
+        assert f.read().startswith("error")
