@@ -59,6 +59,36 @@ def layout_bytes(layout, n, entries, vsize):
     return spmv_bytes(n, entries, vsize, 4, 2)
 
 
+def iteration_bytes(solver, n, op_layout, op_entries):
+    """Algorithmic bytes of one PCG iteration of the mixed solve: the bytes
+    model of every kernel it launches, summed.  FP64 outer loop: operator
+    SpMV with p.Ap (operator bytes + p), x/r update (6 vectors), r.z fused
+    with the cycle output conversion (r, z, FP32 x), p update (3 vectors),
+    cycle input conversion fused with the finest zero-guess sweep (r in; dinv,
+    rhs, x).  FP32 V(1,1) cycle, per level of n_d rows in the layout the cycle
+    streams: residual (SpMV bytes + b), post-smooth (SpMV bytes + b + D^-1),
+    prolongation (x read and written, map, coarse x), and below the finest
+    level the restriction fused with the zero-guess sweep (fine residual and
+    members, offsets, D^-1, b and x written); the dense coarse solve reads
+    its inverse."""
+    stats = solver.level_statistics()
+    nb = layout_bytes(op_layout, n, op_entries, 8) + 8 * n  # SpMV with p.Ap
+    nb += 6 * 8 * n + (8 + 8 + 4) * n + 3 * 8 * n + (8 + 4 + 4 + 4) * n
+    for d, st in enumerate(stats):
+        nd = st["rows"]
+        if d + 1 == len(stats):
+            nb += nd * nd * 8 + 2 * 4 * nd  # dense coarse solve
+            break
+        layout, entries = solver.level_spmv_layout(d)
+        spmv = layout_bytes("sliced" if layout != "csr" else "csr", nd, entries, 4)
+        nc = stats[d + 1]["rows"]
+        nb += (spmv + 4 * nd) + (spmv + 8 * nd) + (8 * nd + 4 * nd + 4 * nc)
+        if d > 0:
+            nf = stats[d - 1]["rows"]
+            nb += 4 * nf + 4 * nf + 4 * (nd + 1) + 4 * nd + 8 * nd
+    return nb
+
+
 def measured_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -547,6 +577,11 @@ def main():
     achieved32 = layout_bytes(layout32, n, entries32, 4) / (spmv32_ms * 1e-3) / 1e9
     achieved_csr = spmv_bytes(n, nnz) / (csr_ms * 1e-3) / 1e9
 
+    # solve-level effective bandwidth: the bytes model of one iteration over
+    # the measured time per iteration
+    it_bytes = iteration_bytes(mixed, n, *mixed.spmv_layout())
+    solve_gbs = it_bytes * rep_mixed["iterations"] / (ms_mixed * 1e-3) / 1e9
+
     cpu = None
     err_vs_oracle = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -581,6 +616,8 @@ def main():
                            "setup_s": setup_plain},
             "speedup_mixed_vs_fp64": ms_plain / ms_mixed,
             "spmv_gbs": {"f64_operator": achieved, "f32_level0": achieved32, "f64_int32_csr": achieved_csr},
+            "solve_effective_gbs": {"value": solve_gbs, "bytes_per_iteration": it_bytes,
+                                    "model": "sum over one iteration's kernels of their algorithmic bytes"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": SPMV_TRAFFIC[layout],
                          "kernel": ("sliced_kernel<double> (SpMV, FP64 Krylov operator, 32-row slices, "
