@@ -612,6 +612,7 @@ def main():
             "iterations": rep_mixed["iterations"], "true_relative_residual": true_rel,
             "relative_error_vs_oracle": err_vs_oracle,
             "setup_s": setup_mixed,
+            "setup_phases_ms": {k: round(v, 3) for k, v in mixed.setup_phases().items()},
             "plain_fp64": {"value": ms_plain / 1e3, "unit": "s", "iterations": rep_plain["iterations"],
                            "setup_s": setup_plain},
             "speedup_mixed_vs_fp64": ms_plain / ms_mixed,

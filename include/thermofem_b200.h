@@ -280,6 +280,16 @@ const char *tf_amg_stop_reason(const tf_amg *m);
 const char *tf_amg_coarse_solver(const tf_amg *m);
 /* Visits per level of the last apply (Amg::lastCycleVisits). */
 int tf_amg_last_visits(const tf_amg *m, int64_t *visits, int capacity);
+/* Setup time per phase of the last setup, in ms from CUDA events on the
+ * context stream (no reference counterpart; the reference driver times the
+ * whole setup with std::chrono, example/solve-matrix.cu:125-128): up to
+ * `capacity` of tf_amg_setup_phase_count() values, named by
+ * tf_amg_setup_phase_name (level copies and diagonals, column and sliced
+ * copies, SpMV shape tuning, strength graphs, aggregation, Galerkin
+ * products, coarse LU, small-level region, layout selection). */
+int tf_amg_setup_phases(const tf_amg *m, double *ms, int capacity);
+int tf_amg_setup_phase_count(void);
+const char *tf_amg_setup_phase_name(int phase);
 /* Level operator and transfer of the hierarchy (read-only device views). */
 int tf_amg_level_matrix(const tf_amg *m, int level, tf_csr *out);
 /* y = A_level x with the level's operator as the cycle streams it (its

@@ -101,3 +101,40 @@ def test_hierarchy_matches_oracle(ctx, gen):
         if d + 1 < ora.levels:
             mp, _, _, nc = amg.level_transfer(d)
             assert np.array_equal(mp.cpu().numpy(), ora.map(d))
+
+
+@pytest.mark.parametrize("hierarchy", ["f64", "f32"])
+def test_setup_and_solve_are_deterministic(hierarchy):
+    # the same setup twice, in two contexts: every level operator, the same
+    # bytes; the same solve: the same report and the same bits
+    m = P.heat3d(24, seed=71)
+    n = len(m[0]) - 1
+    b = torch.tensor(P.rhs_uniform(n, 72), device="cuda")
+    runs = []
+    for _ in range(2):
+        ctx = tf.Context(0)
+        s = tf.Cg(tf.solver_options(), "amg", tf.amg_options(hierarchy_type=hierarchy), ctx=ctx)
+        s.setup(to_device(m))
+        levels = [s.level_matrix(d) for d in range(s.level_count())]
+        x = torch.zeros(n, dtype=torch.float64, device="cuda")
+        rep = s.apply(b, x)
+        runs.append((levels, rep, x))
+    (l0, r0, x0), (l1, r1, x1) = runs
+    assert len(l0) == len(l1) >= 3
+    for a, c in zip(l0, l1):
+        assert torch.equal(a.offsets, c.offsets) and torch.equal(a.indices, c.indices)
+        assert torch.equal(a.values, c.values)
+    assert r0 == r1 and torch.equal(x0, x1)
+
+
+def test_setup_phase_times():
+    # every setup phase is timed and the phases cover the hierarchy build
+    m = P.heat3d(24, seed=73)
+    s = tf.Cg(tf.solver_options(), "amg", tf.amg_options(hierarchy_type="f32"))
+    s.setup(to_device(m))
+    ph = s.setup_phases()
+    assert list(ph) == ["level copies and diagonals", "column and sliced copies", "SpMV shape tuning",
+                        "strength graphs", "aggregation", "Galerkin products", "coarse LU", "small-level region",
+                        "layout selection"]
+    assert all(v >= 0 for v in ph.values())
+    assert ph["aggregation"] > 0 and ph["Galerkin products"] > 0 and ph["strength graphs"] > 0

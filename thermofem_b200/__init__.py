@@ -156,6 +156,9 @@ SIGNATURES = {
     "tf_amg_stop_reason": ([_P], C.c_char_p),
     "tf_amg_coarse_solver": ([_P], C.c_char_p),
     "tf_amg_last_visits": ([_P, _P, _I], _I),
+    "tf_amg_setup_phases": ([_P, _P, _I], _I),
+    "tf_amg_setup_phase_count": ([], _I),
+    "tf_amg_setup_phase_name": ([_I], C.c_char_p),
     "tf_amg_level_matrix": ([_P, _I, C.POINTER(Csr)], _I),
     "tf_amg_level_transfer": ([_P, _I, _PP, _PP, _PP, C.POINTER(C.c_int)], _I),
     "tf_jacobi_create": ([_P, _I, _I, _I, _D, _PP], _I),

@@ -483,6 +483,13 @@ class _AmgView:
             out.append({"rows": r.value, "nonzeros": z.value, "aggregate_sizes": hist.tolist()})
         return out
 
+    def setup_phases(self):
+        """{phase name: ms} of the last setup (CUDA events on the context stream)."""
+        k = lib().tf_amg_setup_phase_count()
+        ms = np.zeros(k, np.float64)
+        check(lib().tf_amg_setup_phases(self._h(), ms.ctypes.data_as(C.c_void_p), k))
+        return {lib().tf_amg_setup_phase_name(i).decode(): float(ms[i]) for i in range(k)}
+
     def stop_reason(self) -> str:
         return lib().tf_amg_stop_reason(self._h()).decode()
 

@@ -63,7 +63,56 @@ std::unique_ptr<tf_dcsr> to_native(tf_ctx *ctx, const tf_csr &a) {
     return canonicalize(ctx, csr_of(*m));
 }
 
+const std::vector<std::string> &setup_phase_names() {
+    static const std::vector<std::string> names = {
+        "level copies and diagonals",  // validation, storage copies, inverse diagonal, learned damping
+        "column and sliced copies",
+        "SpMV shape tuning",
+        "strength graphs",
+        "aggregation",
+        "Galerkin products",
+        "coarse LU",
+        "small-level region",
+        "layout selection"};
+    return names;
+}
+
 namespace {
+
+enum SetupPhase { kPhLevel, kPhColumns, kPhTuning, kPhStrength, kPhAggregate, kPhGalerkin, kPhCoarse, kPhSmall,
+                  kPhLayouts, kPhEnd };
+
+// Events recorded on the context stream where a setup phase starts; the
+// span to the next event is charged to the phase.
+class PhaseMarks {
+  public:
+    ~PhaseMarks() {
+        for (auto &m : marks_) cudaEventDestroy(m.second);
+    }
+    void mark(tf_ctx *ctx, int phase) {
+        cudaEvent_t e = nullptr;
+        if (cudaEventCreate(&e) != cudaSuccess || cudaEventRecord(e, ctx->stream) != cudaSuccess) {
+            if (e) cudaEventDestroy(e);
+            cudaGetLastError();
+            return;
+        }
+        marks_.emplace_back(phase, e);
+    }
+    // after the stream has drained
+    std::vector<double> totals() const {
+        std::vector<double> ms(kPhEnd, 0.0);
+        for (size_t i = 0; i + 1 < marks_.size(); ++i) {
+            float t = 0;
+            if (marks_[i].first < kPhEnd && cudaEventElapsedTime(&t, marks_[i].second, marks_[i + 1].second) == cudaSuccess)
+                ms[marks_[i].first] += t;
+        }
+        cudaGetLastError();
+        return ms;
+    }
+
+  private:
+    std::vector<std::pair<int, cudaEvent_t>> marks_;
+};
 
 template <class S>
 struct Level {
@@ -107,11 +156,13 @@ class HierarchyImpl final : public Hierarchy {
 
     void build(tf_ctx *ctx, const tf_dcsr &fine) {
         const auto &o = cfg_.o;
+        PhaseMarks marks;
         // The native operator of the current level; level 0 borrows `fine`.
         std::unique_ptr<tf_dcsr> owned;
         const tf_dcsr *native = &fine;
         DeviceBuffer<double> row_max;
         for (int depth = 0;; ++depth) {
+            marks.mark(ctx, kPhLevel);
             const auto nc = csr_of(*native);
             row_max.allocate(static_cast<size_t>(nc.rows));
             if (!row_stats(ctx, nc, row_max.data()))
@@ -131,12 +182,14 @@ class HierarchyImpl final : public Hierarchy {
             inverse_diagonal(ctx, l.csr(), l.dinv.data());
             // learned damping: dinv_i scaled by omega_i, sweeps with weight 1
             if (cfg_.model) learned_damping(ctx, *cfg_.model, l.csr(), depth, l.dinv.data());
+            marks.mark(ctx, kPhColumns);
             if (delta_columns_enabled() && l.nnz > 0) {
                 l.cd.allocate(static_cast<size_t>(l.nnz));
                 if (!delta_columns(ctx, l.n, l.rp.data(), l.ci.data(), l.cd.data())) l.cd.release();
             }
             if (l.cd.data() && sliced_enabled()) build_sliced(ctx, l.csr(), l.sl, true);
             // Launch shape of this level's row-tile kernels (cached by shape).
+            marks.mark(ctx, kPhTuning);
             fill_zero(ctx, l.n, l.rhs.data());
             tune_spmv(ctx, l.csr(), static_cast<const S *>(l.rhs.data()), l.r.data());
             LevelStats st;
@@ -151,16 +204,19 @@ class HierarchyImpl final : public Hierarchy {
                 stop_reason = "level limit";
                 break;
             }
+            marks.mark(ctx, kPhStrength);
             auto graph = strength_graph(ctx, nc, row_max.data(), o.strength_threshold);
             if (graph->nnz == 0) {
                 stop_reason = "empty strength graph";
                 break;
             }
+            marks.mark(ctx, kPhAggregate);
             auto t = aggregate(ctx, csr_of(*graph), o.matching_rounds, o.absorb_singletons != 0);
             if (t->coarse_rows >= t->fine_rows) {
                 stop_reason = "no contraction";
                 break;
             }
+            marks.mark(ctx, kPhGalerkin);
             auto coarse = galerkin(ctx, nc, t->map.data(), t->coarse_rows);
             for (int k = 0; k < 4; ++k) stats.back().histogram[k] = t->histogram[k];
             l.map = std::move(t->map);
@@ -170,6 +226,7 @@ class HierarchyImpl final : public Hierarchy {
             owned = std::move(coarse);
             native = owned.get();
         }
+        marks.mark(ctx, kPhCoarse);
         const auto last = csr_of(*native);
         bool singular = false;
         if (last.rows <= o.coarse_lu_rows) {
@@ -185,9 +242,13 @@ class HierarchyImpl final : public Hierarchy {
         }
         coarse_solver = factored_ ? "pivoted GPU LU" : (singular ? "Jacobi (singular LU)" : "Jacobi (coarsening stopped)");
         visits.assign(levels_.size(), 0);
+        marks.mark(ctx, kPhSmall);
         plan_small_levels(ctx);
+        marks.mark(ctx, kPhLayouts);
         select_layouts(ctx);
+        marks.mark(ctx, kPhEnd);
         cuda_check(cudaStreamSynchronize(ctx->stream), "AMG setup");
+        setup_ms = marks.totals();
     }
 
     // Which levels the cycle streams through their sliced copy, decided in

@@ -60,7 +60,13 @@ class Hierarchy {
     std::vector<LevelStats> stats;
     std::vector<int64_t> visits;
     std::string stop_reason, coarse_solver;
+    // Setup time per phase (ms, CUDA events on the context stream), in the
+    // order of setup_phase_names().
+    std::vector<double> setup_ms;
 };
+
+// Names of the setup phases Hierarchy::setup_ms reports.
+const std::vector<std::string> &setup_phase_names();
 
 // Builds the hierarchy from the canonical native fine matrix (Amg::setup,
 // include/Preconditioner/Amg.cuh:81-143).  row_weights (optional, per level)

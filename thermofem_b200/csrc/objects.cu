@@ -165,6 +165,22 @@ int tf_amg_last_visits(const tf_amg *m, int64_t *visits, int capacity) {
     });
 }
 
+int tf_amg_setup_phases(const tf_amg *m, double *ms, int capacity) {
+    return guard([&] {
+        require(m != nullptr && ms != nullptr, "null argument");
+        if (!m->h) fail(TF_ERR_LOGIC, "AMG requires setup");
+        const auto &t = m->h->setup_ms;
+        for (int k = 0; k < capacity && k < static_cast<int>(t.size()); ++k) ms[k] = t[static_cast<size_t>(k)];
+    });
+}
+
+int tf_amg_setup_phase_count(void) { return static_cast<int>(setup_phase_names().size()); }
+
+const char *tf_amg_setup_phase_name(int phase) {
+    const auto &n = setup_phase_names();
+    return phase >= 0 && phase < static_cast<int>(n.size()) ? n[static_cast<size_t>(phase)].c_str() : "";
+}
+
 int tf_amg_level_matrix(const tf_amg *m, int level, tf_csr *out) {
     return guard([&] {
         require(m != nullptr && out != nullptr, "null argument");
