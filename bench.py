@@ -614,7 +614,8 @@ def main():
             "setup_s": setup_mixed,
             "setup_phases_ms": {k: round(v, 3) for k, v in mixed.setup_phases().items()},
             "plain_fp64": {"value": ms_plain / 1e3, "unit": "s", "iterations": rep_plain["iterations"],
-                           "setup_s": setup_plain},
+                           "setup_s": setup_plain,
+                           "setup_phases_ms": {k: round(v, 3) for k, v in plain.setup_phases().items()}},
             "speedup_mixed_vs_fp64": ms_plain / ms_mixed,
             "spmv_gbs": {"f64_operator": achieved, "f32_level0": achieved32, "f64_int32_csr": achieved_csr},
             "solve_effective_gbs": {"value": solve_gbs, "bytes_per_iteration": it_bytes,
