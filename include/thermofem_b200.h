@@ -172,6 +172,26 @@ int tf_dot_multi(tf_ctx *ctx, int value_type, int64_t n, int count, const void *
                  double *out);
 /* y = a x + b y (FP64 scalars). */
 int tf_axpby(tf_ctx *ctx, int value_type, int64_t n, double a, const void *x, double b, void *y);
+/* The Krylov solvers' fused multi-output vector steps, one pass each (the
+ * reference performs each as separate IterationContext axpy/scale/norm calls
+ * with a host round trip per reduction: Cg.cuh:147-158,172-174,
+ * BiCgStab.cuh:170-180,195-198,228-231).  Vectors are device arrays of value_type; the
+ * squared norms rr/ss are device doubles, reduced in FP64 over a fixed
+ * partition of n (the same bits on any GPU).
+ *   cg_update:          x += alpha p;  r -= alpha ap;  *rr = r.r
+ *   cg_direction:       p = z + beta p  (p = z with restart != 0)
+ *   bicgstab_direction: p = r + beta (p - omega v)  (p = r with restart != 0)
+ *   bicgstab_s:         s = r - alpha v;  x += alpha phat;  *ss = s.s
+ *   bicgstab_update:    x += omega shat;  r = s - omega t;  *rr = r.r  */
+int tf_krylov_cg_update(tf_ctx *ctx, int value_type, int64_t n, double alpha, const void *p, const void *ap,
+                        void *x, void *r, double *rr);
+int tf_krylov_cg_direction(tf_ctx *ctx, int value_type, int64_t n, double beta, int restart, const void *z, void *p);
+int tf_krylov_bicgstab_direction(tf_ctx *ctx, int value_type, int64_t n, double beta, double omega, int restart,
+                                 const void *r, const void *v, void *p);
+int tf_krylov_bicgstab_s(tf_ctx *ctx, int value_type, int64_t n, double alpha, const void *r, const void *v,
+                         const void *phat, void *x, void *s, double *ss);
+int tf_krylov_bicgstab_update(tf_ctx *ctx, int value_type, int64_t n, double omega, const void *shat,
+                              const void *s, const void *t, void *x, void *r, double *rr);
 
 /* ---- setup stages (GpuAggregation, include/Multigrid/GpuAggregation.cuh:47-64) */
 /* Row validation (finite values, nonzero diagonal with finite reciprocal)

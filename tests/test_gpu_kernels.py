@@ -348,3 +348,82 @@ def test_set_spmv_config_rejects_bad_shapes(ctx):
     for bad in [(1, 2, 100, 1), (5, 2, 100, 1), (2, 0, 100, 1), (2, 9, 100, 1), (2, 2, 40, 1), (2, 2, 100, 3)]:
         with pytest.raises(tf.InvalidArgument):
             tf.set_spmv_config(a, *bad, ctx=ctx)
+
+
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
+@pytest.mark.parametrize("n", [1, 2047, 300001])
+def test_fused_krylov_steps_match_torch(dtype, n):
+    # the solvers' fused vector steps as standalone entry points, against the
+    # same arithmetic in torch; the squared norms are the same bits as
+    # tf_dot_multi of the result (same fixed partition and order)
+    from thermofem_b200.api import _VT, _p, check, lib, default_context
+    ctx = default_context()
+    g = torch.Generator("cuda").manual_seed(n)
+
+    def vec():
+        return torch.randn(n, dtype=dtype, device="cuda", generator=g)
+
+    vt, L = _VT[dtype], lib()
+    rr = torch.zeros(1, dtype=torch.float64, device="cuda")
+    tol = 1e-13 if dtype == torch.float64 else 1e-5
+
+    def close(a, b):
+        assert torch.allclose(a, b, rtol=tol, atol=tol)
+
+    def same_norm(v):
+        assert torch.equal(rr, tf.dot_multi([v], [v], ctx=ctx))
+        assert float(rr) == pytest.approx(float((v.double() ** 2).sum()), rel=1e-10)
+
+    alpha, beta, omega = 0.37, -1.25, 0.61
+    # CG: x += alpha p, r -= alpha ap, r.r; p = z + beta p (or z)
+    p, ap, x, r = vec(), vec(), vec(), vec()
+    x0, r0 = x.clone(), r.clone()
+    with ctx:
+        check(L.tf_krylov_cg_update(ctx.h, vt, n, alpha, _p(p), _p(ap), _p(x), _p(r), _p(rr)))
+    torch.cuda.synchronize()
+    a = torch.tensor(alpha, dtype=dtype)
+    close(x, x0 + a.item() * p)
+    close(r, r0 - a.item() * ap)
+    same_norm(r)
+    z, pd = vec(), vec()
+    pd0 = pd.clone()
+    for restart in (0, 1):
+        q = pd0.clone()
+        with ctx:
+            check(L.tf_krylov_cg_direction(ctx.h, vt, n, beta, restart, _p(z), _p(q)))
+        torch.cuda.synchronize()
+        close(q, z if restart else z + beta * pd0)
+    # BiCGStab: p = r + beta (p - omega v) (or r); s = r - alpha v, x += alpha phat, s.s;
+    # x += omega shat, r = s - omega t, r.r
+    r, v, pb = vec(), vec(), vec()
+    for restart in (0, 1):
+        q = pb.clone()
+        with ctx:
+            check(L.tf_krylov_bicgstab_direction(ctx.h, vt, n, beta, omega, restart, _p(r), _p(v), _p(q)))
+        torch.cuda.synchronize()
+        close(q, r if restart else r + beta * (pb - omega * v))
+    ph, x, s = vec(), vec(), torch.empty(n, dtype=dtype, device="cuda")
+    x0 = x.clone()
+    with ctx:
+        check(L.tf_krylov_bicgstab_s(ctx.h, vt, n, alpha, _p(r), _p(v), _p(ph), _p(x), _p(s), _p(rr)))
+    torch.cuda.synchronize()
+    close(s, r - alpha * v)
+    close(x, x0 + alpha * ph)
+    same_norm(s)
+    sh, t, x, r2 = vec(), vec(), vec(), torch.empty(n, dtype=dtype, device="cuda")
+    x0 = x.clone()
+    with ctx:
+        check(L.tf_krylov_bicgstab_update(ctx.h, vt, n, omega, _p(sh), _p(s), _p(t), _p(x), _p(r2), _p(rr)))
+    torch.cuda.synchronize()
+    close(x, x0 + omega * sh)
+    close(r2, s - omega * t)
+    same_norm(r2)
+
+
+def test_fused_krylov_steps_reject_aliases():
+    from thermofem_b200.api import _VT, _p, lib, default_context
+    ctx = default_context()
+    v = torch.zeros(8, dtype=torch.float64, device="cuda")
+    rr = torch.zeros(1, dtype=torch.float64, device="cuda")
+    assert lib().tf_krylov_cg_update(ctx.h, _VT[torch.float64], 8, 1.0, _p(v), _p(v), _p(v), _p(v), _p(rr)) == -1
+    assert lib().tf_krylov_cg_direction(ctx.h, _VT[torch.float64], 8, 1.0, 0, _p(v), _p(v)) == -1

@@ -131,6 +131,11 @@ SIGNATURES = {
     "tf_prolong": ([_P, _I, _L, _P, _P, _P], _I),
     "tf_dot_multi": ([_P, _I, _L, _I, _PP, _PP, _P], _I),
     "tf_axpby": ([_P, _I, _L, _D, _P, _D, _P], _I),
+    "tf_krylov_cg_update": ([_P, _I, _L, _D, _P, _P, _P, _P, _P], _I),
+    "tf_krylov_cg_direction": ([_P, _I, _L, _D, _I, _P, _P], _I),
+    "tf_krylov_bicgstab_direction": ([_P, _I, _L, _D, _D, _I, _P, _P, _P], _I),
+    "tf_krylov_bicgstab_s": ([_P, _I, _L, _D, _P, _P, _P, _P, _P, _P], _I),
+    "tf_krylov_bicgstab_update": ([_P, _I, _L, _D, _P, _P, _P, _P, _P, _P], _I),
     "tf_row_stats": ([_P, C.POINTER(Csr), _P, C.POINTER(C.c_int)], _I),
     "tf_strength": ([_P, C.POINTER(Csr), _P, _D, _PP], _I),
     "tf_match": ([_P, C.POINTER(Csr), _I, _P, C.POINTER(C.c_int)], _I),

@@ -395,6 +395,74 @@ int tf_axpby(tf_ctx *ctx, int value_type, int64_t n, double a, const void *x, do
     });
 }
 
+int tf_krylov_cg_update(tf_ctx *ctx, int value_type, int64_t n, double alpha, const void *p, const void *ap,
+                        void *x, void *r, double *rr) {
+    return guard([&] {
+        check_ctx(ctx);
+        require(n >= 0 && p && ap && x && r && rr && x != r, "invalid CG update arguments");
+        DeviceScope scope(ctx->device);
+        with_value_type(value_type, [&](auto t) {
+            using T = decltype(t);
+            krylov_cg_update(ctx, n, alpha, static_cast<const T *>(p), static_cast<const T *>(ap), static_cast<T *>(x),
+                             static_cast<T *>(r), rr);
+        });
+    });
+}
+
+int tf_krylov_cg_direction(tf_ctx *ctx, int value_type, int64_t n, double beta, int restart, const void *z, void *p) {
+    return guard([&] {
+        check_ctx(ctx);
+        require(n >= 0 && z && p && z != p, "invalid CG direction arguments");
+        DeviceScope scope(ctx->device);
+        with_value_type(value_type, [&](auto t) {
+            using T = decltype(t);
+            krylov_cg_direction(ctx, n, beta, restart, static_cast<const T *>(z), static_cast<T *>(p));
+        });
+    });
+}
+
+int tf_krylov_bicgstab_direction(tf_ctx *ctx, int value_type, int64_t n, double beta, double omega, int restart,
+                                 const void *r, const void *v, void *p) {
+    return guard([&] {
+        check_ctx(ctx);
+        require(n >= 0 && r && v && p && p != r && p != v, "invalid BiCGStab direction arguments");
+        DeviceScope scope(ctx->device);
+        with_value_type(value_type, [&](auto t) {
+            using T = decltype(t);
+            krylov_bicgstab_direction(ctx, n, beta, omega, restart, static_cast<const T *>(r),
+                                      static_cast<const T *>(v), static_cast<T *>(p));
+        });
+    });
+}
+
+int tf_krylov_bicgstab_s(tf_ctx *ctx, int value_type, int64_t n, double alpha, const void *r, const void *v,
+                         const void *phat, void *x, void *s, double *ss) {
+    return guard([&] {
+        check_ctx(ctx);
+        require(n >= 0 && r && v && phat && x && s && ss && x != s, "invalid BiCGStab s-step arguments");
+        DeviceScope scope(ctx->device);
+        with_value_type(value_type, [&](auto t) {
+            using T = decltype(t);
+            krylov_bicgstab_s(ctx, n, alpha, static_cast<const T *>(r), static_cast<const T *>(v),
+                              static_cast<const T *>(phat), static_cast<T *>(x), static_cast<T *>(s), ss);
+        });
+    });
+}
+
+int tf_krylov_bicgstab_update(tf_ctx *ctx, int value_type, int64_t n, double omega, const void *shat,
+                              const void *s, const void *t, void *x, void *r, double *rr) {
+    return guard([&] {
+        check_ctx(ctx);
+        require(n >= 0 && shat && s && t && x && r && rr && x != r, "invalid BiCGStab update arguments");
+        DeviceScope scope(ctx->device);
+        with_value_type(value_type, [&](auto tv) {
+            using T = decltype(tv);
+            krylov_bicgstab_update(ctx, n, omega, static_cast<const T *>(shat), static_cast<const T *>(s),
+                                   static_cast<const T *>(t), static_cast<T *>(x), static_cast<T *>(r), rr);
+        });
+    });
+}
+
 int tf_row_stats(tf_ctx *ctx, const tf_csr *a, double *row_max, int *bad) {
     return guard([&] {
         check_ctx(ctx);

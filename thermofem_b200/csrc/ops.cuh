@@ -155,6 +155,21 @@ template <class T>
 void dot_multi(tf_ctx *ctx, int64_t n, int count, const T *const *xs, const T *const *ys, double *out);
 template <class T>
 void axpby(tf_ctx *ctx, int64_t n, double a, const T *x, double b, T *y);
+// The Krylov solvers' fused vector steps (rr, ss: device doubles, FP64
+// squared norms over the fixed dot_multi partition).
+template <class T>
+void krylov_cg_update(tf_ctx *ctx, int64_t n, double alpha, const T *p, const T *ap, T *x, T *r, double *rr);
+template <class T>
+void krylov_cg_direction(tf_ctx *ctx, int64_t n, double beta, int restart, const T *z, T *p);
+template <class T>
+void krylov_bicgstab_direction(tf_ctx *ctx, int64_t n, double beta, double omega, int restart, const T *r,
+                               const T *v, T *p);
+template <class T>
+void krylov_bicgstab_s(tf_ctx *ctx, int64_t n, double alpha, const T *r, const T *v, const T *phat, T *x, T *s,
+                       double *ss);
+template <class T>
+void krylov_bicgstab_update(tf_ctx *ctx, int64_t n, double omega, const T *shat, const T *s, const T *t, T *x, T *r,
+                            double *rr);
 template <class S, class D>
 void convert(tf_ctx *ctx, int64_t n, const S *src, D *dst);
 template <class T>

@@ -328,6 +328,93 @@ __global__ void __launch_bounds__(256) dot_final_kernel(int parts, const double 
         for (int k = 0; k < K; ++k) out[k] = v[k];
 }
 
+// ---- the Krylov solvers' fused vector steps as standalone operations ----
+// (the same arithmetic as the solvers' own kernels in krylov.cu; squared
+// norms in FP64 over the fixed dot_multi partition, then dot_final_kernel)
+
+// x += alpha p; r -= alpha ap; partial sums of r_i^2 (Cg.cuh:172-174)
+template <class T>
+__global__ void __launch_bounds__(256) cg_update_kernel(int64_t n, T alpha, const T *__restrict__ p,
+                                                        const T *__restrict__ ap, T *__restrict__ x,
+                                                        T *__restrict__ r, double *partial) {
+    pdl_enter();
+    __shared__ double shm[32];
+    double v[1] = {0.0};
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        x[i] += alpha * p[i];
+        const T ri = r[i] - alpha * ap[i];
+        r[i] = ri;
+        v[0] += static_cast<double>(ri) * static_cast<double>(ri);
+    }
+    block_sum<1>(v, shm);
+    if (threadIdx.x == 0) partial[blockIdx.x] = v[0];
+}
+
+// p = z + beta p, or p = z when restarting (Cg.cuh:147-158)
+template <class T>
+__global__ void cg_direction_kernel(int64_t n, T beta, int restart, const T *__restrict__ z, T *__restrict__ p) {
+    pdl_enter();
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        p[i] = restart ? z[i] : z[i] + beta * p[i];
+}
+
+// p = r + beta (p - omega v), or p = r when restarting (BiCgStab.cuh:170-180)
+template <class T>
+__global__ void bicgstab_direction_kernel(int64_t n, T beta, T omega, int restart, const T *__restrict__ r,
+                                          const T *__restrict__ v, T *__restrict__ p) {
+    pdl_enter();
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        if (restart) {
+            p[i] = r[i];
+        } else {
+            const T t = p[i] - omega * v[i];
+            p[i] = r[i] + beta * t;
+        }
+    }
+}
+
+// s = r - alpha v; x += alpha phat; partial sums of s_i^2 (BiCgStab.cuh:195-198)
+template <class T>
+__global__ void __launch_bounds__(256) bicgstab_s_kernel(int64_t n, T alpha, const T *__restrict__ r,
+                                                         const T *__restrict__ v, const T *__restrict__ ph,
+                                                         T *__restrict__ x, T *__restrict__ sv, double *partial) {
+    pdl_enter();
+    __shared__ double shm[32];
+    double acc[1] = {0.0};
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const T si = r[i] - alpha * v[i];
+        sv[i] = si;
+        x[i] += alpha * ph[i];
+        acc[0] += static_cast<double>(si) * static_cast<double>(si);
+    }
+    block_sum<1>(acc, shm);
+    if (threadIdx.x == 0) partial[blockIdx.x] = acc[0];
+}
+
+// x += omega shat; r = s - omega t; partial sums of r_i^2 (BiCgStab.cuh:228-231)
+template <class T>
+__global__ void __launch_bounds__(256) bicgstab_update_kernel(int64_t n, T omega, const T *__restrict__ sh,
+                                                              const T *__restrict__ sv, const T *__restrict__ t,
+                                                              T *__restrict__ x, T *__restrict__ r,
+                                                              double *partial) {
+    pdl_enter();
+    __shared__ double shm[32];
+    double acc[1] = {0.0};
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        x[i] += omega * sh[i];
+        const T ri = sv[i] - omega * t[i];
+        r[i] = ri;
+        acc[0] += static_cast<double>(ri) * static_cast<double>(ri);
+    }
+    block_sum<1>(acc, shm);
+    if (threadIdx.x == 0) partial[blockIdx.x] = acc[0];
+}
+
 template <class T>
 __global__ void axpby_kernel(int64_t n, double a, const T *__restrict__ x, double b, T *__restrict__ y) {
     pdl_enter();
@@ -687,6 +774,56 @@ void dot_multi(tf_ctx *ctx, int64_t n, int count, const T *const *xs, const T *c
     }
 }
 
+// The fixed partition of dot_multi: a reduction's value does not depend on the GPU.
+static int reduction_parts(int64_t n) {
+    int64_t parts = (n + 2047) / 2048;
+    return static_cast<int>(parts < 1 ? 1 : (parts > 1184 ? 1184 : parts));
+}
+
+template <class T>
+void krylov_cg_update(tf_ctx *ctx, int64_t n, double alpha, const T *p, const T *ap, T *x, T *r, double *rr) {
+    const int parts = reduction_parts(n);
+    double *partial = static_cast<double *>(ctx->arena(sizeof(double) * parts));
+    launch_kernel(ctx, "krylov_cg_update", cg_update_kernel<T>, parts, 256, 0, n, static_cast<T>(alpha), p, ap, x, r,
+                  partial);
+    launch_kernel(ctx, "dot_final", dot_final_kernel<1>, 1, 256, 0, parts, partial, rr);
+}
+
+template <class T>
+void krylov_cg_direction(tf_ctx *ctx, int64_t n, double beta, int restart, const T *z, T *p) {
+    if (!n) return;
+    launch_kernel(ctx, "krylov_cg_direction", cg_direction_kernel<T>, stride_grid(ctx, n), kBlock, 0, n,
+                  static_cast<T>(beta), restart, z, p);
+}
+
+template <class T>
+void krylov_bicgstab_direction(tf_ctx *ctx, int64_t n, double beta, double omega, int restart, const T *r,
+                               const T *v, T *p) {
+    if (!n) return;
+    launch_kernel(ctx, "krylov_bicgstab_direction", bicgstab_direction_kernel<T>, stride_grid(ctx, n), kBlock, 0, n,
+                  static_cast<T>(beta), static_cast<T>(omega), restart, r, v, p);
+}
+
+template <class T>
+void krylov_bicgstab_s(tf_ctx *ctx, int64_t n, double alpha, const T *r, const T *v, const T *phat, T *x, T *s,
+                       double *ss) {
+    const int parts = reduction_parts(n);
+    double *partial = static_cast<double *>(ctx->arena(sizeof(double) * parts));
+    launch_kernel(ctx, "krylov_bicgstab_s", bicgstab_s_kernel<T>, parts, 256, 0, n, static_cast<T>(alpha), r, v,
+                  phat, x, s, partial);
+    launch_kernel(ctx, "dot_final", dot_final_kernel<1>, 1, 256, 0, parts, partial, ss);
+}
+
+template <class T>
+void krylov_bicgstab_update(tf_ctx *ctx, int64_t n, double omega, const T *shat, const T *s, const T *t, T *x, T *r,
+                            double *rr) {
+    const int parts = reduction_parts(n);
+    double *partial = static_cast<double *>(ctx->arena(sizeof(double) * parts));
+    launch_kernel(ctx, "krylov_bicgstab_update", bicgstab_update_kernel<T>, parts, 256, 0, n, static_cast<T>(omega),
+                  shat, s, t, x, r, partial);
+    launch_kernel(ctx, "dot_final", dot_final_kernel<1>, 1, 256, 0, parts, partial, rr);
+}
+
 template <class T>
 void axpby(tf_ctx *ctx, int64_t n, double a, const T *x, double b, T *y) {
     if (!n) return;
@@ -761,6 +898,13 @@ TF_SPMV_INST(double, int64_t)
     template void prolong_add<T>(tf_ctx *, int64_t, const int32_t *, const T *, T *);                          \
     template void dot_multi<T>(tf_ctx *, int64_t, int, const T *const *, const T *const *, double *);           \
     template void axpby<T>(tf_ctx *, int64_t, double, const T *, double, T *);                                 \
+    template void krylov_cg_update<T>(tf_ctx *, int64_t, double, const T *, const T *, T *, T *, double *);     \
+    template void krylov_cg_direction<T>(tf_ctx *, int64_t, double, int, const T *, T *);                      \
+    template void krylov_bicgstab_direction<T>(tf_ctx *, int64_t, double, double, int, const T *, const T *, T *); \
+    template void krylov_bicgstab_s<T>(tf_ctx *, int64_t, double, const T *, const T *, const T *, T *, T *,     \
+                                       double *);                                                              \
+    template void krylov_bicgstab_update<T>(tf_ctx *, int64_t, double, const T *, const T *, const T *, T *, T *, \
+                                            double *);                                                         \
     template void fill_zero<T>(tf_ctx *, int64_t, T *);
 TF_VEC_INST(float)
 TF_VEC_INST(double)
