@@ -427,3 +427,42 @@ def test_fused_krylov_steps_reject_aliases():
     rr = torch.zeros(1, dtype=torch.float64, device="cuda")
     assert lib().tf_krylov_cg_update(ctx.h, _VT[torch.float64], 8, 1.0, _p(v), _p(v), _p(v), _p(v), _p(rr)) == -1
     assert lib().tf_krylov_cg_direction(ctx.h, _VT[torch.float64], 8, 1.0, 0, _p(v), _p(v)) == -1
+
+
+def test_null_vectors_are_rejected_before_any_launch(ctx):
+    """A NULL device vector (or descriptor) of a nonempty operation comes back
+    as TF_ERR_INVALID from the host checks and launches nothing."""
+    import ctypes as C
+    lib = tf.lib()
+    invalid = -1
+    a = to_device(P.heat3d(8))
+    d = a.desc()
+    n = a.rows
+    v = [torch.zeros(n, dtype=torch.float64, device="cuda") for _ in range(4)]
+    p = [t.data_ptr() for t in v]
+    i32 = torch.zeros(n + 1, dtype=torch.int32, device="cuda").data_ptr()
+    f64 = 1  # TF_F64
+    before = lib.tf_ctx_launch_count(ctx.h)
+    calls = {
+        "spmv x": lambda: lib.tf_spmv(ctx.h, C.byref(d), None, p[1]),
+        "spmv y": lambda: lib.tf_spmv(ctx.h, C.byref(d), p[0], None),
+        "spmv descriptor": lambda: lib.tf_spmv(ctx.h, None, p[0], p[1]),
+        "residual b": lambda: lib.tf_residual(ctx.h, C.byref(d), None, p[1], p[2]),
+        "residual descriptor": lambda: lib.tf_residual(ctx.h, None, p[0], p[1], p[2]),
+        "jacobi dinv": lambda: lib.tf_jacobi_sweep(ctx.h, C.byref(d), None, p[1], p[2], p[3], 0.5, None, None, None),
+        "jacobi descriptor": lambda: lib.tf_jacobi_sweep(ctx.h, None, p[0], p[1], p[2], p[3], 0.5, None, None, None),
+        "zero sweep x": lambda: lib.tf_jacobi_zero(ctx.h, n, f64, p[0], p[1], None, 0.5, None),
+        "zero sweep length": lambda: lib.tf_jacobi_zero(ctx.h, -1, f64, p[0], p[1], p[2], 0.5, None),
+        "inverse diagonal": lambda: lib.tf_inverse_diagonal(ctx.h, C.byref(d), None),
+        "restrict members": lambda: lib.tf_restrict(ctx.h, f64, 4, i32, None, p[0], p[1]),
+        "prolong map": lambda: lib.tf_prolong(ctx.h, f64, n, None, p[0], p[1]),
+        "axpby y": lambda: lib.tf_axpby(ctx.h, f64, n, 1.0, p[0], 1.0, None),
+        "scan out": lambda: lib.tf_scan_exclusive_i32(ctx.h, n, i32, None),
+        "coarse solve lu": lambda: lib.tf_coarse_lu_solve(ctx.h, 4, None, i32, f64, p[0], p[1]),
+    }
+    for what, call in calls.items():
+        assert call() == invalid, what
+    assert lib.tf_ctx_launch_count(ctx.h) == before
+    # the context is untouched: a valid call still runs
+    assert lib.tf_spmv(ctx.h, C.byref(d), p[0], p[1]) == 0
+    assert lib.tf_ctx_synchronize(ctx.h) == 0

@@ -5,6 +5,7 @@
 
 #include <cstdio>
 #include <cstdlib>
+#include <initializer_list>
 
 namespace tfb {
 
@@ -33,6 +34,15 @@ void with_value_type(int t, F &&f) {
     if (t == TF_F64) f(double{});
     else if (t == TF_F32) f(float{});
     else fail(TF_ERR_INVALID, "value type must be TF_F32 or TF_F64");
+}
+
+// Device vector arguments: a length that is not negative, and pointers that
+// are not NULL unless the vectors are empty (a NULL vector would otherwise
+// reach a kernel as an invalid address).
+void require_vectors(int64_t n, std::initializer_list<const void *> vectors, const char *what) {
+    require(n >= 0, what);
+    if (n > 0)
+        for (const void *v : vectors) require(v != nullptr, what);
 }
 
 Csr<double, int32_t> native_csr(const tf_csr *a) {
@@ -86,7 +96,7 @@ int tf_ctx_create(int device, void *stream, tf_ctx **out) {
         int count = 0;
         cuda_check(cudaGetDeviceCount(&count), "cudaGetDeviceCount");
         require(device >= 0 && device < count, "device ordinal out of range");
-        DeviceScope scope(device);
+        DeviceScope scope(device);  // outlives ctx: a failed create releases on this device
         auto ctx = std::make_unique<tf_ctx>();
         ctx->device = device;
         cuda_check(cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device), "SM count");
@@ -111,12 +121,6 @@ int tf_ctx_destroy(tf_ctx *ctx) {
     return guard([&] {
         if (!ctx) return;
         DeviceScope scope(ctx->device);
-        cudaStreamSynchronize(ctx->stream);
-        ctx->scratch.release();
-        ctx->scratch2.release();
-        if (ctx->pinned) cudaFreeHost(ctx->pinned);
-        if (ctx->fault) cudaFree(ctx->fault);
-        if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
         delete ctx;
     });
 }
@@ -235,6 +239,9 @@ int tf_convert(tf_ctx *ctx, int64_t n, int src_type, const void *src, int dst_ty
 int tf_spmv(tf_ctx *ctx, const tf_csr *a, const void *x, void *y) {
     return guard([&] {
         check_ctx(ctx);
+        check_csr(a);
+        require_vectors(a->cols, {x}, "null SpMV vector");
+        require_vectors(a->rows, {y}, "null SpMV vector");
         require(x != y || a->rows == 0, "SpMV shape or alias mismatch");
         DeviceScope scope(ctx->device);
         with_csr_types(a, [&](auto t, auto i) {
@@ -261,6 +268,9 @@ int tf_autotune_spmv(tf_ctx *ctx, const tf_csr *a, const void *x, void *y, int *
                      int *cap_pct, int *rows_per_thread, float *ms) {
     return guard([&] {
         check_ctx(ctx);
+        check_csr(a);
+        require_vectors(a->cols, {x}, "null SpMV vector");
+        require_vectors(a->rows, {y}, "null SpMV vector");
         require(x != y || a->rows == 0, "SpMV shape or alias mismatch");
         DeviceScope scope(ctx->device);
         with_csr_types(a, [&](auto t, auto i) {
@@ -287,8 +297,10 @@ int tf_spmv_set_config(tf_ctx *ctx, const tf_csr *a, int stages, int ctas_per_sm
 int tf_residual(tf_ctx *ctx, const tf_csr *a, const void *b, const void *x, void *r) {
     return guard([&] {
         check_ctx(ctx);
-        require(r != b && r != x, "Residual shape or alias mismatch");
+        check_csr(a);
         require(a->rows == a->cols, "residual needs a square matrix");
+        require_vectors(a->rows, {b, x, r}, "null residual vector");
+        require(r != b && r != x, "Residual shape or alias mismatch");
         DeviceScope scope(ctx->device);
         with_csr_types(a, [&](auto t, auto i) {
             using T = decltype(t);
@@ -302,9 +314,11 @@ int tf_jacobi_sweep(tf_ctx *ctx, const tf_csr *a, const void *dinv, const void *
                     double weight, const float *row_weight, const int32_t *map, const void *coarse) {
     return guard([&] {
         check_ctx(ctx);
-        require(x_out != x, "Jacobi sweep output must not alias its input");
-        require((map == nullptr) == (coarse == nullptr), "map and coarse go together");
+        check_csr(a);
         require(a->rows == a->cols, "Jacobi needs a square matrix");
+        require_vectors(a->rows, {dinv, b, x, x_out}, "null Jacobi vector");
+        require(x_out != x || a->rows == 0, "Jacobi sweep output must not alias its input");
+        require((map == nullptr) == (coarse == nullptr), "map and coarse go together");
         DeviceScope scope(ctx->device);
         with_csr_types(a, [&](auto t, auto i) {
             using T = decltype(t);
@@ -320,6 +334,7 @@ int tf_jacobi_zero(tf_ctx *ctx, int64_t n, int value_type, const void *dinv, con
                    const float *row_weight) {
     return guard([&] {
         check_ctx(ctx);
+        require_vectors(n, {dinv, b, x}, "invalid zero-guess sweep arguments");
         DeviceScope scope(ctx->device);
         with_value_type(value_type, [&](auto t) {
             using T = decltype(t);
@@ -332,6 +347,8 @@ int tf_jacobi_zero(tf_ctx *ctx, int64_t n, int value_type, const void *dinv, con
 int tf_inverse_diagonal(tf_ctx *ctx, const tf_csr *a, void *dinv) {
     return guard([&] {
         check_ctx(ctx);
+        check_csr(a);
+        require_vectors(a->rows, {dinv}, "null inverse diagonal");
         DeviceScope scope(ctx->device);
         with_csr_types(a, [&](auto t, auto i) {
             using T = decltype(t);
@@ -345,7 +362,8 @@ int tf_restrict(tf_ctx *ctx, int value_type, int64_t coarse_rows, const int32_t 
                 const void *fine, void *coarse) {
     return guard([&] {
         check_ctx(ctx);
-        require(fine != coarse, "Invalid aggregate transfer vectors");
+        require_vectors(coarse_rows, {offsets, members, fine, coarse}, "Invalid aggregate transfer vectors");
+        require(fine != coarse || coarse_rows == 0, "Invalid aggregate transfer vectors");
         DeviceScope scope(ctx->device);
         with_value_type(value_type, [&](auto t) {
             using T = decltype(t);
@@ -357,7 +375,8 @@ int tf_restrict(tf_ctx *ctx, int value_type, int64_t coarse_rows, const int32_t 
 int tf_prolong(tf_ctx *ctx, int value_type, int64_t fine_rows, const int32_t *map, const void *coarse, void *fine) {
     return guard([&] {
         check_ctx(ctx);
-        require(fine != coarse, "Invalid aggregate transfer vectors");
+        require_vectors(fine_rows, {map, coarse, fine}, "Invalid aggregate transfer vectors");
+        require(fine != coarse || fine_rows == 0, "Invalid aggregate transfer vectors");
         DeviceScope scope(ctx->device);
         with_value_type(value_type, [&](auto t) {
             using T = decltype(t);
@@ -371,6 +390,7 @@ int tf_dot_multi(tf_ctx *ctx, int value_type, int64_t n, int count, const void *
     return guard([&] {
         check_ctx(ctx);
         require(xs && ys && out && count >= 1 && count <= 4 && n >= 0, "invalid dot arguments");
+        for (int k = 0; k < count; ++k) require_vectors(n, {xs[k], ys[k]}, "null dot vector");
         DeviceScope scope(ctx->device);
         with_value_type(value_type, [&](auto t) {
             using T = decltype(t);
@@ -387,6 +407,7 @@ int tf_dot_multi(tf_ctx *ctx, int value_type, int64_t n, int count, const void *
 int tf_axpby(tf_ctx *ctx, int value_type, int64_t n, double a, const void *x, double b, void *y) {
     return guard([&] {
         check_ctx(ctx);
+        require_vectors(n, {x, y}, "invalid axpby arguments");
         DeviceScope scope(ctx->device);
         with_value_type(value_type, [&](auto t) {
             using T = decltype(t);
@@ -468,6 +489,7 @@ int tf_row_stats(tf_ctx *ctx, const tf_csr *a, double *row_max, int *bad) {
         check_ctx(ctx);
         require(bad != nullptr, "null output");
         auto c = native_csr(a);
+        require_vectors(c.rows, {row_max}, "null row maximum");
         DeviceScope scope(ctx->device);
         *bad = row_stats(ctx, c, row_max) ? 0 : 1;
     });
@@ -564,7 +586,7 @@ int tf_radix_sort_pairs_u64f64(tf_ctx *ctx, int64_t n, const uint64_t *keys_in, 
                                uint64_t *keys_out, double *values_out, int end_bit) {
     return guard([&] {
         check_ctx(ctx);
-        require(n >= 0, "negative size");
+        require_vectors(n, {keys_in, values_in, keys_out, values_out}, "invalid sort arguments");
         require(n == 0 || (keys_in != keys_out && values_in != values_out), "sort outputs must not alias inputs");
         DeviceScope scope(ctx->device);
         radix_sort_pairs(ctx, n, keys_in, values_in, keys_out, values_out, end_bit);
@@ -576,6 +598,7 @@ int tf_reduce_by_key_u64f64(tf_ctx *ctx, int64_t n, const uint64_t *keys, const 
     return guard([&] {
         check_ctx(ctx);
         require(count != nullptr && (op == 0 || op == 1), "invalid reduce arguments");
+        require_vectors(n, {keys, values, keys_out, values_out}, "invalid reduce arguments");
         DeviceScope scope(ctx->device);
         *count = reduce_by_key(ctx, n, keys, values, op, keys_out, values_out);
     });
@@ -584,7 +607,7 @@ int tf_reduce_by_key_u64f64(tf_ctx *ctx, int64_t n, const uint64_t *keys, const 
 int tf_scan_exclusive_i32(tf_ctx *ctx, int64_t n, const int32_t *in, int32_t *out) {
     return guard([&] {
         check_ctx(ctx);
-        require(n >= 0, "negative size");
+        require_vectors(n, {in, out}, "invalid scan arguments");
         DeviceScope scope(ctx->device);
         scan_exclusive(ctx, n, in, out);
     });
@@ -604,6 +627,7 @@ int tf_coarse_lu_solve(tf_ctx *ctx, int rows, const double *lu, const int32_t *p
                        void *x) {
     return guard([&] {
         check_ctx(ctx);
+        require(lu && pivots && b && x, "null argument");
         DeviceScope scope(ctx->device);
         with_value_type(value_type, [&](auto t) {
             using T = decltype(t);

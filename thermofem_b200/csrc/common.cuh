@@ -149,6 +149,19 @@ struct tf_ctx {
     int *fault{nullptr};                        // device word raised by a kernel whose bounded wait expired
     bool pdl{true};                             // launch_kernel adds programmatic dependent launch
     bool stable{false};                         // operators are read-only (solve / cycle enqueue)
+    tf_ctx() = default;
+    tf_ctx(const tf_ctx &) = delete;
+    tf_ctx &operator=(const tf_ctx &) = delete;
+    // Releases what tf_ctx_create acquired, also when it failed part way
+    // (the caller makes the context's device current).
+    ~tf_ctx() {
+        if (stream) cudaStreamSynchronize(stream);
+        scratch.release();
+        scratch2.release();
+        if (pinned) cudaFreeHost(pinned);
+        if (fault) cudaFree(fault);
+        if (own_stream && stream) cudaStreamDestroy(stream);
+    }
     // Returns a scratch region of at least bytes (256-byte aligned start).
     void *arena(size_t bytes, int slot = 0) {
         auto &b = slot ? scratch2 : scratch;
