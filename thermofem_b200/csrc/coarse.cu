@@ -226,9 +226,13 @@ bool coarse_lu_factor(tf_ctx *ctx, const Csr<double, int32_t> &a, double *lu, in
     require(n >= 1 && n <= 256 && a.rows == a.cols, "GPU LU requires order 1..256");
     const bool smem = n <= kSmemRows;
     const size_t bytes = smem ? static_cast<size_t>(n) * n * sizeof(double) : 0;
+    // the attribute is per function and device for the whole process: set
+    // it to the largest size any order needs, so no caller lowers it under
+    // another thread's launch
+    constexpr size_t kMaxBytes = static_cast<size_t>(kSmemRows) * kSmemRows * sizeof(double);
     if (bytes > 48 * 1024)
         cuda_check(cudaFuncSetAttribute(lu_factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        static_cast<int>(bytes)),
+                                        static_cast<int>(kMaxBytes)),
                    "LU shared memory");
     int *bad = static_cast<int *>(ctx->arena(sizeof(int), 1));
     launch_kernel(ctx, "lu_factor", lu_factor_kernel, 1, kLuThreads, bytes, n, a.rp, a.ci, a.val, lu, pivots, bad,

@@ -1068,18 +1068,28 @@ constexpr size_t kTuneFlushBytes = size_t(192) << 20;
 
 // Opts the instantiation into the dynamic shared memory it is launched with
 // (the staged chunk plus the epilogue's static reduction buffer can exceed
-// the 48 KB default); done once per instantiation and device.
+// the 48 KB default).  The attribute belongs to the function on a device,
+// for every thread of the process, so it only ever grows: per device the
+// largest size any thread asked for (a thread that lowered it could make
+// another thread's launch fail).
 template <auto Kernel>
 void allow_smem(size_t bytes) {
-    static thread_local int configured_device = -1;
-    static thread_local size_t configured_bytes = 0;
+    static thread_local int seen_device = -1;
+    static thread_local size_t seen_bytes = 0;  // known granted on seen_device
     int dev = 0;
     cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
-    if (dev == configured_device && bytes <= configured_bytes) return;
-    cuda_check(cudaFuncSetAttribute(Kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes)),
-               "tile shared memory");
-    configured_device = dev;
-    configured_bytes = bytes;
+    if (dev == seen_device && bytes <= seen_bytes) return;
+    static std::mutex m;
+    static std::map<int, size_t> granted;
+    std::lock_guard<std::mutex> lock(m);
+    size_t &g = granted[dev];
+    if (bytes > g) {
+        cuda_check(cudaFuncSetAttribute(Kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes)),
+                   "tile shared memory");
+        g = bytes;
+    }
+    seen_device = dev;
+    seen_bytes = g;
 }
 
 // Epilogues whose launches are usually skipped say so (rarely_runs()).
