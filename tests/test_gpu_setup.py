@@ -138,3 +138,45 @@ def test_setup_phase_times():
                         "layout selection"]
     assert all(v >= 0 for v in ph.values())
     assert ph["aggregation"] > 0 and ph["Galerkin products"] > 0 and ph["strength graphs"] > 0
+
+
+def test_solvers_on_separate_threads_give_the_results_of_one_thread():
+    # Separate solver instances, each with its own context, may be driven
+    # from separate host threads at the same time: setups (tuning, layout
+    # selection, graph captures) and solves interleave, and every report and
+    # solution equals the one the same solve gives alone.
+    import threading
+    m = P.heat3d(20, seed=75)
+    n = len(m[0]) - 1
+    b_host = P.rhs_uniform(n, 76)
+
+    def solve(hierarchy):
+        ctx = tf.Context(0)
+        s = tf.Cg(tf.solver_options(), "amg", tf.amg_options(hierarchy_type=hierarchy), ctx=ctx)
+        s.setup(to_device(m))
+        x = torch.zeros(n, dtype=torch.float64, device="cuda")
+        rep = s.apply(torch.tensor(b_host, device="cuda"), x)
+        torch.cuda.synchronize()
+        assert s.last_execution == 2  # captured as one whole-solve graph, also beside other threads
+        return rep, x.cpu()
+
+    alone = {h: solve(h) for h in ("f64", "f32")}
+    results, errors = {}, []
+
+    def worker(h, k):
+        try:
+            results[(h, k)] = solve(h)
+        except Exception as e:  # reported below, on the main thread
+            errors.append(repr(e))
+
+    threads = [threading.Thread(target=worker, args=(h, k)) for k in range(2) for h in ("f64", "f32")]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join(timeout=300)
+    assert not any(t.is_alive() for t in threads)
+    assert not errors, errors
+    assert len(results) == 4
+    for (h, _), (rep, x) in results.items():
+        assert rep == alone[h][0] and rep["status"] == "Converged"
+        assert torch.equal(x, alone[h][1])
