@@ -83,3 +83,28 @@ def test_driver_fp32_hierarchy(poisson_mtx):
     rc, kv, _, err = run(path, "amg", env={"THERMOFEM_B200_HIERARCHY": "f32"})
     assert rc == 0, err
     assert kv["validation"] == "PASS"
+
+
+EXTRA = ["precision", "device_solve_ms", "operator_spmv_layout", "operator_spmv_gbs",
+         "operator_spmv_roofline_fraction", "peak_gbs", "peak_source"]
+
+
+@pytest.mark.parametrize("hierarchy", ["f64", "f32"])
+def test_driver_performance_keys_are_opt_in(poisson_mtx, hierarchy):
+    # THERMOFEM_B200_DRIVER_EXTRA=1 appends the precision mode, the device
+    # solve time and the operator SpMV's bandwidth after the reference's
+    # keys; without it the report carries the reference's keys only
+    path, _ = poisson_mtx
+    env = {"THERMOFEM_B200_HIERARCHY": hierarchy}
+    rc, kv, order, err = run(path, "amg", env=env)
+    assert rc == 0, err
+    assert not set(EXTRA) & set(order)
+    rc, kv2, order2, err = run(path, "amg", env=dict(env, THERMOFEM_B200_DRIVER_EXTRA="1",
+                                                     THERMOFEM_B200_HBM_GBS="6540.8"))
+    assert rc == 0, err
+    assert order2[:len(order)] == order and order2[len(order):] == EXTRA
+    assert kv2["precision"] == ("f32_hierarchy_f64_outer" if hierarchy == "f32" else "f64")
+    assert float(kv2["device_solve_ms"]) > 0 and float(kv2["operator_spmv_gbs"]) > 0
+    assert float(kv2["operator_spmv_roofline_fraction"]) == pytest.approx(
+        float(kv2["operator_spmv_gbs"]) / 6540.8, rel=1e-4)
+    assert kv2["peak_source"] == "THERMOFEM_B200_HBM_GBS" and kv2["operator_spmv_layout"] in ("sliced", "csr")

@@ -188,6 +188,20 @@ def test_status_semantics(ctx, solver):
     assert z.apply(bad, torch.zeros(3, dtype=torch.float64, device="cuda"))["status"] == "NonFinite"
 
 
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
+def test_jacobi_analytic_sweeps_and_aliased_rhs(ctx, dtype):
+    # solver_test.cpp:56-74: Jacobi(2 sweeps, weight 1) on the 2x2 Poisson
+    # matrix from x = 0 gives (0.5, 0.25); with rhs and x the same vector
+    # (1, 0) the right-hand side is kept before the update: (0.75, 0.25)
+    j = tf.Jacobi(2, 1.0, dtype=dtype, ctx=ctx)
+    j.setup(poisson(2, dtype=dtype)[1])
+    b = torch.tensor([1.0, 0.0], dtype=dtype, device="cuda")
+    x = torch.zeros(2, dtype=dtype, device="cuda")
+    assert j.apply(b, x).cpu().tolist() == [0.5, 0.25]
+    rhs = torch.tensor([1.0, 0.0], dtype=dtype, device="cuda")
+    assert j.apply(rhs, rhs).cpu().tolist() == [0.75, 0.25]
+
+
 def test_solver_lifecycle_errors(ctx):
     s = tf.BiCgStab(ctx=ctx, index_dtype=torch.int64)
     with pytest.raises(tf.LogicError):

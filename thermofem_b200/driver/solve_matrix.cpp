@@ -12,6 +12,11 @@
 // numeric failure, 1 on an input or execution error (message on stderr as
 // error=...).  THERMOFEM_B200_HIERARCHY=f32 runs the AMG cycle in FP32 under
 // the FP64 outer loop (the default is the reference's FP64 hierarchy).
+// THERMOFEM_B200_DRIVER_EXTRA=1 appends, after the reference's keys,
+// precision=, device_solve_ms= (CUDA events around the solve),
+// operator_spmv_gbs= (algorithmic bytes of the FP64 operator SpMV over the
+// mean of 20 event-timed launches), operator_spmv_roofline_fraction= and
+// peak_gbs= (THERMOFEM_B200_HBM_GBS, else 6650 GB/s), peak_source=.
 #include <cuda_runtime.h>
 
 #include <chrono>
@@ -70,12 +75,48 @@ struct Device {
     T *p{nullptr};
     explicit Device(const T *src, size_t n) {
         cuda(cudaMalloc(&p, (n ? n : 1) * sizeof(T)), "cudaMalloc");
-        if (n) cuda(cudaMemcpy(p, src, n * sizeof(T), cudaMemcpyHostToDevice), "cudaMemcpy");
+        if (n && src) cuda(cudaMemcpy(p, src, n * sizeof(T), cudaMemcpyHostToDevice), "cudaMemcpy");
     }
     ~Device() { cudaFree(p); }
     Device(const Device &) = delete;
     Device &operator=(const Device &) = delete;
 };
+
+// The performance keys appended on request: precision, device solve time and
+// the operator SpMV's achieved bandwidth against the HBM peak.
+void report_extra(tf_ctx *ctx, tf_solver *solver, size_t n, size_t nnz, bool mixed) {
+    int sliced = 0;
+    int64_t entries = 0;
+    ok(tf_solver_spmv_layout(solver, &sliced, &entries));
+    // sliced copy: values + 2-byte offsets per entry, one start per 32-row
+    // slice, x and y once; CSR: values + 2-byte columns, row offsets, x, y
+    const double bytes = sliced ? double(entries) * 10 + double((n + 31) / 32 + 1) * 4 + double(n) * 16
+                                : double(nnz) * 10 + double(n) * 20 + 4;
+    Device<double> x(nullptr, n), y(nullptr, n);
+    cuda(cudaMemset(x.p, 0, n * sizeof(double)), "cudaMemset");
+    auto stream = static_cast<cudaStream_t>(tf_ctx_stream(ctx));
+    for (int k = 0; k < 3; ++k) ok(tf_solver_spmv(solver, x.p, y.p));
+    cudaEvent_t e0, e1;
+    cuda(cudaEventCreate(&e0), "cudaEventCreate");
+    cuda(cudaEventCreate(&e1), "cudaEventCreate");
+    constexpr int kReps = 20;
+    cuda(cudaEventRecord(e0, stream), "cudaEventRecord");
+    for (int k = 0; k < kReps; ++k) ok(tf_solver_spmv(solver, x.p, y.p));
+    cuda(cudaEventRecord(e1, stream), "cudaEventRecord");
+    cuda(cudaEventSynchronize(e1), "cudaEventSynchronize");
+    float ms = 0;
+    cuda(cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime");
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    const double gbs = bytes / (double(ms) / kReps * 1e-3) / 1e9;
+    const char *peak_env = std::getenv("THERMOFEM_B200_HBM_GBS");
+    const double peak = peak_env ? std::atof(peak_env) : 6650.0;
+    std::cout << "precision=" << (mixed ? "f32_hierarchy_f64_outer" : "f64")
+              << "\ndevice_solve_ms=" << tf_solver_last_apply_ms(solver) << "\noperator_spmv_layout="
+              << (sliced ? "sliced" : "csr") << "\noperator_spmv_gbs=" << gbs
+              << "\noperator_spmv_roofline_fraction=" << (peak > 0 ? gbs / peak : 0.0) << "\npeak_gbs=" << peak
+              << "\npeak_source=" << (peak_env ? "THERMOFEM_B200_HBM_GBS" : "fallback") << '\n';
+}
 
 }  // namespace
 
@@ -183,6 +224,8 @@ int main(int argc, char **argv) {
         const bool passed =
             finite && report.status == TF_CONVERGED && host_residual <= 1.01e-8 && solution_error <= 1e-4;
         std::cout << "validation=" << (passed ? "PASS" : "FAIL") << '\n';
+        const char *extra = std::getenv("THERMOFEM_B200_DRIVER_EXTRA");
+        if (extra && extra[0] == '1') report_extra(ctx, solver, n, nnz, mode == "amg" && h && std::string(h) == "f32");
         code = passed ? 0 : 2;
     } catch (const std::exception &e) {
         std::cerr << "error=" << e.what() << '\n';
