@@ -466,3 +466,33 @@ def test_null_vectors_are_rejected_before_any_launch(ctx):
     # the context is untouched: a valid call still runs
     assert lib.tf_spmv(ctx.h, C.byref(d), p[0], p[1]) == 0
     assert lib.tf_ctx_synchronize(ctx.h) == 0
+
+
+def test_checked_context_rejects_malformed_operands_before_launching(monkeypatch):
+    # THERMOFEM_B200_CHECKED=1 (read when the context is created): the
+    # kernel-layer entry points validate the caller's CSR on the device
+    # first; a column one past the last comes back as InvalidArgument and
+    # only the validation kernel runs.  A well-formed operand gives the
+    # unchecked result.
+    import ctypes as C
+    monkeypatch.setenv("THERMOFEM_B200_CHECKED", "1")
+    ctx = tf.Context(0)
+    lib = tf.lib()
+    off, idx, val = P.poisson1d(4)
+    good = to_device((off, idx, val))
+    x = torch.arange(1.0, 5.0, dtype=torch.float64, device="cuda")
+    assert torch.equal(tf.spmv(good, x, ctx=ctx), tf.spmv(good, x))
+    bad_idx = idx.copy()
+    bad_idx[-1] = 4  # n: one past the last column
+    bad = to_device((off, bad_idx, val))
+    dinv = tf.inverse_diagonal(good, ctx=ctx)
+    for call in (lambda: tf.spmv(bad, x, ctx=ctx),
+                 lambda: tf.residual(bad, x, x.clone(), ctx=ctx),
+                 lambda: tf.jacobi_sweep(bad, dinv, x, x.clone(), 0.5, ctx=ctx)):
+        before = lib.tf_ctx_launch_count(ctx.h)
+        with pytest.raises(tf.InvalidArgument):
+            call()
+        assert lib.tf_ctx_launch_count(ctx.h) == before + 1  # the validation kernel only
+    # an empty matrix may come without any arrays: valid, nothing to launch
+    empty = tf.Csr(0, 0, 0, 2, 1, None, None, None)  # TF_I32, TF_F64
+    assert lib.tf_csr_validate(ctx.h, C.byref(empty)) == 0

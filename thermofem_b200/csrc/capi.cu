@@ -45,6 +45,25 @@ void require_vectors(int64_t n, std::initializer_list<const void *> vectors, con
         for (const void *v : vectors) require(v != nullptr, what);
 }
 
+// The device check of a CSR's structure (row offsets from 0 to nnz, never
+// decreasing; columns in [0, cols)).
+void validate_structure(tf_ctx *ctx, const tf_csr *a) {
+    const bool ok = a->index_type == TF_I32
+                        ? csr_structure_ok(ctx, a->rows, a->cols, a->nnz, static_cast<const int32_t *>(a->offsets),
+                                           static_cast<const int32_t *>(a->indices))
+                        : csr_structure_ok(ctx, a->rows, a->cols, a->nnz, static_cast<const int64_t *>(a->offsets),
+                                           static_cast<const int64_t *>(a->indices));
+    if (!ok) fail(TF_ERR_INVALID, "Invalid device CSR structure");
+}
+
+// Checked contexts (THERMOFEM_B200_CHECKED=1 at tf_ctx_create) validate a
+// caller's CSR before a kernel-layer entry point gathers through it, so a
+// column or offset out of range comes back as TF_ERR_INVALID instead of an
+// out-of-bounds access.  Setups always validate their input.
+void check_operand(tf_ctx *ctx, const tf_csr *a) {
+    if (ctx->checked) validate_structure(ctx, a);
+}
+
 Csr<double, int32_t> native_csr(const tf_csr *a) {
     check_csr(a);
     require(a->value_type == TF_F64 && a->index_type == TF_I32, "native setup stages take FP64 values and int32 indices");
@@ -103,6 +122,9 @@ int tf_ctx_create(int device, void *stream, tf_ctx **out) {
         // THERMOFEM_B200_PDL=0 launches every kernel with plain stream order.
         const char *pdl = std::getenv("THERMOFEM_B200_PDL");
         ctx->pdl = !(pdl && pdl[0] == '0');
+        // THERMOFEM_B200_CHECKED=1 validates caller CSR operands on every kernel-layer call.
+        const char *checked = std::getenv("THERMOFEM_B200_CHECKED");
+        ctx->checked = checked && checked[0] == '1';
         if (stream) {
             ctx->stream = static_cast<cudaStream_t>(stream);
         } else {
@@ -161,12 +183,7 @@ int tf_csr_validate(tf_ctx *ctx, const tf_csr *a) {
         check_ctx(ctx);
         check_csr(a);
         DeviceScope scope(ctx->device);
-        const bool ok = a->index_type == TF_I32
-                            ? csr_structure_ok(ctx, a->rows, a->cols, a->nnz, static_cast<const int32_t *>(a->offsets),
-                                               static_cast<const int32_t *>(a->indices))
-                            : csr_structure_ok(ctx, a->rows, a->cols, a->nnz, static_cast<const int64_t *>(a->offsets),
-                                               static_cast<const int64_t *>(a->indices));
-        if (!ok) fail(TF_ERR_INVALID, "Invalid device CSR structure");
+        validate_structure(ctx, a);
     });
 }
 
@@ -244,6 +261,7 @@ int tf_spmv(tf_ctx *ctx, const tf_csr *a, const void *x, void *y) {
         require_vectors(a->rows, {y}, "null SpMV vector");
         require(x != y || a->rows == 0, "SpMV shape or alias mismatch");
         DeviceScope scope(ctx->device);
+        check_operand(ctx, a);
         with_csr_types(a, [&](auto t, auto i) {
             using T = decltype(t);
             using I = decltype(i);
@@ -273,6 +291,7 @@ int tf_autotune_spmv(tf_ctx *ctx, const tf_csr *a, const void *x, void *y, int *
         require_vectors(a->rows, {y}, "null SpMV vector");
         require(x != y || a->rows == 0, "SpMV shape or alias mismatch");
         DeviceScope scope(ctx->device);
+        check_operand(ctx, a);
         with_csr_types(a, [&](auto t, auto i) {
             using T = decltype(t);
             using I = decltype(i);
@@ -302,6 +321,7 @@ int tf_residual(tf_ctx *ctx, const tf_csr *a, const void *b, const void *x, void
         require_vectors(a->rows, {b, x, r}, "null residual vector");
         require(r != b && r != x, "Residual shape or alias mismatch");
         DeviceScope scope(ctx->device);
+        check_operand(ctx, a);
         with_csr_types(a, [&](auto t, auto i) {
             using T = decltype(t);
             using I = decltype(i);
@@ -320,6 +340,7 @@ int tf_jacobi_sweep(tf_ctx *ctx, const tf_csr *a, const void *dinv, const void *
         require(x_out != x || a->rows == 0, "Jacobi sweep output must not alias its input");
         require((map == nullptr) == (coarse == nullptr), "map and coarse go together");
         DeviceScope scope(ctx->device);
+        check_operand(ctx, a);
         with_csr_types(a, [&](auto t, auto i) {
             using T = decltype(t);
             using I = decltype(i);
@@ -350,6 +371,7 @@ int tf_inverse_diagonal(tf_ctx *ctx, const tf_csr *a, void *dinv) {
         check_csr(a);
         require_vectors(a->rows, {dinv}, "null inverse diagonal");
         DeviceScope scope(ctx->device);
+        check_operand(ctx, a);
         with_csr_types(a, [&](auto t, auto i) {
             using T = decltype(t);
             using I = decltype(i);

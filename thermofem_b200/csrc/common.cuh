@@ -149,6 +149,7 @@ struct tf_ctx {
     int *fault{nullptr};                        // device word raised by a kernel whose bounded wait expired
     bool pdl{true};                             // launch_kernel adds programmatic dependent launch
     bool stable{false};                         // operators are read-only (solve / cycle enqueue)
+    bool checked{false};                        // caller CSR validated before kernel-layer launches
     tf_ctx() = default;
     tf_ctx(const tf_ctx &) = delete;
     tf_ctx &operator=(const tf_ctx &) = delete;
