@@ -45,6 +45,7 @@ SPMV_TRAFFIC = {"sliced": 163197184 + 4258048, "csr": 171013632 + 13778176}
 # (profiles/sliced_kernel_heat3d_128_fp32_level0.md,
 # profiles/csr_pipe_kernel_heat3d_128_fp32_level0.md)
 SPMV32_TRAFFIC = {"sliced": 96349184 + 4392704, "csr": 104301056 + 5819136}
+SOLVER = "PCG + aggregation AMG V(1,1), Jacobi w=2/3, coarse LU <= 64 rows, rtol 1e-8"
 WORKLOAD = f"heat3d {SIZE}^3 7-point FV, log-normal k (seed {SEED_MATRIX}), Dirichlet x=0, rhs U[-1,1] (seed {SEED_RHS})"
 
 
@@ -198,8 +199,8 @@ def run_reference(args):
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
-            "config": {"workload": WORKLOAD + ", CPU oracle FP64 AMG-PCG", "rows": n, "nnz": int(len(idx)),
-                       "parallelism": "host OpenMP"},
+            "config": {"workload": WORKLOAD, "rows": n, "nnz": int(len(idx)), "solver": SOLVER,
+                       "parallelism": f"host OpenMP, {O.num_threads()} threads (CPU oracle, FP64 hierarchy)"},
             "iterations": rep["iterations"], "setup_s": setup_s,
             "cpu_baseline": {"value": value, "unit": "s", "cores": cores, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -636,7 +637,7 @@ def main():
             "warmup": args.warmup, "ms_per_step": ms_mixed, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64 outer / f32 hierarchy", "data": "synthetic (seeded generator)",
             "config": {"workload": WORKLOAD, "rows": n, "nnz": nnz,
-                       "solver": "PCG + aggregation AMG V(1,1), Jacobi w=2/3, coarse LU <= 64 rows, rtol 1e-8",
+                       "solver": SOLVER,
                        "parallelism": "replicas" if world > 1 else "single GPU",
                        "l2": "inputs larger than L2 (217 MB FP64 operator), no flush"},
             "iterations": rep_mixed["iterations"], "true_relative_residual": true_rel,
