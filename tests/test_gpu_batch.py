@@ -1,7 +1,6 @@
 """Batched solves (tf_batch_*): independent systems as branches of one CUDA
 graph.  Every system's iterations, report and solution must be those of its
 own tf_solver_apply, bit for bit."""
-import numpy as np
 import pytest
 import torch
 

@@ -6,7 +6,6 @@ shared scratch array cannot leak into the second.  Collected last on
 purpose, and self-contained, so it passes alone in a fresh process too."""
 import ctypes
 
-import numpy as np
 import pytest
 import torch
 
