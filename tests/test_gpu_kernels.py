@@ -496,3 +496,25 @@ def test_checked_context_rejects_malformed_operands_before_launching(monkeypatch
     # an empty matrix may come without any arrays: valid, nothing to launch
     empty = tf.Csr(0, 0, 0, 2, 1, None, None, None)  # TF_I32, TF_F64
     assert lib.tf_csr_validate(ctx.h, C.byref(empty)) == 0
+
+
+@pytest.mark.parametrize("dtype,index_dtype", [(torch.float64, torch.int32), (torch.float32, torch.int64)])
+def test_unaligned_arrays_take_the_staged_kernel_with_the_same_bits(ctx, dtype, index_dtype):
+    # A caller's CSR whose arrays start off a 16-byte boundary cannot be
+    # bulk-copied: the staged row-tile kernel reads it (16-byte vector loads
+    # over the aligned interior, scalar head and tail) and gives the bits of
+    # the pipelined kernel on aligned copies of the same arrays.
+    off, idx, val = P.heat3d(16, seed=9)
+    a = to_device((off, idx, val), dtype=dtype, index_dtype=index_dtype)
+    x = torch.randn(a.rows, dtype=dtype, device="cuda", generator=torch.Generator("cuda").manual_seed(3))
+    b = torch.randn(a.rows, dtype=dtype, device="cuda", generator=torch.Generator("cuda").manual_seed(4))
+
+    def shifted(t):  # the same values one element past an aligned start
+        buf = torch.empty(t.numel() + 1, dtype=t.dtype, device="cuda")
+        buf[1:].copy_(t)
+        return buf[1:]
+
+    u = tf.DeviceCsr(shifted(a.offsets), shifted(a.indices), shifted(a.values), a.cols)
+    assert u.offsets.data_ptr() % 16 and u.indices.data_ptr() % 16 and u.values.data_ptr() % 16
+    assert torch.equal(tf.spmv(u, x, ctx=ctx), tf.spmv(a, x, ctx=ctx))
+    assert torch.equal(tf.residual(u, b, x, ctx=ctx), tf.residual(a, b, x, ctx=ctx))

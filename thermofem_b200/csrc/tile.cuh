@@ -161,7 +161,7 @@ __global__ void __launch_bounds__(kThreads) csr_tile_kernel(int64_t rows, const 
     constexpr int K = Epi::kReduce;
     pdl_enter();
     if (epi.skip()) return;
-    extern __shared__ __align__(16) unsigned char smem[];
+    extern __shared__ __align__(128) unsigned char smem[];
     T *sval = reinterpret_cast<T *>(smem);
     I *scol = reinterpret_cast<I *>(smem + static_cast<size_t>(chunk) * sizeof(T));
     const int64_t r0 = static_cast<int64_t>(blockIdx.x) * (kThreads * RPT);
