@@ -53,6 +53,16 @@ def test_four_point_galerkin_known_answer(golden):
     assert c.rows == 1 and list(c.values) == [2.0]
 
 
+def test_four_point_residual_and_jacobi_known_answers(golden):
+    # multigrid_operations_test.cpp:45-59 on the same 4x4 tridiagonal: the
+    # residual of b = 0 at x = ones is (-1, 0, 0, -1); one Jacobi update with
+    # weight 1 from x = 0 and b = ones is 0.5 everywhere
+    a = golden_csr(golden, "galerkin4/input")
+    ones = np.ones(4)
+    assert list(np.zeros(4) - O.spmv(a, ones)) == [-1.0, 0.0, 0.0, -1.0]
+    assert list(O.jacobi(a, 1, 1.0, ones, np.zeros(4))) == [0.5] * 4
+
+
 def test_duplicate_canonicalisation_known_answer():
     # amg_native_test.cpp:115-121: duplicates summed -> {2, -1, -1, 2}
     a = O.Csr(2, np.array([0, 3, 6], np.int32), np.array([1, 0, 0, 1, 0, 1], np.int32),
