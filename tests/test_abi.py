@@ -84,16 +84,16 @@ def test_null_arguments_are_rejected():
     assert b"null" in tf.lib().tf_last_error()
 
 
-def test_problem_generators_match_baseline_sizes():
+def test_problem_generators_match_the_benchmark_sizes():
+    # 2-D 128^2 Poisson: 16,384 rows, 81,408 nonzeros; 3-D 7-point stencil
+    # on n^3 cells: 7 n^3 - 6 n^2 nonzeros
     from thermofem_b200 import problems as P
     off, idx, val = P.laplace2d(128)
     assert len(off) - 1 == 16384 and len(idx) == 81408
     off, idx, val = P.heat3d(32, seed=1)
     assert len(off) - 1 == 32 ** 3 and len(idx) == 7 * 32 ** 3 - 6 * 32 ** 2
-    a = np.zeros(3)
     assert np.array_equal(P.uniform(5, 10), P.uniform(5, 10))  # pure function of (seed, index)
     assert not np.array_equal(P.uniform(5, 10), P.uniform(6, 10))
-    del a
 
 
 def test_solve_matrix_driver_input_errors(tmp_path):
