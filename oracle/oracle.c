@@ -1,7 +1,7 @@
 /*
  * oracle.c -- CPU restatement of ThermoFEM's sparse solve path.
  *
- * TEST INFRASTRUCTURE ONLY (the checker of the CUDA path; see oracle.h).
+ * TEST INFRASTRUCTURE ONLY (the oracle the CUDA path is tested against; see oracle.h).
  * Reference citations are paths inside the Mgepahmge/ThermoFEM project.
  */
 #include "oracle.h"

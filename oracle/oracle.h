@@ -1,7 +1,7 @@
 /*
  * oracle.h -- CPU restatement of ThermoFEM's sparse solve path.
  *
- * TEST INFRASTRUCTURE ONLY.  This library is the checker for the CUDA path:
+ * TEST INFRASTRUCTURE ONLY.  This library is the oracle the CUDA path is tested against:
  * only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg load
  * it.  Nothing in the product (thermofem_b200/) links, imports or calls it.
  *

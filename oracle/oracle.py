@@ -1,5 +1,5 @@
 """ctypes binding of the CPU oracle (oracle/liboracle.so) and of the
-reference-built checker (oracle/_ref/libref_oracle.so).
+oracle built from the reference sources (oracle/_ref/libref_oracle.so).
 
 TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
 cpu_baseline leg of bench.py, never by the product package.
@@ -330,7 +330,7 @@ def num_threads():
 
 
 # --------------------------------------------------------------------------
-# Reference-built checker (oracle/_ref): available where the reference
+# Oracle built from the reference sources (oracle/_ref): available where the reference
 # sources were present at build time.
 # --------------------------------------------------------------------------
 _ref = None
@@ -479,7 +479,7 @@ def mlp_gradient(params, x, target, lo, hi):
 # --------------------------------------------------------------------------
 # The reference's own GPU solve path (oracle/_ref/libref_gpu.so, built by
 # `make -C oracle refgpu` from the reference sources): Cg / BiCgStab with its
-# aggregation Amg in FP64 (ref_gpu_shim.cu).  A checker for the GPU tests.
+# aggregation Amg in FP64 (ref_gpu_shim.cu).  A second oracle for the GPU tests.
 # --------------------------------------------------------------------------
 REF_GPU_LIB = os.path.join(HERE, "_ref", "libref_gpu.so")
 _ref_gpu = None

@@ -1,4 +1,4 @@
-"""Pins the CPU oracle (oracle/oracle.c) before it is trusted as the checker:
+"""Pins the CPU oracle (oracle/oracle.c) before the tests trust it:
 against the golden fixtures generated from the reference's own host oracle,
 and, where this machine has the reference sources, against that oracle
 directly (oracle/_ref).  CPU only."""
