@@ -131,3 +131,30 @@ def test_solve_matrix_driver_input_errors(tmp_path):
         return sorted(zip(r.tolist(), np.asarray(i).tolist(), np.asarray(v).tolist()))
 
     assert triplets(back["offsets"], back["indices"], back["values"]) == triplets(off, idx, val)
+
+
+def test_header_binds_from_strict_c99(tmp_path):
+    # A plain C caller: the header compiles as C99 with -pedantic and every
+    # warning on, links against the library and calls two entry points that
+    # need no device (device count, status strings).
+    import shutil
+    import subprocess
+    gcc = shutil.which("gcc")
+    if gcc is None:
+        pytest.skip("gcc not available")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    libdir = os.path.join(root, "thermofem_b200", "lib")
+    src = tmp_path / "caller.c"
+    src.write_text('#include "thermofem_b200.h"\n'
+                   "int main(void) {\n"
+                   "    int n = -1;\n"
+                   "    if (tf_device_count(&n) != TF_OK || n < 0) return 2;\n"
+                   "    if (tf_status_string(TF_ERR_INVALID)[0] != 'i') return 3;\n"
+                   "    return tf_device_count(0) == TF_ERR_INVALID ? 0 : 4;\n"
+                   "}\n")
+    exe = tmp_path / "caller"
+    r = subprocess.run([gcc, "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror", "-I", os.path.join(root, "include"),
+                        str(src), "-L", libdir, "-lthermofem_b200", f"-Wl,-rpath,{libdir}", "-o", str(exe)],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    assert subprocess.run([str(exe)], timeout=120).returncode == 0
