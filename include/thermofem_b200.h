@@ -239,9 +239,14 @@ int tf_scan_exclusive_i32(tf_ctx *ctx, int64_t n, const int32_t *in, int32_t *ou
  * device that loads the library until the process exits; n is limited to
  * 134,217,728 (2^27) items, larger n returns TF_ERR_LENGTH.  Runs on `stream`
  * (a cudaStream_t, NULL = legacy default stream) of the current device and
- * returns without synchronising.  The first call on a device looks up the
- * scratch array's device address (cudaGetSymbolAddress); make that first
- * call before any stream capture.  All calls on a device share the array:
+ * returns without synchronising.  The first call on a device loads this
+ * library's kernels there if CUDA has not loaded them yet (lazy loading, the
+ * default since CUDA 12.2) -- which allocates the array and the code on the
+ * device and may synchronise it -- and looks up the array's device address
+ * (cudaGetSymbolAddress): make that first call beforehand, where allocating
+ * is allowed and outside any stream capture; later calls allocate nothing.
+ * Not usable after cudaDeviceReset in the same process (the address is kept
+ * per device).  All calls on a device share the array:
  * calls whose kernels may overlap on the GPU race and give undefined results.
  * out may alias in. */
 int tf_scan_exclusive_i32_noalloc(void *stream, int64_t n, const int32_t *in, int32_t *out);
@@ -448,6 +453,12 @@ typedef struct {
  * TF_ERR_RUNTIME with tf_last_error() on malformed input. */
 int tf_read_matrix_market(const char *text, size_t length, tf_host_csr *out);
 int tf_read_matrix_market_file(const char *path, tf_host_csr *out);
+/* The same reader over a caller's byte source (the std::istream overload of
+ * io::readMatrixMarket, include/IO/MatrixMarket.cuh:30): read() fills up to
+ * `capacity` bytes of buf and returns how many, 0 at the end of the input,
+ * (size_t)-1 on a read error ("Matrix Market input read failure"). */
+int tf_read_matrix_market_stream(size_t (*read)(void *user, char *buf, size_t capacity), void *user,
+                                 tf_host_csr *out);
 void tf_host_csr_free(tf_host_csr *m);
 
 #if defined(__GNUC__)

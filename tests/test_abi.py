@@ -54,6 +54,119 @@ def test_matrix_market_matches_reference_reader():
             tf.read_matrix_market(text)
 
 
+def _mm_random_text(rng):
+    """One Matrix Market text built from fields that probe the stream
+    extractors' number grammar, white space, comments, line endings and the
+    header / size / entry rules; most are valid, many are not."""
+    pick = lambda xs: xs[int(rng.integers(len(xs)))]  # noqa: E731
+    sep = lambda: pick([" ", " ", "\t", "  ", " \t "])  # noqa: E731
+    eol = pick(["\n", "\n", "\r\n"])
+    field = pick(["real", "real", "integer", "Real", "complex"])
+    symmetry = pick(["general", "general", "symmetric", "hermitian"])
+    banner = pick(["%%MatrixMarket", "%%MatrixMarket", "%%matrixmarket", " %%MatrixMarket"])
+    words = [banner, "matrix", "coordinate", field, symmetry]
+    if rng.random() < 0.05:
+        words = words[:4]
+    if rng.random() < 0.05:
+        words.append("extra")
+    lines = [sep().join(words)]
+    junk = ["", "   ", "% comment", "  % indented", "\t%", "\r", "\v", "%"]
+    for _ in range(int(rng.integers(3))):
+        lines.append(pick(junk) if rng.random() < 0.8 else "")
+    rows = int(rng.integers(0, 6))
+    cols = rows if rng.random() < 0.8 else int(rng.integers(0, 6))
+    count = int(rng.integers(0, 7))
+    size = [str(rows), str(cols), str(count)]
+    r = rng.random()
+    if r < 0.04:
+        size = size[:2]
+    elif r < 0.08:
+        size.append("1")
+    elif r < 0.12:
+        size[int(rng.integers(3))] = pick(["+3", "-1", "2147483648", "3x", "3.0", "x", "03"])
+    lines.append(sep().join(size))
+    value_pool = ["2", "-1.5", "+3", ".5", "5.", "1e3", "1E-3", "1e", "1e+", "1.5.3", "0x10", "inf", "nan", "-",
+                  "+", "1e400", "1e-400", "1.e5", ".e5", "e5", "-.5", "+-5", "007", "2abc", "1,5", "4", "-0",
+                  "1e5.3", "2.5e-3x", "9" * 30, "4.0"]
+    index_pool = ["+1", "01", "1.0", "-1", "0", "99999999999999999999", "1x", "1"]
+    n_entries = count + (int(rng.integers(-1, 2)) if rng.random() < 0.15 else 0)
+    for _ in range(max(n_entries, 0)):
+        i = str(int(rng.integers(1, max(rows, 1) + 1)))
+        j = str(int(rng.integers(1, max(cols, 1) + 1)))
+        if rng.random() < 0.06:
+            i = pick(index_pool)
+        if rng.random() < 0.06:
+            j = pick(index_pool)
+        v = pick(value_pool) if rng.random() < 0.3 else str(int(rng.integers(-9, 10)))
+        fields = [i, j, v]
+        if rng.random() < 0.03:
+            fields.append(pick(["extra", "1", "%"]))
+        lines.append(sep().join(fields) + (sep() if rng.random() < 0.1 else ""))
+        if rng.random() < 0.1:
+            lines.append(pick(junk))
+    text = eol.join(lines)
+    return text + (eol if rng.random() < 0.9 else "")
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libref_oracle.so")),
+                    reason="the reference reader is built only where the reference sources are")
+def test_matrix_market_reader_agrees_with_the_reference_reader_on_random_inputs():
+    # 8000 seeded texts: every text the reference reader accepts gives the
+    # same CSR here; every text it rejects is rejected with the same message.
+    from oracle import oracle as O
+    rng = np.random.default_rng(2024)
+    accepted = rejected = 0
+    messages = set()
+    for k in range(8000):
+        text = _mm_random_text(rng)
+        try:
+            want = O.ref_read_matrix_market(text)
+        except O.OracleError as e:
+            rejected += 1
+            messages.add(str(e))
+            with pytest.raises(tf.ParseError) as got:
+                tf.read_matrix_market(text)
+            assert str(e) in str(got.value), (k, text)
+            continue
+        accepted += 1
+        m = tf.read_matrix_market(text)
+        assert m["rows"] == want.rows, (k, text)
+        assert np.array_equal(m["offsets"], want.offsets), (k, text)
+        assert np.array_equal(m["indices"], want.indices), (k, text)
+        assert np.array_equal(m["values"], want.values), (k, text)
+    assert accepted > 600 and rejected > 2000
+    # every rule that a text can break was met (the index-range and read-error
+    # rules need inputs larger than these)
+    assert messages == {"Unsupported Matrix Market header", "Unexpected Matrix Market field",
+                        "Invalid Matrix Market dimensions", "Truncated Matrix Market entries",
+                        "Invalid Matrix Market entry", "Mixed triangles in symmetric storage",
+                        "Extra Matrix Market entries"}, messages
+
+
+def test_matrix_market_stream_reader_crosses_block_boundaries(tmp_path):
+    # a file much larger than one read block, with a line longer than a block:
+    # the file reader cuts lines across block boundaries correctly
+    n = 200_000
+    rng = np.random.default_rng(3)
+    cols = rng.integers(1, n + 1, n)
+    vals = rng.standard_normal(n)
+    body = "".join(f"{i + 1} {c} {float(v)!r}\n" for i, (c, v) in enumerate(zip(cols, vals)))
+    long_comment = "%" + "x" * (40 << 20) + "\n"
+    text = "%%MatrixMarket matrix coordinate real general\n" + long_comment + f"{n} {n} {n}\n" + body
+    p = tmp_path / "big.mtx"
+    p.write_text(text)
+    for m in (tf.read_matrix_market_file(str(p)), tf.read_matrix_market_stream(open(p, "rb"))):
+        assert m["offsets"].tolist() == list(range(n + 1))
+        assert np.array_equal(m["indices"], cols - 1)
+        assert np.array_equal(m["values"], vals)
+
+    class Failing:
+        def read(self, k):
+            raise OSError("device gone")
+    with pytest.raises(tf.ParseError, match="read failure"):
+        tf.read_matrix_market_stream(Failing())
+
+
 def test_matrix_market_file_and_known_answers(tmp_path):
     # matrix_market_test.cpp:8-25
     m = tf.read_matrix_market("%%MatrixMarket matrix coordinate real general\n% comment\n3 3 4\n3 1 2\n1 2 4\n1 2 -1\n3 3 5\n")

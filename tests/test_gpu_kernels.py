@@ -206,6 +206,39 @@ def test_scan_exclusive(ctx, n):
     assert np.array_equal(t.cpu().numpy(), want)
 
 
+@pytest.mark.parametrize("src,dst", [(torch.float32, torch.float64), (torch.float64, torch.float32),
+                                     (torch.float32, torch.float32), (torch.float64, torch.float64),
+                                     (torch.int32, torch.int64), (torch.int64, torch.int32),
+                                     (torch.int32, torch.int32), (torch.int64, torch.int64)])
+def test_convert_matches_torch_casts(ctx, src, dst):
+    # tf_convert is an elementwise static_cast, as the reference's convert
+    # kernel (GpuAggregation.cu:1101-1108): FP64 -> FP32 rounds to nearest
+    # even, int64 -> int32 keeps the low 32 bits (two's complement), exactly
+    # what torch's casts do; the index range itself is checked by the
+    # component layer (AMG native index capacity), not per element.
+    g = torch.Generator(device="cuda").manual_seed(5)
+    n = 1_000_003
+    if src.is_floating_point:
+        x = (torch.randn(n, dtype=torch.float64, device="cuda", generator=g) * 1e3).to(src)
+        x[:4] = torch.tensor([0.0, -0.0, 1e-40, 3.4e38], dtype=torch.float64).to(src)
+    else:
+        x = torch.randint(-2**31, 2**31 - 1, (n,), dtype=torch.int64, device="cuda", generator=g).to(src)
+        if src == torch.int64:
+            x[:3] = torch.tensor([2**31, -2**31 - 1, 2**40 + 7], dtype=torch.int64)
+    got = tf.convert(x, dst, ctx=ctx)
+    ctx.synchronize()
+    assert torch.equal(got, x.to(dst))
+    assert tf.convert(x[:0], dst, ctx=ctx).numel() == 0
+
+
+def test_convert_rejects_mixed_kinds(ctx):
+    x = torch.ones(8, dtype=torch.float64, device="cuda")
+    with pytest.raises(tf.InvalidArgument):
+        tf.convert(x, torch.int32, ctx=ctx)
+    with pytest.raises(tf.InvalidArgument):
+        tf.convert(x.to(torch.int64), torch.float32, ctx=ctx)
+
+
 @pytest.mark.parametrize("n,bits", [(1, 8), (1000, 12), (70000, 40), (1_000_003, 64)])
 def test_radix_sort_is_stable_and_reduce_by_key(ctx, n, bits):
     rng = np.random.default_rng(n)

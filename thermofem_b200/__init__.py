@@ -96,6 +96,9 @@ class HostCsr(C.Structure):
                 ("indices", C.POINTER(C.c_int32)), ("values", C.POINTER(C.c_double))]
 
 
+# The byte source of tf_read_matrix_market_stream: read(user, buf, capacity).
+MM_READ = C.CFUNCTYPE(C.c_size_t, C.c_void_p, C.c_void_p, C.c_size_t)
+
 # Every symbol declared in include/thermofem_b200.h with its ctypes signature.
 _P, _I, _L, _D, _S = C.c_void_p, C.c_int, C.c_int64, C.c_double, C.c_size_t
 _PP = C.POINTER(C.c_void_p)
@@ -198,6 +201,7 @@ SIGNATURES = {
     "tf_mlp_sgd": ([_P, _D, _D], _I),
     "tf_read_matrix_market": ([C.c_char_p, _S, C.POINTER(HostCsr)], _I),
     "tf_read_matrix_market_file": ([C.c_char_p, C.POINTER(HostCsr)], _I),
+    "tf_read_matrix_market_stream": ([MM_READ, _P, C.POINTER(HostCsr)], _I),
     "tf_host_csr_free": ([C.POINTER(HostCsr)], None),
 }
 

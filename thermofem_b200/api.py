@@ -14,7 +14,7 @@ from . import (AmgOptions, Csr, HostCsr, SolveResult, SolverOptions, F32, F64, I
 
 __all__ = ["Context", "DeviceCsr", "Transfer", "Amg", "Jacobi", "Cg", "BiCgStab", "Batch", "Mlp", "row_features", "MLP_PARAMS",
            "MLP_FEATURES", "MLP_HIDDEN", "amg_options", "solver_options",
-           "read_matrix_market", "read_matrix_market_file", "spmv", "autotune_spmv", "set_spmv_config", "residual", "jacobi_sweep", "jacobi_zero",
+           "read_matrix_market", "read_matrix_market_file", "read_matrix_market_stream", "spmv", "autotune_spmv", "set_spmv_config", "residual", "jacobi_sweep", "jacobi_zero",
            "inverse_diagonal", "restrict_aggregates", "prolong_aggregates", "dot_multi", "axpby", "convert",
            "csr_validate", "check_canonical", "canonicalize", "row_stats", "strength", "match", "contract",
            "aggregate", "galerkin", "radix_sort_pairs", "reduce_by_key", "scan_exclusive", "coarse_lu_factor",
@@ -700,6 +700,25 @@ def read_matrix_market(text: str):
 def read_matrix_market_file(path: str):
     h = HostCsr()
     check(lib().tf_read_matrix_market_file(path.encode(), C.byref(h)))
+    return _take_host(h)
+
+
+def read_matrix_market_stream(stream):
+    """io::readMatrixMarket over a binary file-like object, read in blocks
+    through tf_read_matrix_market_stream."""
+    from . import MM_READ
+
+    def read(_user, buf, capacity):
+        try:
+            data = stream.read(capacity)
+        except OSError:
+            return C.c_size_t(-1).value
+        C.memmove(buf, data, len(data))
+        return len(data)
+
+    fn = MM_READ(read)
+    h = HostCsr()
+    check(lib().tf_read_matrix_market_stream(fn, None, C.byref(h)))
     return _take_host(h)
 
 

@@ -16,6 +16,17 @@
 // clearing is needed between calls, but two calls whose kernels overlap on
 // the GPU (different streams, no ordering between them) race on the array and
 // both results are undefined.
+//
+// First call on a device: CUDA loads a library's kernels lazily (the default
+// since CUDA 12.2), so the first call on each device loads this module, which
+// allocates the array and the module's code on the device and may
+// synchronise it, and then looks up the array's device address.  A caller
+// that must not allocate at all makes that first call beforehand, at a point
+// where allocating is allowed (and outside any stream capture); every later
+// call on that device allocates nothing.  The address is kept per device
+// ordinal for the life of the process: after cudaDeviceReset the device's
+// memory, the array included, is gone, so the function must not be called
+// again in that process.
 #include <mutex>
 
 #include "common.cuh"
