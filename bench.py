@@ -1,20 +1,26 @@
 """Benchmark: time to a 1e-8 FP64 relative residual of AMG-preconditioned CG
-on the 3-D 7-point variable-coefficient heat-conduction problem, 128^3 cells
-(2,097,152 rows, 14,581,760 nonzeros), log-normal conductivity, Dirichlet on
-one face, Neumann elsewhere (seeded synthetic input).
+and BiCGStab on the 3-D 7-point variable-coefficient heat-conduction
+problem, 256^3 cells (16,777,216 rows, 117,047,296 nonzeros), log-normal
+conductivity, Dirichlet on one face, Neumann elsewhere (seeded synthetic
+input), mixed precision (FP32 AMG hierarchy and V-cycle, FP64 outer Krylov
+loop) against plain FP64 on the same GPU.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl thermofem|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl thermofem|reference] [--size M]
 
 A step is one solve (Solver::apply) from a zero initial guess with the
-hierarchy already built; `value` is seconds per solve of the mixed-precision
-path (FP32 AMG hierarchy and V-cycle, FP64 PCG), `plain_fp64` the same with an
-FP64 hierarchy.  Inputs stay resident in HBM (the 217 MB FP64 operator is
-larger than the 126 MB L2, so nothing is flushed between steps).  `e2e` runs
-the same solve through the C ABI with pinned host buffers (rhs upload, x
-upload and download inside the timed region).  With N > 1 every rank solves
-its own replica (the solve does not shard) and the time is the max over
-ranks.  `--impl reference` times the CPU oracle (the reference has no CPU
-solver; its host restatement is the baseline) on the host cores.
+hierarchy already built.  `value` is seconds per solve of the mixed PCG;
+`plain_fp64` is PCG with an FP64 hierarchy; `bicgstab` holds the same pair
+for BiCGStab; `speedup_mixed_vs_fp64` is the PCG ratio.  Inputs stay resident
+in HBM (the 1.4 GB FP64 operator is far larger than the 126 MB L2, so nothing
+is flushed between steps).  `e2e` runs the mixed PCG through the C ABI with
+pinned host buffers (rhs upload, x upload and download inside the timed
+region).  `reference_gpu` is the reference's own CUDA build (compiled for
+sm_100a from its sources) on the same inputs, where that build is present;
+`heat3d_128` repeats the mixed/plain PCG pair on 128^3 with the error of each
+solution against the CPU oracle's FP64 solve.  With N > 1 every rank solves
+its own replica (a single system does not shard) and the time is the max
+over ranks.  `--impl reference` times the CPU oracle (the reference has no
+CPU solver; its host restatement is the baseline) on the host cores.
 """
 from __future__ import annotations
 
@@ -31,22 +37,28 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-SIZE = 128
+SIZE = 256
+EXTRA_SIZE = 128
 SEED_MATRIX, SEED_RHS = 1001, 1002
 AMG = dict(jacobi_weight=2.0 / 3.0, pre_sweeps=1, post_sweeps=1, cycle="v", coarse_rows=64)
 METRIC = "time-to-1e-8 FP64 relative residual (s), AMG-PCG V-cycle, FP32 hierarchy / FP64 outer"
-# DRAM bytes (read + write) of one launch of the FP64 operator SpMV on the
-# 128^3 problem, from the ncu captures summarised in
-# profiles/sliced_kernel_heat3d_128_fp64_operator.md (sliced copy) and
-# profiles/csr_pipe_kernel_heat3d_128_fp64_operator.md (CSR row tiles)
+# DRAM bytes (read + write) of one launch, from ncu captures on the 128^3
+# problem: the FP64 Krylov operator SpMV (its sliced copy, or CSR row tiles)
+# and the FP32 finest-level SpMV of the mixed hierarchy (sliced copy or row
+# tiles), the kernel family that takes most of the mixed solve's time.  On
+# other sizes the traffic per algorithmic byte of the same kernel is applied
+# (the operators are the same stencil, so traffic grows with the bytes).
 SPMV_TRAFFIC = {"sliced": 163197184 + 4258048, "csr": 171013632 + 13778176}
-# the same for the FP32 finest-level SpMV of the mixed hierarchy, the kernel
-# family that takes most of the mixed solve's time
-# (profiles/sliced_kernel_heat3d_128_fp32_level0.md,
-# profiles/csr_pipe_kernel_heat3d_128_fp32_level0.md)
 SPMV32_TRAFFIC = {"sliced": 96349184 + 4392704, "csr": 104301056 + 5819136}
-SOLVER = "PCG + aggregation AMG V(1,1), Jacobi w=2/3, coarse LU <= 64 rows, rtol 1e-8"
-WORKLOAD = f"heat3d {SIZE}^3 7-point FV, log-normal k (seed {SEED_MATRIX}), Dirichlet x=0, rhs U[-1,1] (seed {SEED_RHS})"
+# the algorithmic bytes of those captured launches (128^3)
+SPMV_BYTES_128 = {"sliced": 179961860, "csr": 187760644}
+SPMV32_BYTES_128 = {"sliced": 104726532, "csr": 112656388}
+SOLVER = "PCG / BiCGStab + aggregation AMG V(1,1), Jacobi w=2/3, coarse LU <= 64 rows, rtol 1e-8"
+
+
+def workload_name(m):
+    return (f"heat3d {m}^3 7-point FV, log-normal k (seed {SEED_MATRIX}), Dirichlet x=0, "
+            f"rhs U[-1,1] (seed {SEED_RHS})")
 
 
 def spmv_bytes(n, nnz, vsize=8, isize=4, csize=None):
@@ -159,53 +171,74 @@ class Clocks:
                 "power_w_max": max(r[2] for r in rows), "samples": len(rows), "reasons": reasons}
 
 
-def cpu_solve_once(A, amg, b, O, keep=None):
+def oracle_baseline(A, b, iterations, sample_iterations=10, repeats=1):
+    """The CPU oracle's FP64 AMG-PCG on the host cores: its setup, then
+    `repeats` bounded samples of `sample_iterations` PCG iterations, each
+    scaled to `iterations` (the full solve's count).  Returns (setup_s,
+    [seconds per full solve, one per sample], threads)."""
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle")], check=True)
+    from oracle import oracle as O
     t0 = time.perf_counter()
-    x, rep = O.cg(A, amg, b, np.zeros(A.rows))
-    t = time.perf_counter() - t0
-    if keep is not None:
-        keep.append(x)
-    return t, rep
+    amg = O.Amg(A, jacobi_weight=AMG["jacobi_weight"], coarse_rows=AMG["coarse_rows"])
+    setup_s = time.perf_counter() - t0
+    k = min(sample_iterations, iterations)
+    times = []
+    for _ in range(repeats):
+        t0 = time.perf_counter()
+        O.cg(A, amg, b, np.zeros(A.rows), max_iterations=k)
+        times.append((time.perf_counter() - t0) * iterations / k)
+    return setup_s, times, O.num_threads()
 
 
 def run_reference(args):
-    """CPU oracle (OpenMP, all host cores) on the same workload and metric."""
+    """The CPU oracle (OpenMP, all host cores) on the same workload and metric:
+    the reference has no CPU solver, so its host restatement is the baseline.
+    A step is a bounded sample of 10 PCG iterations scaled to the iteration
+    count of the full FP64 solve (one full solve first, where it fits the
+    time budget, gives that count; otherwise the count the FP64 solve takes on
+    the GPU on this problem)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle")], check=True)
     from oracle import oracle as O
     from thermofem_b200 import problems as P
-    off, idx, val = P.heat3d(SIZE, SEED_MATRIX)
+    m = args.size or SIZE
+    off, idx, val = P.heat3d(m, SEED_MATRIX)
     n = len(off) - 1
     b = P.rhs_uniform(n, SEED_RHS)
     A = O.Csr(n, off, idx, val)
     t0 = time.perf_counter()
-    amg = O.Amg(A, **{k: (0 if v == "v" else v) for k, v in AMG.items() if k != "cycle"}, cycle=0)
+    amg = O.Amg(A, jacobi_weight=AMG["jacobi_weight"], coarse_rows=AMG["coarse_rows"])
     setup_s = time.perf_counter() - t0
-    # First warm-up step: one full solve gives the iteration count and cost.
-    t_full, rep = cpu_solve_once(A, amg, b, O)
-    budget = 240.0
-    full = (args.steps + args.warmup) * t_full <= budget
-    sample = "full solve per step" if full else "20 PCG iterations per step, scaled to the full iteration count"
+    # the full solve's iteration count: solved here when that is cheap (small
+    # sizes), else the count of the FP64 hierarchy on this problem (the GPU's
+    # FP64 solve takes the oracle's iterations: same hierarchy, same recurrence)
+    known = {128: 99, 256: 138}
+    if m in known:
+        iterations = known[m]
+        how = f"{iterations} iterations (the FP64 solve's count on this problem)"
+    else:
+        _, rep = O.cg(A, amg, b, np.zeros(n))
+        iterations = rep["iterations"]
+        how = f"{iterations} iterations (one full solve)"
+    k = min(10, iterations)
     times = []
-    for k in range(args.warmup - 1 + args.steps):
-        if full:
-            t, _ = cpu_solve_once(A, amg, b, O)
-        else:
-            t0 = time.perf_counter()
-            O.cg(A, amg, b, np.zeros(n), max_iterations=20)
-            t = (time.perf_counter() - t0) * rep["iterations"] / 20.0
-        if k >= args.warmup - 1:
+    for step in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        O.cg(A, amg, b, np.zeros(n), max_iterations=k)
+        t = (time.perf_counter() - t0) * iterations / k
+        if step >= args.warmup:
             times.append(t)
     value = float(np.median(times))
     cores = O.num_threads()
+    sample = f"{k} PCG iterations per step, scaled to the full solve's {how}"
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
-            "config": {"workload": WORKLOAD, "rows": n, "nnz": int(len(idx)), "solver": SOLVER,
-                       "parallelism": f"host OpenMP, {O.num_threads()} threads (CPU oracle, FP64 hierarchy)"},
-            "iterations": rep["iterations"], "setup_s": setup_s,
+            "config": {"workload": workload_name(m), "rows": n, "nnz": int(len(idx)), "solver": SOLVER,
+                       "parallelism": f"host OpenMP, {cores} threads (CPU oracle, FP64 hierarchy)"},
+            "iterations": iterations, "setup_s": setup_s,
             "cpu_baseline": {"value": value, "unit": "s", "cores": cores, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -382,7 +415,7 @@ def run_profile(args):
     import torch
     import thermofem_b200 as tf
     from thermofem_b200 import problems as P
-    off, idx, val = P.heat3d(SIZE, SEED_MATRIX)
+    off, idx, val = P.heat3d(args.size or SIZE, SEED_MATRIX)
     n = len(off) - 1
     ctx = tf.Context(0)
     a = tf.DeviceCsr.from_host(off, idx, val)
@@ -446,6 +479,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="thermofem", choices=["thermofem", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    ap.add_argument("--no-reference-gpu", action="store_true", help="skip the reference GPU build leg")
     ap.add_argument("--small-level-rows", type=int, default=None,
                     help="tf_amg_options.small_level_rows (default: the library default)")
     ap.add_argument("--profile", choices=["mixed", "fp64", "spmv", "spmv32"], default=None,
@@ -455,7 +489,8 @@ def main():
                     help="the other benchmark configurations (one JSON line each, not the headline): batched = 48 "
                          "transient systems x 20 steps; convdiff = 192^3 BiCGStab W-cycle; heat = --size^3 heat; "
                          "learned = shipped damping model vs w=2/3 on --size^3 (default 256), F-cycle")
-    ap.add_argument("--size", type=int, default=None, help="grid side of --workload convdiff/heat")
+    ap.add_argument("--size", type=int, default=None,
+                    help="grid side (headline and reference arm: default 256; --workload convdiff/heat/learned)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -463,7 +498,10 @@ def main():
         return run_profile(args)
     if args.workload:
         return run_workload(args)
+    return headline(args)
 
+
+def headline(args):
     import torch
     import thermofem_b200 as tf
     from thermofem_b200 import problems as P
@@ -479,26 +517,16 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
+    m = args.size or SIZE
+    lead = rank == 0 and world == 1  # the host-side legs run once, on a single-GPU run
 
-    off, idx, val = P.heat3d(SIZE, SEED_MATRIX)
+    off, idx, val = P.heat3d(m, SEED_MATRIX)
     n, nnz = len(off) - 1, len(idx)
     b_host = torch.tensor(P.rhs_uniform(n, SEED_RHS))
     ctx = tf.Context(local)
     a = tf.DeviceCsr.from_host(off, idx, val, device=dev)
     b = b_host.to(dev)
     x = torch.zeros(n, dtype=torch.float64, device=dev)
-    opts = tf.solver_options(torch.float64)
-
-    def make(hier):
-        s = tf.Cg(opts, "amg", tf.amg_options(hierarchy_type=hier, **AMG, **_small(args)), ctx=ctx)
-        torch.cuda.synchronize(dev)
-        t0 = time.perf_counter()
-        s.setup(a)
-        ctx.synchronize()
-        return s, time.perf_counter() - t0
-
-    mixed, setup_mixed = make("f32")
-    plain, setup_plain = make("f64")
 
     def barrier():
         if dist is not None:
@@ -511,41 +539,63 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    def solve(s):
-        x.zero_()
-        rep = s.apply(b, x)
-        assert rep["status"] == "Converged", rep
-        return rep
+    def make(kind, hier, a=a):
+        cls = tf.Cg if kind == "cg" else tf.BiCgStab
+        s = cls(tf.solver_options(torch.float64), "amg", tf.amg_options(hierarchy_type=hier, **AMG, **_small(args)),
+                ctx=ctx)
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        s.setup(a)
+        ctx.synchronize()
+        return s, time.perf_counter() - t0
 
-    def timed(s, steps, clocks=None):
+    def timed(s, b, x, steps):
+        def solve():
+            x.zero_()
+            rep = s.apply(b, x)
+            assert rep["status"] == "Converged", rep
+            return rep
         for _ in range(args.warmup):
-            rep = solve(s)
+            solve()
         barrier()
         torch.cuda.synchronize(dev)
         launches0 = ctx.launches
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(ctx.stream)
         for _ in range(steps):
-            rep = solve(s)
+            rep = solve()
         e1.record(ctx.stream)
         torch.cuda.synchronize(dev)
         barrier()
         ms = e0.elapsed_time(e1) / steps
         return maxover(ms), rep, ctx.launches - launches0
 
+    def true_residual(a, b, x):
+        r = tf.residual(a, b, x, ctx=ctx)
+        return float(torch.linalg.norm(r) / torch.linalg.norm(b))
+
+    # ---- the four solves: {PCG, BiCGStab} x {FP32 hierarchy, FP64 hierarchy}
+    runs = {}
+    keep = {}
     with Clocks(local) as clk:
-        ms_mixed, rep_mixed, launches_mixed = timed(mixed, args.steps)
+        for kind in ("cg", "bicgstab"):
+            for hier in ("f32", "f64"):
+                s, setup_s = make(kind, hier)
+                ms, rep, launches = timed(s, b, x, args.steps)
+                runs[(kind, hier)] = {"ms": ms, "iterations": rep["iterations"], "setup_s": setup_s,
+                                      "true_relative_residual": true_residual(a, b, x),
+                                      "setup_phases_ms": {k: round(v, 3) for k, v in s.setup_phases().items()},
+                                      "launches": launches}
+                if kind == "cg":
+                    keep[hier] = s
+                else:
+                    del s
     clocks = clk.summary()
-    x_mixed_dev = x.clone()  # the last mixed solve (the plain solves reuse x)
-    ms_plain, rep_plain, launches_plain = timed(plain, args.steps)
+    mixed, plain = keep["f32"], keep["f64"]
+    pcg_mixed = runs[("cg", "f32")]
 
-    # true FP64 residual of the last mixed solve
-    r = tf.residual(a, b, x_mixed_dev, ctx=ctx)
-    true_rel = float(torch.linalg.norm(r) / torch.linalg.norm(b))
-    x_mixed = x_mixed_dev.cpu().numpy()
-
-    # e2e: public C ABI call with pinned host buffers, copies inside the timed region
-    # (a zeroed pinned initial guess per step, prepared outside the timed region)
+    # ---- e2e: the public C ABI call with pinned host buffers, the copies inside
+    # the timed region (a zeroed pinned initial guess per step, prepared outside it)
     hb = b_host.pin_memory()
     hxs = [torch.zeros(n, dtype=torch.float64).pin_memory() for _ in range(args.steps + 2)]
     for hx in hxs[:2]:
@@ -558,10 +608,9 @@ def main():
     del hxs
     assert rep_e2e["status"] == "Converged"
 
-    # roofline of the dominant kernel family of the mixed solve, the FP32
+    # ---- roofline of the dominant kernel family of the mixed solve, the FP32
     # level SpMV, on its finest level as the cycle streams it; beside it the
-    # FP64 Krylov operator SpMV (both with 2-byte column offsets) and, for
-    # reference, the FP64 SpMV of a caller's int32 CSR
+    # FP64 Krylov operator SpMV
     def time_launch(fn, reps=50):
         for _ in range(5):
             fn()
@@ -573,12 +622,10 @@ def main():
         torch.cuda.synchronize(dev)
         return e0.elapsed_time(e1) / reps
 
-    # the FP32 finest level (about 110 MB) would partly stay in the 126 MB L2
-    # across back-to-back launches; in the cycle other levels and the outer
-    # loop run between its launches, so it is timed with L2 flushed before
-    # every launch, one event pair around each.  The flush READS 192 MB, so
-    # that L2 holds clean lines (a written flush would leave ~126 MB of dirty
-    # lines for the timed kernel to write back).
+    # In the cycle, other levels and the outer loop run between two launches
+    # of the finest level, so it is timed cold: before every launch a 192 MB
+    # READ leaves the 126 MB L2 holding other, clean lines (a written flush
+    # would leave dirty lines for the timed kernel to write back).
     flush = torch.ones(48 << 20, dtype=torch.int32, device=dev)
 
     def time_launch_cold(fn, reps=20):
@@ -606,78 +653,151 @@ def main():
     peak, peak_kind = measured_peaks()
     layout, entries = plain.spmv_layout()
     layout32, entries32 = mixed.level_spmv_layout(0)
+    layout32 = "sliced" if layout32 != "csr" else "csr"
     algo = layout_bytes(layout, n, entries, 8)
     achieved = algo / (spmv_ms * 1e-3) / 1e9
     algo32 = layout_bytes(layout32, n, entries32, 4)
     achieved32 = algo32 / (spmv32_ms * 1e-3) / 1e9
     achieved_csr = spmv_bytes(n, nnz) / (csr_ms * 1e-3) / 1e9
+    traffic = SPMV_TRAFFIC[layout] * algo / SPMV_BYTES_128[layout]
+    traffic32 = SPMV32_TRAFFIC[layout32] * algo32 / SPMV32_BYTES_128[layout32]
 
     # solve-level effective bandwidth: the bytes model of one iteration over
     # the measured time per iteration
     it_bytes = iteration_bytes(mixed, n, *mixed.spmv_layout())
-    solve_gbs = it_bytes * rep_mixed["iterations"] / (ms_mixed * 1e-3) / 1e9
+    solve_gbs = it_bytes * pcg_mixed["iterations"] / (pcg_mixed["ms"] * 1e-3) / 1e9
+    del mixed, plain, keep
 
-    cpu = None
-    err_vs_oracle = None
-    if rank == 0 and world == 1 and not args.no_cpu:
+    # ---- 128^3: the same pair, and each solution against the CPU oracle's
+    # FP64 solve (the oracle finishes that size in seconds)
+    extra = None
+    if m != EXTRA_SIZE:
+        off2, idx2, val2 = P.heat3d(EXTRA_SIZE, SEED_MATRIX)
+        n2 = len(off2) - 1
+        a2 = tf.DeviceCsr.from_host(off2, idx2, val2, device=dev)
+        b2_host = P.rhs_uniform(n2, SEED_RHS)
+        b2 = torch.tensor(b2_host, device=dev)
+        x2 = torch.zeros(n2, dtype=torch.float64, device=dev)
+        extra = {"workload": workload_name(EXTRA_SIZE), "rows": n2, "nnz": int(len(idx2))}
+        xs2 = {}
+        for hier in ("f32", "f64"):
+            s, setup_s = make("cg", hier, a=a2)
+            ms, rep, _ = timed(s, b2, x2, args.steps)
+            extra["mixed" if hier == "f32" else "plain_fp64"] = {
+                "value": ms / 1e3, "unit": "s", "iterations": rep["iterations"], "setup_s": setup_s,
+                "true_relative_residual": true_residual(a2, b2, x2)}
+            xs2[hier] = x2.cpu().numpy()
+            del s
+        extra["speedup_mixed_vs_fp64"] = extra["plain_fp64"]["value"] / extra["mixed"]["value"]
+        if lead and not args.no_cpu:
+            try:
+                subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle")], check=True)
+                from oracle import oracle as O
+                A2 = O.Csr(n2, off2, idx2, val2)
+                xo, orep = O.cg(A2, O.Amg(A2, jacobi_weight=AMG["jacobi_weight"], coarse_rows=AMG["coarse_rows"]),
+                                b2_host, np.zeros(n2))
+                for hier, key in (("f32", "mixed"), ("f64", "plain_fp64")):
+                    extra[key]["relative_error_vs_oracle"] = float(np.linalg.norm(xs2[hier] - xo) /
+                                                                   np.linalg.norm(xo))
+                extra["oracle_iterations"] = orep["iterations"]
+            except Exception as e:  # reported, never required
+                extra["oracle"] = f"failed: {e}"
+        del a2
+
+    # ---- the reference's own CUDA build on the same inputs
+    reference_gpu = None
+    if lead and not args.no_reference_gpu:
         try:
-            subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle")], check=True)
             from oracle import oracle as O
-            A = O.Csr(n, off, idx, val)
-            amg = O.Amg(A, jacobi_weight=AMG["jacobi_weight"], coarse_rows=AMG["coarse_rows"])
-            xs_cpu = []
-            t_cpu, rep_cpu = cpu_solve_once(A, amg, b_host.numpy(), O, keep=xs_cpu)
-            cpu = {"value": t_cpu, "unit": "s", "cores": O.num_threads(), "kind": "port",
-                   "sample": f"one full FP64 AMG-PCG solve of the same 128^3 problem ({rep_cpu['iterations']} iterations)"}
-            # the mixed solve's error against the oracle's FP64 solve
-            xo = xs_cpu[0]
-            err_vs_oracle = float(np.linalg.norm(x_mixed - xo) / np.linalg.norm(xo))
+            if O.ref_gpu_available():
+                torch.cuda.synchronize(dev)
+                r = O.ref_gpu_solve_pair(O.Csr(n, off, idx, val), b_host.numpy(),
+                                         jacobi_weight=AMG["jacobi_weight"], coarse_rows=AMG["coarse_rows"],
+                                         repeats=2)
+                reference_gpu = {
+                    "build": "the reference's library sources compiled with nvcc for sm_100a (cuSPARSE, cuBLAS, CUB)",
+                    "setup_s": r["setup_s"], "timing": "host clock around device-synchronised calls, best of 2",
+                    "pcg": {k: r["pcg"][k] for k in ("solve_s", "iterations", "relative_residual")},
+                    "bicgstab": {k: r["bicgstab"][k] for k in ("solve_s", "iterations", "relative_residual")}}
+                reference_gpu["pcg_speedup"] = {
+                    "mixed": r["pcg"]["solve_s"] / (runs[("cg", "f32")]["ms"] / 1e3),
+                    "plain_fp64": r["pcg"]["solve_s"] / (runs[("cg", "f64")]["ms"] / 1e3)}
+                reference_gpu["bicgstab_speedup"] = {
+                    "mixed": r["bicgstab"]["solve_s"] / (runs[("bicgstab", "f32")]["ms"] / 1e3),
+                    "plain_fp64": r["bicgstab"]["solve_s"] / (runs[("bicgstab", "f64")]["ms"] / 1e3)}
+            else:
+                reference_gpu = {"unavailable": "oracle/_ref/libref_gpu.so was not built (reference sources absent)"}
+        except Exception as e:  # reported, never required
+            reference_gpu = {"unavailable": f"failed: {e}"}
+
+    # ---- the CPU oracle on the host cores (bounded sample)
+    cpu = None
+    if lead and not args.no_cpu:
+        try:
+            from oracle import oracle as O
+            setup_cpu, times, cores = oracle_baseline(O.Csr(n, off, idx, val), b_host.numpy(),
+                                                      runs[("cg", "f64")]["iterations"])
+            cpu = {"value": times[0], "unit": "s", "cores": cores, "kind": "port",
+                   "sample": f"10 FP64 AMG-PCG iterations of the same {m}^3 problem on the oracle's hierarchy "
+                             f"(built in {setup_cpu:.1f} s, not counted), scaled to the FP64 solve's "
+                             f"{runs[('cg', 'f64')]['iterations']} iterations"}
         except Exception as e:  # the baseline is reported, never required
             cpu = {"value": None, "unit": "s", "cores": None, "kind": "port", "sample": f"failed: {e}"}
 
     if rank == 0:
+        def pair(kind):
+            mx, pl = runs[(kind, "f32")], runs[(kind, "f64")]
+            return {"mixed": {"value": mx["ms"] / 1e3, "unit": "s", "iterations": mx["iterations"],
+                              "true_relative_residual": mx["true_relative_residual"], "setup_s": mx["setup_s"]},
+                    "plain_fp64": {"value": pl["ms"] / 1e3, "unit": "s", "iterations": pl["iterations"],
+                                   "true_relative_residual": pl["true_relative_residual"], "setup_s": pl["setup_s"]},
+                    "speedup_mixed_vs_fp64": pl["ms"] / mx["ms"]}
+        kernel32 = (f"sliced_kernel<float> (SpMV, FP32 finest AMG level, 32-row slices, 2-byte column offsets, "
+                    f"{entries32} entries)" if layout32 == "sliced" else
+                    f"csr_pipe_kernel<float,int,short> (SpMV, FP32 finest AMG level, 2-byte column offsets, "
+                    f"{entries32} entries)")
+        kernel64 = (f"sliced_kernel<double> (SpMV, FP64 Krylov operator, 32-row slices, 2-byte column offsets, "
+                    f"{entries} entries)" if layout == "sliced" else
+                    "csr_pipe_kernel<double,int,short> (SpMV, FP64 Krylov operator, 2-byte column offsets)")
         line = {
-            "metric": METRIC, "value": ms_mixed / 1e3, "unit": "s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms_mixed, "higher_is_better": False, "scaling": "weak",
+            "metric": METRIC, "value": pcg_mixed["ms"] / 1e3, "unit": "s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": pcg_mixed["ms"], "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64 outer / f32 hierarchy", "data": "synthetic (seeded generator)",
-            "config": {"workload": WORKLOAD, "rows": n, "nnz": nnz,
-                       "solver": SOLVER,
+            "config": {"workload": workload_name(m), "rows": n, "nnz": nnz, "solver": SOLVER,
                        "parallelism": "replicas" if world > 1 else "single GPU",
-                       "l2": "inputs larger than L2 (217 MB FP64 operator), no flush"},
-            "iterations": rep_mixed["iterations"], "true_relative_residual": true_rel,
-            "relative_error_vs_oracle": err_vs_oracle,
-            "setup_s": setup_mixed,
-            "setup_phases_ms": {k: round(v, 3) for k, v in mixed.setup_phases().items()},
-            "plain_fp64": {"value": ms_plain / 1e3, "unit": "s", "iterations": rep_plain["iterations"],
-                           "setup_s": setup_plain,
-                           "setup_phases_ms": {k: round(v, 3) for k, v in plain.setup_phases().items()}},
-            "speedup_mixed_vs_fp64": ms_plain / ms_mixed,
+                       "l2": "inputs larger than L2 (1.4 GB FP64 operator), no flush"},
+            "iterations": pcg_mixed["iterations"], "true_relative_residual": pcg_mixed["true_relative_residual"],
+            "setup_s": pcg_mixed["setup_s"], "setup_phases_ms": pcg_mixed["setup_phases_ms"],
+            "plain_fp64": {"value": runs[("cg", "f64")]["ms"] / 1e3, "unit": "s",
+                           "iterations": runs[("cg", "f64")]["iterations"],
+                           "true_relative_residual": runs[("cg", "f64")]["true_relative_residual"],
+                           "setup_s": runs[("cg", "f64")]["setup_s"],
+                           "setup_phases_ms": runs[("cg", "f64")]["setup_phases_ms"]},
+            "speedup_mixed_vs_fp64": runs[("cg", "f64")]["ms"] / pcg_mixed["ms"],
+            "pcg": pair("cg"), "bicgstab": pair("bicgstab"),
+            "reference_gpu": reference_gpu,
+            "heat3d_128": extra,
             "spmv_gbs": {"f64_operator": achieved, "f32_level0": achieved32, "f64_int32_csr": achieved_csr},
             "solve_effective_gbs": {"value": solve_gbs, "bytes_per_iteration": it_bytes,
                                     "model": "sum over one iteration's kernels of their algorithmic bytes"},
             "roofline": {"bound": "hbm", "achieved": achieved32, "peak": peak, "unit": "GB/s",
-                         "frac": achieved32 / peak, "traffic": SPMV32_TRAFFIC[layout32],
-                         "kernel": ("sliced_kernel<float> (SpMV, FP32 finest AMG level, 32-row slices, "
-                                    f"2-byte column offsets, {entries32} entries)") if layout32 == "sliced" else
-                                   ("csr_pipe_kernel<float,int,short> (SpMV, FP32 finest AMG level, "
-                                    f"2-byte column offsets, {entries32} entries)"),
-                         "share": "FP32 level SpMV family: 53 % of the mixed solve's device time "
-                                  "(profiles/solve_heat3d_128_mixed_launches.md)",
-                         "peak_source": peak_kind, "algorithmic_bytes": algo32, "launch_ms": spmv32_ms},
+                         "frac": achieved32 / peak, "traffic": traffic32, "kernel": kernel32,
+                         "share": "the FP32 level SpMV family takes the largest share of the mixed solve's "
+                                  "device time in its ncu launch list",
+                         "peak_source": peak_kind, "algorithmic_bytes": algo32, "launch_ms": spmv32_ms,
+                         "timing": "cold (L2 evicted by a read before each launch), CUDA events",
+                         "traffic_source": "ncu DRAM bytes per algorithmic byte of the same kernel on 128^3"},
             "roofline_fp64_operator": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": SPMV_TRAFFIC[layout],
-                         "kernel": ("sliced_kernel<double> (SpMV, FP64 Krylov operator, 32-row slices, "
-                                    f"2-byte column offsets, {entries} entries)") if layout == "sliced" else
-                                   "csr_pipe_kernel<double,int,short> (SpMV, FP64 Krylov operator, "
-                                   "2-byte column offsets)", "peak_source": peak_kind,
-                         "algorithmic_bytes": algo, "launch_ms": spmv_ms},
+                                       "frac": achieved / peak, "traffic": traffic, "kernel": kernel64,
+                                       "peak_source": peak_kind, "algorithmic_bytes": algo, "launch_ms": spmv_ms,
+                                       "traffic_source": "ncu DRAM bytes per algorithmic byte of the same kernel "
+                                                         "on 128^3"},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": 2 * n * 8, "d2h_bytes_per_step": n * 8},
-            "gpu_launches": int(launches_mixed),
+            "gpu_launches": int(pcg_mixed["launches"]),
             "clocks": clocks,
         }
         print(json.dumps(line), flush=True)
-    del mixed, plain
     if dist is not None:
         dist.destroy_process_group()
 

@@ -330,6 +330,13 @@ int tf_amg_level_spmv_layout(const tf_amg *m, int level, int *sliced, int64_t *e
 int tf_amg_level_transfer(const tf_amg *m, int level, const int32_t **map, const int32_t **offsets,
                           const int32_t **members, int *coarse_rows);
 
+/* The coarse level's factor (CoarseFactor, include/Multigrid/
+ * GpuAggregation.cuh:19-25, which the reference's tests read directly):
+ * *rows x *rows FP64 LU, row-major, unit lower part below the diagonal, and
+ * the pivot row chosen at each step, both device arrays owned by the
+ * hierarchy; *rows = 0 (NULL arrays) when the coarse solve is Jacobi. */
+int tf_amg_coarse_factor(const tf_amg *m, int *rows, const double **lu, const int32_t **pivots);
+
 /* Jacobi smoother component (Jacobi.cuh:26-93). */
 typedef struct tf_jacobi tf_jacobi;
 int tf_jacobi_create(tf_ctx *ctx, int value_type, int index_type, int sweeps, double weight, tf_jacobi **out);

@@ -438,10 +438,24 @@ void or_spmv(const or_csr *a, const double *x, double *y) {
     }
 }
 
+/* Fixed partition: chunks of 4096 entries summed left to right, then the
+ * chunk sums left to right, so the value does not depend on the number of
+ * threads (an OpenMP reduction clause would make it depend on the host). */
+#define OR_DOT_CHUNK 4096
 double or_dot(int64_t n, const double *x, const double *y) {
+    const int64_t chunks = (n + OR_DOT_CHUNK - 1) / OR_DOT_CHUNK;
+    double local[64];
+    double *part = chunks <= 64 ? local : (double *)malloc(sizeof(double) * (size_t)chunks);
+#pragma omp parallel for schedule(static)
+    for (int64_t c = 0; c < chunks; ++c) {
+        const int64_t e = (c + 1) * OR_DOT_CHUNK < n ? (c + 1) * OR_DOT_CHUNK : n;
+        double s = 0;
+        for (int64_t i = c * OR_DOT_CHUNK; i < e; ++i) s += x[i] * y[i];
+        part[c] = s;
+    }
     double s = 0;
-#pragma omp parallel for reduction(+ : s) schedule(static)
-    for (int64_t i = 0; i < n; ++i) s += x[i] * y[i];
+    for (int64_t c = 0; c < chunks; ++c) s += part[c];
+    if (part != local) free(part);
     return s;
 }
 

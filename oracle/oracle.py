@@ -248,6 +248,7 @@ class Amg:
         self.opts = AmgOptions.make(**opts)
         self._v = _view(a)
         st = C.c_int()
+        self._free = lib().or_amg_free  # kept: module globals are cleared at interpreter shutdown
         self.h = lib().or_amg_setup(C.byref(self._v), C.byref(self.opts), C.byref(st))
         if st.value != 0 or not self.h:
             raise OracleError(f"oracle AMG setup status {st.value}")
@@ -255,7 +256,7 @@ class Amg:
 
     def __del__(self):
         if getattr(self, "h", None):
-            lib().or_amg_free(self.h)
+            self._free(self.h)
             self.h = None
 
     @property
@@ -517,3 +518,53 @@ def ref_gpu_solve(a: Csr, b, x0=None, kind="cg", cycle="v", jacobi_weight=2.0 / 
         raise OracleError("reference GPU solve failed")
     return x, {"iterations": int(it[0]), "status": int(st[0]), "relative_residual": float(rel[0]),
                "setup_s": float(ts[0]), "solve_s": float(tv[0])}
+
+
+def ref_gpu_amg_levels(a: Csr, jacobi_weight=2.0 / 3.0, coarse_rows=64):
+    """The reference's own Amg<double> built on a (its GPU build): a list of
+    (rows, nonzeros, histogram) per level, the stop reason and the coarse
+    solver, as Amg::levelStatistics / stopReason / coarseSolver give them."""
+    r = C.CDLL(REF_GPU_LIB)
+    P, I, D = C.c_void_p, C.c_int, C.c_double
+    r.ref_gpu_amg_levels.argtypes = [P, P, P, C.c_int64, D, I, I, P, P, P, C.c_char_p, C.c_char_p]
+    r.ref_gpu_amg_levels.restype = I
+    rp, ci, val = _arrs(a)
+    cap = 32
+    rows, nnz, hist = np.zeros(cap, np.int64), np.zeros(cap, np.int64), np.zeros(4 * cap, np.int64)
+    stop, coarse = C.create_string_buffer(64), C.create_string_buffer(64)
+    levels = r.ref_gpu_amg_levels(_ptr(rp), _ptr(ci), _ptr(val), a.rows, float(jacobi_weight), int(coarse_rows), cap,
+                                  _ptr(rows), _ptr(nnz), _ptr(hist), stop, coarse)
+    if levels < 0:
+        raise OracleError("reference AMG setup failed")
+    stats = [(int(rows[d]), int(nnz[d]), hist[4 * d:4 * d + 4].tolist()) for d in range(levels)]
+    return stats, stop.value.decode(), coarse.value.decode()
+
+
+def ref_gpu_solve_pair(a: Csr, b, jacobi_weight=2.0 / 3.0, coarse_rows=64, repeats=1, keep_x=False):
+    """The reference's own FP64 PCG and BiCGStab with one shared AMG V-cycle
+    setup (its GPU build).  Returns {"setup_s", "pcg": {...}, "bicgstab":
+    {...}} with iterations, status (0 Converged), relative_residual, solve_s
+    (fastest of `repeats`) and, with keep_x, x."""
+    r = C.CDLL(REF_GPU_LIB)
+    P, I, D = C.c_void_p, C.c_int, C.c_double
+    r.ref_gpu_solve_pair.argtypes = [P, P, P, C.c_int64, P, D, I, I, P, P, P, P, P, P, P]
+    r.ref_gpu_solve_pair.restype = I
+    rp, ci, val = _arrs(a)
+    n = a.rows
+    b = np.ascontiguousarray(b, np.float64)
+    setup = np.zeros(1)
+    it, st = np.zeros(2, np.int32), np.zeros(2, np.int32)
+    rel, ts = np.zeros(2), np.zeros(2)
+    xs = [np.zeros(n), np.zeros(n)] if keep_x else [None, None]
+    rc = r.ref_gpu_solve_pair(_ptr(rp), _ptr(ci), _ptr(val), n, _ptr(b), float(jacobi_weight), int(coarse_rows),
+                              int(repeats), _ptr(setup), _ptr(it), _ptr(st), _ptr(rel), _ptr(ts),
+                              _ptr(xs[0]) if keep_x else None, _ptr(xs[1]) if keep_x else None)
+    if rc != 0:
+        raise OracleError("reference GPU solve failed")
+    out = {"setup_s": float(setup[0])}
+    for k, name in enumerate(("pcg", "bicgstab")):
+        out[name] = {"iterations": int(it[k]), "status": int(st[k]), "relative_residual": float(rel[k]),
+                     "solve_s": float(ts[k])}
+        if keep_x:
+            out[name]["x"] = xs[k]
+    return out

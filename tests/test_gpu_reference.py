@@ -4,10 +4,11 @@ The reference library (its Cg / BiCgStab with its aggregation Amg on
 cuSPARSE, cuBLAS and CUB) is compiled for sm_100a from its sources by
 `make -C oracle refgpu` into oracle/_ref/libref_gpu.so; these tests skip
 where that build is absent.  Same inputs, same options (FP64 hierarchy,
-Jacobi w = 2/3, coarse LU <= 64 rows, tolerance 1e-8): the iteration
-counts agree within one and the solutions within 1e-6, as the CPU-oracle
-parity tests require.  The last test also reports both solve times on the
-128^3 benchmark problem.
+Jacobi w = 2/3, coarse LU <= 64 rows, tolerance 1e-8): AMG-preconditioned
+CG takes the same iterations and its solution agrees to 1e-12 relative;
+BiCGStab, which amplifies the two implementations' different reduction
+orders, agrees within one iteration and 1e-6.  The last test also reports
+both solve times on the 128^3 benchmark problem.
 """
 import json
 import os
@@ -52,9 +53,20 @@ def test_solves_match_the_reference_gpu_build(problem, kind, cycle):
     xr, rr = O.ref_gpu_solve(O.Csr(n, *m), b, kind=kind, cycle=cycle)
     _, x, _, rep = _ours(m, b, kind, cycle)
     assert rr["status"] == 0 and rep["status"] == "Converged"
-    assert abs(rep["iterations"] - rr["iterations"]) <= 1, (rep["iterations"], rr["iterations"])
     xo = x.cpu().numpy()
-    assert np.linalg.norm(xo - xr) / np.linalg.norm(xr) < 1e-6
+    err = np.linalg.norm(xo - xr) / np.linalg.norm(xr)
+    print(f"\nvs reference GPU build {problem} {kind}-{cycle}: {rep['iterations']} vs {rr['iterations']} "
+          f"iterations, relative difference {err:.3e}")
+    if kind == "cg":
+        # PCG on the same hierarchy: rounding differences (cuBLAS/cuSPARSE
+        # reduction orders against this library's) stay at rounding level
+        assert rep["iterations"] == rr["iterations"]
+        assert err <= 1e-12
+    else:
+        # BiCGStab amplifies them over the iterations (measured 1e-12 on
+        # heat 24^3, 1e-9 on convection-diffusion 20^3)
+        assert abs(rep["iterations"] - rr["iterations"]) <= 1, (rep["iterations"], rr["iterations"])
+        assert err < 1e-6
 
 
 @pytest.mark.parametrize("case", ["laplace2d-128", "w-0.75", "coarse-16", "identity-cg", "identity-bicgstab"])
@@ -87,10 +99,13 @@ def test_more_solves_match_the_reference_gpu_build(case):
     if precond == "identity":
         slack = max(1, rr["iterations"] // (50 if kind == "cg" else 4))
         tol = 1e-4
-    else:
-        slack, tol = 1, 1e-6
+    else:  # AMG-preconditioned CG: rounding level, as above
+        slack, tol = 0, 1e-12
     assert abs(rep["iterations"] - rr["iterations"]) <= slack, (rep["iterations"], rr["iterations"])
-    assert np.linalg.norm(x.cpu().numpy() - xr) / np.linalg.norm(xr) < tol
+    err = np.linalg.norm(x.cpu().numpy() - xr) / np.linalg.norm(xr)
+    print(f"\nvs reference GPU build {case}: {rep['iterations']} vs {rr['iterations']} iterations, "
+          f"relative difference {err:.3e}")
+    assert err <= tol
 
 
 def test_reference_gpu_build_on_the_benchmark_problem(capsys):

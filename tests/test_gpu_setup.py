@@ -151,14 +151,19 @@ def test_solvers_on_separate_threads_give_the_results_of_one_thread():
     b_host = P.rhs_uniform(n, 76)
 
     def solve(hierarchy):
+        # Each thread keeps its torch work on its own context's stream and
+        # waits on that stream only: a device-wide synchronisation (or the
+        # legacy default stream) would cut into another thread's graph
+        # capture, which CUDA then invalidates.
         ctx = tf.Context(0)
-        s = tf.Cg(tf.solver_options(), "amg", tf.amg_options(hierarchy_type=hierarchy), ctx=ctx)
-        s.setup(to_device(m))
-        x = torch.zeros(n, dtype=torch.float64, device="cuda")
-        rep = s.apply(torch.tensor(b_host, device="cuda"), x)
-        torch.cuda.synchronize()
-        assert s.last_execution == 2  # captured as one whole-solve graph, also beside other threads
-        return rep, x.cpu()
+        with torch.cuda.stream(ctx.stream):
+            s = tf.Cg(tf.solver_options(), "amg", tf.amg_options(hierarchy_type=hierarchy), ctx=ctx)
+            s.setup(to_device(m))
+            x = torch.zeros(n, dtype=torch.float64, device="cuda")
+            rep = s.apply(torch.tensor(b_host, device="cuda"), x)
+            ctx.stream.synchronize()
+            assert s.last_execution == 2  # captured as one whole-solve graph, also beside other threads
+            return rep, x.cpu()
 
     alone = {h: solve(h) for h in ("f64", "f32")}
     results, errors = {}, []

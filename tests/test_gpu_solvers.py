@@ -236,11 +236,17 @@ def test_heat3d_solve_matches_oracle(ctx, kind, hierarchy):
     ora = O.Amg(A, **opts)
     xo, orep = (O.cg if kind == "cg" else O.bicgstab)(A, ora, b, np.zeros(n))
     assert orep["status"] == "Converged"
-    if hierarchy is None:  # same precision, same recurrence: same iteration count up to rounding
-        assert abs(rep["iterations"] - orep["iterations"]) <= 1
+    err = np.linalg.norm(xv - xo) / np.linalg.norm(xo)
+    print(f"\nheat3d 24^3 {kind} hierarchy={hierarchy}: {rep['iterations']} vs oracle {orep['iterations']} "
+          f"iterations, relative difference {err:.3e}")
+    if hierarchy is None:
+        # same precision, same hierarchy bits, same recurrence: the same
+        # iterations, and the solutions differ only by rounding
+        assert rep["iterations"] == orep["iterations"]
+        assert err <= 1e-12
     else:  # FP32 cycle: a different trajectory, but no more than 25% more iterations
         assert rep["iterations"] <= 1.25 * orep["iterations"] + 2
-    assert np.linalg.norm(xv - xo) / np.linalg.norm(xo) < 1e-6
+        assert err < 1e-6
 
 
 def test_host_buffer_apply(ctx):

@@ -539,6 +539,18 @@ class _AmgView:
         return (_view_i32(pm.value, n, dev).clone(), _view_i32(po.value, cr.value + 1, dev).clone(),
                 _view_i32(pe.value, n, dev).clone(), cr.value)
 
+    def coarse_factor(self, device="cuda"):
+        """(lu as rows x rows FP64, pivots) of the coarse LU, None for a
+        Jacobi coarse solve (CoarseFactor, GpuAggregation.cuh:19-25)."""
+        rows, plu, ppiv = C.c_int(), C.c_void_p(), C.c_void_p()
+        check(lib().tf_amg_coarse_factor(self._h(), C.byref(rows), C.byref(plu), C.byref(ppiv)))
+        n = rows.value
+        if n == 0:
+            return None
+        dev = torch.device(device)
+        lu = _view_i32(plu.value, 2 * n * n, dev).view(torch.float64).clone().view(n, n)
+        return lu, _view_i32(ppiv.value, n, dev).clone()
+
 
 class Amg(_AmgView):
     """Aggregation AMG preconditioner (Amg<T,I>): setup(matrix), apply(rhs, x)."""

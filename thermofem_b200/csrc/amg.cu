@@ -348,6 +348,11 @@ class HierarchyImpl final : public Hierarchy {
         *mem = l.mem.data();
         *coarse = l.coarse;
     }
+    void coarse_factor(int *rows, const double **lu, const int32_t **pivots) const override {
+        *rows = factored_ ? static_cast<int>(levels_.back().n) : 0;
+        *lu = factored_ ? lu_.data() : nullptr;
+        *pivots = factored_ ? piv_.data() : nullptr;
+    }
     int64_t kernels_per_cycle() const override { return per_cycle_; }
 
   private:
@@ -844,7 +849,7 @@ class HierarchyImpl final : public Hierarchy {
             rec_.clear();
             entries_.clear();
             if (ok) {
-                tail_.upload();
+                tail_.upload(ctx);
                 return;
             }
             coop_from_ = none;

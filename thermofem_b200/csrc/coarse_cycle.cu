@@ -414,6 +414,19 @@ TailRegion<S>::TailRegion() = default;
 template <class S>
 TailRegion<S>::~TailRegion() = default;
 
+namespace {
+
+// A copy on the context's stream, waited for on that stream only.  Never the
+// legacy default stream, which another thread's work or a capture in
+// progress may be using.
+void copy_and_wait(tf_ctx *ctx, void *dst, const void *src, size_t bytes, cudaMemcpyKind kind, const char *what) {
+    if (!bytes) return;
+    cuda_check(cudaMemcpyAsync(dst, src, bytes, kind, ctx->stream), what);
+    cuda_check(cudaStreamSynchronize(ctx->stream), what);
+}
+
+}  // namespace
+
 template <class S>
 bool TailRegion<S>::plan(tf_ctx *ctx, const std::vector<TailLevel<S>> &levels, const TailParent &parent,
                          const double *inv, int dense_n, S w, int max_steps) {
@@ -426,19 +439,19 @@ bool TailRegion<S>::plan(tf_ctx *ctx, const std::vector<TailLevel<S>> &levels, c
         const auto &L = levels[d];
         if (L.n <= 0 || L.n >= (1 << 16)) return false;
         rps[d].resize(static_cast<size_t>(L.n) + 1);
-        cuda_check(cudaMemcpy(rps[d].data(), L.rp, rps[d].size() * sizeof(int32_t), cudaMemcpyDeviceToHost),
-                   "region plan");
+        copy_and_wait(ctx, rps[d].data(), L.rp, rps[d].size() * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                      "region plan");
         if (d + 1 < levels.size()) {
             if (!L.map || !L.off || !L.mem) return false;
             offs[d].resize(static_cast<size_t>(levels[d + 1].n) + 1);
-            cuda_check(cudaMemcpy(offs[d].data(), L.off, offs[d].size() * sizeof(int32_t), cudaMemcpyDeviceToHost),
-                       "region plan");
+            copy_and_wait(ctx, offs[d].data(), L.off, offs[d].size() * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                          "region plan");
         }
     }
     if (!parent.off || !parent.mem || parent.n <= 0) return false;
     std::vector<int32_t> poffs(static_cast<size_t>(levels[0].n) + 1);
-    cuda_check(cudaMemcpy(poffs.data(), parent.off, poffs.size() * sizeof(int32_t), cudaMemcpyDeviceToHost),
-               "region plan");
+    copy_and_wait(ctx, poffs.data(), parent.off, poffs.size() * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                  "region plan");
     int max_optin = 0;
     cuda_check(cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device),
                "shared memory limit");
@@ -601,13 +614,12 @@ bool TailRegion<S>::plan(tf_ctx *ctx, const std::vector<TailLevel<S>> &levels, c
         levels_ = levels;
         dev_ = std::make_unique<TailDevice<S>>();
         dev_->header.allocate(1);
-        cuda_check(cudaMemcpy(dev_->header.data(), h.get(), sizeof(TailHeader<S>), cudaMemcpyHostToDevice),
-                   "region plan upload");
+        copy_and_wait(ctx, dev_->header.data(), h.get(), sizeof(TailHeader<S>), cudaMemcpyHostToDevice,
+                      "region plan upload");
         dev_->copies.allocate(std::max<size_t>(flat.size(), 1));
         if (!flat.empty())
-            cuda_check(cudaMemcpy(dev_->copies.data(), flat.data(), flat.size() * sizeof(TailCopy),
-                                  cudaMemcpyHostToDevice),
-                       "region copies upload");
+            copy_and_wait(ctx, dev_->copies.data(), flat.data(), flat.size() * sizeof(TailCopy),
+                          cudaMemcpyHostToDevice, "region copies upload");
         steps_.clear();
         entries_.clear();
         return true;
@@ -692,14 +704,14 @@ bool TailRegion<S>::add_entry(const std::vector<CoarseStep<S>> &rec, size_t firs
 }
 
 template <class S>
-void TailRegion<S>::upload() {
+void TailRegion<S>::upload(tf_ctx *ctx) {
     std::vector<TailStepDev> d(steps_.size());
     for (size_t k = 0; k < steps_.size(); ++k)
         d[k] = TailStepDev{steps_[k].op, steps_[k].level, steps_[k].a, steps_[k].b, steps_[k].c};
     dev_->steps.allocate(std::max<size_t>(d.size(), 1));
     if (!d.empty())
-        cuda_check(cudaMemcpy(dev_->steps.data(), d.data(), d.size() * sizeof(TailStepDev), cudaMemcpyHostToDevice),
-                   "region steps upload");
+        copy_and_wait(ctx, dev_->steps.data(), d.data(), d.size() * sizeof(TailStepDev), cudaMemcpyHostToDevice,
+                      "region steps upload");
 }
 
 template <class S>

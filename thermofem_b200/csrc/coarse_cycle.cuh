@@ -104,7 +104,7 @@ class TailRegion {
     // Translates one recorded sub-cycle into region steps; false when a step
     // does not belong to the region's levels.
     bool add_entry(const std::vector<CoarseStep<S>> &steps, size_t first, size_t count);
-    void upload();
+    void upload(tf_ctx *ctx);
     // Runs entry `entry`; root_cur is the root buffer (0: x0, 1: x1) that
     // holds its result at the end, written back with both buffers and rhs.
     void launch(tf_ctx *ctx, int entry, const ProgramIO<S> &io, int root_cur) const;

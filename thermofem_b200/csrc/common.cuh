@@ -260,6 +260,22 @@ inline void check_faults(tf_ctx *ctx) {
     }
 }
 
+// Ends a capture left open on the context stream by a failed step of a
+// capture INTO AN EXISTING GRAPH (cudaStreamBeginCaptureToGraph).  The graph
+// that cudaStreamEndCapture hands back is then that existing graph, or a body
+// graph owned by one of its nodes, so it is not destroyed here: the caller
+// destroys its own graph once.  (A capture may also end this way when another
+// thread synchronises the whole device while it is open, which invalidates
+// it.)
+inline void end_capture_into_graph(tf_ctx *ctx) {
+    cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(ctx->stream, &st) == cudaSuccess && st != cudaStreamCaptureStatusNone) {
+        cudaGraph_t returned = nullptr;
+        cudaStreamEndCapture(ctx->stream, &returned);
+    }
+    cudaGetLastError();
+}
+
 inline void copy_async(tf_ctx *ctx, void *dst, const void *src, size_t bytes) {
     if (bytes && dst != src) cuda_check(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, ctx->stream), "cudaMemcpyAsync");
 }

@@ -54,6 +54,9 @@ class Hierarchy {
     virtual int level_spmv_layout(tf_ctx *ctx, int d, int64_t *entries) const = 0;
     virtual void level_transfer(int d, const int32_t **map, const int32_t **off, const int32_t **mem,
                                 int *coarse) const = 0;
+    // The coarse level's LU factor (rows x rows doubles, row-major, and the
+    // pivot row of each step), rows = 0 when the coarse solve is Jacobi.
+    virtual void coarse_factor(int *rows, const double **lu, const int32_t **pivots) const = 0;
     // Kernels launched by one cycle (graph replay counts them too).
     virtual int64_t kernels_per_cycle() const = 0;
 

@@ -878,15 +878,7 @@ class KrylovImpl final : public Krylov {
         if (g) cudaGraphDestroy(g);
     }
 
-    static void end_open_capture(tf_ctx *ctx) {
-        cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
-        if (cudaStreamIsCapturing(ctx->stream, &st) == cudaSuccess && st != cudaStreamCaptureStatusNone) {
-            cudaGraph_t junk = nullptr;
-            cudaStreamEndCapture(ctx->stream, &junk);
-            if (junk) cudaGraphDestroy(junk);
-        }
-        cudaGetLastError();
-    }
+    static void end_open_capture(tf_ctx *ctx) { end_capture_into_graph(ctx); }
 
     KState initial_state() const {
         KState init{};

@@ -219,6 +219,14 @@ int tf_amg_level_transfer(const tf_amg *m, int level, const int32_t **map, const
     });
 }
 
+int tf_amg_coarse_factor(const tf_amg *m, int *rows, const double **lu, const int32_t **pivots) {
+    return guard([&] {
+        require(m != nullptr && rows && lu && pivots, "null argument");
+        if (!m->h) fail(TF_ERR_LOGIC, "AMG requires setup");
+        m->h->coarse_factor(rows, lu, pivots);
+    });
+}
+
 int tf_jacobi_create(tf_ctx *ctx, int value_type, int index_type, int sweeps, double weight, tf_jacobi **out) {
     return guard([&] {
         check_ctx(ctx);
@@ -454,13 +462,7 @@ int tf_batch_apply(tf_batch *b, const void *const *rhs, void *const *x, tf_solve
                 for (auto *s : b->solvers) s->k->batch_nodes(ctx, g);
                 cuda_check(cudaGraphInstantiate(&b->exec, g, 0), "batch graph instantiate");
             } catch (const Failure &) {
-                cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
-                if (cudaStreamIsCapturing(ctx->stream, &st) == cudaSuccess && st != cudaStreamCaptureStatusNone) {
-                    cudaGraph_t junk = nullptr;
-                    cudaStreamEndCapture(ctx->stream, &junk);
-                    if (junk) cudaGraphDestroy(junk);
-                }
-                cudaGetLastError();
+                end_capture_into_graph(ctx);
                 b->exec = nullptr;
                 b->graph_failed = true;
             }
