@@ -54,6 +54,10 @@ extern "C" {
 const char *tf_version(void);
 /* Message of the last failing call on this thread. */
 const char *tf_last_error(void);
+/* The cudaError_t behind the last failing call on this thread when it
+ * failed with TF_ERR_CUDA or TF_ERR_NOMEM, else 0 (the code the
+ * reference's CudaError carries, include/DataStructure/Memory.cuh:52-66). */
+int tf_last_cuda_error(void);
 const char *tf_status_string(int status);
 
 /* ---- execution context ------------------------------------------------- */
@@ -151,6 +155,11 @@ int tf_jacobi_sweep(tf_ctx *ctx, const tf_csr *a, const void *dinv, const void *
 /* Zero-guess sweep x = w * Dinv * b (no SpMV). */
 int tf_jacobi_zero(tf_ctx *ctx, int64_t n, int value_type, const void *dinv, const void *b, void *x, double weight,
                    const float *row_weight);
+/* The Jacobi update on its own, x += w * dinv * (b - ax) with ax = A x formed
+ * by the caller (IterationContext::jacobi, src/LinearAlgebra/
+ * IterationContext.cu:26-32,251-269); x must not alias an input. */
+int tf_jacobi_update(tf_ctx *ctx, int value_type, int64_t n, double weight, const void *dinv, const void *b,
+                     const void *ax, void *x);
 /* Inverse diagonal with duplicate diagonals summed; TF_ERR_INVALID on a
  * missing, zero or nonfinite diagonal or reciprocal (LinearAlgebra/
  * Diagonal.cuh:13-36), computed on the device. */
@@ -218,6 +227,10 @@ int tf_transfer_arrays(const tf_transfer *t, const int32_t **map, const int32_t 
 int tf_transfer_free(tf_transfer *t);
 /* Ac = P^T A P by coordinate mapping and sum (GpuAggregation.cu:136-234). */
 int tf_galerkin(tf_ctx *ctx, const tf_csr *a, const tf_transfer *t, tf_dcsr **out);
+/* The same product from an aggregate map held by the caller
+ * (multigrid::galerkin(a, AggregateTransfer), GpuAggregation.cu:1029-1036):
+ * map[rows] (device) gives each fine row's aggregate in 0..coarse_rows-1. */
+int tf_galerkin_map(tf_ctx *ctx, const tf_csr *a, const int32_t *map, int coarse_rows, tf_dcsr **out);
 
 /* ---- sort / reduce / scan primitives (replace CUB, GpuAggregation.cu:116-211) */
 /* Stable LSD radix sort of (u64 key, f64 value) pairs on bits

@@ -105,6 +105,7 @@ _PP = C.POINTER(C.c_void_p)
 SIGNATURES = {
     "tf_version": ([], C.c_char_p),
     "tf_last_error": ([], C.c_char_p),
+    "tf_last_cuda_error": ([], _I),
     "tf_status_string": ([_I], C.c_char_p),
     "tf_ctx_create": ([_I, _P, _PP], _I),
     "tf_ctx_destroy": ([_P], _I),
@@ -129,6 +130,7 @@ SIGNATURES = {
     "tf_spmv_set_config": ([_P, C.POINTER(Csr), _I, _I, _I, _I], _I),
     "tf_jacobi_sweep": ([_P, C.POINTER(Csr), _P, _P, _P, _P, _D, _P, _P, _P], _I),
     "tf_jacobi_zero": ([_P, _L, _I, _P, _P, _P, _D, _P], _I),
+    "tf_jacobi_update": ([_P, _I, _L, _D, _P, _P, _P, _P], _I),
     "tf_inverse_diagonal": ([_P, C.POINTER(Csr), _P], _I),
     "tf_restrict": ([_P, _I, _L, _P, _P, _P, _P], _I),
     "tf_prolong": ([_P, _I, _L, _P, _P, _P], _I),
@@ -148,6 +150,7 @@ SIGNATURES = {
     "tf_transfer_arrays": ([_P, _PP, _PP, _PP], _I),
     "tf_transfer_free": ([_P], _I),
     "tf_galerkin": ([_P, C.POINTER(Csr), _P, _PP], _I),
+    "tf_galerkin_map": ([_P, C.POINTER(Csr), _P, _I, _PP], _I),
     "tf_radix_sort_pairs_u64f64": ([_P, _L, _P, _P, _P, _P, _I], _I),
     "tf_reduce_by_key_u64f64": ([_P, _L, _P, _P, _I, _P, _P, C.POINTER(C.c_int64)], _I),
     "tf_scan_exclusive_i32": ([_P, _L, _P, _P], _I),

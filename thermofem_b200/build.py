@@ -37,7 +37,8 @@ def _sources():
 def _headers():
     hs = glob.glob(os.path.join(CSRC, "**", "*.cuh"), recursive=True)
     hs += glob.glob(os.path.join(CSRC, "**", "*.h"), recursive=True)
-    hs += glob.glob(os.path.join(ROOT, "include", "**", "*.h*"), recursive=True)
+    # the C ABI header (the C++ component headers under include/ are not part of the library build)
+    hs += glob.glob(os.path.join(ROOT, "include", "*.h"))
     return hs
 
 

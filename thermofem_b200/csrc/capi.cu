@@ -11,9 +11,14 @@ namespace tfb {
 
 namespace {
 thread_local std::string g_last_error;
+thread_local int g_last_cuda = 0;
 }
 
-void set_last_error(const char *msg) { g_last_error = msg ? msg : ""; }
+void set_last_error(const char *msg, int cuda) {
+    g_last_error = msg ? msg : "";
+    g_last_cuda = cuda;
+}
+
 
 namespace {
 
@@ -80,6 +85,7 @@ extern "C" {
 
 const char *tf_version(void) { return "thermofem_b200 0.1.0 (sm_100a)"; }
 const char *tf_last_error(void) { return g_last_error.c_str(); }
+int tf_last_cuda_error(void) { return g_last_cuda; }
 
 const char *tf_status_string(int status) {
     switch (status) {
@@ -365,6 +371,21 @@ int tf_jacobi_zero(tf_ctx *ctx, int64_t n, int value_type, const void *dinv, con
     });
 }
 
+int tf_jacobi_update(tf_ctx *ctx, int value_type, int64_t n, double weight, const void *dinv, const void *b,
+                     const void *ax, void *x) {
+    return guard([&] {
+        check_ctx(ctx);
+        require_vectors(n, {dinv, b, ax, x}, "invalid Jacobi update arguments");
+        require(n == 0 || (x != ax && x != b && x != dinv), "Jacobi update output aliases an input");
+        DeviceScope scope(ctx->device);
+        with_value_type(value_type, [&](auto t) {
+            using T = decltype(t);
+            jacobi_update(ctx, n, static_cast<T>(weight), static_cast<const T *>(dinv), static_cast<const T *>(b),
+                          static_cast<const T *>(ax), static_cast<T *>(x));
+        });
+    });
+}
+
 int tf_inverse_diagonal(tf_ctx *ctx, const tf_csr *a, void *dinv) {
     return guard([&] {
         check_ctx(ctx);
@@ -599,6 +620,22 @@ int tf_galerkin(tf_ctx *ctx, const tf_csr *a, const tf_transfer *t, tf_dcsr **ou
         require(c.rows == t->fine_rows && t->coarse_rows >= 1, "AMG transfer dimension mismatch");
         DeviceScope scope(ctx->device);
         auto m = galerkin(ctx, c, t->map.data(), t->coarse_rows);
+        cuda_check(cudaStreamSynchronize(ctx->stream), "galerkin");
+        *out = m.release();
+    });
+}
+
+int tf_galerkin_map(tf_ctx *ctx, const tf_csr *a, const int32_t *map, int coarse_rows, tf_dcsr **out) {
+    return guard([&] {
+        check_ctx(ctx);
+        require(out && map, "null argument");
+        *out = nullptr;
+        auto c = native_csr(a);
+        require(coarse_rows >= 1 && coarse_rows <= c.rows, "AMG transfer dimension mismatch");
+        DeviceScope scope(ctx->device);
+        if (indices_out_of_range(ctx, c.rows, map, coarse_rows))
+            fail(TF_ERR_INVALID, "aggregate map entry outside 0..coarse_rows-1");
+        auto m = galerkin(ctx, c, map, coarse_rows);
         cuda_check(cudaStreamSynchronize(ctx->stream), "galerkin");
         *out = m.release();
     });

@@ -21,7 +21,8 @@ namespace tfb {
 struct Failure : std::exception {
     int code;
     std::string message;
-    Failure(int c, std::string m) : code(c), message(std::move(m)) {}
+    int cuda{0};  // the cudaError_t behind a TF_ERR_CUDA / TF_ERR_NOMEM, 0 otherwise
+    Failure(int c, std::string m, int cu = 0) : code(c), message(std::move(m)), cuda(cu) {}
     const char *what() const noexcept override { return message.c_str(); }
 };
 
@@ -31,12 +32,14 @@ inline void require(bool ok, const char *msg, int code = TF_ERR_INVALID) {
 }
 inline void cuda_check(cudaError_t e, const char *what) {
     if (e != cudaSuccess) {
-        if (e == cudaErrorMemoryAllocation) fail(TF_ERR_NOMEM, std::string(what) + ": " + cudaGetErrorString(e));
-        fail(TF_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+        const std::string msg = std::string(what) + ": " + cudaGetErrorString(e);
+        throw Failure(e == cudaErrorMemoryAllocation ? TF_ERR_NOMEM : TF_ERR_CUDA, msg, static_cast<int>(e));
     }
 }
 
-void set_last_error(const char *msg);
+// Records the message (and CUDA error code, 0 for none) of a failing call on
+// this thread: tf_last_error / tf_last_cuda_error.
+void set_last_error(const char *msg, int cuda = 0);
 
 // Runs f and converts exceptions to a status (the ABI never throws).
 template <class F>
@@ -45,7 +48,7 @@ int guard(F &&f) noexcept {
         f();
         return TF_OK;
     } catch (const Failure &e) {
-        set_last_error(e.message.c_str());
+        set_last_error(e.message.c_str(), e.cuda);
         return e.code;
     } catch (const std::bad_alloc &) {
         set_last_error("host allocation failed");

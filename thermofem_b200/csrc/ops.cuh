@@ -116,6 +116,10 @@ void restrict_jacobi_zero(tf_ctx *ctx, int64_t nc, const int32_t *off, const int
 // x = w Dinv b
 template <class T>
 void jacobi_zero(tf_ctx *ctx, int64_t n, const T *dinv, const T *b, T *x, T w, const float *row_w);
+template <class T>
+void jacobi_update(tf_ctx *ctx, int64_t n, T w, const T *dinv, const T *b, const T *ax, T *x);
+// True when some of the n indices lies outside [0, limit) (synchronises).
+bool indices_out_of_range(tf_ctx *ctx, int64_t n, const int32_t *idx, int32_t limit);
 // b = S(in), x = w Dinv b (a cycle's input conversion fused with its first sweep)
 template <class S, class T>
 void jacobi_zero_convert(tf_ctx *ctx, int64_t n, const S *dinv, const T *in, S *b, S *x, S w);

@@ -125,6 +125,26 @@ __global__ void jacobi_zero_kernel(int64_t n, const T *__restrict__ dinv, const 
     }
 }
 
+// *bad = 1 when some idx[i] lies outside [0, limit).
+__global__ void index_range_kernel(int64_t n, const int32_t *__restrict__ idx, int32_t limit, int *bad) {
+    pdl_enter();
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        if (idx[i] < 0 || idx[i] >= limit) atomicExch(bad, 1);
+}
+
+// x += w d (b - ax) with ax = A x computed before (IterationContext::jacobi,
+// src/LinearAlgebra/IterationContext.cu:26-32,251-269): the Jacobi update on
+// its own, for callers that form A x themselves.
+template <class T>
+__global__ void jacobi_update_kernel(int64_t n, T w, const T *__restrict__ dinv, const T *__restrict__ b,
+                                     const T *__restrict__ ax, T *__restrict__ x) {
+    pdl_enter();
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        x[i] += w * dinv[i] * (b[i] - ax[i]);
+}
+
 template <class T, class I>
 __global__ void inverse_diagonal_kernel(int64_t n, const I *__restrict__ rp, const I *__restrict__ ci,
                                         const T *__restrict__ val, T *__restrict__ dinv, int *bad) {
@@ -575,6 +595,23 @@ void restrict_jacobi_zero(tf_ctx *ctx, int64_t nc, const int32_t *off, const int
     launch_kernel(ctx, "restrict_jacobi_zero", restrict_jacobi_zero_kernel<T>, grid_for(nc), kBlock, 0, nc, off, mem,
                   fine, b, dinv, x, w);
 }
+
+bool indices_out_of_range(tf_ctx *ctx, int64_t n, const int32_t *idx, int32_t limit) {
+    if (!n) return false;
+    int *bad = static_cast<int *>(ctx->arena(sizeof(int), 1));
+    memset_async(ctx, bad, 0, sizeof(int));
+    launch_kernel(ctx, "index_range", index_range_kernel, stride_grid(ctx, n), kBlock, 0, n, idx, limit, bad);
+    return read_scalar(ctx, bad) != 0;
+}
+
+template <class T>
+void jacobi_update(tf_ctx *ctx, int64_t n, T w, const T *dinv, const T *b, const T *ax, T *x) {
+    if (!n) return;
+    launch_kernel(ctx, "jacobi_update", jacobi_update_kernel<T>, stride_grid(ctx, n), kBlock, 0, n, w, dinv, b, ax, x);
+}
+template void jacobi_update<float>(tf_ctx *, int64_t, float, const float *, const float *, const float *, float *);
+template void jacobi_update<double>(tf_ctx *, int64_t, double, const double *, const double *, const double *,
+                                    double *);
 
 template <class T>
 void jacobi_zero(tf_ctx *ctx, int64_t n, const T *dinv, const T *b, T *x, T w, const float *row_w) {
