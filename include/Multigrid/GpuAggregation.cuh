@@ -87,7 +87,7 @@ class GpuAggregation {
         if (!a.rowCount() || a.rowCount() >= std::size_t(INT_MAX) || a.rowCount() != a.columnCount() ||
             a.nonZeroCount() > std::size_t(INT_MAX / 2) || a.rowOffsets().deviceId() != device())
             throw std::invalid_argument("AMG requires nonempty square int32-capacity CSR on workspace device");
-        return run([&] {
+        return b200::onContext(*ctx_, [&] {
             const tf_csr v = b200::describe(a);
             tf_dcsr *out = nullptr;
             b200::check(tf_canonicalize(ctx_->get(), &v, &out));
@@ -97,14 +97,14 @@ class GpuAggregation {
 
     /// Finite values, a nonzero diagonal with a finite reciprocal on every row.
     void validate(const CsrMatrix<double> &a) {
-        run([&] { rowMaxima(a); });
+        b200::onContext(*ctx_, [&] { rowMaxima(a); });
     }
 
     /// Symmetric strength graph of a (max-merged couplings above threshold).
     CsrMatrix<double> strength(const CsrMatrix<double> &a, double threshold) {
         if (!std::isfinite(threshold) || threshold < 0 || threshold > 1)
             throw std::invalid_argument("Invalid strength threshold");
-        return run([&] {
+        return b200::onContext(*ctx_, [&] {
             CudaBuffer<double> rowMax = rowMaxima(a);
             const tf_csr v = b200::describe(a);
             tf_dcsr *out = nullptr;
@@ -117,7 +117,7 @@ class GpuAggregation {
     /// singleton absorption, aggregates of at most four rows.
     AggregateTransfer aggregate(const CsrMatrix<double> &graph, int rounds, bool absorbSingletons) {
         if (rounds < 1 || rounds > 8 || !graph.rowCount()) throw std::invalid_argument("Invalid matching configuration");
-        return run([&] {
+        return b200::onContext(*ctx_, [&] {
             struct Free {
                 void operator()(tf_transfer *t) const noexcept { tf_transfer_free(t); }
             };
@@ -146,7 +146,7 @@ class GpuAggregation {
     CsrMatrix<double> galerkin(const CsrMatrix<double> &a, const AggregateTransfer &t) {
         if (a.rowCount() != std::size_t(t.fineRows_) || t.coarseRows_ < 1)
             throw std::invalid_argument("AMG transfer dimension mismatch");
-        return run([&] {
+        return b200::onContext(*ctx_, [&] {
             const tf_csr v = b200::describe(a);
             tf_dcsr *out = nullptr;
             b200::check(tf_galerkin_map(ctx_->get(), &v, detail::onDevice(t.aggregate_), t.coarseRows_, &out));
@@ -157,10 +157,6 @@ class GpuAggregation {
   private:
     int device() const noexcept { return ctx_->device(); }
 
-    template <class F>
-    auto run(F &&f) {
-        return b200::onContext(*ctx_, std::forward<F>(f));
-    }
     void copy(void *dst, const void *src, std::size_t bytes) {
         if (bytes)
             thermofem::detail::cudaCall(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, ctx_->stream()),
