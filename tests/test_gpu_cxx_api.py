@@ -19,7 +19,6 @@ import subprocess
 
 import pytest
 
-from oracle import oracle as O
 from thermofem_b200 import problems as P
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -121,3 +120,19 @@ def test_reference_driver_on_these_headers_reports_what_the_reference_reports(tm
             assert float(vo) == pytest.approx(float(vr), rel=1e-9), (k, vo, vr)
         else:
             assert vo == vr, (k, vo, vr)
+
+
+COMPONENT_TESTS = os.path.join(HERE, "cxx", "bin", "component-tests")
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not os.path.exists(COMPONENT_TESTS), reason="component tests not built (make -C tests/cxx)")
+def test_host_driven_component_paths(capsys):
+    # this repository's own C++ tests of what the reference's tests do not
+    # reach: caller-written preconditioners and factory smoothers, which run
+    # the Krylov loop and the cycle from the host, against the fused paths
+    r = subprocess.run([COMPONENT_TESTS], capture_output=True, text=True, timeout=600)
+    ran, passed, skipped, failed = _summary(r.stdout)
+    with capsys.disabled():
+        print(f"\ncomponent tests: {ran} ran, {passed} passed, {skipped} skipped, {failed} failed")
+    assert r.returncode == 0 and failed == 0 and skipped == 0, r.stdout[-6000:]
