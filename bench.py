@@ -42,17 +42,17 @@ EXTRA_SIZE = 128
 SEED_MATRIX, SEED_RHS = 1001, 1002
 AMG = dict(jacobi_weight=2.0 / 3.0, pre_sweeps=1, post_sweeps=1, cycle="v", coarse_rows=64)
 METRIC = "time-to-1e-8 FP64 relative residual (s), AMG-PCG V-cycle, FP32 hierarchy / FP64 outer"
-# DRAM bytes (read + write) of one launch, from ncu captures on the 128^3
-# problem: the FP64 Krylov operator SpMV (its sliced copy, or CSR row tiles)
-# and the FP32 finest-level SpMV of the mixed hierarchy (sliced copy or row
-# tiles), the kernel family that takes most of the mixed solve's time.  On
-# other sizes the traffic per algorithmic byte of the same kernel is applied
-# (the operators are the same stencil, so traffic grows with the bytes).
-SPMV_TRAFFIC = {"sliced": 163197184 + 4258048, "csr": 171013632 + 13778176}
-SPMV32_TRAFFIC = {"sliced": 96349184 + 4392704, "csr": 104301056 + 5819136}
-# the algorithmic bytes of those captured launches (128^3)
-SPMV_BYTES_128 = {"sliced": 179961860, "csr": 187760644}
-SPMV32_BYTES_128 = {"sliced": 104726532, "csr": 112656388}
+# DRAM bytes (read + write) per algorithmic byte of one launch, from ncu
+# captures of the same kernel and layout on the 128^3 problem (FP64 Krylov
+# operator, FP32 finest level of the mixed hierarchy; profiles/).  The
+# operators are one stencil at every size, so traffic grows with the bytes;
+# layouts without a capture report null.
+TRAFFIC_RATIO = {
+    ("f64", "sliced"): (163197184 + 4258048) / 179961860,
+    ("f64", "csr"): (171013632 + 13778176) / 187760644,
+    ("f32", "sliced"): (96349184 + 4392704) / 104726532,
+    ("f32", "csr"): (104301056 + 5819136) / 112656388,
+}
 SOLVER = "PCG / BiCGStab + aggregation AMG V(1,1), Jacobi w=2/3, coarse LU <= 64 rows, rtol 1e-8"
 
 
@@ -69,12 +69,32 @@ def spmv_bytes(n, nnz, vsize=8, isize=4, csize=None):
 
 
 def layout_bytes(layout, n, entries, vsize):
-    """Algorithmic bytes of one SpMV over the storage it streams: the sliced
-    copy (entries incl. padding x (value + 2-byte column), one 4-byte start
-    per 32-row slice, x and y once) or the CSR with 2-byte columns."""
-    if layout == "sliced":
-        return entries * (vsize + 2) + ((n + 31) // 32 + 1) * 4 + 2 * n * vsize
+    """Algorithmic bytes of one SpMV over the storage it streams, x and y once:
+    sliced / sorted copy: entries incl. padding x (value + 2-byte column
+    offset), one 4-byte start per 32-row slice; banded copy: entries incl.
+    padding x value, one 8-byte {offset, mask} per 32 entries, the slice
+    starts; CSR: row offsets and per entry the value and a 2-byte column
+    offset ("csr") or a 4-byte column index ("csr32")."""
+    slices = ((n + 31) // 32 + 1) * 4
+    if layout in ("sliced", "sorted"):
+        return entries * (vsize + 2) + slices + 2 * n * vsize
+    if layout == "banded":
+        return entries * vsize + (entries // 32) * 8 + slices + 2 * n * vsize
+    if layout == "csr32":
+        return spmv_bytes(n, entries, vsize, 4, 4)
     return spmv_bytes(n, entries, vsize, 4, 2)
+
+
+def kernel_name(layout, t, entries):
+    """The kernel that streams a layout, and what it streams."""
+    return {
+        "sliced": f"sliced_kernel<{t}> over the sliced copy (32-row slices, 2-byte column offsets, {entries} entries)",
+        "sorted": f"sliced_kernel<{t}> over the sorted sliced copy ({entries} entries)",
+        "banded": f"sliced_kernel<{t}, BandCols> over the banded copy (32-row slices, one shared column offset per "
+                  f"entry slot, {entries} entries)",
+        "csr": f"csr_pipe_kernel<{t},int,short> over the CSR arrays (2-byte column offsets)",
+        "csr32": f"csr_pipe_kernel<{t},int,int> over the CSR arrays (4-byte column indices)",
+    }[layout]
 
 
 def iteration_bytes(solver, n, op_layout, op_entries):
@@ -98,7 +118,7 @@ def iteration_bytes(solver, n, op_layout, op_entries):
             nb += nd * nd * 8 + 2 * 4 * nd  # dense coarse solve
             break
         layout, entries = solver.level_spmv_layout(d)
-        spmv = layout_bytes("sliced" if layout != "csr" else "csr", nd, entries, 4)
+        spmv = layout_bytes(layout, nd, entries, 4)
         nc = stats[d + 1]["rows"]
         nb += (spmv + 4 * nd) + (spmv + 8 * nd) + (8 * nd + 4 * nd + 4 * nc)
         if d > 0:
@@ -653,14 +673,13 @@ def headline(args):
     peak, peak_kind = measured_peaks()
     layout, entries = plain.spmv_layout()
     layout32, entries32 = mixed.level_spmv_layout(0)
-    layout32 = "sliced" if layout32 != "csr" else "csr"
     algo = layout_bytes(layout, n, entries, 8)
     achieved = algo / (spmv_ms * 1e-3) / 1e9
     algo32 = layout_bytes(layout32, n, entries32, 4)
     achieved32 = algo32 / (spmv32_ms * 1e-3) / 1e9
     achieved_csr = spmv_bytes(n, nnz) / (csr_ms * 1e-3) / 1e9
-    traffic = SPMV_TRAFFIC[layout] * algo / SPMV_BYTES_128[layout]
-    traffic32 = SPMV32_TRAFFIC[layout32] * algo32 / SPMV32_BYTES_128[layout32]
+    traffic = TRAFFIC_RATIO[("f64", layout)] * algo if ("f64", layout) in TRAFFIC_RATIO else None
+    traffic32 = TRAFFIC_RATIO[("f32", layout32)] * algo32 if ("f32", layout32) in TRAFFIC_RATIO else None
 
     # solve-level effective bandwidth: the bytes model of one iteration over
     # the measured time per iteration
@@ -752,13 +771,8 @@ def headline(args):
                     "plain_fp64": {"value": pl["ms"] / 1e3, "unit": "s", "iterations": pl["iterations"],
                                    "true_relative_residual": pl["true_relative_residual"], "setup_s": pl["setup_s"]},
                     "speedup_mixed_vs_fp64": pl["ms"] / mx["ms"]}
-        kernel32 = (f"sliced_kernel<float> (SpMV, FP32 finest AMG level, 32-row slices, 2-byte column offsets, "
-                    f"{entries32} entries)" if layout32 == "sliced" else
-                    f"csr_pipe_kernel<float,int,short> (SpMV, FP32 finest AMG level, 2-byte column offsets, "
-                    f"{entries32} entries)")
-        kernel64 = (f"sliced_kernel<double> (SpMV, FP64 Krylov operator, 32-row slices, 2-byte column offsets, "
-                    f"{entries} entries)" if layout == "sliced" else
-                    "csr_pipe_kernel<double,int,short> (SpMV, FP64 Krylov operator, 2-byte column offsets)")
+        kernel32 = f"SpMV, FP32 finest AMG level: {kernel_name(layout32, 'float', entries32)}"
+        kernel64 = f"SpMV, FP64 Krylov operator: {kernel_name(layout, 'double', entries)}"
         line = {
             "metric": METRIC, "value": pcg_mixed["ms"] / 1e3, "unit": "s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": pcg_mixed["ms"], "higher_is_better": False, "scaling": "weak",

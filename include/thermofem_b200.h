@@ -337,8 +337,11 @@ int tf_amg_level_spmv(const tf_amg *amg, int level, const void *x, void *y);
 /* The storage that SpMV streams (no reference counterpart): *sliced = 1
  * for the operator's sliced copy (32-row slices, entries column-major,
  * 2-byte column offsets; *entries counts its padding too), 2 for a sliced
- * copy whose rows are ordered longest first within each 256-row tile, 0 for
- * the CSR arrays (*entries = nnz). */
+ * copy whose rows are ordered longest first within each 256-row tile, 3 for
+ * a banded copy (32-row slices whose rows share one column offset per entry
+ * slot: values plus one 8-byte {offset, padding mask} pair per 32 entries),
+ * 0 for the CSR arrays with 2-byte column offsets, 4 for the CSR arrays with
+ * their 4-byte column indices (*entries = nnz for 0 and 4). */
 int tf_amg_level_spmv_layout(const tf_amg *m, int level, int *sliced, int64_t *entries);
 int tf_amg_level_transfer(const tf_amg *m, int level, const int32_t **map, const int32_t **offsets,
                           const int32_t **members, int *coarse_rows);

@@ -27,9 +27,10 @@ def test_reference_arm_prints_one_contract_line():
 
 
 def test_algorithmic_bytes_of_the_reported_kernels():
-    # The per-launch byte counts that roofline.achieved divides by, for the
-    # 128^3 benchmark operator: FP64 operator on its sliced copy, FP32
-    # finest level on row tiles (2-byte columns) and on its sliced copy.
+    # The per-launch byte counts that roofline.achieved divides by: the 128^3
+    # benchmark operator on its sliced copy (FP64) and its FP32 finest level
+    # on row tiles and on its sliced copy; the banded copy and 4-byte-column
+    # CSR on the 256^3 operator.
     import sys
     sys.path.insert(0, ROOT)
     import bench
@@ -37,7 +38,11 @@ def test_algorithmic_bytes_of_the_reported_kernels():
     assert bench.layout_bytes("sliced", n, entries, 8) == 179961860
     assert bench.layout_bytes("csr", n, nnz, 4) == 112656388
     assert bench.layout_bytes("sliced", n, entries, 4) == 104726532
+    n2, nnz2 = 16777216, 117047296
+    assert bench.layout_bytes("csr32", n2, nnz2, 8) == 1740111876  # the CSR-int32 bytes of the 256^3 operator
+    banded = bench.layout_bytes("banded", n2, 7 * n2, 8)
+    assert banded == 7 * n2 * 8 + 7 * n2 // 32 * 8 + (n2 // 32 + 1) * 4 + 2 * n2 * 8
+    assert banded < 0.72 * 1740111876
     # ncu traffic per launch sits just below the algorithmic bytes (x partly in L2)
-    assert 0.9 < bench.SPMV_TRAFFIC["sliced"] / 179961860 < 1.0
-    assert 0.9 < bench.SPMV32_TRAFFIC["csr"] / 112656388 < 1.0
-    assert 0.9 < bench.SPMV32_TRAFFIC["sliced"] / 104726532 < 1.0
+    for ratio in bench.TRAFFIC_RATIO.values():
+        assert 0.9 < ratio < 1.0

@@ -427,6 +427,7 @@ def test_sliced_layout_gives_identical_solves(ctx, case, shape, monkeypatch):
     out = []
     # padding bound 10 %: the aggregated levels (30-50 % in row order) keep
     # CSR unless sorted; 50 % (the default): they take row-order slices too
+    monkeypatch.setenv("THERMOFEM_B200_BANDED", "0")  # the 2-byte-offset sliced copy, not the banded one
     for flag, pad in (("0", "10"), ("1", "10"), ("sorted", "10"), ("1", "50")):
         monkeypatch.setenv("THERMOFEM_B200_SLICED", flag)
         monkeypatch.setenv("THERMOFEM_B200_SLICED_PAD", pad)
@@ -453,6 +454,46 @@ def test_sliced_layout_gives_identical_solves(ctx, case, shape, monkeypatch):
         assert out[0][0] == other[0]
         assert torch.equal(out[0][1], other[1])
         assert torch.equal(out[0][2], other[2])
+
+
+@pytest.mark.parametrize("shape", ["0,2", "1,3", "1,8", "0,5", None])
+@pytest.mark.parametrize("case", ["heat3d25-cg-f32", "heat3d25-bicgstab-f64", "heat3d184-cg-f32"])
+def test_banded_layout_gives_identical_solves(ctx, case, shape, monkeypatch):
+    # Stencil operators (the solver's operator, the finest level) carry a
+    # banded copy: 32-row slices whose rows share one column offset per entry
+    # slot, with a padding mask, so SpMV streams values and an 8-byte pair
+    # per 32 entries.  Each row still sums its entries left to right from +0
+    # (padding lanes gather nothing): the same bits as the CSR arrays
+    # (THERMOFEM_B200_SLICED=0), whatever the launch shape.  184^3: couplings
+    # 33,856 rows apart, beyond 2-byte offsets, so the CSR arrays stream
+    # 4-byte columns there.
+    side = int(case.split("-")[0][6:])
+    if side > 100 and shape not in (None, "1,3"):
+        pytest.skip("the large case runs two launch shapes")
+    m = P.heat3d(side, seed=85)
+    n = len(m[0]) - 1
+    b = torch.tensor(P.rhs_uniform(n, 86), device="cuda")
+    solver = tf.BiCgStab if "bicgstab" in case else tf.Cg
+    if shape:
+        monkeypatch.setenv("THERMOFEM_B200_SLICED_SHAPE", shape)
+    out = []
+    for flag in ("0", "1"):
+        monkeypatch.setenv("THERMOFEM_B200_SLICED", flag)
+        s = solver(tf.solver_options(), "amg", tf.amg_options(hierarchy_type=case[-3:], jacobi_weight=2 / 3),
+                   ctx=ctx)
+        s.setup(to_device(m))
+        x = torch.zeros(n, dtype=torch.float64, device="cuda")
+        rep = s.apply(b, x)
+        xs = torch.randn(n, dtype=torch.float64, device="cuda", generator=torch.Generator("cuda").manual_seed(6))
+        out.append((rep, x, s.spmv(xs), s.level_spmv_layout(0)[0], s.spmv_layout()))
+        del s
+    (r0, x0, y0, l0, op0), (r1, x1, y1, l1, op1) = out
+    assert op0[0] == ("csr" if side < 100 else "csr32")
+    if shape:  # a forced shape streams the copy
+        assert op1[0] == "banded" and l1 == "banded"
+        assert len(m[1]) <= op1[1] <= len(m[1]) * 1.1
+    assert r0["status"] == "Converged" and r0 == r1
+    assert torch.equal(x0, x1) and torch.equal(y0, y1)
 
 
 @pytest.mark.parametrize("shape", [None, "1,4", "0,3", "2,2,4", "2,3,2"])

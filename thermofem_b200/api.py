@@ -465,6 +465,10 @@ def solver_options(dtype=torch.float64, **kw) -> SolverOptions:
     return o
 
 
+# tf_*_spmv_layout codes
+LAYOUTS = ("csr", "sliced", "sorted", "banded", "csr32")
+
+
 class _AmgView:
     """Read access to a hierarchy (statistics, level operators, transfers)."""
 
@@ -524,10 +528,11 @@ class _AmgView:
         return y
 
     def level_spmv_layout(self, d):
-        """("sliced" | "sorted" | "csr", entries streamed) of level d's SpMV."""
+        """(layout, entries streamed) of level d's SpMV: "sliced", "sorted",
+        "banded", "csr" (2-byte column offsets) or "csr32" (4-byte columns)."""
         sl, n = C.c_int(), C.c_int64()
         check(lib().tf_amg_level_spmv_layout(self._h(), int(d), C.byref(sl), C.byref(n)))
-        return ("csr", "sliced", "sorted")[sl.value], n.value
+        return LAYOUTS[sl.value], n.value
 
     def level_transfer(self, d, device="cuda"):
         pm, po, pe = C.c_void_p(), C.c_void_p(), C.c_void_p()
@@ -669,10 +674,11 @@ class _Solver(_AmgView):
         return y
 
     def spmv_layout(self):
-        """("sliced" | "csr", entries streamed) of the solver's operator SpMV."""
+        """(layout, entries streamed) of the solver's operator SpMV, as
+        level_spmv_layout names them."""
         sl, n = C.c_int(), C.c_int64()
         check(lib().tf_solver_spmv_layout(self.h, C.byref(sl), C.byref(n)))
-        return ("sliced" if sl.value else "csr"), n.value
+        return LAYOUTS[sl.value], n.value
 
     @property
     def last_execution(self) -> int:

@@ -187,7 +187,8 @@ class HierarchyImpl final : public Hierarchy {
                 l.cd.allocate(static_cast<size_t>(l.nnz));
                 if (!delta_columns(ctx, l.n, l.rp.data(), l.ci.data(), l.cd.data())) l.cd.release();
             }
-            if (l.cd.data() && sliced_enabled()) build_sliced(ctx, l.csr(), l.sl, true);
+            if (sliced_enabled() && !(banded_enabled() && build_banded(ctx, l.csr(), l.sl)) && l.cd.data())
+                build_sliced(ctx, l.csr(), l.sl, true);
             // Launch shape of this level's row-tile kernels (cached by shape).
             marks.mark(ctx, kPhTuning);
             fill_zero(ctx, l.n, l.rhs.data());
@@ -337,8 +338,8 @@ class HierarchyImpl final : public Hierarchy {
     }
     int level_spmv_layout(tf_ctx *ctx, int d, int64_t *entries) const override {
         const auto &l = levels_.at(static_cast<size_t>(d));
-        if (!streams_sliced(ctx, l.csr(), l.sl.entries, entries)) return 0;
-        return l.sl.perm.data() ? 2 : 1;
+        if (!streams_sliced(ctx, l.csr(), l.sl.entries, entries)) return l.cd.data() ? 0 : 4;
+        return l.sl.perm.data() ? 2 : (l.sl.banded() ? 3 : 1);
     }
     void level_transfer(int d, const int32_t **map, const int32_t **off, const int32_t **mem,
                         int *coarse) const override {

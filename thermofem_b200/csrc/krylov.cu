@@ -34,16 +34,22 @@ int parts_for(int64_t n) {
     return static_cast<int>(p < 1 ? 1 : (p > kParts ? kParts : p));
 }
 
-// Fixed-order sum of K partial arrays [K][parts]; valid in thread 0.  Each
-// thread adds entries t, t + blockDim, t + 2 blockDim, ... in that order, the
-// loads issued eight at a time (they come from L2, written by other CTAs).
+// Fixed-order sum of K partial arrays [K][parts]; valid in thread 0.  Thread
+// t < 256 adds entries t, t + 256, t + 512, ... in that order, the loads
+// issued eight at a time (they come from L2, written by other CTAs).  The
+// stride is fixed, not blockDim: the finisher runs in the last CTA of
+// whichever kernel produced the partials (256 threads for the sliced SpMV,
+// 288 for the pipelined CSR one, 1024 for the one-CTA steps), and the sum
+// must not depend on which.  Threads past 256 contribute +0.0, which leaves
+// the block reduction's value unchanged.  Needs blockDim.x >= 256.
 template <int K>
 __device__ __forceinline__ void sum_partials(const double *part, int parts, double (&v)[K]) {
     constexpr int kBatch = 8;
-    const int step = static_cast<int>(blockDim.x);
+    constexpr int step = tile::kThreads;
 #pragma unroll
     for (int k = 0; k < K; ++k) {
         v[k] = 0.0;
+        if (threadIdx.x >= step) continue;
         for (int p0 = threadIdx.x; p0 < parts; p0 += step * kBatch) {
             double t[kBatch];
 #pragma unroll
@@ -635,7 +641,10 @@ class KrylovImpl final : public Krylov {
         }
         sl_.release();
         if constexpr (std::is_same_v<I, int32_t>) {
-            if (cd_.data() && sliced_enabled()) build_sliced(ctx, csr(), sl_, false);
+            // a banded copy where the operator's slices share their column
+            // offsets (stencils), else the 2-byte-offset sliced copy
+            if (sliced_enabled() && !(banded_enabled() && build_banded(ctx, csr(), sl_)) && cd_.data())
+                build_sliced(ctx, csr(), sl_, false);
         }
         hier_.reset();
         if (precond_ == TF_PRECOND_AMG) {
@@ -752,7 +761,8 @@ class KrylovImpl final : public Krylov {
     }
     int spmv_layout(tf_ctx *ctx, int64_t *entries) const override {
         if (!ready_) fail(TF_ERR_LOGIC, "solver requires setup");
-        return streams_sliced(ctx, csr(), sl_.entries, entries) ? 1 : 0;
+        if (!streams_sliced(ctx, csr(), sl_.entries, entries)) return cd_.data() ? 0 : 4;
+        return sl_.banded() ? 3 : 1;
     }
     int64_t rows() const override { return n_; }
 

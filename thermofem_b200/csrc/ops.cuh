@@ -26,6 +26,12 @@ struct Csr {
     const int32_t *sp{nullptr};
     const T *sv{nullptr};
     const int16_t *sc{nullptr};
+    // Banded slices instead of per-entry offsets (SlicedCopy::band): entry
+    // slot j of slice s holds one column offset shared by the slice's 32
+    // rows and the mask of its padding lanes, bd[sp[s] / 32 + j] = {offset,
+    // mask}; sc is then null.  Stencil operators have a handful of slots per
+    // slice, so the copy streams values and almost nothing else.
+    const int2 *bd{nullptr};
     // With sorted slices: the row at position t of the sliced order (rows
     // permuted within their 256-row tile, longest first).  Only epilogues
     // without partial sums stream a sorted copy.
@@ -42,7 +48,8 @@ template <class T>
 struct SlicedCopy {
     DeviceBuffer<int32_t> sp;
     DeviceBuffer<T> val;
-    DeviceBuffer<int16_t> col;
+    DeviceBuffer<int16_t> col;   // per-entry column offsets (sliced), or
+    DeviceBuffer<int2> band;     // per-slot shared offsets and padding masks (banded)
     DeviceBuffer<int32_t> perm;  // sorted slices only
     int64_t entries{0};
     int64_t tile_max{0};  // most entries of any 256-row tile
@@ -50,16 +57,19 @@ struct SlicedCopy {
         sp.release();
         val.release();
         col.release();
+        band.release();
         perm.release();
         entries = 0;
         tile_max = 0;
     }
+    bool banded() const { return band.data() != nullptr; }
     template <class I>
     void attach(Csr<T, I> &c) const {
         if (sp.data()) {
             c.sp = sp.data();
             c.sv = val.data();
             c.sc = col.data();
+            c.bd = band.data();
             c.perm = perm.data();
             c.sl_tile_max = tile_max;
         }
@@ -146,6 +156,14 @@ bool delta_columns_enabled();
 template <class T>
 bool build_sliced(tf_ctx *ctx, const Csr<T, int32_t> &a, SlicedCopy<T> &out, bool allow_sort);
 bool sliced_enabled();
+// A banded copy of a (slices of 32 rows whose entries share their column
+// offsets slot by slot, SlicedCopy::band) when every row is sorted without
+// repeated columns, no slice needs more than 32 slots and the padding stays
+// within THERMOFEM_B200_BANDED_PAD percent of nnz (default 10); false (and
+// out released) otherwise.  THERMOFEM_B200_BANDED=0 turns it off.
+template <class T>
+bool build_banded(tf_ctx *ctx, const Csr<T, int32_t> &a, SlicedCopy<T> &out);
+bool banded_enabled();
 // Self-check of the bounded device waits: a kernel whose wait nothing ends
 // gives up after `polls` polls and raises the context's fault word; throws
 // TF_ERR_TIMEOUT from check_faults (the word is cleared).

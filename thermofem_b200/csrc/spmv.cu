@@ -277,6 +277,81 @@ __global__ void slice_fill_kernel(int64_t rows, int64_t nslices, const I *__rest
     }
 }
 
+// Banded copy.  A warp walks one slice: lane l holds row 32 s + l and a
+// cursor into its (sorted) entries; at each step the warp takes the smallest
+// column offset among the lanes' next entries as the slot's shared offset,
+// and the lanes whose next entry has it advance.  The slot count is the
+// number of distinct offsets of the slice.  bad: 1 a row with unsorted or
+// repeated columns, 2 a slice wider than kBandMaxSlots.
+constexpr int kBandMaxSlots = 32;
+
+__device__ __forceinline__ int band_next(int64_t p, int64_t e, const int32_t *__restrict__ ci, int row) {
+    return p < e ? ci[p] - row : INT_MAX;
+}
+
+__global__ void band_width_kernel(int64_t rows, int64_t nslices, const int32_t *__restrict__ rp,
+                                  const int32_t *__restrict__ ci, int32_t *__restrict__ entries,
+                                  unsigned long long *total, int *bad) {
+    pdl_enter();
+    const int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    const int64_t s = t >> 5;  // uniform across the warp
+    if (s >= nslices) return;
+    const int lane = static_cast<int>(t & 31);
+    const int row = static_cast<int>(t);
+    int64_t p = 0, e = 0;
+    if (t < rows) {
+        p = rp[t];
+        e = rp[t + 1];
+        for (int64_t k = p + 1; k < e; ++k)
+            if (ci[k] <= ci[k - 1]) atomicOr(bad, 1);
+    }
+    int slots = 0;
+    for (;;) {
+        const int mine = band_next(p, e, ci, row);
+        int m = mine;
+        for (int o = 16; o > 0; o >>= 1) m = min(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if (m == INT_MAX) break;
+        if (mine == m) ++p;
+        if (++slots > kBandMaxSlots) {
+            if (lane == 0) atomicOr(bad, 2);
+            return;
+        }
+    }
+    if (lane == 0) {
+        entries[s] = slots * 32;
+        atomicAdd(total, static_cast<unsigned long long>(slots) * 32ull);
+    }
+}
+
+template <class T>
+__global__ void band_fill_kernel(int64_t rows, int64_t nslices, const int32_t *__restrict__ rp,
+                                 const int32_t *__restrict__ ci, const T *__restrict__ val,
+                                 const int32_t *__restrict__ sp, T *__restrict__ sv, int2 *__restrict__ bd) {
+    pdl_enter();
+    const int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    const int64_t s = t >> 5;
+    if (s >= nslices) return;
+    const int lane = static_cast<int>(t & 31);
+    const int row = static_cast<int>(t);
+    int64_t p = 0, e = 0;
+    if (t < rows) {
+        p = rp[t];
+        e = rp[t + 1];
+    }
+    const int64_t base = sp[s];
+    for (int j = 0;; ++j) {
+        const int mine = band_next(p, e, ci, row);
+        int m = mine;
+        for (int o = 16; o > 0; o >>= 1) m = min(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if (m == INT_MAX) break;
+        const bool has = mine == m;
+        const unsigned pad = __ballot_sync(0xffffffffu, !has);
+        sv[base + j * 32 + lane] = has ? val[p] : T(0);
+        if (lane == 0) bd[(base >> 5) + j] = make_int2(m, static_cast<int>(pad));
+        if (has) ++p;
+    }
+}
+
 template <class T>
 __global__ void prolong_kernel(int64_t nf, const int32_t *__restrict__ map, const T *__restrict__ coarse,
                                T *__restrict__ fine) {
@@ -556,7 +631,7 @@ template <class T, class I>
 bool streams_sliced(tf_ctx *ctx, const Csr<T, I> &a, int64_t entries_if_sliced, int64_t *entries) {
     bool sliced = false;
     if constexpr (std::is_same_v<I, int32_t>) {
-        if (a.sp && a.cd) sliced = tile::tuned_config<T, I, int16_t>(a.rows, a.nnz, ctx->sm_count).sliced != 0;
+        if (a.sp && (a.cd || a.bd)) sliced = tile::copy_config(ctx, a).sliced != 0;
     }
     *entries = sliced ? entries_if_sliced : a.nnz;
     return sliced;
@@ -695,6 +770,11 @@ void bounded_wait_check(tf_ctx *ctx, int64_t polls) {
     check_faults(ctx);  // TF_ERR_TIMEOUT, fault word cleared
 }
 
+bool banded_enabled() {
+    const char *v = std::getenv("THERMOFEM_B200_BANDED");
+    return !(v && v[0] == '0');
+}
+
 bool sliced_enabled() {
     const char *v = std::getenv("THERMOFEM_B200_SLICED");
     return !(v && v[0] == '0');
@@ -770,6 +850,41 @@ bool build_sliced(tf_ctx *ctx, const Csr<T, int32_t> &a, SlicedCopy<T> &out, boo
 }
 template bool build_sliced<float>(tf_ctx *, const Csr<float, int32_t> &, SlicedCopy<float> &, bool);
 template bool build_sliced<double>(tf_ctx *, const Csr<double, int32_t> &, SlicedCopy<double> &, bool);
+
+template <class T>
+bool build_banded(tf_ctx *ctx, const Csr<T, int32_t> &a, SlicedCopy<T> &out) {
+    out.release();
+    if (!a.rows || !a.nnz || a.rows >= INT32_MAX) return false;
+    const int64_t nslices = (a.rows + 31) / 32;
+    int pad_pct = 10;
+    if (const char *v = std::getenv("THERMOFEM_B200_BANDED_PAD")) pad_pct = std::atoi(v);
+    DeviceBuffer<int32_t> entries(static_cast<size_t>(nslices) + 1);
+    DeviceBuffer<unsigned long long> total(1);
+    int *bad = static_cast<int *>(ctx->arena(sizeof(int), 1));
+    memset_async(ctx, entries.data(), 0, (nslices + 1) * sizeof(int32_t));
+    memset_async(ctx, total.data(), 0, sizeof(unsigned long long));
+    memset_async(ctx, bad, 0, sizeof(int));
+    launch_kernel(ctx, "band_width", band_width_kernel, grid_for(nslices * 32), kBlock, 0, a.rows, nslices, a.rp,
+                  a.ci, entries.data(), total.data(), bad);
+    if (read_scalar(ctx, bad)) return false;
+    const int64_t n = static_cast<int64_t>(read_scalar(ctx, total.data()));
+    if (n >= INT32_MAX || n > a.nnz + a.nnz * pad_pct / 100) return false;
+    out.sp.allocate(static_cast<size_t>(nslices) + 1);
+    scan_exclusive(ctx, nslices + 1, entries.data(), out.sp.data());
+    out.val.allocate(static_cast<size_t>(n));
+    out.band.allocate(static_cast<size_t>(n / 32));
+    launch_kernel(ctx, "band_fill", band_fill_kernel<T>, grid_for(nslices * 32), kBlock, 0, a.rows, nslices, a.rp,
+                  a.ci, a.val, out.sp.data(), out.val.data(), out.band.data());
+    DeviceBuffer<unsigned long long> tmax(1);
+    memset_async(ctx, tmax.data(), 0, sizeof(unsigned long long));
+    launch_kernel(ctx, "slice_tile_max", slice_tile_max_kernel, grid_for((nslices + 7) / 8), kBlock, 0, nslices,
+                  out.sp.data(), tmax.data());
+    out.tile_max = static_cast<int64_t>(read_scalar(ctx, tmax.data()));
+    out.entries = n;
+    return true;
+}
+template bool build_banded<float>(tf_ctx *, const Csr<float, int32_t> &, SlicedCopy<float> &);
+template bool build_banded<double>(tf_ctx *, const Csr<double, int32_t> &, SlicedCopy<double> &);
 
 template <class T>
 void restrict_sum(tf_ctx *ctx, int64_t nc, const int32_t *off, const int32_t *mem, const T *fine, T *coarse) {

@@ -18,6 +18,7 @@
 // reduces into per-tile partial sums (deterministic: fixed tile partition and
 // fixed reduction tree), and may gate the whole launch on a device flag.
 #pragma once
+#include <climits>
 #include <cstdio>
 #include <cstdlib>
 #include <map>
@@ -616,17 +617,41 @@ __global__ void __launch_bounds__(kThreads + 32) csr_pipe_kernel(int64_t rows, i
 // (every output is still the same bits; only epilogues without partial sums
 // are launched on it).
 // ---------------------------------------------------------------------------
-template <class T, int G>
-struct SliceHead {
-    T v[G];
-    int16_t c[G];
-    int32_t base, width;
+// Where a slice entry's column offset comes from.  c = cols.at(base, j,
+// lane) is the offset from the lane's row of entry j of the slice that
+// starts at entry base, or kColPad for a padding entry (no gather).
+constexpr int kColPad = INT_MIN;
+
+// Sliced copy: one 2-byte offset per entry, loaded with the values.
+struct OffsetCols {
+    const int16_t *__restrict__ sc;
+    __device__ __forceinline__ int at(int base, int j, int lane) const {
+        const int16_t c = __ldcs(sc + base + j * 32 + lane);
+        return c == kSlicePad ? kColPad : c;
+    }
+};
+
+// Banded copy: one {offset, padding mask} pair per slot, shared by the
+// slice's 32 rows (a broadcast load per warp, cached).
+struct BandCols {
+    const int2 *__restrict__ bd;
+    __device__ __forceinline__ int at(int base, int j, int lane) const {
+        const int2 q = __ldg(bd + (base >> 5) + j);
+        return (static_cast<unsigned>(q.y) >> lane) & 1u ? kColPad : q.x;
+    }
 };
 
 template <class T, int G>
+struct SliceHead {
+    T v[G];
+    int c[G];
+    int32_t base, width;
+};
+
+template <class T, int G, class Cols>
 __device__ __forceinline__ void load_slice_head(SliceHead<T, G> &h, int64_t slice, int64_t nslices,
                                                 const int32_t *__restrict__ sp, const T *__restrict__ sv,
-                                                const int16_t *__restrict__ sc, int lane) {
+                                                const Cols &cols, int lane) {
     h.base = 0;
     h.width = 0;
     if (slice < nslices) {
@@ -634,22 +659,21 @@ __device__ __forceinline__ void load_slice_head(SliceHead<T, G> &h, int64_t slic
         h.width = (__ldg(sp + slice + 1) - h.base) >> 5;
     }
     const T *pv = sv + h.base + lane;  // entry g of this lane's row at pv[32 g]
-    const int16_t *pc = sc + h.base + lane;
 #pragma unroll
     for (int g = 0; g < G; ++g) {
         if (g < h.width) {
             h.v[g] = __ldcs(pv + g * 32);
-            h.c[g] = __ldcs(pc + g * 32);
+            h.c[g] = cols.at(h.base, g, lane);
         } else {
             h.v[g] = T(0);
-            h.c[g] = kSlicePad;
+            h.c[g] = kColPad;
         }
     }
 }
 
-template <class T, int G, bool PF, class XS, class Epi>
+template <class T, int G, bool PF, class XS, class Epi, class Cols>
 __global__ void __launch_bounds__(kThreads) sliced_kernel(int64_t rows, const int32_t *__restrict__ sp,
-                                                          const T *__restrict__ sv, const int16_t *__restrict__ sc,
+                                                          const T *__restrict__ sv, Cols cols,
                                                           const int32_t *__restrict__ perm, int early, XS xs,
                                                           Epi epi) {
     constexpr int K = Epi::kReduce;
@@ -664,10 +688,10 @@ __global__ void __launch_bounds__(kThreads) sliced_kernel(int64_t rows, const in
     const int nslices = (nrows + 31) / 32;
     int tile = blockIdx.x;
     SliceHead<T, G> h;
-    if (early) load_slice_head(h, tile * kWarps + warp, nslices, sp, sv, sc, lane);
+    if (early) load_slice_head(h, tile * kWarps + warp, nslices, sp, sv, cols, lane);
     pdl_enter();
     if (epi.skip()) return;  // the gate reads the same device word in every CTA
-    if (!early) load_slice_head(h, tile * kWarps + warp, nslices, sp, sv, sc, lane);
+    if (!early) load_slice_head(h, tile * kWarps + warp, nslices, sp, sv, cols, lane);
     for (int parity = 0; tile < ntiles; tile += gridDim.x, parity ^= 1) {
         const int slot = tile * kThreads + threadIdx.x;  // position in the sliced order
         const bool live = slot < nrows;
@@ -675,31 +699,30 @@ __global__ void __launch_bounds__(kThreads) sliced_kernel(int64_t rows, const in
         typename Epi::Pre pre{};
         if (live) pre = epi.pre(row, xs);
         SliceHead<T, G> next;
-        if constexpr (PF) load_slice_head(next, (tile + gridDim.x) * kWarps + warp, nslices, sp, sv, sc, lane);
+        if constexpr (PF) load_slice_head(next, (tile + gridDim.x) * kWarps + warp, nslices, sp, sv, cols, lane);
         const auto xr = xs.row(row);  // x~ around this lane's row, indexed by column offset
         T y[G];
 #pragma unroll
-        for (int g = 0; g < G; ++g) y[g] = h.c[g] != kSlicePad ? xr(h.c[g]) : T(0);
+        for (int g = 0; g < G; ++g) y[g] = h.c[g] != kColPad ? xr(h.c[g]) : T(0);
         T acc = T(0);
 #pragma unroll
         for (int g = 0; g < G; ++g) acc += h.v[g] * y[g];
         for (int j0 = G; j0 < h.width; j0 += G) {
             T v[G];
-            int16_t c[G];
+            int c[G];
             const T *pv = sv + h.base + lane + j0 * 32;
-            const int16_t *pc = sc + h.base + lane + j0 * 32;
 #pragma unroll
             for (int g = 0; g < G; ++g) {
                 if (j0 + g < h.width) {
                     v[g] = __ldcs(pv + g * 32);
-                    c[g] = __ldcs(pc + g * 32);
+                    c[g] = cols.at(h.base, j0 + g, lane);
                 } else {
                     v[g] = T(0);
-                    c[g] = kSlicePad;
+                    c[g] = kColPad;
                 }
             }
 #pragma unroll
-            for (int g = 0; g < G; ++g) y[g] = c[g] != kSlicePad ? xr(c[g]) : T(0);
+            for (int g = 0; g < G; ++g) y[g] = c[g] != kColPad ? xr(c[g]) : T(0);
 #pragma unroll
             for (int g = 0; g < G; ++g) acc += v[g] * y[g];
         }
@@ -725,7 +748,7 @@ __global__ void __launch_bounds__(kThreads) sliced_kernel(int64_t rows, const in
         }
         if constexpr (PF) h = next;
         else if (tile + static_cast<int>(gridDim.x) < ntiles)
-            load_slice_head(h, (tile + gridDim.x) * kWarps + warp, nslices, sp, sv, sc, lane);
+            load_slice_head(h, (tile + gridDim.x) * kWarps + warp, nslices, sp, sv, cols, lane);
     }
     if constexpr (K > 0) finish(epi.fin, epi.partial, ntiles);
 }
@@ -946,6 +969,7 @@ struct PipeConfig {
 // largest tile, or 0 when a stage would exceed 64 KB.
 template <class T, class I>
 int sliced_stage_cap(const Csr<T, I> &a) {
+    if (a.bd) return 0;  // the staged kernel streams per-entry offsets only
     const int64_t cap = (a.sl_tile_max + 255) & ~int64_t(255);
     if (cap <= 0 || cap > (int64_t(64) << 10)) return 0;
     return SlicedStage<T>(static_cast<int>(cap)).bytes <= (64 << 10) ? static_cast<int>(cap) : 0;
@@ -1149,14 +1173,28 @@ void launch_sliced(tf_ctx *ctx, const Csr<T, I> &a, const XS &xs, const Epi &epi
         const int64_t g = static_cast<int64_t>(ctx->sm_count) * per_sm;
         return static_cast<int>(ntiles < g ? ntiles : g);
     };
-    if (cfg.prefetch)
-        launch_kernel(ctx, name, sliced_kernel<T, 8, true, XS, Epi>,
-                      grid(resident_ctas<sliced_kernel<T, 8, true, XS, Epi>>(kThreads, 0)), kThreads, 0, a.rows, a.sp,
-                      a.sv, a.sc, a.perm, early, xs, epi);
-    else
-        launch_kernel(ctx, name, sliced_kernel<T, 8, false, XS, Epi>,
-                      grid(resident_ctas<sliced_kernel<T, 8, false, XS, Epi>>(kThreads, 0)), kThreads, 0, a.rows,
-                      a.sp, a.sv, a.sc, a.perm, early, xs, epi);
+    auto go = [&](auto cols) {
+        using Cols = decltype(cols);
+        if (cfg.prefetch)
+            launch_kernel(ctx, name, sliced_kernel<T, 8, true, XS, Epi, Cols>,
+                          grid(resident_ctas<sliced_kernel<T, 8, true, XS, Epi, Cols>>(kThreads, 0)), kThreads, 0,
+                          a.rows, a.sp, a.sv, cols, a.perm, early, xs, epi);
+        else
+            launch_kernel(ctx, name, sliced_kernel<T, 8, false, XS, Epi, Cols>,
+                          grid(resident_ctas<sliced_kernel<T, 8, false, XS, Epi, Cols>>(kThreads, 0)), kThreads, 0,
+                          a.rows, a.sp, a.sv, cols, a.perm, early, xs, epi);
+    };
+    if (a.bd) go(BandCols{a.bd});
+    else go(OffsetCols{a.sc});
+}
+
+// The launch shape cached for an operator's sliced or banded copy: it is
+// stored under the column stream its row-tile kernel reads (2-byte offsets
+// when the operator has them, else its indices).
+template <class T, class I>
+PipeConfig copy_config(tf_ctx *ctx, const Csr<T, I> &a) {
+    return a.cd ? tuned_config<T, I, int16_t>(a.rows, a.nnz, ctx->sm_count)
+                : tuned_config<T, I, I>(a.rows, a.nnz, ctx->sm_count);
 }
 
 // Launches the sliced kernel when the operator carries a sliced copy and its
@@ -1171,8 +1209,8 @@ void launch(tf_ctx *ctx, const Csr<T, I> &a, const XS &xs, const Epi &epi, const
     if constexpr (std::is_same_v<I, int32_t>) {
         // a sorted copy permutes rows within their tile, which would change
         // the order of a reducing epilogue's partial sums: row tiles then
-        if (a.sp && a.cd && (!a.perm || Epi::kReduce == 0)) {
-            const PipeConfig cfg = force ? *force : tuned_config<T, I, int16_t>(a.rows, a.nnz, ctx->sm_count);
+        if (a.sp && (a.cd || a.bd) && (!a.perm || Epi::kReduce == 0)) {
+            const PipeConfig cfg = force ? *force : copy_config(ctx, a);
             if (cfg.sliced) {
                 launch_sliced(ctx, a, xs, epi, name, cfg);
                 return;
@@ -1311,8 +1349,9 @@ PipeConfig autotune_columns(tf_ctx *ctx, const Csr<T, I> &a, const T *x, T *y, f
             }
         }
     }
-    if constexpr (std::is_same_v<I, int32_t> && std::is_same_v<C, int16_t>) {
-        if (a.sp) {
+    if constexpr (std::is_same_v<I, int32_t>) {
+        // a sliced copy (2-byte offsets: tuned under C = int16_t) or a banded one
+        if (a.sp && (a.bd || std::is_same_v<C, int16_t>)) {
             // The sliced copy: next-tile prefetch on/off x resident CTAs per
             // SM, unless THERMOFEM_B200_SLICED_SHAPE="prefetch,ctas" forces one.
             int forced_pf = -1, forced_ctas = 0;
@@ -1354,17 +1393,20 @@ PipeConfig autotune_columns(tf_ctx *ctx, const Csr<T, I> &a, const T *x, T *y, f
                         resident = resident_ctas<sliced_pipe_kernel<T, PlainX<T>, TuneStore<T>>>(kThreads + 32, smem);
                     } else {
                         cfg.prefetch = knob;
-                        resident = knob ? resident_ctas<sliced_kernel<T, 8, true, PlainX<T>, TuneStore<T>>>(kThreads, 0)
-                                        : resident_ctas<sliced_kernel<T, 8, false, PlainX<T>, TuneStore<T>>>(kThreads, 0);
+                        // (the column source does not change the kernel's registers much; offsets bound it)
+                        resident = knob ? resident_ctas<sliced_kernel<T, 8, true, PlainX<T>, TuneStore<T>, OffsetCols>>(
+                                              kThreads, 0)
+                                        : resident_ctas<sliced_kernel<T, 8, false, PlainX<T>, TuneStore<T>, OffsetCols>>(
+                                              kThreads, 0);
                     }
                     if (resident < ctas && forced_pf < 0) continue;
                     const float ms = time_cfg(cfg);
                     if (tune_log())
                         std::fprintf(stderr,
-                                     "tf_autotune_spmv rows=%lld nnz=%lld T=%d sliced %s=%d ctas=%d %.2f us\n",
+                                     "tf_autotune_spmv rows=%lld nnz=%lld T=%d %s %s=%d ctas=%d %.2f us\n",
                                      static_cast<long long>(a.rows), static_cast<long long>(a.nnz),
-                                     static_cast<int>(sizeof(T)), kind == 2 ? "staged stages" : "prefetch", knob,
-                                     ctas, ms * 1e3f);
+                                     static_cast<int>(sizeof(T)), a.bd ? "banded" : "sliced",
+                                     kind == 2 ? "staged stages" : "prefetch", knob, ctas, ms * 1e3f);
                     if (sfirst || ms < sbest_t) {
                         sbest_t = ms;
                         sbest = cfg;
