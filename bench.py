@@ -90,8 +90,9 @@ def kernel_name(layout, t, entries):
     return {
         "sliced": f"sliced_kernel<{t}> over the sliced copy (32-row slices, 2-byte column offsets, {entries} entries)",
         "sorted": f"sliced_kernel<{t}> over the sorted sliced copy ({entries} entries)",
-        "banded": f"sliced_kernel<{t}, BandCols> over the banded copy (32-row slices, one shared column offset per "
-                  f"entry slot, {entries} entries)",
+        "banded": f"the banded copy's tuned kernel over {entries} entries (32-row slices, one shared column offset "
+                  f"per entry slot): sliced_pipe_kernel<{t}, group, ..., StagedBand> (values and slots bulk-copied "
+                  f"into shared memory) or sliced_kernel<{t}, ..., BandCols>",
         "csr": f"csr_pipe_kernel<{t},int,short> over the CSR arrays (2-byte column offsets)",
         "csr32": f"csr_pipe_kernel<{t},int,int> over the CSR arrays (4-byte column indices)",
     }[layout]

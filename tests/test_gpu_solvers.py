@@ -456,7 +456,7 @@ def test_sliced_layout_gives_identical_solves(ctx, case, shape, monkeypatch):
         assert torch.equal(out[0][2], other[2])
 
 
-@pytest.mark.parametrize("shape", ["0,2", "1,3", "1,8", "0,5", None])
+@pytest.mark.parametrize("shape", ["0,2", "1,3", "1,8", "0,5", "2,2,3", "2,3,2", "2,3,3,2", "2,2,2,4", None])
 @pytest.mark.parametrize("case", ["heat3d25-cg-f32", "heat3d25-bicgstab-f64", "heat3d184-cg-f32"])
 def test_banded_layout_gives_identical_solves(ctx, case, shape, monkeypatch):
     # Stencil operators (the solver's operator, the finest level) carry a
@@ -464,12 +464,14 @@ def test_banded_layout_gives_identical_solves(ctx, case, shape, monkeypatch):
     # slot, with a padding mask, so SpMV streams values and an 8-byte pair
     # per 32 entries.  Each row still sums its entries left to right from +0
     # (padding lanes gather nothing): the same bits as the CSR arrays
-    # (THERMOFEM_B200_SLICED=0), whatever the launch shape.  184^3: couplings
-    # 33,856 rows apart, beyond 2-byte offsets, so the CSR arrays stream
-    # 4-byte columns there.
+    # (THERMOFEM_B200_SLICED=0), whatever the launch shape: "p,c" the direct
+    # kernel (prefetch p, c CTAs per SM), "2,s,c[,g]" the staged one (s stages
+    # of g tiles' values and slots copied in bulk into shared memory).  184^3:
+    # couplings 33,856 rows apart, beyond 2-byte offsets, so the CSR arrays
+    # stream 4-byte columns there.
     side = int(case.split("-")[0][6:])
-    if side > 100 and shape not in (None, "1,3"):
-        pytest.skip("the large case runs two launch shapes")
+    if side > 100 and shape not in (None, "1,3", "2,2,3", "2,3,3,2"):
+        pytest.skip("the large case runs four launch shapes")
     m = P.heat3d(side, seed=85)
     n = len(m[0]) - 1
     b = torch.tensor(P.rhs_uniform(n, 86), device="cuda")
@@ -496,7 +498,7 @@ def test_banded_layout_gives_identical_solves(ctx, case, shape, monkeypatch):
     assert torch.equal(x0, x1) and torch.equal(y0, y1)
 
 
-@pytest.mark.parametrize("shape", [None, "1,4", "0,3", "2,2,4", "2,3,2"])
+@pytest.mark.parametrize("shape", [None, "1,4", "0,3", "2,2,4", "2,3,2", "2,3,2,2", "2,2,2,4"])
 def test_operator_spmv_entry_points(ctx, shape, monkeypatch):
     # The solver's and the hierarchy's own operators (2-byte column stream,
     # sliced copy when the tuner picks it or a shape forces it) give the same

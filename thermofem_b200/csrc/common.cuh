@@ -198,12 +198,22 @@ inline void launched(tf_ctx *ctx, const char *name) {
 // kernel writes or reads; pdl_trigger() lets the next kernel be scheduled
 // (its CTAs then wait in their own pdl_wait).  Both are no-ops in a kernel
 // launched without the attribute.
+//
+// The next kernel is scheduled once every CTA of this one has triggered or
+// exited.  Kernels here do not trigger at entry: a next kernel scheduled
+// while this one still runs takes SM slots, registers and shared memory
+// (and with it L1) that this one needs.  Measured on B200 (PCG + AMG, FP32
+// hierarchy), triggers at entry everywhere made the 256^3 solve 12 % slower
+// than triggers after the work; entry triggers in the small kernels only
+// gained 1 ms at 128^3 and lost 1.5 % at 256^3.  So a kernel enters with
+// pdl_enter() (the wait alone) and triggers by exiting -- or, for the
+// persistent row-tile SpMV kernels (tile.cuh), by pdl_trigger() after the
+// main loop, so that the next kernel's launch and prologue overlap their
+// tail (draining copies, a last-CTA scalar step).  The small-level region
+// (coarse_cycle.cu), one CTA or cluster, triggers once it has loaded.
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 __device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
-__device__ __forceinline__ void pdl_enter() {
-    pdl_wait();
-    pdl_trigger();
-}
+__device__ __forceinline__ void pdl_enter() { pdl_wait(); }
 
 // Launches kernel<<<grid, block, smem, ctx->stream>>>(args...) with the
 // programmatic-serialization attribute (when ctx->pdl) and counts it.  Every

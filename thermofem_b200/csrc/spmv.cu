@@ -872,7 +872,10 @@ bool build_banded(tf_ctx *ctx, const Csr<T, int32_t> &a, SlicedCopy<T> &out) {
     out.sp.allocate(static_cast<size_t>(nslices) + 1);
     scan_exclusive(ctx, nslices + 1, entries.data(), out.sp.data());
     out.val.allocate(static_cast<size_t>(n));
-    out.band.allocate(static_cast<size_t>(n / 32));
+    // an even number of slots: the staged kernel copies whole 16-byte pairs
+    const int64_t slots = n / 32, slots_even = (slots + 1) & ~int64_t(1);
+    out.band.allocate(static_cast<size_t>(slots_even));
+    if (slots_even > slots) memset_async(ctx, out.band.data() + slots, 0, sizeof(int2));
     launch_kernel(ctx, "band_fill", band_fill_kernel<T>, grid_for(nslices * 32), kBlock, 0, a.rows, nslices, a.rp,
                   a.ci, a.val, out.sp.data(), out.val.data(), out.band.data());
     DeviceBuffer<unsigned long long> tmax(1);

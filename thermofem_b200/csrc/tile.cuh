@@ -18,6 +18,7 @@
 // reduces into per-tile partial sums (deterministic: fixed tile partition and
 // fixed reduction tree), and may gate the whole launch on a device flag.
 #pragma once
+#include <algorithm>
 #include <climits>
 #include <cstdio>
 #include <cstdlib>
@@ -583,6 +584,7 @@ __global__ void __launch_bounds__(kThreads + 32) csr_pipe_kernel(int64_t rows, i
         }
     }
     __syncthreads();
+    pdl_trigger();  // the main loop is done: the next kernel may be scheduled
     if (tid == kThreads) {
         // No copy of this CTA may still be in flight when it exits: wait
         // (bounded; immediate when the consumers consumed everything) for the
@@ -750,67 +752,137 @@ __global__ void __launch_bounds__(kThreads) sliced_kernel(int64_t rows, const in
         else if (tile + static_cast<int>(gridDim.x) < ntiles)
             load_slice_head(h, (tile + gridDim.x) * kWarps + warp, nslices, sp, sv, cols, lane);
     }
+    pdl_trigger();  // the main loop is done: the next kernel may be scheduled
     if constexpr (K > 0) finish(epi.fin, epi.partial, ntiles);
 }
 
 // ---------------------------------------------------------------------------
-// Staged sliced kernel: the sliced copy streamed through shared memory.
+// Staged sliced kernel: the sliced or banded copy streamed through shared
+// memory.
 //
-// A tile's 8 slices are contiguous in the copy (entries [sp[8t], sp[8t+8])
-// of the values and of the column offsets), so the producer thread (warp 8,
-// lane 0) moves a whole tile with two bulk copies into a ring stage.  Slice
-// starts are multiples of 32 entries, so both copies start and end on
-// 16-byte boundaries (no ragged edges).  The producer also writes the
-// tile's 9 slice starts into the stage header before arming the stage.
-// Each consumer warp then reads its slice from shared memory lane by lane
-// (consecutive addresses: no bank conflicts) and only the x gathers leave
-// the SM.  Row sums, epilogues and the per-256-row-block partial sums are
-// those of the kernels above: the same bits.  Every wait is bounded as in
-// csr_pipe_kernel (fault word, drain of the CTA's own copies).
+// A group of R tiles (8 R slices, 256 R rows) is contiguous in the copy
+// (entries [sp[8 R g], sp[8 R (g + 1)]) of the values and of the column
+// source), so the producer thread (warp 8, lane 0) moves a whole group with
+// two bulk copies into a ring stage.  Slice starts are multiples of 32
+// entries, so the value copy starts and ends on 16-byte boundaries (the
+// column sources keep theirs, see below).  The producer also writes the
+// group's 8 R + 1 slice starts into the stage header before arming the
+// stage.  Consumer warp w owns slice w of each of the group's tiles, lane l
+// its row, and reads its slices from shared memory lane by lane (consecutive
+// addresses: no bank conflicts); only the x gathers leave the SM.  R amortises
+// the per-stage work (the waits, the header, the producer's copies) over R
+// slices per warp.  Row sums, epilogues and the per-256-row-block partial
+// sums are those of the kernels above: the same bits.  Every wait is bounded
+// as in csr_pipe_kernel (fault word, drain of the CTA's own copies).
 // ---------------------------------------------------------------------------
-template <class T>
+// Column sources of the staged kernel: what the producer copies next to a
+// group's values (entries [e0, e1) of the copy) and how a consumer lane
+// reads slot j of its slice from the stage: take(j, c) is false for a
+// padding entry, else sets c to the column offset from the lane's row.
+//
+// Sliced copy: the group's 2-byte offsets, one per entry.
+struct StagedOffsets {
+    const int16_t *__restrict__ sc;
+    static __host__ __device__ int stage_bytes(int cap) { return (cap * 2 + 127) & ~127; }
+    __device__ __forceinline__ uint32_t bytes(int64_t e0, int64_t e1) const {
+        return static_cast<uint32_t>((e1 - e0) * 2);
+    }
+    __device__ __forceinline__ void copy(void *dst, int64_t e0, int64_t e1, uint64_t *bar) const {
+        bulk_load(dst, sc + e0, bytes(e0, e1), bar);
+    }
+    struct View {
+        const int16_t *p;
+        __device__ __forceinline__ bool take(int j, int &c) const {
+            const int16_t v = p[j * 32];
+            c = v;
+            return v != kSlicePad;
+        }
+    };
+    // base: the slice's first entry, relative to e0
+    __device__ __forceinline__ View view(const void *stage, int64_t, int base, int lane) const {
+        return {static_cast<const int16_t *>(stage) + base + lane};
+    }
+};
+
+// Banded copy: the group's {offset, padding mask} slots (one per 32
+// entries), copied from the even slot at or below e0 / 32 to the even slot
+// at or above e1 / 32, so that both ends sit on 16-byte boundaries (the band
+// array is allocated to an even number of slots).  A lane reads the slot as
+// a broadcast (one shared-memory word for the whole warp) and tests its own
+// bit of the mask.
+struct StagedBand {
+    const int2 *__restrict__ bd;
+    static __host__ __device__ int stage_bytes(int cap) { return ((cap / 32 + 2) * 8 + 127) & ~127; }
+    static __device__ __forceinline__ int64_t lo(int64_t e0) { return (e0 >> 5) & ~int64_t(1); }
+    static __device__ __forceinline__ int64_t hi(int64_t e1) { return ((e1 >> 5) + 1) & ~int64_t(1); }
+    __device__ __forceinline__ uint32_t bytes(int64_t e0, int64_t e1) const {
+        return static_cast<uint32_t>((hi(e1) - lo(e0)) * 8);
+    }
+    __device__ __forceinline__ void copy(void *dst, int64_t e0, int64_t e1, uint64_t *bar) const {
+        bulk_load(dst, bd + lo(e0), bytes(e0, e1), bar);
+    }
+    struct View {
+        const int2 *q;
+        unsigned bit;
+        __device__ __forceinline__ bool take(int j, int &c) const {
+            const int2 v = q[j];
+            c = v.x;
+            return (static_cast<unsigned>(v.y) & bit) == 0u;
+        }
+    };
+    __device__ __forceinline__ View view(const void *stage, int64_t e0, int base, int lane) const {
+        return {static_cast<const int2 *>(stage) + ((e0 >> 5) - lo(e0)) + (base >> 5), 1u << lane};
+    }
+};
+
+// One ring stage: the header of R * 8 + 1 slice starts, the values, the
+// column source.  cap: the stage's entry capacity.
+template <class T, class Cols, int R>
 struct SlicedStage {
-    static constexpr int kHeader = 64;  // 9 int32 slice starts, padded
+    static constexpr int kHeader = ((R * 8 + 1) * 4 + 63) & ~63;
     int val_bytes, col_bytes, bytes;
     __host__ __device__ explicit SlicedStage(int cap) {
         val_bytes = (cap * static_cast<int>(sizeof(T)) + 127) & ~127;
-        col_bytes = (cap * 2 + 127) & ~127;
+        col_bytes = Cols::stage_bytes(cap);
         bytes = (kHeader + val_bytes + col_bytes + 127) & ~127;
     }
 };
 
-template <class T, class XS, class Epi>
+template <class T, int R, class XS, class Epi, class Cols>
 __global__ void __launch_bounds__(kThreads + 32)
-    sliced_pipe_kernel(int64_t rows, const int32_t *__restrict__ sp, const T *__restrict__ sv,
-                       const int16_t *__restrict__ sc, int cap, int stages, int early, XS xs, Epi epi, int *fault) {
+    sliced_pipe_kernel(int64_t rows, const int32_t *__restrict__ sp, const T *__restrict__ sv, Cols cols, int cap,
+                       int stages, int early, XS xs, Epi epi, int *fault) {
     constexpr int K = Epi::kReduce;
     constexpr int KK = K > 0 ? K : 1;
     constexpr int kWarps = kThreads / 32;
+    constexpr int kSlices = kWarps * R;  // slices per group
+    constexpr int kRing = kMaxStages * R + 1;
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ uint64_t full_bar[kMaxStages], empty_bar[kMaxStages];
-    __shared__ double warp_sums[kMaxStages + 1][kWarps][KK];
-    __shared__ int warp_done[kMaxStages + 1];
+    __shared__ double warp_sums[kRing][kWarps][KK];
+    __shared__ int warp_done[kRing];
     __shared__ int skipped_cta;
-    const SlicedStage<T> L(cap);
+    using Stage = SlicedStage<T, Cols, R>;
+    const Stage L(cap);
     const int tid = threadIdx.x;
     if (tid == 0) {
         for (int st = 0; st < stages; ++st) {
             mbar_init(&full_bar[st], 1);
             mbar_init(&empty_bar[st], kWarps);
         }
-        for (int st = 0; st < kMaxStages + 1; ++st) warp_done[st] = 0;
+        for (int st = 0; st < kRing; ++st) warp_done[st] = 0;
         mbar_fence_init();
     }
     __syncthreads();
     auto stage_hdr = [&](int st) { return reinterpret_cast<int32_t *>(smem + static_cast<size_t>(st) * L.bytes); };
     auto stage_val = [&](int st) {
-        return reinterpret_cast<T *>(smem + static_cast<size_t>(st) * L.bytes + SlicedStage<T>::kHeader);
+        return reinterpret_cast<T *>(smem + static_cast<size_t>(st) * L.bytes + Stage::kHeader);
     };
     auto stage_col = [&](int st) {
-        return reinterpret_cast<int16_t *>(smem + static_cast<size_t>(st) * L.bytes + SlicedStage<T>::kHeader +
-                                           L.val_bytes);
+        return static_cast<void *>(smem + static_cast<size_t>(st) * L.bytes + Stage::kHeader + L.val_bytes);
     };
     const int64_t ntiles = (rows + kThreads - 1) / kThreads;  // = 256-row blocks of partial sums
+    const int64_t ngroups = (ntiles + R - 1) / R;
     const int64_t nslices = (rows + 31) / 32;
     bool ok = true;
     uint32_t armed[kMaxStages] = {0, 0, 0, 0};  // producer: completions requested per stage
@@ -828,20 +900,25 @@ __global__ void __launch_bounds__(kThreads + 32)
             return stop;
         };
         if (!early) enter();
-        // the slice starts of the CTA's next tile are loaded one tile ahead,
-        // so their latency overlaps the wait for a free stage
-        int32_t starts[kWarps + 1];
-        auto load_starts = [&](int64_t tile) {
-            const int64_t s0 = tile * kWarps;
+        // the group's first and last slice starts are loaded one group
+        // ahead, so their latency overlaps the wait for a free stage; the
+        // others are loaded before that wait
+        auto start_at = [&](int64_t s) { return __ldg(sp + (s < nslices ? s : nslices)); };
+        int32_t next0 = 0, next1 = 0;
+        if (static_cast<int64_t>(blockIdx.x) < ngroups) {
+            next0 = start_at(blockIdx.x * static_cast<int64_t>(kSlices));
+            next1 = start_at((blockIdx.x + 1) * static_cast<int64_t>(kSlices));
+        }
+        for (int64_t grp = blockIdx.x; grp < ngroups && ok && !stop; grp += gridDim.x, ++it) {
+            const int64_t e0 = next0, e1 = next1;
+            const int64_t s0 = grp * kSlices;
+            if (grp + gridDim.x < ngroups) {
+                next0 = start_at((grp + gridDim.x) * kSlices);
+                next1 = start_at((grp + gridDim.x + 1) * kSlices);
+            }
+            int32_t mid[kSlices - 1];
 #pragma unroll
-            for (int k = 0; k <= kWarps; ++k) starts[k] = __ldg(sp + (s0 + k < nslices ? s0 + k : nslices));
-        };
-        if (static_cast<int64_t>(blockIdx.x) < ntiles) load_starts(blockIdx.x);
-        for (int64_t tile = blockIdx.x; tile < ntiles && ok && !stop; tile += gridDim.x, ++it) {
-            int32_t cur[kWarps + 1];
-#pragma unroll
-            for (int k = 0; k <= kWarps; ++k) cur[k] = starts[k];
-            if (tile + gridDim.x < ntiles) load_starts(tile + gridDim.x);
+            for (int k = 1; k < kSlices; ++k) mid[k - 1] = start_at(s0 + k);
             const int st = static_cast<int>(it % stages);
             if (it >= static_cast<uint32_t>(stages)) {
                 if (enter()) break;
@@ -851,33 +928,37 @@ __global__ void __launch_bounds__(kThreads + 32)
                 }
             }
             int32_t *hdr = stage_hdr(st);
+            hdr[0] = static_cast<int32_t>(e0);
 #pragma unroll
-            for (int k = 0; k <= kWarps; ++k) hdr[k] = cur[k];
-            const int64_t e0 = cur[0], e1 = cur[kWarps];
+            for (int k = 1; k < kSlices; ++k) hdr[k] = mid[k - 1];
+            hdr[kSlices] = static_cast<int32_t>(e1);
             const uint32_t nv = static_cast<uint32_t>((e1 - e0) * static_cast<int64_t>(sizeof(T)));
-            const uint32_t nc = static_cast<uint32_t>((e1 - e0) * 2);
+            const uint32_t nc = e1 > e0 ? cols.bytes(e0, e1) : 0;
             mbar_arrive_expect_tx(&full_bar[st], nv + nc);
             ++armed[st];
             if (e1 > e0) {
                 bulk_load(stage_val(st), sv + e0, nv, &full_bar[st]);
-                bulk_load(stage_col(st), sc + e0, nc, &full_bar[st]);
+                cols.copy(stage_col(st), e0, e1, &full_bar[st]);
             }
         }
         enter();
         if (!ok) atomicExch(fault, 1);
     } else if (tid < kThreads) {
-        // ---- consumers: warp w owns slice 8 tile + w, lane l its row ----
+        // ---- consumers: warp w owns slice w of each tile of the group ----
         pdl_enter();
         const int lane = tid & 31, warp = tid >> 5;
-        uint32_t it = 0, local_tile = 0;
+        uint32_t it = 0, local_block = 0;
         const bool skipped = epi.skip();
         if (tid == 0) skipped_cta = skipped ? 1 : 0;
-        const int64_t first = skipped ? ntiles : blockIdx.x;
-        for (int64_t tile = first; tile < ntiles && ok; tile += gridDim.x, ++it) {
-            const int64_t row = tile * kThreads + tid;
-            const bool live = row < rows;
-            typename Epi::Pre pre{};
-            if (live) pre = epi.pre(row, xs);
+        const int64_t first = skipped ? ngroups : blockIdx.x;
+        for (int64_t grp = first; grp < ngroups && ok; grp += gridDim.x, ++it) {
+            typename Epi::Pre pre[R];
+#pragma unroll
+            for (int k = 0; k < R; ++k) {
+                const int64_t row = (grp * R + k) * kThreads + tid;
+                pre[k] = typename Epi::Pre{};
+                if (row < rows) pre[k] = epi.pre(row, xs);
+            }
             const int st = static_cast<int>(it % stages);
             if (__any_sync(0xffffffffu, !mbar_wait(&full_bar[st], (it / stages) & 1))) {
                 ok = false;
@@ -885,55 +966,73 @@ __global__ void __launch_bounds__(kThreads + 32)
                 break;
             }
             const int32_t *hdr = stage_hdr(st);
-            const int base = hdr[warp] - hdr[0];
-            const int width = (hdr[warp + 1] - hdr[warp]) >> 5;
-            const T *vs = stage_val(st) + base + lane;
-            const int16_t *cs = stage_col(st) + base + lane;
-            T acc = T(0);
-            const auto xr = xs.row(row);
-            for (int j0 = 0; j0 < width; j0 += 8) {
-                int16_t c[8];
-                T y[8];
+            T acc[R];
 #pragma unroll
-                for (int g = 0; g < 8; ++g) c[g] = j0 + g < width ? cs[(j0 + g) * 32] : kSlicePad;
+            for (int k = 0; k < R; ++k) {
+                const int64_t row = (grp * R + k) * kThreads + tid;
+                const int s = k * kWarps + warp;
+                const int base = hdr[s] - hdr[0];
+                const int width = (hdr[s + 1] - hdr[s]) >> 5;
+                const T *vs = stage_val(st) + base + lane;
+                const auto cs = cols.view(stage_col(st), hdr[0], base, lane);
+                const auto xr = xs.row(row);
+                T a = T(0);
+                for (int j0 = 0; j0 < width; j0 += 8) {
+                    bool on[8];
+                    T y[8];
 #pragma unroll
-                for (int g = 0; g < 8; ++g) y[g] = c[g] != kSlicePad ? xr(c[g]) : T(0);
+                    for (int g = 0; g < 8; ++g) {
+                        int c = 0;
+                        on[g] = j0 + g < width && cs.take(j0 + g, c);
+                        y[g] = on[g] ? xr(c) : T(0);
+                    }
 #pragma unroll
-                for (int g = 0; g < 8; ++g) acc += (j0 + g < width ? vs[(j0 + g) * 32] : T(0)) * y[g];
+                    for (int g = 0; g < 8; ++g)
+                        if (on[g]) a += vs[(j0 + g) * 32] * y[g];
+                }
+                acc[k] = a;
             }
             __syncwarp();
             if (lane == 0) mbar_arrive(&empty_bar[st]);
-            double red[KK];
 #pragma unroll
-            for (int q = 0; q < KK; ++q) red[q] = 0.0;
-            if (live) epi(row, acc, pre, red);
-            if constexpr (K > 0) {
-                // as in csr_pipe_kernel: the last warp of the tile adds the
-                // eight warp sums in warp order (ring of kMaxStages + 1 slots)
-                const int slot = static_cast<int>(local_tile % (kMaxStages + 1));
+            for (int k = 0; k < R; ++k) {
+                const int64_t block = grp * R + k;
+                const int64_t row = block * kThreads + tid;
+                double red[KK];
 #pragma unroll
-                for (int q = 0; q < K; ++q)
-                    for (int o = 16; o > 0; o >>= 1) red[q] += __shfl_down_sync(0xffffffffu, red[q], o);
-                if (lane == 0) {
+                for (int q = 0; q < KK; ++q) red[q] = 0.0;
+                if (row < rows) epi(row, acc[k], pre[k], red);
+                if constexpr (K > 0) {
+                    // as in csr_pipe_kernel: the last warp of the block adds
+                    // the eight warp sums in warp order; warps are at most
+                    // `stages` groups apart, so a ring of kMaxStages R + 1
+                    // slots never overwrites a slot still being read
+                    const int slot = static_cast<int>(local_block % kRing);
 #pragma unroll
-                    for (int q = 0; q < K; ++q) warp_sums[slot][warp][q] = red[q];
-                    __threadfence_block();
-                    if (atomicAdd(&warp_done[slot], 1) == kWarps - 1) {
+                    for (int q = 0; q < K; ++q)
+                        for (int o = 16; o > 0; o >>= 1) red[q] += __shfl_down_sync(0xffffffffu, red[q], o);
+                    if (lane == 0 && block < ntiles) {
+#pragma unroll
+                        for (int q = 0; q < K; ++q) warp_sums[slot][warp][q] = red[q];
                         __threadfence_block();
+                        if (atomicAdd(&warp_done[slot], 1) == kWarps - 1) {
+                            __threadfence_block();
 #pragma unroll
-                        for (int q = 0; q < K; ++q) {
-                            double v = 0.0;
-                            for (int w = 0; w < kWarps; ++w) v += warp_sums[slot][w][q];
-                            epi.partial[q * ntiles + tile] = v;
+                            for (int q = 0; q < K; ++q) {
+                                double v = 0.0;
+                                for (int w = 0; w < kWarps; ++w) v += warp_sums[slot][w][q];
+                                epi.partial[q * ntiles + block] = v;
+                            }
+                            warp_done[slot] = 0;
                         }
-                        warp_done[slot] = 0;
                     }
                 }
+                ++local_block;
             }
-            ++local_tile;
         }
     }
     __syncthreads();
+    pdl_trigger();  // the main loop is done: the next kernel may be scheduled
     if (tid == kThreads) {
         for (int st = 0; st < stages; ++st)
             if (armed[st]) mbar_wait(&full_bar[st], (armed[st] - 1) & 1);
@@ -962,17 +1061,69 @@ struct PipeConfig {
     // per SM, sliced = 1 directly (sliced_kernel, next-tile prefetch when
     // set), sliced = 2 through a ring of sliced_stages shared-memory stages
     // (sliced_pipe_kernel).
-    int sliced{0}, sliced_ctas{4}, prefetch{1}, sliced_stages{2};
+    // sliced_group: tiles per stage of the staged kernel (1, 2 or 4).
+    int sliced{0}, sliced_ctas{4}, prefetch{1}, sliced_stages{2}, sliced_group{1};
 };
 
-// Stage capacity (entries) of the staged sliced kernel for a's copy: its
-// largest tile, or 0 when a stage would exceed 64 KB.
+// Stage capacity (entries) of the staged sliced kernel for a's copy in
+// groups of R tiles: R times its largest tile, or 0 when a stage would
+// exceed 96 KB.
+template <class T, class Cols, int R>
+int sliced_stage_cap_for(int64_t tile_max) {
+    const int64_t cap = (tile_max * R + 255) & ~int64_t(255);
+    if (cap <= 0 || cap > (int64_t(96) << 10)) return 0;
+    return SlicedStage<T, Cols, R>(static_cast<int>(cap)).bytes <= (96 << 10) ? static_cast<int>(cap) : 0;
+}
 template <class T, class I>
-int sliced_stage_cap(const Csr<T, I> &a) {
-    if (a.bd) return 0;  // the staged kernel streams per-entry offsets only
-    const int64_t cap = (a.sl_tile_max + 255) & ~int64_t(255);
-    if (cap <= 0 || cap > (int64_t(64) << 10)) return 0;
-    return SlicedStage<T>(static_cast<int>(cap)).bytes <= (64 << 10) ? static_cast<int>(cap) : 0;
+int sliced_stage_cap(const Csr<T, I> &a, int group) {
+    switch (group) {
+        case 4: return a.bd ? sliced_stage_cap_for<T, StagedBand, 4>(a.sl_tile_max)
+                            : sliced_stage_cap_for<T, StagedOffsets, 4>(a.sl_tile_max);
+        case 2: return a.bd ? sliced_stage_cap_for<T, StagedBand, 2>(a.sl_tile_max)
+                            : sliced_stage_cap_for<T, StagedOffsets, 2>(a.sl_tile_max);
+        default: return a.bd ? sliced_stage_cap_for<T, StagedBand, 1>(a.sl_tile_max)
+                             : sliced_stage_cap_for<T, StagedOffsets, 1>(a.sl_tile_max);
+    }
+}
+
+// Dynamic shared memory the staged kernel's ring may take (the per-block
+// opt-in limit, 227 KB on B200, less its static barriers and sums).
+constexpr size_t kStagedSmemMax = size_t(200) << 10;
+
+// Shared memory of one stage of the staged kernel over a's copy.
+template <class T, class I>
+size_t sliced_stage_bytes(const Csr<T, I> &a, int group, int cap) {
+    auto bytes = [&](auto cols) -> size_t {
+        using Cols = decltype(cols);
+        switch (group) {
+            case 4: return SlicedStage<T, Cols, 4>(cap).bytes;
+            case 2: return SlicedStage<T, Cols, 2>(cap).bytes;
+            default: return SlicedStage<T, Cols, 1>(cap).bytes;
+        }
+    };
+    return a.bd ? bytes(StagedBand{}) : bytes(StagedOffsets{});
+}
+
+// A kernel as a type, for the helpers that take it as a template argument.
+template <auto K>
+struct KernelTag {
+    static constexpr auto kernel = K;
+};
+
+// Calls f(KernelTag<kernel>, cols) with the staged kernel instantiation for
+// a's column source and the group size.
+template <class T, class I, class XS, class Epi, class F>
+decltype(auto) with_staged_kernel(const Csr<T, I> &a, int group, F &&f) {
+    auto pick = [&](auto cols) -> decltype(auto) {
+        using Cols = decltype(cols);
+        switch (group) {
+            case 4: return f(KernelTag<sliced_pipe_kernel<T, 4, XS, Epi, Cols>>{}, cols);
+            case 2: return f(KernelTag<sliced_pipe_kernel<T, 2, XS, Epi, Cols>>{}, cols);
+            default: return f(KernelTag<sliced_pipe_kernel<T, 1, XS, Epi, Cols>>{}, cols);
+        }
+    };
+    if (a.bd) return pick(StagedBand{a.bd});
+    return pick(StagedOffsets{a.sc});
 }
 
 template <class T, class I, class C = I>
@@ -1155,16 +1306,23 @@ void launch_sliced(tf_ctx *ctx, const Csr<T, I> &a, const XS &xs, const Epi &epi
     const int64_t ntiles = (a.rows + kThreads - 1) / kThreads;
     const int early = ctx->stable && !rarely_runs(epi, 0) ? 1 : 0;
     if (cfg.sliced == 2 && !a.perm) {
-        const int cap = sliced_stage_cap(a);
-        if (cap > 0) {
-            const size_t smem = static_cast<size_t>(SlicedStage<T>(cap).bytes) * cfg.sliced_stages;
-            allow_smem<sliced_pipe_kernel<T, XS, Epi>>(smem);
-            const int resident = resident_ctas<sliced_pipe_kernel<T, XS, Epi>>(kThreads + 32, smem);
-            const int per_sm = cfg.sliced_ctas < resident || resident < 1 ? cfg.sliced_ctas : resident;
-            const int64_t g = static_cast<int64_t>(ctx->sm_count) * per_sm;
-            launch_kernel(ctx, name, sliced_pipe_kernel<T, XS, Epi>, static_cast<int>(ntiles < g ? ntiles : g),
-                          kThreads + 32, smem, a.rows, a.sp, a.sv, a.sc, cap, cfg.sliced_stages, early, xs, epi,
-                          ctx->fault);
+        const int cap = sliced_stage_cap(a, cfg.sliced_group);
+        const size_t stage = cap > 0 ? sliced_stage_bytes(a, cfg.sliced_group, cap) : 0;
+        // a ring deeper than the shared memory holds runs with fewer stages
+        // (the stage count changes the speed only)
+        const int stages = stage ? std::min<int>(cfg.sliced_stages, static_cast<int>(kStagedSmemMax / stage)) : 0;
+        if (stages >= 2) {
+            const size_t smem = stage * stages;
+            const int64_t ngroups = (ntiles + cfg.sliced_group - 1) / cfg.sliced_group;
+            with_staged_kernel<T, I, XS, Epi>(a, cfg.sliced_group, [&](auto tag, auto cols) {
+                constexpr auto kernel = decltype(tag)::kernel;
+                allow_smem<kernel>(smem);
+                const int resident = resident_ctas<kernel>(kThreads + 32, smem);
+                const int per_sm = cfg.sliced_ctas < resident || resident < 1 ? cfg.sliced_ctas : resident;
+                const int64_t g = static_cast<int64_t>(ctx->sm_count) * per_sm;
+                launch_kernel(ctx, name, kernel, static_cast<int>(ngroups < g ? ngroups : g), kThreads + 32, smem,
+                              a.rows, a.sp, a.sv, cols, cap, stages, early, xs, epi, ctx->fault);
+            });
             return;
         }
     }
@@ -1360,26 +1518,29 @@ PipeConfig autotune_columns(tf_ctx *ctx, const Csr<T, I> &a, const T *x, T *y, f
             PipeConfig sbest = best;
             float sbest_t = 0;
             bool sfirst = true;
-            // shapes: (kind, prefetch or stages, ctas); kind 1 direct, 2 staged
-            std::vector<std::tuple<int, int, int>> shapes;
-            const int cap = sliced_stage_cap(a);
+            // shapes: (kind, prefetch or stages, ctas, group); kind 1 direct,
+            // 2 staged (group: tiles per stage)
+            std::vector<std::tuple<int, int, int, int>> shapes;
             if (forced_pf >= 0) {
-                // "prefetch,ctas" forces the direct kernel, "2,stages,ctas" the staged one
-                int a3 = 0;
+                // "prefetch,ctas" forces the direct kernel, "2,stages,ctas[,group]" the staged one
+                int a3 = 0, a4 = 1;
                 const char *v = std::getenv("THERMOFEM_B200_SLICED_SHAPE");
-                if (v && std::sscanf(v, "%d,%d,%d", &forced_pf, &forced_ctas, &a3) == 3 && forced_pf == 2 && cap)
+                const int got = v ? std::sscanf(v, "%d,%d,%d,%d", &forced_pf, &forced_ctas, &a3, &a4) : 0;
+                const int group = got == 4 && (a4 == 2 || a4 == 4) ? a4 : 1;
+                if (got >= 3 && forced_pf == 2 && sliced_stage_cap(a, group))
                     shapes.emplace_back(2, forced_ctas < 2 ? 2 : (forced_ctas > kMaxStages ? kMaxStages : forced_ctas),
-                                        a3 < 1 ? 1 : a3);
+                                        a3 < 1 ? 1 : a3, group);
                 else
-                    shapes.emplace_back(1, forced_pf ? 1 : 0, forced_ctas < 1 ? 1 : forced_ctas);
+                    shapes.emplace_back(1, forced_pf ? 1 : 0, forced_ctas < 1 ? 1 : forced_ctas, 1);
             } else {
                 for (int pf : {0, 1})
-                    for (int ctas : {2, 3, 4, 5, 6}) shapes.emplace_back(1, pf, ctas);
-                if (cap)
-                    for (int stg : {2, 3})
-                        for (int ctas : {2, 3, 4, 5}) shapes.emplace_back(2, stg, ctas);
+                    for (int ctas : {2, 3, 4, 5, 6}) shapes.emplace_back(1, pf, ctas, 1);
+                for (int group : {1, 2, 4})
+                    if (sliced_stage_cap(a, group))
+                        for (int stg : {2, 3, 4})
+                            for (int ctas : {1, 2, 3, 4, 5}) shapes.emplace_back(2, stg, ctas, group);
             }
-            for (const auto &[kind, knob, ctas] : shapes) {
+            for (const auto &[kind, knob, ctas, group] : shapes) {
                 {
                     PipeConfig cfg = best;
                     cfg.sliced = kind;
@@ -1387,10 +1548,17 @@ PipeConfig autotune_columns(tf_ctx *ctx, const Csr<T, I> &a, const T *x, T *y, f
                     int resident = 0;
                     if (kind == 2) {
                         cfg.sliced_stages = knob;
-                        const size_t smem = static_cast<size_t>(SlicedStage<T>(cap).bytes) * knob;
-                        if (smem * ctas > 220 * 1024 && forced_pf < 0) continue;
-                        allow_smem<sliced_pipe_kernel<T, PlainX<T>, TuneStore<T>>>(smem);
-                        resident = resident_ctas<sliced_pipe_kernel<T, PlainX<T>, TuneStore<T>>>(kThreads + 32, smem);
+                        cfg.sliced_group = group;
+                        const size_t stage = sliced_stage_bytes(a, group, sliced_stage_cap(a, group));
+                        if ((stage * knob > kStagedSmemMax || stage * knob * ctas > 220 * 1024) && forced_pf < 0)
+                            continue;
+                        // (a forced ring deeper than the shared memory runs shallower, as launch_sliced does)
+                        const size_t smem = stage * std::min<int>(knob, static_cast<int>(kStagedSmemMax / stage));
+                        resident = with_staged_kernel<T, I, PlainX<T>, TuneStore<T>>(a, group, [&](auto tag, auto) {
+                            constexpr auto kernel = decltype(tag)::kernel;
+                            allow_smem<kernel>(smem);
+                            return resident_ctas<kernel>(kThreads + 32, smem);
+                        });
                     } else {
                         cfg.prefetch = knob;
                         // (the column source does not change the kernel's registers much; offsets bound it)
@@ -1403,10 +1571,10 @@ PipeConfig autotune_columns(tf_ctx *ctx, const Csr<T, I> &a, const T *x, T *y, f
                     const float ms = time_cfg(cfg);
                     if (tune_log())
                         std::fprintf(stderr,
-                                     "tf_autotune_spmv rows=%lld nnz=%lld T=%d %s %s=%d ctas=%d %.2f us\n",
+                                     "tf_autotune_spmv rows=%lld nnz=%lld T=%d %s %s=%d ctas=%d group=%d %.2f us\n",
                                      static_cast<long long>(a.rows), static_cast<long long>(a.nnz),
                                      static_cast<int>(sizeof(T)), a.bd ? "banded" : "sliced",
-                                     kind == 2 ? "staged stages" : "prefetch", knob, ctas, ms * 1e3f);
+                                     kind == 2 ? "staged stages" : "prefetch", knob, ctas, group, ms * 1e3f);
                     if (sfirst || ms < sbest_t) {
                         sbest_t = ms;
                         sbest = cfg;
