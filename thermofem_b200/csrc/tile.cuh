@@ -966,29 +966,49 @@ __global__ void __launch_bounds__(kThreads + 32)
                 break;
             }
             const int32_t *hdr = stage_hdr(st);
+            // The first 8 slots of all R slices are gathered before any
+            // product is added (8 R loads in flight per lane: the x gathers'
+            // L2 latency, not the bytes, bounds this loop), then each row
+            // adds its products left to right, slots past 8 in a second loop.
+            // A padding entry (value 0 in the copy) gathers nothing and adds
+            // 0 * 0 = +0: a row sum starts at +0 and never becomes -0 (an
+            // exact cancellation rounds to +0), so adding +0 leaves every
+            // bit of it as the entry-by-entry sum of the CSR kernels.
             T acc[R];
+            T y[R][8];
+            int base[R], width[R];
 #pragma unroll
             for (int k = 0; k < R; ++k) {
-                const int64_t row = (grp * R + k) * kThreads + tid;
                 const int s = k * kWarps + warp;
-                const int base = hdr[s] - hdr[0];
-                const int width = (hdr[s + 1] - hdr[s]) >> 5;
-                const T *vs = stage_val(st) + base + lane;
-                const auto cs = cols.view(stage_col(st), hdr[0], base, lane);
-                const auto xr = xs.row(row);
+                base[k] = hdr[s] - hdr[0];
+                width[k] = (hdr[s + 1] - hdr[s]) >> 5;
+                const auto cs = cols.view(stage_col(st), hdr[0], base[k], lane);
+                const auto xr = xs.row((grp * R + k) * kThreads + tid);
+#pragma unroll
+                for (int g = 0; g < 8; ++g) {
+                    int c = 0;
+                    y[k][g] = g < width[k] && cs.take(g, c) ? xr(c) : T(0);
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < R; ++k) {
+                const T *vs = stage_val(st) + base[k] + lane;
                 T a = T(0);
-                for (int j0 = 0; j0 < width; j0 += 8) {
-                    bool on[8];
-                    T y[8];
 #pragma unroll
-                    for (int g = 0; g < 8; ++g) {
-                        int c = 0;
-                        on[g] = j0 + g < width && cs.take(j0 + g, c);
-                        y[g] = on[g] ? xr(c) : T(0);
+                for (int g = 0; g < 8; ++g) a += (g < width[k] ? vs[g * 32] : T(0)) * y[k][g];
+                if (width[k] > 8) {
+                    const auto cs = cols.view(stage_col(st), hdr[0], base[k], lane);
+                    const auto xr = xs.row((grp * R + k) * kThreads + tid);
+                    for (int j0 = 8; j0 < width[k]; j0 += 8) {
+                        T z[8];
+#pragma unroll
+                        for (int g = 0; g < 8; ++g) {
+                            int c = 0;
+                            z[g] = j0 + g < width[k] && cs.take(j0 + g, c) ? xr(c) : T(0);
+                        }
+#pragma unroll
+                        for (int g = 0; g < 8; ++g) a += (j0 + g < width[k] ? vs[(j0 + g) * 32] : T(0)) * z[g];
                     }
-#pragma unroll
-                    for (int g = 0; g < 8; ++g)
-                        if (on[g]) a += vs[(j0 + g) * 32] * y[g];
                 }
                 acc[k] = a;
             }
