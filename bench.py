@@ -43,8 +43,9 @@ SEED_MATRIX, SEED_RHS = 1001, 1002
 AMG = dict(jacobi_weight=2.0 / 3.0, pre_sweeps=1, post_sweeps=1, cycle="v", coarse_rows=64)
 METRIC = "time-to-1e-8 FP64 relative residual (s), AMG-PCG V-cycle, FP32 hierarchy / FP64 outer"
 # DRAM bytes (read + write) per algorithmic byte of one launch, from ncu
-# captures of the same kernel and layout on the 128^3 problem (FP64 Krylov
-# operator, FP32 finest level of the mixed hierarchy; profiles/).  The
+# captures of the same kernel and layout on a smaller case of the same
+# stencil (FP64 Krylov operator, FP32 finest level of the mixed hierarchy;
+# sliced and CSR row tiles on 128^3, the staged banded kernel on 192^3).  The
 # operators are one stencil at every size, so traffic grows with the bytes;
 # layouts without a capture report null.
 TRAFFIC_RATIO = {
@@ -52,7 +53,17 @@ TRAFFIC_RATIO = {
     ("f64", "csr"): (171013632 + 13778176) / 187760644,
     ("f32", "sliced"): (96349184 + 4392704) / 104726532,
     ("f32", "csr"): (104301056 + 5819136) / 112656388,
+    ("f64", "banded"): 516795905 / 521662468,
+    ("f32", "banded"): 262385128 / 267448324,
 }
+TRAFFIC_SOURCE = {"banded": "192^3"}
+
+
+def traffic_source(layout):
+    return (f"ncu DRAM bytes per algorithmic byte of the same kernel and layout on "
+            f"{TRAFFIC_SOURCE.get(layout, '128^3')}, times this launch's algorithmic bytes")
+
+
 SOLVER = "PCG / BiCGStab + aggregation AMG V(1,1), Jacobi w=2/3, coarse LU <= 64 rows, rtol 1e-8"
 
 
@@ -801,12 +812,11 @@ def headline(args):
                                   "device time in its ncu launch list",
                          "peak_source": peak_kind, "algorithmic_bytes": algo32, "launch_ms": spmv32_ms,
                          "timing": "cold (L2 evicted by a read before each launch), CUDA events",
-                         "traffic_source": "ncu DRAM bytes per algorithmic byte of the same kernel on 128^3"},
+                         "traffic_source": traffic_source(layout32)},
             "roofline_fp64_operator": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                                        "frac": achieved / peak, "traffic": traffic, "kernel": kernel64,
                                        "peak_source": peak_kind, "algorithmic_bytes": algo, "launch_ms": spmv_ms,
-                                       "traffic_source": "ncu DRAM bytes per algorithmic byte of the same kernel "
-                                                         "on 128^3"},
+                                       "traffic_source": traffic_source(layout)},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": 2 * n * 8, "d2h_bytes_per_step": n * 8},
             "gpu_launches": int(pcg_mixed["launches"]),
