@@ -456,7 +456,8 @@ def test_sliced_layout_gives_identical_solves(ctx, case, shape, monkeypatch):
         assert torch.equal(out[0][2], other[2])
 
 
-@pytest.mark.parametrize("shape", ["0,2", "1,3", "1,8", "0,5", "2,2,3", "2,3,2", "2,3,3,2", "2,2,2,4", None])
+@pytest.mark.parametrize("shape", ["0,2", "1,3", "1,8", "0,5", "2,2,3", "2,3,2", "2,3,3,2", "2,2,2,4", "3,2,3",
+                                   "3,3,2", None])
 @pytest.mark.parametrize("case", ["heat3d25-cg-f32", "heat3d25-bicgstab-f64", "heat3d184-cg-f32"])
 def test_banded_layout_gives_identical_solves(ctx, case, shape, monkeypatch):
     # Stencil operators (the solver's operator, the finest level) carry a
@@ -466,12 +467,14 @@ def test_banded_layout_gives_identical_solves(ctx, case, shape, monkeypatch):
     # (padding lanes gather nothing): the same bits as the CSR arrays
     # (THERMOFEM_B200_SLICED=0), whatever the launch shape: "p,c" the direct
     # kernel (prefetch p, c CTAs per SM), "2,s,c[,g]" the staged one (s stages
-    # of g tiles' values and slots copied in bulk into shared memory).  184^3:
+    # of g tiles' values and slots copied in bulk into shared memory), "3,s,c"
+    # the staged one with four rows per lane (reducing epilogues: one row per
+    # lane, the same stages).  184^3:
     # couplings 33,856 rows apart, beyond 2-byte offsets, so the CSR arrays
     # stream 4-byte columns there.
     side = int(case.split("-")[0][6:])
-    if side > 100 and shape not in (None, "1,3", "2,2,3", "2,3,3,2"):
-        pytest.skip("the large case runs four launch shapes")
+    if side > 100 and shape not in (None, "1,3", "2,2,3", "2,3,3,2", "3,2,3"):
+        pytest.skip("the large case runs five launch shapes")
     m = P.heat3d(side, seed=85)
     n = len(m[0]) - 1
     b = torch.tensor(P.rhs_uniform(n, 86), device="cuda")

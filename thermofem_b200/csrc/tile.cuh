@@ -848,10 +848,38 @@ struct SlicedStage {
     }
 };
 
-template <class T, int R, class XS, class Epi, class Cols>
+// Four values of a stage, 16-byte aligned, into registers.
+template <class T>
+__device__ __forceinline__ void load4(T (&v)[4], const T *p) {
+    if constexpr (sizeof(T) == 4) {
+        const float4 t = *reinterpret_cast<const float4 *>(p);
+        v[0] = t.x;
+        v[1] = t.y;
+        v[2] = t.z;
+        v[3] = t.w;
+    } else {
+        const double2 a = *reinterpret_cast<const double2 *>(p), b = *reinterpret_cast<const double2 *>(p + 2);
+        v[0] = a.x;
+        v[1] = a.y;
+        v[2] = b.x;
+        v[3] = b.y;
+    }
+}
+
+// kQuad (banded copies, R = 4, epilogues without partial sums): consumer
+// lanes take four consecutive rows each instead of one -- warp w owns
+// slices 4w..4w+3 of the group, lane 8q + p rows 4p..4p+3 of slice 4w + q.
+// Per slot a lane reads the slot pair once for its four rows, their four
+// values with one 16-byte load (slices start on 32-entry boundaries, so a
+// row quad's values are 16-byte aligned in the stage) and gathers x at four
+// consecutive addresses, which cuts the instructions per entry about in
+// half; each row still adds its products slot by slot from +0.
+template <class T, int R, class XS, class Epi, class Cols, bool kQuad = false>
 __global__ void __launch_bounds__(kThreads + 32)
     sliced_pipe_kernel(int64_t rows, const int32_t *__restrict__ sp, const T *__restrict__ sv, Cols cols, int cap,
                        int stages, int early, XS xs, Epi epi, int *fault) {
+    static_assert(!kQuad || (R == 4 && Epi::kReduce == 0 && std::is_same_v<Cols, StagedBand>),
+                  "the four-rows-per-lane form serves banded copies in groups of 4 tiles without partial sums");
     constexpr int K = Epi::kReduce;
     constexpr int KK = K > 0 ? K : 1;
     constexpr int kWarps = kThreads / 32;
@@ -943,6 +971,71 @@ __global__ void __launch_bounds__(kThreads + 32)
         }
         enter();
         if (!ok) atomicExch(fault, 1);
+    } else if (kQuad && tid < kThreads) {
+        if constexpr (kQuad) {
+            // ---- consumers, four rows per lane ----
+            pdl_enter();
+            const int lane = tid & 31, warp = tid >> 5;
+            const int q = lane >> 3, p = lane & 7;
+            const int s = warp * 4 + q;  // the lane's slice within the group
+            uint32_t it = 0;
+            const bool skipped = epi.skip();
+            if (tid == 0) skipped_cta = skipped ? 1 : 0;
+            const int64_t first = skipped ? ngroups : blockIdx.x;
+            for (int64_t grp = first; grp < ngroups && ok; grp += gridDim.x, ++it) {
+                const int64_t row0 = grp * (R * kThreads) + s * 32 + 4 * p;
+                typename Epi::Pre pre[4];
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    pre[k] = typename Epi::Pre{};
+                    if (row0 + k < rows) pre[k] = epi.pre(row0 + k, xs);
+                }
+                const int st = static_cast<int>(it % stages);
+                if (__any_sync(0xffffffffu, !mbar_wait(&full_bar[st], (it / stages) & 1))) {
+                    ok = false;
+                    if (lane == 0) atomicExch(fault, 1);
+                    break;
+                }
+                const int32_t *hdr = stage_hdr(st);
+                const int base = hdr[s] - hdr[0];
+                const int width = (hdr[s + 1] - hdr[s]) >> 5;
+                const int2 *band = static_cast<const int2 *>(stage_col(st)) +
+                                   static_cast<int>((hdr[0] >> 5) - StagedBand::lo(hdr[0])) + (base >> 5);
+                const T *vs = stage_val(st) + base + 4 * p;
+                const auto xr = xs.row(row0);
+                T acc[4] = {T(0), T(0), T(0), T(0)};
+                for (int j0 = 0; j0 < width; j0 += 8) {
+                    T y[8][4];
+#pragma unroll
+                    for (int g = 0; g < 8; ++g) {
+                        int c = 0;
+                        unsigned pad = 0xFu;  // bit k: row 4p + k has no entry in this slot
+                        if (j0 + g < width) {
+                            const int2 v = band[j0 + g];
+                            c = v.x;
+                            pad = (static_cast<unsigned>(v.y) >> (4 * p)) & 0xFu;
+                        }
+#pragma unroll
+                        for (int k = 0; k < 4; ++k) y[g][k] = (pad >> k) & 1u ? T(0) : xr(c + k);
+                    }
+#pragma unroll
+                    for (int g = 0; g < 8; ++g) {
+                        if (j0 + g < width) {
+                            T v[4];
+                            load4(v, vs + (j0 + g) * 32);
+#pragma unroll
+                            for (int k = 0; k < 4; ++k) acc[k] += v[k] * y[g][k];
+                        }
+                    }
+                }
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&empty_bar[st]);
+                double red[1] = {0.0};
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
+                    if (row0 + k < rows) epi(row0 + k, acc[k], pre[k], red);
+            }
+        }
     } else if (tid < kThreads) {
         // ---- consumers: warp w owns slice w of each tile of the group ----
         pdl_enter();
@@ -1080,8 +1173,9 @@ struct PipeConfig {
     // Operators with a sliced copy: stream it with sliced_ctas resident CTAs
     // per SM, sliced = 1 directly (sliced_kernel, next-tile prefetch when
     // set), sliced = 2 through a ring of sliced_stages shared-memory stages
-    // (sliced_pipe_kernel).
-    // sliced_group: tiles per stage of the staged kernel (1, 2 or 4).
+    // (sliced_pipe_kernel, sliced_group tiles per stage: 1, 2 or 4), sliced =
+    // 3 the same with four rows per consumer lane (banded copies, 4 tiles
+    // per stage).
     int sliced{0}, sliced_ctas{4}, prefetch{1}, sliced_stages{2}, sliced_group{1};
 };
 
@@ -1131,11 +1225,15 @@ struct KernelTag {
 };
 
 // Calls f(KernelTag<kernel>, cols) with the staged kernel instantiation for
-// a's column source and the group size.
+// a's column source and the group size; quad: the four-rows-per-lane form,
+// where it applies (a banded copy, an epilogue without partial sums; group
+// 4 is then implied).
 template <class T, class I, class XS, class Epi, class F>
-decltype(auto) with_staged_kernel(const Csr<T, I> &a, int group, F &&f) {
+decltype(auto) with_staged_kernel(const Csr<T, I> &a, int group, F &&f, bool quad = false) {
     auto pick = [&](auto cols) -> decltype(auto) {
         using Cols = decltype(cols);
+        if constexpr (std::is_same_v<Cols, StagedBand> && Epi::kReduce == 0)
+            if (quad) return f(KernelTag<sliced_pipe_kernel<T, 4, XS, Epi, Cols, true>>{}, cols);
         switch (group) {
             case 4: return f(KernelTag<sliced_pipe_kernel<T, 4, XS, Epi, Cols>>{}, cols);
             case 2: return f(KernelTag<sliced_pipe_kernel<T, 2, XS, Epi, Cols>>{}, cols);
@@ -1325,16 +1423,20 @@ void launch_sliced(tf_ctx *ctx, const Csr<T, I> &a, const XS &xs, const Epi &epi
                    const PipeConfig &cfg) {
     const int64_t ntiles = (a.rows + kThreads - 1) / kThreads;
     const int early = ctx->stable && !rarely_runs(epi, 0) ? 1 : 0;
-    if (cfg.sliced == 2 && !a.perm) {
-        const int cap = sliced_stage_cap(a, cfg.sliced_group);
-        const size_t stage = cap > 0 ? sliced_stage_bytes(a, cfg.sliced_group, cap) : 0;
+    if (cfg.sliced >= 2 && !a.perm) {
+        // sliced = 3: four rows per lane over a banded copy (epilogues with
+        // partial sums take the one-row form with the same stages)
+        const bool quad = cfg.sliced == 3 && a.bd && Epi::kReduce == 0;
+        const int group = cfg.sliced == 3 ? 4 : cfg.sliced_group;
+        const int cap = sliced_stage_cap(a, group);
+        const size_t stage = cap > 0 ? sliced_stage_bytes(a, group, cap) : 0;
         // a ring deeper than the shared memory holds runs with fewer stages
         // (the stage count changes the speed only)
         const int stages = stage ? std::min<int>(cfg.sliced_stages, static_cast<int>(kStagedSmemMax / stage)) : 0;
         if (stages >= 2) {
             const size_t smem = stage * stages;
-            const int64_t ngroups = (ntiles + cfg.sliced_group - 1) / cfg.sliced_group;
-            with_staged_kernel<T, I, XS, Epi>(a, cfg.sliced_group, [&](auto tag, auto cols) {
+            const int64_t ngroups = (ntiles + group - 1) / group;
+            with_staged_kernel<T, I, XS, Epi>(a, group, [&](auto tag, auto cols) {
                 constexpr auto kernel = decltype(tag)::kernel;
                 allow_smem<kernel>(smem);
                 const int resident = resident_ctas<kernel>(kThreads + 32, smem);
@@ -1342,7 +1444,7 @@ void launch_sliced(tf_ctx *ctx, const Csr<T, I> &a, const XS &xs, const Epi &epi
                 const int64_t g = static_cast<int64_t>(ctx->sm_count) * per_sm;
                 launch_kernel(ctx, name, kernel, static_cast<int>(ngroups < g ? ngroups : g), kThreads + 32, smem,
                               a.rows, a.sp, a.sv, cols, cap, stages, early, xs, epi, ctx->fault);
-            });
+            }, quad);
             return;
         }
     }
@@ -1546,8 +1648,11 @@ PipeConfig autotune_columns(tf_ctx *ctx, const Csr<T, I> &a, const T *x, T *y, f
                 int a3 = 0, a4 = 1;
                 const char *v = std::getenv("THERMOFEM_B200_SLICED_SHAPE");
                 const int got = v ? std::sscanf(v, "%d,%d,%d,%d", &forced_pf, &forced_ctas, &a3, &a4) : 0;
-                const int group = got == 4 && (a4 == 2 || a4 == 4) ? a4 : 1;
-                if (got >= 3 && forced_pf == 2 && sliced_stage_cap(a, group))
+                const int group = forced_pf == 3 ? 4 : (got == 4 && (a4 == 2 || a4 == 4) ? a4 : 1);
+                if (got >= 3 && forced_pf == 3 && a.bd && sliced_stage_cap(a, 4))
+                    shapes.emplace_back(3, forced_ctas < 2 ? 2 : (forced_ctas > kMaxStages ? kMaxStages : forced_ctas),
+                                        a3 < 1 ? 1 : a3, 4);
+                else if (got >= 3 && forced_pf == 2 && sliced_stage_cap(a, group))
                     shapes.emplace_back(2, forced_ctas < 2 ? 2 : (forced_ctas > kMaxStages ? kMaxStages : forced_ctas),
                                         a3 < 1 ? 1 : a3, group);
                 else
@@ -1559,6 +1664,9 @@ PipeConfig autotune_columns(tf_ctx *ctx, const Csr<T, I> &a, const T *x, T *y, f
                     if (sliced_stage_cap(a, group))
                         for (int stg : {2, 3, 4})
                             for (int ctas : {1, 2, 3, 4, 5}) shapes.emplace_back(2, stg, ctas, group);
+                if (a.bd && sliced_stage_cap(a, 4))
+                    for (int stg : {2, 3, 4})
+                        for (int ctas : {1, 2, 3, 4}) shapes.emplace_back(3, stg, ctas, 4);
             }
             for (const auto &[kind, knob, ctas, group] : shapes) {
                 {
@@ -1566,7 +1674,7 @@ PipeConfig autotune_columns(tf_ctx *ctx, const Csr<T, I> &a, const T *x, T *y, f
                     cfg.sliced = kind;
                     cfg.sliced_ctas = ctas;
                     int resident = 0;
-                    if (kind == 2) {
+                    if (kind >= 2) {
                         cfg.sliced_stages = knob;
                         cfg.sliced_group = group;
                         const size_t stage = sliced_stage_bytes(a, group, sliced_stage_cap(a, group));
@@ -1574,11 +1682,14 @@ PipeConfig autotune_columns(tf_ctx *ctx, const Csr<T, I> &a, const T *x, T *y, f
                             continue;
                         // (a forced ring deeper than the shared memory runs shallower, as launch_sliced does)
                         const size_t smem = stage * std::min<int>(knob, static_cast<int>(kStagedSmemMax / stage));
-                        resident = with_staged_kernel<T, I, PlainX<T>, TuneStore<T>>(a, group, [&](auto tag, auto) {
-                            constexpr auto kernel = decltype(tag)::kernel;
-                            allow_smem<kernel>(smem);
-                            return resident_ctas<kernel>(kThreads + 32, smem);
-                        });
+                        resident = with_staged_kernel<T, I, PlainX<T>, TuneStore<T>>(
+                            a, group,
+                            [&](auto tag, auto) {
+                                constexpr auto kernel = decltype(tag)::kernel;
+                                allow_smem<kernel>(smem);
+                                return resident_ctas<kernel>(kThreads + 32, smem);
+                            },
+                            kind == 3);
                     } else {
                         cfg.prefetch = knob;
                         // (the column source does not change the kernel's registers much; offsets bound it)
@@ -1594,7 +1705,8 @@ PipeConfig autotune_columns(tf_ctx *ctx, const Csr<T, I> &a, const T *x, T *y, f
                                      "tf_autotune_spmv rows=%lld nnz=%lld T=%d %s %s=%d ctas=%d group=%d %.2f us\n",
                                      static_cast<long long>(a.rows), static_cast<long long>(a.nnz),
                                      static_cast<int>(sizeof(T)), a.bd ? "banded" : "sliced",
-                                     kind == 2 ? "staged stages" : "prefetch", knob, ctas, group, ms * 1e3f);
+                                     kind == 3 ? "quad stages" : (kind == 2 ? "staged stages" : "prefetch"), knob, ctas,
+                                     group, ms * 1e3f);
                     if (sfirst || ms < sbest_t) {
                         sbest_t = ms;
                         sbest = cfg;
