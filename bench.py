@@ -406,7 +406,7 @@ def run_workload(args):
     del off, idx, val
     b = torch.tensor(P.rhs_uniform(n, SEED_RHS), device="cuda")
     res = {}
-    for hier in ("f32", "f64"):
+    for hier in ("f32", "f64", "f32v"):
         opts = dict(AMG, cycle=cycle)
         s = kind(tf.solver_options(), "amg", tf.amg_options(hierarchy_type=hier, **opts, **_small(args)), ctx=ctx)
         t0 = time.perf_counter()
@@ -432,7 +432,9 @@ def run_workload(args):
         "workload": f"{args.workload} {m}^3 ({n} rows, {a.nnz} nnz), {label}, Jacobi w=2/3 V/W(1,1), rtol 1e-8",
         "metric": "time-to-1e-8 FP64 relative residual (s), median", "unit": "s",
         "mixed_f32_hierarchy": res["f32"], "plain_fp64": res["f64"],
-        "speedup_mixed_vs_fp64": res["f64"]["s"] / res["f32"]["s"], "data": "synthetic (seeded generator)"}),
+        "speedup_mixed_vs_fp64": res["f64"]["s"] / res["f32"]["s"],
+        "f32_operators_f64_cycle": res["f32v"], "speedup_f32_operators_vs_fp64": res["f64"]["s"] / res["f32v"]["s"],
+        "data": "synthetic (seeded generator)"}),
         flush=True)
 
 

@@ -38,6 +38,9 @@ extern "C" {
 #define TF_F64 1
 #define TF_I32 2
 #define TF_I64 3
+/* tf_amg_options.hierarchy_type only: operators stored in FP32, the cycle's
+ * vectors and arithmetic in FP64 (no reference counterpart). */
+#define TF_F32_VALUES 4
 
 /* Solve status, values of thermofem::SolveStatus (include/Solver/
  * Interfaces.cuh:10). */
@@ -290,7 +293,8 @@ typedef struct {
     int absorb_singletons;   /* default 1 */
     int compact_sort_keys;   /* default 0; does not change results */
     int cycle;               /* TF_CYCLE_V */
-    int hierarchy_type;      /* TF_F64 or TF_F32 storage/arithmetic of the cycle; -1 = same as vectors */
+    int hierarchy_type;      /* TF_F64 or TF_F32 storage/arithmetic of the cycle, TF_F32_VALUES (FP32 operators,
+                                FP64 cycle); -1 = same as vectors */
     int coarse_lu_rows;      /* LU when the last level has <= this many rows; default 64, max 256 */
     int small_level_rows;    /* levels (below the finest) with <= this many rows run each sub-cycle as one
                                 launch out of shared memory (one CTA when they fit, else a thread-block

@@ -19,6 +19,7 @@ LIB_PATH = os.path.join(_PKG, "lib", "libthermofem_b200.so")
 
 OK, ERR_INVALID, ERR_CUDA, ERR_LENGTH, ERR_LOGIC, ERR_TIMEOUT, ERR_NOMEM, ERR_RUNTIME = 0, -1, -2, -3, -4, -5, -6, -7
 F32, F64, I32, I64 = 0, 1, 2, 3
+F32_VALUES = 4  # tf_amg_options.hierarchy_type: FP32 operators under an FP64 cycle
 CYCLE = {"v": 0, "w": 1, "f": 2}
 SOLVER_CG, SOLVER_BICGSTAB = 0, 1
 PRECOND_IDENTITY, PRECOND_AMG = 0, 1

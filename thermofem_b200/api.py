@@ -9,7 +9,7 @@ from dataclasses import dataclass
 import numpy as np
 import torch
 
-from . import (AmgOptions, Csr, HostCsr, SolveResult, SolverOptions, F32, F64, I32, I64, CYCLE, SOLVER_CG,
+from . import (AmgOptions, Csr, HostCsr, SolveResult, SolverOptions, F32, F64, F32_VALUES, I32, I64, CYCLE, SOLVER_CG,
                SOLVER_BICGSTAB, PRECOND_AMG, PRECOND_IDENTITY, check, lib)
 
 __all__ = ["Context", "DeviceCsr", "Transfer", "Amg", "Jacobi", "Cg", "BiCgStab", "Batch", "Mlp", "row_features", "MLP_PARAMS",
@@ -448,7 +448,7 @@ def amg_options(**kw) -> AmgOptions:
             o._damping_model_ref = v  # the model must live until the options are used
             v = v.h.value if v is not None else None
         if k == "hierarchy_type" and not isinstance(v, int):
-            v = {torch.float32: F32, torch.float64: F64, "f32": F32, "f64": F64, None: -1}[v]
+            v = {torch.float32: F32, torch.float64: F64, "f32": F32, "f64": F64, "f32v": F32_VALUES, None: -1}[v]
         if not hasattr(o, k):
             raise TypeError(f"unknown AMG option {k}")
         setattr(o, k, v)

@@ -29,7 +29,8 @@ AmgConfig::AmgConfig(const tf_amg_options &opt) : o(opt) {
         !std::isfinite(p.strength_threshold) || p.strength_threshold < 0 || p.strength_threshold > 1 ||
         !std::isfinite(p.jacobi_weight) || p.jacobi_weight <= 0 || p.jacobi_weight >= 2 ||
         (p.cycle != TF_CYCLE_V && p.cycle != TF_CYCLE_W && p.cycle != TF_CYCLE_F) ||
-        (p.hierarchy_type != -1 && p.hierarchy_type != TF_F32 && p.hierarchy_type != TF_F64) ||
+        (p.hierarchy_type != -1 && p.hierarchy_type != TF_F32 && p.hierarchy_type != TF_F64 &&
+         p.hierarchy_type != TF_F32_VALUES) ||
         p.coarse_lu_rows < 1 || p.coarse_lu_rows > 256 || p.small_level_rows < 0)
         fail(TF_ERR_INVALID, "Invalid AMG options");
     model = damping_model_of(p.damping_model);
@@ -114,21 +115,23 @@ class PhaseMarks {
     std::vector<std::pair<int, cudaEvent_t>> marks_;
 };
 
-template <class S>
+template <class S, class V = S>
 struct Level {
     int64_t n{0}, nnz{0};
     DeviceBuffer<int32_t> rp, ci;
-    DeviceBuffer<S> val, dinv, rhs, x0, x1, r;
+    DeviceBuffer<V> val;  // values, stored in V (FP32 under an FP64 cycle, or S)
+    DeviceBuffer<S> val_s;  // V != S: the values widened to S, for the small-level region only
+    DeviceBuffer<S> dinv, rhs, x0, x1, r;
     DeviceBuffer<int32_t> map, off, mem;
     DeviceBuffer<int16_t> cd;  // columns as row offsets, when they fit
-    SlicedCopy<S> sl;          // sliced copy for the SpMV family, when built
+    SlicedCopy<V> sl;          // sliced copy for the SpMV family, when built
     bool sliced_on{true};      // the cycle streams sl (chosen at setup, select_layouts)
     int coarse{0};
     int cur{0};
     S *x() const { return cur ? x1.data() : x0.data(); }
     S *other() const { return cur ? x0.data() : x1.data(); }
-    Csr<S, int32_t> csr() const {
-        Csr<S, int32_t> c;
+    Csr<S, int32_t, V> csr() const {
+        Csr<S, int32_t, V> c;
         c.rows = c.cols = n;
         c.nnz = nnz;
         c.rp = rp.data();
@@ -138,9 +141,22 @@ struct Level {
         if (sliced_on) sl.attach(c);
         return c;
     }
+    // Values and structure alone, in V (what the copy builders read).
+    Csr<V, int32_t> values() const {
+        Csr<V, int32_t> c;
+        c.rows = c.cols = n;
+        c.nnz = nnz;
+        c.rp = rp.data();
+        c.ci = ci.data();
+        c.val = val.data();
+        c.cd = cd.data();
+        return c;
+    }
 };
 
-template <class S>
+// S: the cycle's vectors and arithmetic; V: how the level operators' values
+// are stored (V = S, or FP32 values under an FP64 cycle).
+template <class S, class V = S>
 class HierarchyImpl final : public Hierarchy {
   public:
     HierarchyImpl(const AmgConfig &cfg) : cfg_(cfg), w_(static_cast<S>(cfg.model ? 1.0 : cfg.o.jacobi_weight)) {
@@ -168,7 +184,7 @@ class HierarchyImpl final : public Hierarchy {
             if (!row_stats(ctx, nc, row_max.data()))
                 fail(TF_ERR_INVALID, "Native AMG: missing/zero diagonal, non-finite value or reciprocal in hierarchy");
             levels_.emplace_back();
-            Level<S> &l = levels_.back();
+            Level<S, V> &l = levels_.back();
             l.n = nc.rows;
             l.nnz = nc.nnz;
             l.rp.allocate(static_cast<size_t>(l.n) + 1);
@@ -181,14 +197,16 @@ class HierarchyImpl final : public Hierarchy {
             // The diagonal must also invert in the iteration precision.
             inverse_diagonal(ctx, l.csr(), l.dinv.data());
             // learned damping: dinv_i scaled by omega_i, sweeps with weight 1
-            if (cfg_.model) learned_damping(ctx, *cfg_.model, l.csr(), depth, l.dinv.data());
+            if constexpr (std::is_same_v<S, V>) {
+                if (cfg_.model) learned_damping(ctx, *cfg_.model, l.csr(), depth, l.dinv.data());
+            }
             marks.mark(ctx, kPhColumns);
             if (delta_columns_enabled() && l.nnz > 0) {
                 l.cd.allocate(static_cast<size_t>(l.nnz));
                 if (!delta_columns(ctx, l.n, l.rp.data(), l.ci.data(), l.cd.data())) l.cd.release();
             }
-            if (sliced_enabled() && !(banded_enabled() && build_banded(ctx, l.csr(), l.sl)) && l.cd.data())
-                build_sliced(ctx, l.csr(), l.sl, true);
+            if (sliced_enabled() && !(banded_enabled() && build_banded(ctx, l.values(), l.sl)) && l.cd.data())
+                build_sliced(ctx, l.values(), l.sl, true);
             // Launch shape of this level's row-tile kernels (cached by shape).
             marks.mark(ctx, kPhTuning);
             fill_zero(ctx, l.n, l.rhs.data());
@@ -328,7 +346,8 @@ class HierarchyImpl final : public Hierarchy {
     int level_count() const override { return static_cast<int>(levels_.size()); }
     tf_csr level_matrix(int d) const override {
         const auto &l = levels_.at(static_cast<size_t>(d));
-        tf_csr c{l.n, l.n, l.nnz, TF_I32, storage_type(), l.rp.data(), l.ci.data(), l.val.data()};
+        const int vt = std::is_same_v<V, double> ? TF_F64 : TF_F32;
+        tf_csr c{l.n, l.n, l.nnz, TF_I32, vt, l.rp.data(), l.ci.data(), l.val.data()};
         return c;
     }
     void level_spmv(tf_ctx *ctx, int d, const void *x, void *y) const override {
@@ -360,7 +379,7 @@ class HierarchyImpl final : public Hierarchy {
     template <class T>
     void apply_t(tf_ctx *ctx, const T *rhs, T *x) {
         StableScope stable(ctx);  // level operators are read-only from here on
-        Level<S> &f = levels_.front();
+        Level<S, V> &f = levels_.front();
         convert(ctx, f.n, rhs, f.rhs.data());
         run_cycle(ctx);
         convert(ctx, f.n, levels_.front().x(), x);
@@ -370,7 +389,7 @@ class HierarchyImpl final : public Hierarchy {
     template <class T>
     const void *open_t(tf_ctx *ctx, const T *rhs) {
         StableScope stable(ctx);
-        Level<S> &f = levels_.front();
+        Level<S, V> &f = levels_.front();
         cudaStreamCaptureStatus capturing;
         cuda_check(cudaStreamIsCapturing(ctx->stream, &capturing), "capture status");
         if (capturing != cudaStreamCaptureStatusNone && fuse_ > 0) {
@@ -451,7 +470,7 @@ class HierarchyImpl final : public Hierarchy {
     }
 
     // ---- level operations: launched, or recorded as a small-level program step ----
-    void op_jacobi_zero(tf_ctx *ctx, Level<S> &l) {
+    void op_jacobi_zero(tf_ctx *ctx, Level<S, V> &l) {
         if (recording_) {
             if (rec_.size() > region_start_) {
                 CoarseStep<S> &prev = rec_.back();
@@ -495,7 +514,7 @@ class HierarchyImpl final : public Hierarchy {
         }
     }
 
-    void op_zero(tf_ctx *ctx, Level<S> &l) {
+    void op_zero(tf_ctx *ctx, Level<S, V> &l) {
         if (recording_) {
             CoarseStep<S> s;
             s.op = kStepZero;
@@ -508,7 +527,7 @@ class HierarchyImpl final : public Hierarchy {
         }
     }
 
-    void sweep(tf_ctx *ctx, Level<S> &l, const int32_t *map = nullptr, const S *e = nullptr) {
+    void sweep(tf_ctx *ctx, Level<S, V> &l, const int32_t *map = nullptr, const S *e = nullptr) {
         if (recording_) {
             CoarseStep<S> s;
             s.op = kStepSweep;
@@ -516,7 +535,7 @@ class HierarchyImpl final : public Hierarchy {
             s.w = w_;
             s.rp = l.rp.data();
             s.ci = l.ci.data();
-            s.val = l.val.data();
+            if constexpr (std::is_same_v<S, V>) s.val = l.val.data();
             s.dinv = l.dinv.data();
             s.rhs = l.rhs.data();
             s.xin = l.x();
@@ -532,7 +551,7 @@ class HierarchyImpl final : public Hierarchy {
         l.cur ^= 1;
     }
 
-    void op_residual_restrict(tf_ctx *ctx, Level<S> &l, Level<S> &c) {
+    void op_residual_restrict(tf_ctx *ctx, Level<S, V> &l, Level<S, V> &c) {
         if (recording_) {
             CoarseStep<S> s;
             s.op = kStepResidualRestrict;
@@ -540,7 +559,7 @@ class HierarchyImpl final : public Hierarchy {
             s.nc = l.coarse;
             s.rp = l.rp.data();
             s.ci = l.ci.data();
-            s.val = l.val.data();
+            if constexpr (std::is_same_v<S, V>) s.val = l.val.data();
             s.rhs = l.rhs.data();
             s.xin = l.x();
             s.off = l.off.data();
@@ -555,7 +574,7 @@ class HierarchyImpl final : public Hierarchy {
         }
     }
 
-    void op_restrict_rhs(tf_ctx *ctx, Level<S> &l, Level<S> &c) {
+    void op_restrict_rhs(tf_ctx *ctx, Level<S, V> &l, Level<S, V> &c) {
         if (recording_) {
             CoarseStep<S> s;
             s.op = kStepRestrict;
@@ -572,7 +591,7 @@ class HierarchyImpl final : public Hierarchy {
         }
     }
 
-    void op_prolong(tf_ctx *ctx, Level<S> &l, Level<S> &c) {
+    void op_prolong(tf_ctx *ctx, Level<S, V> &l, Level<S, V> &c) {
         if (recording_) {
             CoarseStep<S> s;
             s.op = kStepProlong;
@@ -592,7 +611,7 @@ class HierarchyImpl final : public Hierarchy {
         }
     }
 
-    void op_dense(tf_ctx *ctx, Level<S> &l) {
+    void op_dense(tf_ctx *ctx, Level<S, V> &l) {
         if (recording_) {
             CoarseStep<S> s;
             s.op = kStepDense;
@@ -621,13 +640,13 @@ class HierarchyImpl final : public Hierarchy {
     // dense with scatter).  Anything held is launched before any other op, so
     // the kernel order and every value are those of the unfused cycle.
     struct PendingRestrict {
-        Level<S> *fine{nullptr}, *coarse{nullptr};
+        Level<S, V> *fine{nullptr}, *coarse{nullptr};
         const S *src{nullptr};
     };
     static constexpr int kWriteNone = 0, kWriteSweep = 1, kWriteDense = 2, kWriteProgram = 3;
     struct PendingWrite {
         int kind{kWriteNone};
-        Level<S> *l{nullptr};
+        Level<S, V> *l{nullptr};
         const S *xin{nullptr};
         S *xout{nullptr};
         PendingRestrict r;
@@ -639,20 +658,20 @@ class HierarchyImpl final : public Hierarchy {
 
     bool fusing() const { return fuse_ > 0 && !recording_ && !dry_; }
 
-    bool prolong_fusable(const Level<S> &l, const Level<S> &c) const {
+    bool prolong_fusable(const Level<S, V> &l, const Level<S, V> &c) const {
         return fusing() && pw_.kind != kWriteNone && pw_.l == &c && pw_.xout == c.x() &&
                (fuse_ >= 2 || l.n <= kScatterRows);
     }
 
     // Launches the held write; with `fine` set, fused with the prolongation
     // of its result into fine->x().
-    void launch_write(tf_ctx *ctx, Level<S> *fine) {
+    void launch_write(tf_ctx *ctx, Level<S, V> *fine) {
         const PendingWrite w = pw_;
         pw_ = {};
         const int32_t *off = fine ? fine->off.data() : nullptr;
         const int32_t *mem = fine ? fine->mem.data() : nullptr;
         S *fx = fine ? fine->x() : nullptr;
-        Level<S> &l = *w.l;
+        Level<S, V> &l = *w.l;
         if (w.kind == kWriteProgram) {
             ProgramIO<S> io = w.io;
             io.soff = off;
@@ -684,7 +703,7 @@ class HierarchyImpl final : public Hierarchy {
         if (pin_.src) {
             const PendingInput in = pin_;
             pin_ = {};
-            Level<S> &f = levels_.front();
+            Level<S, V> &f = levels_.front();
             if (in.f64) convert(ctx, f.n, static_cast<const double *>(in.src), f.rhs.data());
             else convert(ctx, f.n, static_cast<const float *>(in.src), f.rhs.data());
         }
@@ -697,7 +716,7 @@ class HierarchyImpl final : public Hierarchy {
     }
 
     // `sweeps` Jacobi sweeps; cleared: x is the zero vector on entry.
-    void smooth(tf_ctx *ctx, Level<S> &l, int sweeps, bool cleared) {
+    void smooth(tf_ctx *ctx, Level<S, V> &l, int sweeps, bool cleared) {
         int done = 0;
         if (cleared) {
             if (sweeps > 0) {
@@ -718,7 +737,7 @@ class HierarchyImpl final : public Hierarchy {
     // prolongation of its result can go into it too.
     void cycle(tf_ctx *ctx, int kind, size_t d, bool zero) {
         if (recording_ || d != coop_from_) return cycle_body(ctx, kind, d, zero);
-        Level<S> &l = levels_[d];
+        Level<S, V> &l = levels_[d];
         ProgramIO<S> io;
         if (!dry_ && fusing() && pr_.coarse == &l) {
             io.rsrc = pr_.src;
@@ -756,7 +775,7 @@ class HierarchyImpl final : public Hierarchy {
     }
 
     void cycle_body(tf_ctx *ctx, int kind, size_t d, bool zero) {
-        Level<S> &l = levels_[d];
+        Level<S, V> &l = levels_[d];
         ++visits[d];
         const bool cleared = zero || kind == TF_CYCLE_F;
         if (d + 1 == levels_.size()) {
@@ -764,7 +783,7 @@ class HierarchyImpl final : public Hierarchy {
             else smooth(ctx, l, cfg_.o.coarse_sweeps, cleared);
             return;
         }
-        Level<S> &c = levels_[d + 1];
+        Level<S, V> &c = levels_[d + 1];
         if (kind == TF_CYCLE_F) {
             op_restrict_rhs(ctx, l, c);
             cycle(ctx, TF_CYCLE_F, d + 1, true);
@@ -804,6 +823,7 @@ class HierarchyImpl final : public Hierarchy {
         const size_t none = levels_.size();
         coop_from_ = none;
         if (cfg_.o.small_level_rows <= 0) return;
+        {
         size_t root = none;
         for (size_t d = 1; d < levels_.size(); ++d)
             if (levels_[d].n <= cfg_.o.small_level_rows) {
@@ -821,13 +841,25 @@ class HierarchyImpl final : public Hierarchy {
             for (const auto &e : entries_) max_steps = std::max(max_steps, e.second);
             std::vector<TailLevel<S>> tl;
             for (size_t d = root; d < levels_.size(); ++d) {
-                const Level<S> &l = levels_[d];
+                const Level<S, V> &l = levels_[d];
                 TailLevel<S> t;
                 t.n = l.n;
                 t.rp = l.rp.data();
                 t.ci = l.ci.data();
                 t.cd = l.cd.data();
-                t.val = l.val.data();
+                if constexpr (std::is_same_v<S, V>) {
+                    t.val = l.val.data();
+                } else {
+                    // the region computes in S from its own copy of the values
+                    // (widening FP32 to FP64 is exact: the same products as the
+                    // launched kernels, which widen each value as they read it)
+                    Level<S, V> &lw = levels_[d];
+                    if (!lw.val_s.data()) {
+                        lw.val_s.allocate(static_cast<size_t>(lw.nnz));
+                        convert(ctx, lw.nnz, lw.val.data(), lw.val_s.data());
+                    }
+                    t.val = lw.val_s.data();
+                }
                 t.dinv = l.dinv.data();
                 t.rhs = l.rhs.data();
                 t.x0 = l.x0.data();
@@ -855,6 +887,7 @@ class HierarchyImpl final : public Hierarchy {
             }
             coop_from_ = none;
         }
+        }
     }
 
     static constexpr int64_t kFusedProlongRows = 131072;
@@ -862,7 +895,7 @@ class HierarchyImpl final : public Hierarchy {
 
     AmgConfig cfg_;
     S w_;
-    std::vector<Level<S>> levels_;
+    std::vector<Level<S, V>> levels_;
     DeviceBuffer<double> lu_, inv_;
     DeviceBuffer<int32_t> piv_;
     bool factored_{false};
@@ -895,6 +928,12 @@ class HierarchyImpl final : public Hierarchy {
 
 std::unique_ptr<Hierarchy> build_hierarchy(tf_ctx *ctx, const AmgConfig &cfg, int storage_type,
                                            const tf_dcsr &native) {
+    if (storage_type == TF_F32_VALUES) {
+        require(cfg.model == nullptr, "learned damping needs a hierarchy whose values and vectors share a type");
+        auto h = std::make_unique<HierarchyImpl<double, float>>(cfg);
+        h->build(ctx, native);
+        return h;
+    }
     if (storage_type == TF_F32) {
         auto h = std::make_unique<HierarchyImpl<float>>(cfg);
         h->build(ctx, native);

@@ -7,13 +7,17 @@
 
 namespace tfb {
 
-// Device CSR view with typed arrays.
-template <class T, class I>
+// Device CSR view with typed arrays.  T is the type of the vectors an SpMV
+// over it reads and writes, and of its accumulators; V the type its values
+// are stored in (V = T, or FP32 values under FP64 vectors: each value is
+// widened before its product, so a row sums exactly as with FP64 values
+// equal to the FP32 ones).
+template <class T, class I, class V = T>
 struct Csr {
     int64_t rows{0}, cols{0}, nnz{0};
     const I *rp{nullptr};
     const I *ci{nullptr};
-    const T *val{nullptr};
+    const V *val{nullptr};
     // Optional second copy of the columns as offsets from the row
     // (ci[j] - row, int16): the pipelined row-tile kernels stream it instead
     // of ci when set (see delta_columns).
@@ -24,7 +28,7 @@ struct Csr {
     // family may stream it instead of the CSR arrays; results are the same
     // bits either way.
     const int32_t *sp{nullptr};
-    const T *sv{nullptr};
+    const V *sv{nullptr};
     const int16_t *sc{nullptr};
     // Banded slices instead of per-entry offsets (SlicedCopy::band): entry
     // slot j of slice s holds one column offset shared by the slice's 32
@@ -63,8 +67,8 @@ struct SlicedCopy {
         tile_max = 0;
     }
     bool banded() const { return band.data() != nullptr; }
-    template <class I>
-    void attach(Csr<T, I> &c) const {
+    template <class U, class I>
+    void attach(Csr<U, I, T> &c) const {
         if (sp.data()) {
             c.sp = sp.data();
             c.sv = val.data();
@@ -86,8 +90,8 @@ struct SpmvShape {
 SpmvShape spmv_shape(int64_t rows, int64_t nnz, size_t value_size, size_t index_size);
 
 // y = A x
-template <class T, class I>
-void spmv(tf_ctx *ctx, const Csr<T, I> &a, const T *x, T *y);
+template <class T, class I, class V = T>
+void spmv(tf_ctx *ctx, const Csr<T, I, V> &a, const T *x, T *y);
 // Picks and caches the fastest pipelined launch shape for operators of this
 // shape (y is overwritten).  Writes the chosen ring depth, CTAs per SM, chunk
 // capacity percentage, rows per thread and the best time per launch (ms)
@@ -98,26 +102,26 @@ void autotune_spmv(tf_ctx *ctx, const Csr<T, I> &a, const T *x, T *y, int *stage
 // autotune_spmv the first time an operator of a's shape and storage is set
 // up in the process; later setups reuse the cached shape
 // (THERMOFEM_B200_SLICED_SHAPE forces the timing, and with it that shape).
-template <class T, class I>
-void tune_spmv(tf_ctx *ctx, const Csr<T, I> &a, const T *x, T *y);
+template <class T, class I, class V = T>
+void tune_spmv(tf_ctx *ctx, const Csr<T, I, V> &a, const T *x, T *y);
 // The storage the SpMV family streams for a under its cached shape: true
 // (sliced copy, *entries its padded entry count) or false (CSR, *entries = nnz).
-template <class T, class I>
-bool streams_sliced(tf_ctx *ctx, const Csr<T, I> &a, int64_t entries_if_sliced, int64_t *entries);
+template <class T, class I, class V = T>
+bool streams_sliced(tf_ctx *ctx, const Csr<T, I, V> &a, int64_t entries_if_sliced, int64_t *entries);
 // Stores a launch shape for operators of a's shape (validated, not timed).
 template <class T, class I>
 void set_spmv_config(tf_ctx *ctx, const Csr<T, I> &a, int stages, int ctas_per_sm, int cap_pct, int rows_per_thread);
 // r = b - A x
-template <class T, class I>
-void residual(tf_ctx *ctx, const Csr<T, I> &a, const T *b, const T *x, T *r);
+template <class T, class I, class V = T>
+void residual(tf_ctx *ctx, const Csr<T, I, V> &a, const T *b, const T *x, T *r);
 // xo = x~ + w Dinv (b - A x~), x~ = x (+ e[map] when map != nullptr)
-template <class T, class I>
-void jacobi_sweep(tf_ctx *ctx, const Csr<T, I> &a, const T *dinv, const T *b, const T *x, T *xo, T w,
+template <class T, class I, class V = T>
+void jacobi_sweep(tf_ctx *ctx, const Csr<T, I, V> &a, const T *dinv, const T *b, const T *x, T *xo, T w,
                   const float *row_w, const int32_t *map, const T *e);
 // xo = x + w Dinv (b - A x), and fine[mem[k]] += xo[c] for k in
 // [off[c], off[c+1]) (the prolongation of the result fused in).
-template <class T, class I>
-void jacobi_sweep_scatter(tf_ctx *ctx, const Csr<T, I> &a, const T *dinv, const T *b, const T *x, T *xo, T w,
+template <class T, class I, class V = T>
+void jacobi_sweep_scatter(tf_ctx *ctx, const Csr<T, I, V> &a, const T *dinv, const T *b, const T *x, T *xo, T w,
                           const int32_t *off, const int32_t *mem, T *fine);
 // b[c] = sum_k fine[mem[k]] (k in [off[c], off[c+1])), x = w Dinv b.
 template <class T>
@@ -134,8 +138,8 @@ bool indices_out_of_range(tf_ctx *ctx, int64_t n, const int32_t *idx, int32_t li
 template <class S, class T>
 void jacobi_zero_convert(tf_ctx *ctx, int64_t n, const S *dinv, const T *in, S *b, S *x, S w);
 // Dinv from summed diagonal entries; throws TF_ERR_INVALID on a bad diagonal.
-template <class T, class I>
-void inverse_diagonal(tf_ctx *ctx, const Csr<T, I> &a, T *dinv);
+template <class T, class I, class V = T>
+void inverse_diagonal(tf_ctx *ctx, const Csr<T, I, V> &a, T *dinv);
 // cd[j] = ci[j] - row(j) as int16_t (the pipelined kernels' 2-byte column
 // stream).  False, with cd unusable, when a coupling lies more than 32767
 // rows from the diagonal.  THERMOFEM_B200_DELTA16=0 turns the stream off

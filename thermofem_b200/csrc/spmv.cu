@@ -107,8 +107,8 @@ struct JacobiScatter {
     }
 };
 
-template <class T, class I, class XS, class Epi>
-void launch_tile(tf_ctx *ctx, const Csr<T, I> &a, const XS &xs, const Epi &epi, const char *name) {
+template <class T, class I, class V, class XS, class Epi>
+void launch_tile(tf_ctx *ctx, const Csr<T, I, V> &a, const XS &xs, const Epi &epi, const char *name) {
     tile::launch(ctx, a, xs, epi, name);
 }
 
@@ -145,9 +145,9 @@ __global__ void jacobi_update_kernel(int64_t n, T w, const T *__restrict__ dinv,
         x[i] += w * dinv[i] * (b[i] - ax[i]);
 }
 
-template <class T, class I>
+template <class T, class I, class V>
 __global__ void inverse_diagonal_kernel(int64_t n, const I *__restrict__ rp, const I *__restrict__ ci,
-                                        const T *__restrict__ val, T *__restrict__ dinv, int *bad) {
+                                        const V *__restrict__ val, T *__restrict__ dinv, int *bad) {
     pdl_enter();
     const int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
     if (i >= n) return;
@@ -606,8 +606,8 @@ SpmvShape spmv_shape(int64_t rows, int64_t nnz, size_t value_size, size_t index_
     return s;
 }
 
-template <class T, class I>
-void spmv(tf_ctx *ctx, const Csr<T, I> &a, const T *x, T *y) {
+template <class T, class I, class V>
+void spmv(tf_ctx *ctx, const Csr<T, I, V> &a, const T *x, T *y) {
     launch_tile(ctx, a, PlainX<T>{x}, StoreY<T>{y, nullptr}, "spmv");
 }
 
@@ -621,14 +621,14 @@ void autotune_spmv(tf_ctx *ctx, const Csr<T, I> &a, const T *x, T *y, int *stage
     if (rows_per_thread) *rows_per_thread = c.rpt;
 }
 
-template <class T, class I>
-void tune_spmv(tf_ctx *ctx, const Csr<T, I> &a, const T *x, T *y) {
+template <class T, class I, class V>
+void tune_spmv(tf_ctx *ctx, const Csr<T, I, V> &a, const T *x, T *y) {
     if (!std::getenv("THERMOFEM_B200_SLICED_SHAPE") && tile::tuned(ctx, a)) return;
     tile::autotune(ctx, a, x, y, nullptr);
 }
 
-template <class T, class I>
-bool streams_sliced(tf_ctx *ctx, const Csr<T, I> &a, int64_t entries_if_sliced, int64_t *entries) {
+template <class T, class I, class V>
+bool streams_sliced(tf_ctx *ctx, const Csr<T, I, V> &a, int64_t entries_if_sliced, int64_t *entries) {
     bool sliced = false;
     if constexpr (std::is_same_v<I, int32_t>) {
         if (a.sp && (a.cd || a.bd)) sliced = tile::copy_config(ctx, a).sliced != 0;
@@ -642,13 +642,13 @@ void set_spmv_config(tf_ctx *ctx, const Csr<T, I> &a, int stages, int ctas_per_s
     tile::configure(ctx, a, tile::PipeConfig{stages, ctas_per_sm, cap_pct, rows_per_thread});
 }
 
-template <class T, class I>
-void residual(tf_ctx *ctx, const Csr<T, I> &a, const T *b, const T *x, T *r) {
+template <class T, class I, class V>
+void residual(tf_ctx *ctx, const Csr<T, I, V> &a, const T *b, const T *x, T *r) {
     launch_tile(ctx, a, PlainX<T>{x}, ResidualOut<T>{b, r, nullptr}, "residual");
 }
 
-template <class T, class I>
-void jacobi_sweep(tf_ctx *ctx, const Csr<T, I> &a, const T *dinv, const T *b, const T *x, T *xo, T w,
+template <class T, class I, class V>
+void jacobi_sweep(tf_ctx *ctx, const Csr<T, I, V> &a, const T *dinv, const T *b, const T *x, T *xo, T w,
                   const float *row_w, const int32_t *map, const T *e) {
     JacobiOut<T> epi{dinv, b, xo, row_w, w, nullptr};
     if (map)
@@ -657,8 +657,8 @@ void jacobi_sweep(tf_ctx *ctx, const Csr<T, I> &a, const T *dinv, const T *b, co
         launch_tile(ctx, a, PlainX<T>{x}, epi, "jacobi");
 }
 
-template <class T, class I>
-void jacobi_sweep_scatter(tf_ctx *ctx, const Csr<T, I> &a, const T *dinv, const T *b, const T *x, T *xo, T w,
+template <class T, class I, class V>
+void jacobi_sweep_scatter(tf_ctx *ctx, const Csr<T, I, V> &a, const T *dinv, const T *b, const T *x, T *xo, T w,
                           const int32_t *off, const int32_t *mem, T *fine) {
     launch_tile(ctx, a, PlainX<T>{x}, JacobiScatter<T>{dinv, b, xo, w, off, mem, fine, nullptr}, "jacobi_scatter");
 }
@@ -724,12 +724,12 @@ template void jacobi_zero_convert<double, double>(tf_ctx *, int64_t, const doubl
 template void jacobi_zero_convert<double, float>(tf_ctx *, int64_t, const double *, const float *, double *,
                                                  double *, double);
 
-template <class T, class I>
-void inverse_diagonal(tf_ctx *ctx, const Csr<T, I> &a, T *dinv) {
+template <class T, class I, class V>
+void inverse_diagonal(tf_ctx *ctx, const Csr<T, I, V> &a, T *dinv) {
     require(a.rows > 0 && a.rows == a.cols, "Inverse diagonal requires a nonempty square matrix");
     int *bad = static_cast<int *>(ctx->arena(sizeof(int), 1));
     memset_async(ctx, bad, 0, sizeof(int));
-    launch_kernel(ctx, "inverse_diagonal", inverse_diagonal_kernel<T, I>, grid_for(a.rows), kBlock, 0, a.rows, a.rp,
+    launch_kernel(ctx, "inverse_diagonal", inverse_diagonal_kernel<T, I, V>, grid_for(a.rows), kBlock, 0, a.rows, a.rp,
                   a.ci, a.val, dinv, bad);
     if (read_scalar(ctx, bad)) fail(TF_ERR_INVALID, "Missing or invalid diagonal");
 }
@@ -1045,6 +1045,23 @@ TF_SPMV_INST(double, int32_t)
 TF_SPMV_INST(float, int64_t)
 TF_SPMV_INST(double, int64_t)
 #undef TF_SPMV_INST
+
+// FP32 values under FP64 vectors (the hierarchy whose operators are stored
+// in FP32 and whose cycle runs in FP64).
+template void spmv<double, int32_t, float>(tf_ctx *, const Csr<double, int32_t, float> &, const double *, double *);
+template void tune_spmv<double, int32_t, float>(tf_ctx *, const Csr<double, int32_t, float> &, const double *,
+                                               double *);
+template bool streams_sliced<double, int32_t, float>(tf_ctx *, const Csr<double, int32_t, float> &, int64_t,
+                                                    int64_t *);
+template void residual<double, int32_t, float>(tf_ctx *, const Csr<double, int32_t, float> &, const double *,
+                                              const double *, double *);
+template void jacobi_sweep<double, int32_t, float>(tf_ctx *, const Csr<double, int32_t, float> &, const double *,
+                                                  const double *, const double *, double *, double, const float *,
+                                                  const int32_t *, const double *);
+template void jacobi_sweep_scatter<double, int32_t, float>(tf_ctx *, const Csr<double, int32_t, float> &,
+                                                          const double *, const double *, const double *, double *,
+                                                          double, const int32_t *, const int32_t *, double *);
+template void inverse_diagonal<double, int32_t, float>(tf_ctx *, const Csr<double, int32_t, float> &, double *);
 
 #define TF_VEC_INST(T)                                                                                        \
     template void jacobi_zero<T>(tf_ctx *, int64_t, const T *, const T *, T *, T, const float *);              \

@@ -156,16 +156,16 @@ __device__ __forceinline__ void finish(const Fin &fin, const double *part, int p
 //   __device__ void operator()(int64_t i, T acc, const XS &xs, double (&red)[kReduce or 1]) const;
 //   double *partial;                        [kReduce][gridDim.x] when kReduce > 0
 // (the pipelined kernel also needs `fin`, a tile::finish step, when kReduce > 0)
-template <class T, class I, int RPT, class XS, class Epi>
+template <class T, class I, int RPT, class XS, class Epi, class V = T>
 __global__ void __launch_bounds__(kThreads) csr_tile_kernel(int64_t rows, const I *__restrict__ rp,
-                                                             const I *__restrict__ ci, const T *__restrict__ val,
+                                                             const I *__restrict__ ci, const V *__restrict__ val,
                                                              int chunk, XS xs, Epi epi) {
     constexpr int K = Epi::kReduce;
     pdl_enter();
     if (epi.skip()) return;
     extern __shared__ __align__(128) unsigned char smem[];
-    T *sval = reinterpret_cast<T *>(smem);
-    I *scol = reinterpret_cast<I *>(smem + static_cast<size_t>(chunk) * sizeof(T));
+    V *sval = reinterpret_cast<V *>(smem);
+    I *scol = reinterpret_cast<I *>(smem + static_cast<size_t>(chunk) * sizeof(V));
     const int64_t r0 = static_cast<int64_t>(blockIdx.x) * (kThreads * RPT);
     const int64_t rend = min(r0 + static_cast<int64_t>(kThreads * RPT), rows);
     const int64_t t0 = rp[r0], t1 = rp[rend];
@@ -356,14 +356,14 @@ __device__ __forceinline__ int64_t column_of(int64_t row, C entry) {
     else return static_cast<int64_t>(entry);
 }
 
-template <class T, class I, class C, int RPT, class XS, class Epi>
+template <class T, class I, class C, int RPT, class XS, class Epi, class V = T>
 __global__ void __launch_bounds__(kThreads + 32) csr_pipe_kernel(int64_t rows, int64_t nnz, const I *__restrict__ rp,
                                                                   const C *__restrict__ ci,
-                                                                  const T *__restrict__ val, int cap, int stages,
+                                                                  const V *__restrict__ val, int cap, int stages,
                                                                   int early, XS xs, Epi epi, int *fault) {
     constexpr int K = Epi::kReduce;
     constexpr int KK = K > 0 ? K : 1;
-    constexpr int kVT = 16 / sizeof(T), kVC = 16 / sizeof(C);
+    constexpr int kVT = 16 / sizeof(V), kVC = 16 / sizeof(C);
     constexpr int kTileRows = kThreads * RPT;
     constexpr int kWarps = kThreads / 32;
     extern __shared__ __align__(128) unsigned char smem[];
@@ -371,7 +371,7 @@ __global__ void __launch_bounds__(kThreads + 32) csr_pipe_kernel(int64_t rows, i
     __shared__ double warp_sums[kMaxStages + 1][RPT][kWarps][KK];
     __shared__ int warp_done[kMaxStages + 1];
     __shared__ int skipped_cta;
-    const StageLayout<T, I, C> L(cap, kTileRows);
+    const StageLayout<V, I, C> L(cap, kTileRows);
     const int tid = threadIdx.x;
     if (tid == 0) {
         for (int s = 0; s < stages; ++s) {
@@ -384,7 +384,7 @@ __global__ void __launch_bounds__(kThreads + 32) csr_pipe_kernel(int64_t rows, i
     __syncthreads();
     auto stage_rp = [&](int s) { return reinterpret_cast<I *>(smem + static_cast<size_t>(s) * L.bytes); };
     auto stage_val = [&](int s) {
-        return reinterpret_cast<T *>(smem + static_cast<size_t>(s) * L.bytes + L.rp_bytes);
+        return reinterpret_cast<V *>(smem + static_cast<size_t>(s) * L.bytes + L.rp_bytes);
     };
     auto stage_col = [&](int s) {
         return reinterpret_cast<C *>(smem + static_cast<size_t>(s) * L.bytes + L.rp_bytes + L.val_bytes);
@@ -425,7 +425,7 @@ __global__ void __launch_bounds__(kThreads + 32) csr_pipe_kernel(int64_t rows, i
                 Range<I> rr;
                 if (c == 0) rr.plan(r0, r0 + nr + 1, rows + 1);
                 else rr.plan(r0, r0, rows + 1);
-                Range<T> rv;
+                Range<V> rv;
                 rv.plan(cs, ce, nnz);
                 Range<C> rc;
                 rc.plan(cs, ce, nnz);
@@ -495,7 +495,7 @@ __global__ void __launch_bounds__(kThreads + 32) csr_pipe_kernel(int64_t rows, i
                         }
                 }
                 const Off cs = s + static_cast<Off>(c) * cap, ce = min(e, cs + static_cast<Off>(cap));
-                const T *sv = stage_val(st) + (cs % kVT);  // sv[j - cs]
+                const V *sv = stage_val(st) + (cs % kVT);  // sv[j - cs]
                 const C *sc = stage_col(st) + (cs % kVC);  // sc[j - cs]
                 constexpr int kGather = 8;
                 int lo[RPT], hi[RPT];
@@ -673,9 +673,9 @@ __device__ __forceinline__ void load_slice_head(SliceHead<T, G> &h, int64_t slic
     }
 }
 
-template <class T, int G, bool PF, class XS, class Epi, class Cols>
+template <class T, int G, bool PF, class XS, class Epi, class Cols, class V = T>
 __global__ void __launch_bounds__(kThreads) sliced_kernel(int64_t rows, const int32_t *__restrict__ sp,
-                                                          const T *__restrict__ sv, Cols cols,
+                                                          const V *__restrict__ sv, Cols cols,
                                                           const int32_t *__restrict__ perm, int early, XS xs,
                                                           Epi epi) {
     constexpr int K = Epi::kReduce;
@@ -689,7 +689,7 @@ __global__ void __launch_bounds__(kThreads) sliced_kernel(int64_t rows, const in
     const int ntiles = (nrows + kThreads - 1) / kThreads;  // = 256-row blocks of partial sums
     const int nslices = (nrows + 31) / 32;
     int tile = blockIdx.x;
-    SliceHead<T, G> h;
+    SliceHead<V, G> h;
     if (early) load_slice_head(h, tile * kWarps + warp, nslices, sp, sv, cols, lane);
     pdl_enter();
     if (epi.skip()) return;  // the gate reads the same device word in every CTA
@@ -700,7 +700,7 @@ __global__ void __launch_bounds__(kThreads) sliced_kernel(int64_t rows, const in
         const int row = live && perm ? __ldg(perm + slot) : slot;
         typename Epi::Pre pre{};
         if (live) pre = epi.pre(row, xs);
-        SliceHead<T, G> next;
+        SliceHead<V, G> next;
         if constexpr (PF) load_slice_head(next, (tile + gridDim.x) * kWarps + warp, nslices, sp, sv, cols, lane);
         const auto xr = xs.row(row);  // x~ around this lane's row, indexed by column offset
         T y[G];
@@ -710,16 +710,16 @@ __global__ void __launch_bounds__(kThreads) sliced_kernel(int64_t rows, const in
 #pragma unroll
         for (int g = 0; g < G; ++g) acc += h.v[g] * y[g];
         for (int j0 = G; j0 < h.width; j0 += G) {
-            T v[G];
+            V v[G];
             int c[G];
-            const T *pv = sv + h.base + lane + j0 * 32;
+            const V *pv = sv + h.base + lane + j0 * 32;
 #pragma unroll
             for (int g = 0; g < G; ++g) {
                 if (j0 + g < h.width) {
                     v[g] = __ldcs(pv + g * 32);
                     c[g] = cols.at(h.base, j0 + g, lane);
                 } else {
-                    v[g] = T(0);
+                    v[g] = V(0);
                     c[g] = kColPad;
                 }
             }
@@ -874,9 +874,9 @@ __device__ __forceinline__ void load4(T (&v)[4], const T *p) {
 // row quad's values are 16-byte aligned in the stage) and gathers x at four
 // consecutive addresses, which cuts the instructions per entry about in
 // half; each row still adds its products slot by slot from +0.
-template <class T, int R, class XS, class Epi, class Cols, bool kQuad = false>
+template <class T, int R, class XS, class Epi, class Cols, bool kQuad = false, class V = T>
 __global__ void __launch_bounds__(kThreads + 32)
-    sliced_pipe_kernel(int64_t rows, const int32_t *__restrict__ sp, const T *__restrict__ sv, Cols cols, int cap,
+    sliced_pipe_kernel(int64_t rows, const int32_t *__restrict__ sp, const V *__restrict__ sv, Cols cols, int cap,
                        int stages, int early, XS xs, Epi epi, int *fault) {
     static_assert(!kQuad || (R == 4 && Epi::kReduce == 0 && std::is_same_v<Cols, StagedBand>),
                   "the four-rows-per-lane form serves banded copies in groups of 4 tiles without partial sums");
@@ -890,7 +890,7 @@ __global__ void __launch_bounds__(kThreads + 32)
     __shared__ double warp_sums[kRing][kWarps][KK];
     __shared__ int warp_done[kRing];
     __shared__ int skipped_cta;
-    using Stage = SlicedStage<T, Cols, R>;
+    using Stage = SlicedStage<V, Cols, R>;
     const Stage L(cap);
     const int tid = threadIdx.x;
     if (tid == 0) {
@@ -904,7 +904,7 @@ __global__ void __launch_bounds__(kThreads + 32)
     __syncthreads();
     auto stage_hdr = [&](int st) { return reinterpret_cast<int32_t *>(smem + static_cast<size_t>(st) * L.bytes); };
     auto stage_val = [&](int st) {
-        return reinterpret_cast<T *>(smem + static_cast<size_t>(st) * L.bytes + Stage::kHeader);
+        return reinterpret_cast<V *>(smem + static_cast<size_t>(st) * L.bytes + Stage::kHeader);
     };
     auto stage_col = [&](int st) {
         return static_cast<void *>(smem + static_cast<size_t>(st) * L.bytes + Stage::kHeader + L.val_bytes);
@@ -960,7 +960,7 @@ __global__ void __launch_bounds__(kThreads + 32)
 #pragma unroll
             for (int k = 1; k < kSlices; ++k) hdr[k] = mid[k - 1];
             hdr[kSlices] = static_cast<int32_t>(e1);
-            const uint32_t nv = static_cast<uint32_t>((e1 - e0) * static_cast<int64_t>(sizeof(T)));
+            const uint32_t nv = static_cast<uint32_t>((e1 - e0) * static_cast<int64_t>(sizeof(V)));
             const uint32_t nc = e1 > e0 ? cols.bytes(e0, e1) : 0;
             mbar_arrive_expect_tx(&full_bar[st], nv + nc);
             ++armed[st];
@@ -1001,7 +1001,7 @@ __global__ void __launch_bounds__(kThreads + 32)
                 const int width = (hdr[s + 1] - hdr[s]) >> 5;
                 const int2 *band = static_cast<const int2 *>(stage_col(st)) +
                                    static_cast<int>((hdr[0] >> 5) - StagedBand::lo(hdr[0])) + (base >> 5);
-                const T *vs = stage_val(st) + base + 4 * p;
+                const V *vs = stage_val(st) + base + 4 * p;
                 const auto xr = xs.row(row0);
                 T acc[4] = {T(0), T(0), T(0), T(0)};
                 for (int j0 = 0; j0 < width; j0 += 8) {
@@ -1021,7 +1021,7 @@ __global__ void __launch_bounds__(kThreads + 32)
 #pragma unroll
                     for (int g = 0; g < 8; ++g) {
                         if (j0 + g < width) {
-                            T v[4];
+                            V v[4];
                             load4(v, vs + (j0 + g) * 32);
 #pragma unroll
                             for (int k = 0; k < 4; ++k) acc[k] += v[k] * y[g][k];
@@ -1085,7 +1085,7 @@ __global__ void __launch_bounds__(kThreads + 32)
             }
 #pragma unroll
             for (int k = 0; k < R; ++k) {
-                const T *vs = stage_val(st) + base[k] + lane;
+                const V *vs = stage_val(st) + base[k] + lane;
                 T a = T(0);
 #pragma unroll
                 for (int g = 0; g < 8; ++g) a += (g < width[k] ? vs[g * 32] : T(0)) * y[k][g];
@@ -1188,15 +1188,15 @@ int sliced_stage_cap_for(int64_t tile_max) {
     if (cap <= 0 || cap > (int64_t(96) << 10)) return 0;
     return SlicedStage<T, Cols, R>(static_cast<int>(cap)).bytes <= (96 << 10) ? static_cast<int>(cap) : 0;
 }
-template <class T, class I>
-int sliced_stage_cap(const Csr<T, I> &a, int group) {
+template <class T, class I, class V>
+int sliced_stage_cap(const Csr<T, I, V> &a, int group) {
     switch (group) {
-        case 4: return a.bd ? sliced_stage_cap_for<T, StagedBand, 4>(a.sl_tile_max)
-                            : sliced_stage_cap_for<T, StagedOffsets, 4>(a.sl_tile_max);
-        case 2: return a.bd ? sliced_stage_cap_for<T, StagedBand, 2>(a.sl_tile_max)
-                            : sliced_stage_cap_for<T, StagedOffsets, 2>(a.sl_tile_max);
-        default: return a.bd ? sliced_stage_cap_for<T, StagedBand, 1>(a.sl_tile_max)
-                             : sliced_stage_cap_for<T, StagedOffsets, 1>(a.sl_tile_max);
+        case 4: return a.bd ? sliced_stage_cap_for<V, StagedBand, 4>(a.sl_tile_max)
+                            : sliced_stage_cap_for<V, StagedOffsets, 4>(a.sl_tile_max);
+        case 2: return a.bd ? sliced_stage_cap_for<V, StagedBand, 2>(a.sl_tile_max)
+                            : sliced_stage_cap_for<V, StagedOffsets, 2>(a.sl_tile_max);
+        default: return a.bd ? sliced_stage_cap_for<V, StagedBand, 1>(a.sl_tile_max)
+                             : sliced_stage_cap_for<V, StagedOffsets, 1>(a.sl_tile_max);
     }
 }
 
@@ -1205,14 +1205,14 @@ int sliced_stage_cap(const Csr<T, I> &a, int group) {
 constexpr size_t kStagedSmemMax = size_t(200) << 10;
 
 // Shared memory of one stage of the staged kernel over a's copy.
-template <class T, class I>
-size_t sliced_stage_bytes(const Csr<T, I> &a, int group, int cap) {
+template <class T, class I, class V>
+size_t sliced_stage_bytes(const Csr<T, I, V> &a, int group, int cap) {
     auto bytes = [&](auto cols) -> size_t {
         using Cols = decltype(cols);
         switch (group) {
-            case 4: return SlicedStage<T, Cols, 4>(cap).bytes;
-            case 2: return SlicedStage<T, Cols, 2>(cap).bytes;
-            default: return SlicedStage<T, Cols, 1>(cap).bytes;
+            case 4: return SlicedStage<V, Cols, 4>(cap).bytes;
+            case 2: return SlicedStage<V, Cols, 2>(cap).bytes;
+            default: return SlicedStage<V, Cols, 1>(cap).bytes;
         }
     };
     return a.bd ? bytes(StagedBand{}) : bytes(StagedOffsets{});
@@ -1228,16 +1228,16 @@ struct KernelTag {
 // a's column source and the group size; quad: the four-rows-per-lane form,
 // where it applies (a banded copy, an epilogue without partial sums; group
 // 4 is then implied).
-template <class T, class I, class XS, class Epi, class F>
-decltype(auto) with_staged_kernel(const Csr<T, I> &a, int group, F &&f, bool quad = false) {
+template <class T, class I, class XS, class Epi, class F, class V>
+decltype(auto) with_staged_kernel(const Csr<T, I, V> &a, int group, F &&f, bool quad = false) {
     auto pick = [&](auto cols) -> decltype(auto) {
         using Cols = decltype(cols);
         if constexpr (std::is_same_v<Cols, StagedBand> && Epi::kReduce == 0)
-            if (quad) return f(KernelTag<sliced_pipe_kernel<T, 4, XS, Epi, Cols, true>>{}, cols);
+            if (quad) return f(KernelTag<sliced_pipe_kernel<T, 4, XS, Epi, Cols, true, V>>{}, cols);
         switch (group) {
-            case 4: return f(KernelTag<sliced_pipe_kernel<T, 4, XS, Epi, Cols>>{}, cols);
-            case 2: return f(KernelTag<sliced_pipe_kernel<T, 2, XS, Epi, Cols>>{}, cols);
-            default: return f(KernelTag<sliced_pipe_kernel<T, 1, XS, Epi, Cols>>{}, cols);
+            case 4: return f(KernelTag<sliced_pipe_kernel<T, 4, XS, Epi, Cols, false, V>>{}, cols);
+            case 2: return f(KernelTag<sliced_pipe_kernel<T, 2, XS, Epi, Cols, false, V>>{}, cols);
+            default: return f(KernelTag<sliced_pipe_kernel<T, 1, XS, Epi, Cols, false, V>>{}, cols);
         }
     };
     if (a.bd) return pick(StagedBand{a.bd});
@@ -1287,34 +1287,36 @@ inline std::map<TuneKey, PipeConfig> &tune_cache() {
     static std::map<TuneKey, PipeConfig> m;
     return m;
 }
-template <class T, class I, class C>
+// (values of type V under vectors of type T: V's size, plus 100 when the
+// two differ, so FP32 values under FP64 vectors keep shapes of their own)
+template <class T, class I, class C, class V = T>
 TuneKey tune_key(int64_t rows, int64_t nnz, int sm_count) {
-    return TuneKey{rows, nnz, static_cast<int>(sizeof(T)), static_cast<int>(sizeof(I)), static_cast<int>(sizeof(C)),
-                   sm_count};
+    return TuneKey{rows, nnz, static_cast<int>(sizeof(V)) + (std::is_same_v<T, V> ? 0 : 100),
+                   static_cast<int>(sizeof(I)), static_cast<int>(sizeof(C)), sm_count};
 }
-template <class T, class I, class C>
+template <class T, class I, class C, class V = T>
 PipeConfig tuned_config(int64_t rows, int64_t nnz, int sm_count) {
     std::lock_guard<std::mutex> lock(tune_mutex());
-    auto it = tune_cache().find(tune_key<T, I, C>(rows, nnz, sm_count));
+    auto it = tune_cache().find(tune_key<T, I, C, V>(rows, nnz, sm_count));
     return it == tune_cache().end() ? PipeConfig{} : it->second;
 }
-template <class T, class I, class C>
+template <class T, class I, class C, class V = T>
 bool has_config(int64_t rows, int64_t nnz, int sm_count) {
     std::lock_guard<std::mutex> lock(tune_mutex());
-    return tune_cache().count(tune_key<T, I, C>(rows, nnz, sm_count)) != 0;
+    return tune_cache().count(tune_key<T, I, C, V>(rows, nnz, sm_count)) != 0;
 }
-template <class T, class I, class C>
+template <class T, class I, class C, class V = T>
 void store_config(int64_t rows, int64_t nnz, int sm_count, const PipeConfig &cfg) {
     std::lock_guard<std::mutex> lock(tune_mutex());
-    tune_cache()[tune_key<T, I, C>(rows, nnz, sm_count)] = cfg;
+    tune_cache()[tune_key<T, I, C, V>(rows, nnz, sm_count)] = cfg;
 }
 
 inline bool aligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
 // Calls f(cols) with the column stream the pipelined kernel reads for a:
 // the 2-byte row offsets when the operator carries them, else the indices.
-template <class T, class I, class F>
-decltype(auto) with_columns(const Csr<T, I> &a, F &&f) {
+template <class T, class I, class F, class V>
+decltype(auto) with_columns(const Csr<T, I, V> &a, F &&f) {
     if constexpr (std::is_same_v<I, int32_t>) {
         if (a.cd && aligned16(a.cd)) return f(a.cd);
     }
@@ -1322,17 +1324,17 @@ decltype(auto) with_columns(const Csr<T, I> &a, F &&f) {
 }
 
 // Validates and caches a launch shape for operators of a's shape.
-template <class T, class I>
-void configure(tf_ctx *ctx, const Csr<T, I> &a, const PipeConfig &cfg) {
+template <class T, class I, class V>
+void configure(tf_ctx *ctx, const Csr<T, I, V> &a, const PipeConfig &cfg) {
     require(cfg.rpt == 1 || cfg.rpt == 2, "rows_per_thread must be 1 or 2");
     require(cfg.stages >= 2 && cfg.stages <= kMaxStages, "stages must be 2..4");
     require(cfg.ctas_per_sm >= 1 && cfg.ctas_per_sm <= 8, "ctas_per_sm must be 1..8");
     require(cfg.cap_pct >= 50 && cfg.cap_pct <= 400, "cap_pct must be 50..400");
     with_columns(a, [&](auto cols) {
         using C = std::remove_cv_t<std::remove_pointer_t<decltype(cols)>>;
-        const PipeShape p = pipe_shape<T, I, C>(a.rows, a.nnz, ctx->sm_count, cfg);
+        const PipeShape p = pipe_shape<V, I, C>(a.rows, a.nnz, ctx->sm_count, cfg);
         require(p.smem <= 200 * 1024, "stage ring exceeds shared memory");
-        store_config<T, I, C>(a.rows, a.nnz, ctx->sm_count, cfg);
+        store_config<T, I, C, V>(a.rows, a.nnz, ctx->sm_count, cfg);
     });
 }
 
@@ -1395,31 +1397,31 @@ bool rarely_runs(const E &, long) {
     return false;
 }
 
-template <class T, class I, class C, class XS, class Epi>
-void launch_pipe(tf_ctx *ctx, const Csr<T, I> &a, const C *cols, const XS &xs, const Epi &epi, const char *name,
+template <class T, class I, class C, class XS, class Epi, class V>
+void launch_pipe(tf_ctx *ctx, const Csr<T, I, V> &a, const C *cols, const XS &xs, const Epi &epi, const char *name,
                  const PipeConfig *force) {
-    const PipeConfig cfg = force ? *force : tuned_config<T, I, C>(a.rows, a.nnz, ctx->sm_count);
-    const PipeShape p = pipe_shape<T, I, C>(a.rows, a.nnz, ctx->sm_count, cfg);
+    const PipeConfig cfg = force ? *force : tuned_config<T, I, C, V>(a.rows, a.nnz, ctx->sm_count);
+    const PipeShape p = pipe_shape<V, I, C>(a.rows, a.nnz, ctx->sm_count, cfg);
     const int early = ctx->stable && !rarely_runs(epi, 0) ? 1 : 0;
     auto grid = [&](int resident) {
         const int64_t g = static_cast<int64_t>(ctx->sm_count) * (resident > 0 ? resident : 1);
         return static_cast<int>(p.grid < g ? p.grid : g);
     };
     if (p.rpt == 2) {
-        allow_smem<csr_pipe_kernel<T, I, C, 2, XS, Epi>>(p.smem);
-        const int g = grid(resident_ctas<csr_pipe_kernel<T, I, C, 2, XS, Epi>>(kThreads + 32, p.smem));
-        launch_kernel(ctx, name, csr_pipe_kernel<T, I, C, 2, XS, Epi>, g, kThreads + 32, p.smem, a.rows, a.nnz, a.rp,
+        allow_smem<csr_pipe_kernel<T, I, C, 2, XS, Epi, V>>(p.smem);
+        const int g = grid(resident_ctas<csr_pipe_kernel<T, I, C, 2, XS, Epi, V>>(kThreads + 32, p.smem));
+        launch_kernel(ctx, name, csr_pipe_kernel<T, I, C, 2, XS, Epi, V>, g, kThreads + 32, p.smem, a.rows, a.nnz, a.rp,
                       cols, a.val, p.cap, p.stages, early, xs, epi, ctx->fault);
     } else {
-        allow_smem<csr_pipe_kernel<T, I, C, 1, XS, Epi>>(p.smem);
-        const int g = grid(resident_ctas<csr_pipe_kernel<T, I, C, 1, XS, Epi>>(kThreads + 32, p.smem));
-        launch_kernel(ctx, name, csr_pipe_kernel<T, I, C, 1, XS, Epi>, g, kThreads + 32, p.smem, a.rows, a.nnz, a.rp,
+        allow_smem<csr_pipe_kernel<T, I, C, 1, XS, Epi, V>>(p.smem);
+        const int g = grid(resident_ctas<csr_pipe_kernel<T, I, C, 1, XS, Epi, V>>(kThreads + 32, p.smem));
+        launch_kernel(ctx, name, csr_pipe_kernel<T, I, C, 1, XS, Epi, V>, g, kThreads + 32, p.smem, a.rows, a.nnz, a.rp,
                       cols, a.val, p.cap, p.stages, early, xs, epi, ctx->fault);
     }
 }
 
-template <class T, class I, class XS, class Epi>
-void launch_sliced(tf_ctx *ctx, const Csr<T, I> &a, const XS &xs, const Epi &epi, const char *name,
+template <class T, class I, class XS, class Epi, class V>
+void launch_sliced(tf_ctx *ctx, const Csr<T, I, V> &a, const XS &xs, const Epi &epi, const char *name,
                    const PipeConfig &cfg) {
     const int64_t ntiles = (a.rows + kThreads - 1) / kThreads;
     const int early = ctx->stable && !rarely_runs(epi, 0) ? 1 : 0;
@@ -1456,12 +1458,12 @@ void launch_sliced(tf_ctx *ctx, const Csr<T, I> &a, const XS &xs, const Epi &epi
     auto go = [&](auto cols) {
         using Cols = decltype(cols);
         if (cfg.prefetch)
-            launch_kernel(ctx, name, sliced_kernel<T, 8, true, XS, Epi, Cols>,
-                          grid(resident_ctas<sliced_kernel<T, 8, true, XS, Epi, Cols>>(kThreads, 0)), kThreads, 0,
+            launch_kernel(ctx, name, sliced_kernel<T, 8, true, XS, Epi, Cols, V>,
+                          grid(resident_ctas<sliced_kernel<T, 8, true, XS, Epi, Cols, V>>(kThreads, 0)), kThreads, 0,
                           a.rows, a.sp, a.sv, cols, a.perm, early, xs, epi);
         else
-            launch_kernel(ctx, name, sliced_kernel<T, 8, false, XS, Epi, Cols>,
-                          grid(resident_ctas<sliced_kernel<T, 8, false, XS, Epi, Cols>>(kThreads, 0)), kThreads, 0,
+            launch_kernel(ctx, name, sliced_kernel<T, 8, false, XS, Epi, Cols, V>,
+                          grid(resident_ctas<sliced_kernel<T, 8, false, XS, Epi, Cols, V>>(kThreads, 0)), kThreads, 0,
                           a.rows, a.sp, a.sv, cols, a.perm, early, xs, epi);
     };
     if (a.bd) go(BandCols{a.bd});
@@ -1471,10 +1473,10 @@ void launch_sliced(tf_ctx *ctx, const Csr<T, I> &a, const XS &xs, const Epi &epi
 // The launch shape cached for an operator's sliced or banded copy: it is
 // stored under the column stream its row-tile kernel reads (2-byte offsets
 // when the operator has them, else its indices).
-template <class T, class I>
-PipeConfig copy_config(tf_ctx *ctx, const Csr<T, I> &a) {
-    return a.cd ? tuned_config<T, I, int16_t>(a.rows, a.nnz, ctx->sm_count)
-                : tuned_config<T, I, I>(a.rows, a.nnz, ctx->sm_count);
+template <class T, class I, class V>
+PipeConfig copy_config(tf_ctx *ctx, const Csr<T, I, V> &a) {
+    return a.cd ? tuned_config<T, I, int16_t, V>(a.rows, a.nnz, ctx->sm_count)
+                : tuned_config<T, I, I, V>(a.rows, a.nnz, ctx->sm_count);
 }
 
 // Launches the sliced kernel when the operator carries a sliced copy and its
@@ -1482,8 +1484,8 @@ PipeConfig copy_config(tf_ctx *ctx, const Csr<T, I> &a) {
 // start on 16-byte boundaries (every buffer this library allocates does),
 // the staged kernel otherwise.  Reducing epilogues need one of the first
 // two: they write their partial sums per 256-row block (tile::partials).
-template <class T, class I, class XS, class Epi>
-void launch(tf_ctx *ctx, const Csr<T, I> &a, const XS &xs, const Epi &epi, const char *name,
+template <class T, class I, class XS, class Epi, class V>
+void launch(tf_ctx *ctx, const Csr<T, I, V> &a, const XS &xs, const Epi &epi, const char *name,
             const PipeConfig *force = nullptr) {
     if (a.rows == 0) return;
     if constexpr (std::is_same_v<I, int32_t>) {
@@ -1503,17 +1505,17 @@ void launch(tf_ctx *ctx, const Csr<T, I> &a, const XS &xs, const Epi &epi, const
         return;
     }
     require(Epi::kReduce == 0, "reducing SpMV epilogues need 16-byte aligned CSR arrays");
-    const SpmvShape shape = spmv_shape(a.rows, a.nnz, sizeof(T), sizeof(I));
+    const SpmvShape shape = spmv_shape(a.rows, a.nnz, sizeof(V), sizeof(I));
     const int64_t tile_rows = static_cast<int64_t>(kThreads) * shape.rows_per_thread;
     const unsigned g = static_cast<unsigned>((a.rows + tile_rows - 1) / tile_rows);
-    const size_t smem = static_cast<size_t>(shape.chunk) * (sizeof(T) + sizeof(I));
+    const size_t smem = static_cast<size_t>(shape.chunk) * (sizeof(V) + sizeof(I));
     if (shape.rows_per_thread == 2) {
-        allow_smem<csr_tile_kernel<T, I, 2, XS, Epi>>(smem);
-        launch_kernel(ctx, name, csr_tile_kernel<T, I, 2, XS, Epi>, g, kThreads, smem, a.rows, a.rp, a.ci, a.val,
+        allow_smem<csr_tile_kernel<T, I, 2, XS, Epi, V>>(smem);
+        launch_kernel(ctx, name, csr_tile_kernel<T, I, 2, XS, Epi, V>, g, kThreads, smem, a.rows, a.rp, a.ci, a.val,
                       shape.chunk, xs, epi);
     } else {
-        allow_smem<csr_tile_kernel<T, I, 1, XS, Epi>>(smem);
-        launch_kernel(ctx, name, csr_tile_kernel<T, I, 1, XS, Epi>, g, kThreads, smem, a.rows, a.rp, a.ci, a.val,
+        allow_smem<csr_tile_kernel<T, I, 1, XS, Epi, V>>(smem);
+        launch_kernel(ctx, name, csr_tile_kernel<T, I, 1, XS, Epi, V>, g, kThreads, smem, a.rows, a.rp, a.ci, a.val,
                       shape.chunk, xs, epi);
     }
 }
@@ -1548,8 +1550,8 @@ inline bool tune_log() {
     return on;
 }
 
-template <class T, class I, class C>
-PipeConfig autotune_columns(tf_ctx *ctx, const Csr<T, I> &a, const T *x, T *y, float *best_ms) {
+template <class T, class I, class C, class V>
+PipeConfig autotune_columns(tf_ctx *ctx, const Csr<T, I, V> &a, const T *x, T *y, float *best_ms) {
     PipeConfig best{};
     float best_t = 0;
     cudaEvent_t e0, e1;
@@ -1560,7 +1562,7 @@ PipeConfig autotune_columns(tf_ctx *ctx, const Csr<T, I> &a, const T *x, T *y, f
     // next use: it is timed cold (a write of more than the L2 size before
     // every launch, then a copy x -> y, so x and y are recently touched);
     // smaller ones are timed back to back.
-    const bool cold = static_cast<double>(a.nnz) * (sizeof(T) + sizeof(C)) +
+    const bool cold = static_cast<double>(a.nnz) * (sizeof(V) + sizeof(C)) +
                           static_cast<double>(a.rows) * (sizeof(I) + 2 * sizeof(T)) >
                       static_cast<double>(kTuneFlushBytes) / 3;
     // (the context's second scratch arena: allocated once, kept for later setups)
@@ -1598,17 +1600,17 @@ PipeConfig autotune_columns(tf_ctx *ctx, const Csr<T, I> &a, const T *x, T *y, f
             for (int ctas : {1, 2, 3, 4, 5, 6}) {
                 for (int pct : {100, 125}) {
                     const PipeConfig cfg{stages, ctas, pct, rpt};
-                    const PipeShape p = pipe_shape<T, I, C>(a.rows, a.nnz, ctx->sm_count, cfg);
+                    const PipeShape p = pipe_shape<V, I, C>(a.rows, a.nnz, ctx->sm_count, cfg);
                     if (p.smem * ctas > 220 * 1024) continue;
                     if ((rpt == 1 && ctas < 2) || (rpt == 2 && ctas > 3)) continue;
                     int resident = 0;
                     if (rpt == 2) {
-                        allow_smem<csr_pipe_kernel<T, I, C, 2, PlainX<T>, TuneStore<T>>>(p.smem);
-                        resident = resident_ctas<csr_pipe_kernel<T, I, C, 2, PlainX<T>, TuneStore<T>>>(kThreads + 32,
+                        allow_smem<csr_pipe_kernel<T, I, C, 2, PlainX<T>, TuneStore<T>, V>>(p.smem);
+                        resident = resident_ctas<csr_pipe_kernel<T, I, C, 2, PlainX<T>, TuneStore<T>, V>>(kThreads + 32,
                                                                                                        p.smem);
                     } else {
-                        allow_smem<csr_pipe_kernel<T, I, C, 1, PlainX<T>, TuneStore<T>>>(p.smem);
-                        resident = resident_ctas<csr_pipe_kernel<T, I, C, 1, PlainX<T>, TuneStore<T>>>(kThreads + 32,
+                        allow_smem<csr_pipe_kernel<T, I, C, 1, PlainX<T>, TuneStore<T>, V>>(p.smem);
+                        resident = resident_ctas<csr_pipe_kernel<T, I, C, 1, PlainX<T>, TuneStore<T>, V>>(kThreads + 32,
                                                                                                        p.smem);
                     }
                     if (resident < ctas) continue;
@@ -1693,9 +1695,9 @@ PipeConfig autotune_columns(tf_ctx *ctx, const Csr<T, I> &a, const T *x, T *y, f
                     } else {
                         cfg.prefetch = knob;
                         // (the column source does not change the kernel's registers much; offsets bound it)
-                        resident = knob ? resident_ctas<sliced_kernel<T, 8, true, PlainX<T>, TuneStore<T>, OffsetCols>>(
+                        resident = knob ? resident_ctas<sliced_kernel<T, 8, true, PlainX<T>, TuneStore<T>, OffsetCols, V>>(
                                               kThreads, 0)
-                                        : resident_ctas<sliced_kernel<T, 8, false, PlainX<T>, TuneStore<T>, OffsetCols>>(
+                                        : resident_ctas<sliced_kernel<T, 8, false, PlainX<T>, TuneStore<T>, OffsetCols, V>>(
                                               kThreads, 0);
                     }
                     if (resident < ctas && forced_pf < 0) continue;
@@ -1723,7 +1725,7 @@ PipeConfig autotune_columns(tf_ctx *ctx, const Csr<T, I> &a, const T *x, T *y, f
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     check_faults(ctx);
-    store_config<T, I, C>(a.rows, a.nnz, ctx->sm_count, best);
+    store_config<T, I, C, V>(a.rows, a.nnz, ctx->sm_count, best);
     if (best_ms) *best_ms = best_t;
     return best;
 }
@@ -1732,21 +1734,21 @@ PipeConfig autotune_columns(tf_ctx *ctx, const Csr<T, I> &a, const T *x, T *y, f
 // capacities on this operator (two warm-up and five timed launches each,
 // CUDA events on the context stream) and caches the fastest for every later
 // launch over an operator of the same shape and storage.  y is overwritten.
-template <class T, class I>
-PipeConfig autotune(tf_ctx *ctx, const Csr<T, I> &a, const T *x, T *y, float *best_ms) {
+template <class T, class I, class V>
+PipeConfig autotune(tf_ctx *ctx, const Csr<T, I, V> &a, const T *x, T *y, float *best_ms) {
     if (a.rows == 0 || !aligned16(a.rp) || (a.nnz && (!aligned16(a.ci) || !aligned16(a.val)))) return PipeConfig{};
     return with_columns(a, [&](auto cols) {
         using C = std::remove_cv_t<std::remove_pointer_t<decltype(cols)>>;
-        return autotune_columns<T, I, C>(ctx, a, x, y, best_ms);
+        return autotune_columns<T, I, C, V>(ctx, a, x, y, best_ms);
     });
 }
 
 // True when operators of a's shape and storage already have a cached shape.
-template <class T, class I>
-bool tuned(tf_ctx *ctx, const Csr<T, I> &a) {
+template <class T, class I, class V>
+bool tuned(tf_ctx *ctx, const Csr<T, I, V> &a) {
     return with_columns(a, [&](auto cols) {
         using C = std::remove_cv_t<std::remove_pointer_t<decltype(cols)>>;
-        return has_config<T, I, C>(a.rows, a.nnz, ctx->sm_count);
+        return has_config<T, I, C, V>(a.rows, a.nnz, ctx->sm_count);
     });
 }
 
