@@ -522,3 +522,25 @@ def test_operator_spmv_entry_points(ctx, shape, monkeypatch):
         lm = h.level_matrix(d)
         xd = torch.tensor(np.random.default_rng(d).standard_normal(lm.rows), dtype=torch.float32, device="cuda")
         assert torch.equal(h.level_spmv(d, xd), tf.spmv(lm, xd, ctx=ctx))
+
+
+@pytest.mark.parametrize("dtype", ["f32", "f64"])
+def test_banded_level_spmv_on_unaligned_vectors(ctx, dtype, monkeypatch):
+    # The four-rows-per-lane banded kernel reads four x values with one
+    # 16-byte load where they are aligned; an x that starts one element into
+    # its buffer takes the one-load-per-entry path: the same bits as the CSR
+    # arrays either way.
+    m = P.heat3d(25, seed=85)
+    n = len(m[0]) - 1
+    t = torch.float32 if dtype == "f32" else torch.float64
+    base = torch.randn(n + 1, dtype=t, device="cuda", generator=torch.Generator("cuda").manual_seed(3))
+    out = []
+    monkeypatch.setenv("THERMOFEM_B200_SLICED_SHAPE", "3,2,3")
+    for flag in ("1", "0"):
+        monkeypatch.setenv("THERMOFEM_B200_SLICED", flag)
+        s = tf.Cg(tf.solver_options(), "amg", tf.amg_options(hierarchy_type=dtype, jacobi_weight=2 / 3), ctx=ctx)
+        s.setup(to_device(m))
+        assert s.level_spmv_layout(0)[0] == ("banded" if flag == "1" else "csr")
+        out.append((s.level_spmv(0, base[1:]).clone(), s.level_spmv(0, base[:n]).clone()))
+        del s
+    assert torch.equal(out[0][0], out[1][0]) and torch.equal(out[0][1], out[1][1])

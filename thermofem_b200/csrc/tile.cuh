@@ -866,6 +866,25 @@ __device__ __forceinline__ void load4(T (&v)[4], const T *p) {
     }
 }
 
+// Four consecutive x values from global memory, 16-byte aligned, through
+// the read-only path.
+template <class T>
+__device__ __forceinline__ void load4_ldg(T (&v)[4], const T *p) {
+    if constexpr (sizeof(T) == 4) {
+        const float4 t = __ldg(reinterpret_cast<const float4 *>(p));
+        v[0] = t.x;
+        v[1] = t.y;
+        v[2] = t.z;
+        v[3] = t.w;
+    } else {
+        const double2 a = __ldg(reinterpret_cast<const double2 *>(p)), b = __ldg(reinterpret_cast<const double2 *>(p + 2));
+        v[0] = a.x;
+        v[1] = a.y;
+        v[2] = b.x;
+        v[3] = b.y;
+    }
+}
+
 // kQuad (banded copies, R = 4, epilogues without partial sums): consumer
 // lanes take four consecutive rows each instead of one -- warp w owns
 // slices 4w..4w+3 of the group, lane 8q + p rows 4p..4p+3 of slice 4w + q.
@@ -1014,6 +1033,15 @@ __global__ void __launch_bounds__(kThreads + 32)
                             const int2 v = band[j0 + g];
                             c = v.x;
                             pad = (static_cast<unsigned>(v.y) >> (4 * p)) & 0xFu;
+                        }
+                        if constexpr (std::is_same_v<std::remove_cv_t<decltype(xr)>, typename PlainX<T>::View>) {
+                            // the four rows' x values in one 16-byte load when they
+                            // are all entries (no index outside x) and their address
+                            // is 16-byte aligned; else one load per entry
+                            if (pad == 0u && (reinterpret_cast<uintptr_t>(xr.p + c) & 15u) == 0) {
+                                load4_ldg(y[g], xr.p + c);
+                                continue;
+                            }
                         }
 #pragma unroll
                         for (int k = 0; k < 4; ++k) y[g][k] = (pad >> k) & 1u ? T(0) : xr(c + k);
