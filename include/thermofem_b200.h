@@ -356,6 +356,18 @@ int tf_amg_level_transfer(const tf_amg *m, int level, const int32_t **map, const
  * the pivot row chosen at each step, both device arrays owned by the
  * hierarchy; *rows = 0 (NULL arrays) when the coarse solve is Jacobi. */
 int tf_amg_coarse_factor(const tf_amg *m, int *rows, const double **lu, const int32_t **pivots);
+/* Hierarchy checkpoint (no reference counterpart; the reference rebuilds
+ * the hierarchy on every setup): tf_amg_save writes the built hierarchy --
+ * every level's operator in its storage type, its damped inverse diagonal,
+ * the aggregates, the coarse factor and the level statistics -- to a file;
+ * tf_amg_load restores it into a component created with the same value,
+ * index and hierarchy types and the same smoothing (TF_ERR_INVALID
+ * otherwise, and for a truncated or foreign file), re-deriving the column
+ * copies, launch shapes and small-level region as setup does, so that the
+ * restored component applies with the same bits.  Load is transactional:
+ * on failure the previous hierarchy is kept. */
+int tf_amg_save(const tf_amg *m, const char *path);
+int tf_amg_load(tf_amg *m, const char *path);
 
 /* Jacobi smoother component (Jacobi.cuh:26-93). */
 typedef struct tf_jacobi tf_jacobi;

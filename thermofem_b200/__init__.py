@@ -174,6 +174,8 @@ SIGNATURES = {
     "tf_amg_level_matrix": ([_P, _I, C.POINTER(Csr)], _I),
     "tf_amg_level_transfer": ([_P, _I, _PP, _PP, _PP, C.POINTER(C.c_int)], _I),
     "tf_amg_coarse_factor": ([_P, C.POINTER(C.c_int), _PP, _PP], _I),
+    "tf_amg_save": ([C.c_void_p, C.c_char_p], C.c_int),
+    "tf_amg_load": ([C.c_void_p, C.c_char_p], C.c_int),
     "tf_jacobi_create": ([_P, _I, _I, _I, _D, _PP], _I),
     "tf_jacobi_destroy": ([_P], _I),
     "tf_jacobi_setup": ([_P, C.POINTER(Csr)], _I),

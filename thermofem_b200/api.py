@@ -4,6 +4,7 @@ BiCgStab), named after the reference's C++ components."""
 from __future__ import annotations
 
 import ctypes as C
+import os
 from dataclasses import dataclass
 
 import numpy as np
@@ -587,6 +588,17 @@ class Amg(_AmgView):
         with self.ctx:
             check(lib().tf_amg_apply(self.h, _p(rhs), _p(x)))
         return x
+
+    def save(self, path):
+        """Writes the built hierarchy to `path` (tf_amg_save)."""
+        with self.ctx:
+            check(lib().tf_amg_save(self.h, os.fsencode(path)))
+
+    def load(self, path):
+        """Restores a hierarchy written by save() into this component, which
+        must have the same types and smoothing (tf_amg_load)."""
+        with self.ctx:
+            check(lib().tf_amg_load(self.h, os.fsencode(path)))
 
 
 class Jacobi:

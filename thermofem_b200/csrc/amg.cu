@@ -15,6 +15,10 @@
 // fly instead of running a separate prolongation.  The whole cycle is
 // captured once into a CUDA graph and replayed on every apply.
 #include <algorithm>
+#include <cstring>
+#include <istream>
+#include <ostream>
+#include <vector>
 
 #include "coarse_cycle.cuh"
 #include "engine.cuh"
@@ -115,6 +119,66 @@ class PhaseMarks {
     std::vector<std::pair<int, cudaEvent_t>> marks_;
 };
 
+// Checkpoint streams: sized arrays, device arrays staged through host
+// memory on the context stream; a short or failed stream is an error.
+struct Writer {
+    tf_ctx *ctx;
+    std::ostream &out;
+    void bytes(const void *p, size_t n) {
+        out.write(static_cast<const char *>(p), static_cast<std::streamsize>(n));
+        if (!out) fail(TF_ERR_RUNTIME, "AMG checkpoint: write failed");
+    }
+    template <class P>
+    void pod(const P &v) {
+        bytes(&v, sizeof v);
+    }
+    void str(const std::string &v) {
+        pod(static_cast<int32_t>(v.size()));
+        bytes(v.data(), v.size());
+    }
+    void device(const void *d, int64_t n) {
+        std::vector<char> h(static_cast<size_t>(n));
+        if (n) {
+            cuda_check(cudaMemcpyAsync(h.data(), d, static_cast<size_t>(n), cudaMemcpyDeviceToHost, ctx->stream),
+                       "AMG checkpoint");
+            cuda_check(cudaStreamSynchronize(ctx->stream), "AMG checkpoint");
+        }
+        pod(n);
+        bytes(h.data(), h.size());
+    }
+};
+struct Reader {
+    tf_ctx *ctx;
+    std::istream &in;
+    void bytes(void *p, size_t n) {
+        in.read(static_cast<char *>(p), static_cast<std::streamsize>(n));
+        if (!in || static_cast<size_t>(in.gcount()) != n) fail(TF_ERR_INVALID, "AMG checkpoint: file truncated or unreadable");
+    }
+    template <class P>
+    P pod() {
+        P v{};
+        bytes(&v, sizeof v);
+        return v;
+    }
+    std::string str() {
+        const int32_t n = pod<int32_t>();
+        if (n < 0 || n > 256) fail(TF_ERR_INVALID, "AMG checkpoint: bad string");
+        std::string v(static_cast<size_t>(n), '\0');
+        bytes(v.data(), v.size());
+        return v;
+    }
+    void device(void *d, int64_t n) {
+        if (pod<int64_t>() != n) fail(TF_ERR_INVALID, "AMG checkpoint: array size does not match its level");
+        std::vector<char> h(static_cast<size_t>(n));
+        bytes(h.data(), h.size());
+        if (n) {
+            cuda_check(cudaMemcpyAsync(d, h.data(), static_cast<size_t>(n), cudaMemcpyHostToDevice, ctx->stream),
+                       "AMG checkpoint");
+            cuda_check(cudaStreamSynchronize(ctx->stream), "AMG checkpoint");
+        }
+    }
+};
+
 template <class S, class V = S>
 struct Level {
     int64_t n{0}, nnz{0};
@@ -201,16 +265,9 @@ class HierarchyImpl final : public Hierarchy {
                 if (cfg_.model) learned_damping(ctx, *cfg_.model, l.csr(), depth, l.dinv.data());
             }
             marks.mark(ctx, kPhColumns);
-            if (delta_columns_enabled() && l.nnz > 0) {
-                l.cd.allocate(static_cast<size_t>(l.nnz));
-                if (!delta_columns(ctx, l.n, l.rp.data(), l.ci.data(), l.cd.data())) l.cd.release();
-            }
-            if (sliced_enabled() && !(banded_enabled() && build_banded(ctx, l.values(), l.sl)) && l.cd.data())
-                build_sliced(ctx, l.values(), l.sl, true);
-            // Launch shape of this level's row-tile kernels (cached by shape).
+            column_copies(ctx, l);
             marks.mark(ctx, kPhTuning);
-            fill_zero(ctx, l.n, l.rhs.data());
-            tune_spmv(ctx, l.csr(), static_cast<const S *>(l.rhs.data()), l.r.data());
+            tune_level(ctx, l);
             LevelStats st;
             st.rows = l.n;
             st.nnz = l.nnz;
@@ -260,6 +317,25 @@ class HierarchyImpl final : public Hierarchy {
             }
         }
         coarse_solver = factored_ ? "pivoted GPU LU" : (singular ? "Jacobi (singular LU)" : "Jacobi (coarsening stopped)");
+        finish_setup(ctx, marks);
+    }
+
+    // The 2-byte column stream and the banded or sliced copy of a level
+    // (derived from its structure and values alone).
+    void column_copies(tf_ctx *ctx, Level<S, V> &l) {
+        if (delta_columns_enabled() && l.nnz > 0) {
+            l.cd.allocate(static_cast<size_t>(l.nnz));
+            if (!delta_columns(ctx, l.n, l.rp.data(), l.ci.data(), l.cd.data())) l.cd.release();
+        }
+        if (sliced_enabled() && !(banded_enabled() && build_banded(ctx, l.values(), l.sl)) && l.cd.data())
+            build_sliced(ctx, l.values(), l.sl, true);
+    }
+    // Launch shape of this level's row-tile kernels (cached by shape).
+    void tune_level(tf_ctx *ctx, Level<S, V> &l) {
+        fill_zero(ctx, l.n, l.rhs.data());
+        tune_spmv(ctx, l.csr(), static_cast<const S *>(l.rhs.data()), l.r.data());
+    }
+    void finish_setup(tf_ctx *ctx, PhaseMarks &marks) {
         visits.assign(levels_.size(), 0);
         marks.mark(ctx, kPhSmall);
         plan_small_levels(ctx);
@@ -268,6 +344,123 @@ class HierarchyImpl final : public Hierarchy {
         marks.mark(ctx, kPhEnd);
         cuda_check(cudaStreamSynchronize(ctx->stream), "AMG setup");
         setup_ms = marks.totals();
+    }
+
+    // ---- checkpoint: the results of the setup phases that coarsen (each
+    // level's operator in its storage, its damped inverse diagonal, the
+    // aggregates, the coarse factor, the statistics) -- everything else is
+    // derived again on restore by the code that derives it in build, so a
+    // restored hierarchy applies with the same bits.
+    static constexpr char kMagic[8] = {'T', 'F', 'B', 'A', 'M', 'G', '0', '1'};
+
+    void save(tf_ctx *ctx, std::ostream &out) const override {
+        Writer w{ctx, out};
+        w.bytes(kMagic, sizeof kMagic);
+        w.pod(static_cast<int32_t>(sizeof(S)));
+        w.pod(static_cast<int32_t>(sizeof(V)));
+        w.pod(static_cast<double>(w_));
+        w.pod(static_cast<int32_t>(levels_.size()));
+        w.str(stop_reason);
+        w.str(coarse_solver);
+        for (size_t d = 0; d < levels_.size(); ++d) {
+            const Level<S, V> &l = levels_[d];
+            const bool last = d + 1 == levels_.size();
+            w.pod(l.n);
+            w.pod(l.nnz);
+            w.pod(static_cast<int32_t>(last ? 0 : l.coarse));
+            w.bytes(stats[d].histogram, sizeof stats[d].histogram);
+            w.device(l.rp.data(), (l.n + 1) * sizeof(int32_t));
+            w.device(l.ci.data(), l.nnz * sizeof(int32_t));
+            w.device(l.val.data(), l.nnz * sizeof(V));
+            w.device(l.dinv.data(), l.n * sizeof(S));
+            if (!last) {
+                w.device(l.map.data(), l.n * sizeof(int32_t));
+                w.device(l.off.data(), (static_cast<int64_t>(l.coarse) + 1) * sizeof(int32_t));
+                w.device(l.mem.data(), l.n * sizeof(int32_t));
+            }
+        }
+        const int32_t nlu = factored_ ? static_cast<int32_t>(levels_.back().n) : 0;
+        w.pod(nlu);
+        if (nlu) {
+            w.device(lu_.data(), static_cast<size_t>(nlu) * nlu * sizeof(double));
+            w.device(piv_.data(), static_cast<size_t>(nlu) * sizeof(int32_t));
+            w.device(inv_.data(), static_cast<size_t>(nlu) * nlu * sizeof(double));
+        }
+        out.flush();
+        if (!out) fail(TF_ERR_RUNTIME, "AMG checkpoint: write failed");
+    }
+
+    void restore(tf_ctx *ctx, std::istream &in) {
+        PhaseMarks marks;
+        Reader r{ctx, in};
+        char magic[sizeof kMagic];
+        r.bytes(magic, sizeof magic);
+        if (std::memcmp(magic, kMagic, sizeof kMagic) != 0) fail(TF_ERR_INVALID, "AMG checkpoint: not a hierarchy file");
+        const auto sv = r.pod<int32_t>(), vv = r.pod<int32_t>();
+        if (sv != static_cast<int32_t>(sizeof(S)) || vv != static_cast<int32_t>(sizeof(V)))
+            fail(TF_ERR_INVALID, "AMG checkpoint: the hierarchy type differs from this component's");
+        if (r.pod<double>() != static_cast<double>(w_))
+            fail(TF_ERR_INVALID, "AMG checkpoint: built with another Jacobi weight or damping model");
+        const int32_t nl = r.pod<int32_t>();
+        if (nl < 1 || nl > cfg_.o.max_levels) fail(TF_ERR_INVALID, "AMG checkpoint: bad level count");
+        stop_reason = r.str();
+        coarse_solver = r.str();
+        for (int32_t d = 0; d < nl; ++d) {
+            marks.mark(ctx, kPhLevel);
+            const bool last = d + 1 == nl;
+            levels_.emplace_back();
+            Level<S, V> &l = levels_.back();
+            l.n = r.pod<int64_t>();
+            l.nnz = r.pod<int64_t>();
+            l.coarse = r.pod<int32_t>();
+            if (l.n < 1 || l.n >= INT32_MAX || l.nnz < 0 || l.nnz >= INT32_MAX || (!last && (l.coarse < 1 || l.coarse >= l.n)))
+                fail(TF_ERR_INVALID, "AMG checkpoint: bad level sizes");
+            if (d > 0 && l.n != levels_[d - 1].coarse) fail(TF_ERR_INVALID, "AMG checkpoint: levels do not chain");
+            LevelStats st;
+            st.rows = l.n;
+            st.nnz = l.nnz;
+            r.bytes(st.histogram, sizeof st.histogram);
+            stats.push_back(st);
+            l.rp.allocate(static_cast<size_t>(l.n) + 1);
+            l.ci.allocate(static_cast<size_t>(l.nnz));
+            l.val.allocate(static_cast<size_t>(l.nnz));
+            for (auto *b : {&l.dinv, &l.rhs, &l.x0, &l.x1, &l.r}) b->allocate(static_cast<size_t>(l.n));
+            r.device(l.rp.data(), (l.n + 1) * sizeof(int32_t));
+            r.device(l.ci.data(), l.nnz * sizeof(int32_t));
+            r.device(l.val.data(), l.nnz * sizeof(V));
+            r.device(l.dinv.data(), l.n * sizeof(S));
+            if (!last) {
+                l.map.allocate(static_cast<size_t>(l.n));
+                l.off.allocate(static_cast<size_t>(l.coarse) + 1);
+                l.mem.allocate(static_cast<size_t>(l.n));
+                r.device(l.map.data(), l.n * sizeof(int32_t));
+                r.device(l.off.data(), (static_cast<int64_t>(l.coarse) + 1) * sizeof(int32_t));
+                r.device(l.mem.data(), l.n * sizeof(int32_t));
+            }
+            // the operator's structure is checked as a caller's would be
+            // (every later kernel trusts it), then its copies are derived
+            if (!csr_structure_ok(ctx, l.n, l.n, l.nnz, l.rp.data(), l.ci.data()))
+                fail(TF_ERR_INVALID, "AMG checkpoint: level operator structure is invalid");
+            if (!last && indices_out_of_range(ctx, l.n, l.map.data(), l.coarse))
+                fail(TF_ERR_INVALID, "AMG checkpoint: aggregate map entry out of range");
+            marks.mark(ctx, kPhColumns);
+            column_copies(ctx, l);
+            marks.mark(ctx, kPhTuning);
+            tune_level(ctx, l);
+        }
+        marks.mark(ctx, kPhCoarse);
+        const int32_t nlu = r.pod<int32_t>();
+        if (nlu) {
+            if (nlu != levels_.back().n) fail(TF_ERR_INVALID, "AMG checkpoint: coarse factor size");
+            lu_.allocate(static_cast<size_t>(nlu) * nlu);
+            piv_.allocate(static_cast<size_t>(nlu));
+            inv_.allocate(static_cast<size_t>(nlu) * nlu);
+            r.device(lu_.data(), static_cast<size_t>(nlu) * nlu * sizeof(double));
+            r.device(piv_.data(), static_cast<size_t>(nlu) * sizeof(int32_t));
+            r.device(inv_.data(), static_cast<size_t>(nlu) * nlu * sizeof(double));
+        }
+        factored_ = nlu > 0;
+        finish_setup(ctx, marks);
     }
 
     // Which levels the cycle streams through their sliced copy, decided in
@@ -925,6 +1118,23 @@ class HierarchyImpl final : public Hierarchy {
 };
 
 }  // namespace
+
+std::unique_ptr<Hierarchy> restore_hierarchy(tf_ctx *ctx, const AmgConfig &cfg, int storage_type,
+                                             std::istream &in) {
+    if (storage_type == TF_F32_VALUES) {
+        auto h = std::make_unique<HierarchyImpl<double, float>>(cfg);
+        h->restore(ctx, in);
+        return h;
+    }
+    if (storage_type == TF_F32) {
+        auto h = std::make_unique<HierarchyImpl<float>>(cfg);
+        h->restore(ctx, in);
+        return h;
+    }
+    auto h = std::make_unique<HierarchyImpl<double>>(cfg);
+    h->restore(ctx, in);
+    return h;
+}
 
 std::unique_ptr<Hierarchy> build_hierarchy(tf_ctx *ctx, const AmgConfig &cfg, int storage_type,
                                            const tf_dcsr &native) {

@@ -2,7 +2,9 @@
 // component API (include/Preconditioner/Amg.cuh, include/Solver/Cg.cuh,
 // include/Solver/BiCgStab.cuh of the reference).
 #pragma once
+#include <istream>
 #include <memory>
+#include <ostream>
 #include <string>
 #include <vector>
 
@@ -59,6 +61,8 @@ class Hierarchy {
     virtual void coarse_factor(int *rows, const double **lu, const int32_t **pivots) const = 0;
     // Kernels launched by one cycle (graph replay counts them too).
     virtual int64_t kernels_per_cycle() const = 0;
+    // Writes the hierarchy (restore_hierarchy reads it back).
+    virtual void save(tf_ctx *ctx, std::ostream &out) const = 0;
 
     std::vector<LevelStats> stats;
     std::vector<int64_t> visits;
@@ -76,6 +80,11 @@ const std::vector<std::string> &setup_phase_names();
 // give per-row Jacobi damping for the smoothers.
 std::unique_ptr<Hierarchy> build_hierarchy(tf_ctx *ctx, const AmgConfig &cfg, int storage_type,
                                            const tf_dcsr &native);
+// A hierarchy written by Hierarchy::save, for a component of the same types
+// and smoothing; the per-level copies, launch shapes and the small-level
+// region are derived again as build_hierarchy derives them.
+std::unique_ptr<Hierarchy> restore_hierarchy(tf_ctx *ctx, const AmgConfig &cfg, int storage_type,
+                                             std::istream &in);
 
 // Krylov solver (kind TF_SOLVER_CG or TF_SOLVER_BICGSTAB) over vectors of T.
 class Krylov {

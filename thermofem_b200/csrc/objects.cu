@@ -4,6 +4,9 @@
 // include/Solver/{Cg,BiCgStab}.cuh).  Setup is transactional for AMG and
 // Jacobi (a failure keeps the previous state) and invalidating for solvers,
 // as in the reference.
+#include <fstream>
+#include <string>
+
 #include "engine.cuh"
 
 using namespace tfb;
@@ -224,6 +227,31 @@ int tf_amg_coarse_factor(const tf_amg *m, int *rows, const double **lu, const in
         require(m != nullptr && rows && lu && pivots, "null argument");
         if (!m->h) fail(TF_ERR_LOGIC, "AMG requires setup");
         m->h->coarse_factor(rows, lu, pivots);
+    });
+}
+
+int tf_amg_save(const tf_amg *m, const char *path) {
+    return guard([&] {
+        require(m != nullptr && path != nullptr, "null argument");
+        if (!m->h) fail(TF_ERR_LOGIC, "AMG requires setup");
+        DeviceScope scope(m->ctx->device);
+        std::ofstream out(path, std::ios::binary | std::ios::trunc);
+        if (!out) fail(TF_ERR_RUNTIME, std::string("AMG checkpoint: cannot open ") + path);
+        m->h->save(m->ctx, out);
+    });
+}
+
+int tf_amg_load(tf_amg *m, const char *path) {
+    return guard([&] {
+        require(m != nullptr && path != nullptr, "null argument");
+        DeviceScope scope(m->ctx->device);
+        std::ifstream in(path, std::ios::binary);
+        if (!in) fail(TF_ERR_INVALID, std::string("AMG checkpoint: cannot open ") + path);
+        const int storage = m->cfg.o.hierarchy_type == -1 ? m->value_type : m->cfg.o.hierarchy_type;
+        // transactional, as setup: the previous hierarchy stays on failure
+        auto h = restore_hierarchy(m->ctx, m->cfg, storage, in);
+        m->owned = std::move(h);
+        m->h = m->owned.get();
     });
 }
 
