@@ -159,7 +159,7 @@ __global__ void k_dot_from(int64_t n, const T *__restrict__ r, const S *__restri
     for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
          i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
         const T zi = static_cast<T>(xs[i]);
-        z[i] = zi;
+        if (z) z[i] = zi;  // (null: the next step reads xs itself)
         v[0] += static_cast<double>(r[i]) * static_cast<double>(zi);
     }
     tile::block_reduce<1>(v);
@@ -308,15 +308,17 @@ __device__ void cg_rho_step(KState *s, const double *part, int parts) {
     }
 }
 
-template <class T>
-__global__ void cg_p(const KState *s, int64_t n, const T *__restrict__ z, T *__restrict__ p) {
+template <class T, class S = T>
+__global__ void cg_p(const KState *s, int64_t n, const S *__restrict__ z, T *__restrict__ p) {
     pdl_enter();
     if (!s->running) return;
     const int mode = s->pmode;
     const T beta = static_cast<T>(s->beta);
     for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
-         i += static_cast<int64_t>(gridDim.x) * blockDim.x)
-        p[i] = mode ? z[i] + beta * p[i] : z[i];
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const T zi = static_cast<T>(z[i]);  // exact: z is the preconditioner's output in its storage S
+        p[i] = mode ? zi + beta * p[i] : zi;
+    }
 }
 
 __device__ void cg_curv_step(KState *s, const double *part, int parts) {
@@ -948,19 +950,26 @@ class KrylovImpl final : public Krylov {
         const unsigned pg = static_cast<unsigned>(parts_);
         if (kind_ == TF_SOLVER_CG) {
             if (fuse_outer()) {
+                // z = M^-1 r stays in the hierarchy's finest level (its
+                // storage): the dot and the direction update read it there
                 const void *zs = hier_->apply_open(ctx, static_cast<const T *>(r_.data()));
-                if (hier_->storage_type() == TF_F32)
+                if (hier_->storage_type() == TF_F32) {
                     launch_kernel(ctx, "dot_rho_from", k_dot_from<T, float, CgRho>, pg, 256, 0, n_, r_.data(),
-                                  static_cast<const float *>(zs), z_.data(), part, CgRho{s, tk + 0});
-                else
+                                  static_cast<const float *>(zs), static_cast<T *>(nullptr), part, CgRho{s, tk + 0});
+                    launch_kernel(ctx, "cg_p", cg_p<T, float>, pg, 256, 0, s, n_, static_cast<const float *>(zs),
+                                  p_.data());
+                } else {
                     launch_kernel(ctx, "dot_rho_from", k_dot_from<T, double, CgRho>, pg, 256, 0, n_, r_.data(),
-                                  static_cast<const double *>(zs), z_.data(), part, CgRho{s, tk + 0});
+                                  static_cast<const double *>(zs), static_cast<T *>(nullptr), part, CgRho{s, tk + 0});
+                    launch_kernel(ctx, "cg_p", cg_p<T, double>, pg, 256, 0, s, n_, static_cast<const double *>(zs),
+                                  p_.data());
+                }
             } else {
                 precondition(ctx, r_.data(), z_.data());
                 launch_kernel(ctx, "dot_rho", k_dot<T, CgRho>, pg, 256, 0, n_, r_.data(), z_.data(), part,
                               CgRho{s, tk + 0});
+                launch_kernel(ctx, "cg_p", cg_p<T>, pg, 256, 0, s, n_, z_.data(), p_.data());
             }
-            launch_kernel(ctx, "cg_p", cg_p<T>, pg, 256, 0, s, n_, z_.data(), p_.data());
             tile::launch(ctx, csr(), tile::PlainX<T>{p_.data()},
                          SpmvDot<T, CgCurv>{q_.data(), p_.data(), &s->running, part, CgCurv{s, tk + 1}},
                          "spmv_dot_curv");
